@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the Schulze widest-path closure on B200 (the headline workload).
+
+Workload: one election with C = 16384 candidates and V = 4096 voters whose ballots are drawn
+from a Mallows model (dispersion 0.8) around a seeded reference order. Ballots are drawn on
+the GPU, tallied on the GPU, and the tally stays in HBM. A "step" is one full widest-path
+closure of that C x C matrix (u16 lanes, legal because every count is at most V < 65536).
+
+  value  C^3 relaxations per second ("cells/s", the reference's metric,
+         scaling_elections.py:499), device-resident input and output, max over ranks.
+  e2e    the same metric through the public host API compute_strongest_paths(): the
+         preference matrix starts in pinned host memory and the strongest-path matrix returns
+         to pinned host memory every step (1 GiB each way).
+
+The matrix (0.5 GiB in u16, 1 GiB in u32) is larger than the 126 MB L2, so no flush is
+needed between steps. ``--impl reference`` times the reference's own CPU closure (its OpenMP
+path compiled unmodified into oracle/_ref) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank closes its own independent election (elections are the
+unit of parallelism; there is no collective on the data path), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcells/s (C^3/t), single-election widest-path closure, C=16384"
+UNIT = "Gcells/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--candidates", type=int, default=16384)
+    ap.add_argument("--voters", type=int, default=4096)
+    ap.add_argument("--phi", type=float, default=0.8)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
+    ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(args, world):
+    return {
+        "workload": f"Schulze widest-path closure, one election per GPU: C={args.candidates} candidates, "
+                    f"V={args.voters} Mallows(phi={args.phi}) ballots",
+        "candidates": args.candidates,
+        "voters": args.voters,
+        "phi": args.phi,
+        "lanes": f"u{args.lanes}" if args.lanes else "auto",
+        "tile": 128,
+        "parallelism": f"replicas{world}" if world > 1 else "single",
+        "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
+    }
+
+
+# ------------------------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples: list[list[str]] = []
+        self._stop = threading.Event()
+        self._thr = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thr.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._thr.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[4 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baselines (the reference's own OpenMP closure, else the oracle's port)
+# ------------------------------------------------------------------------------------------
+def cpu_sample_matrix(args):
+    """Preference matrix of the bounded CPU sample: a Mallows election with C = args.cpu_sample
+    candidates and 512 voters, drawn and tallied on the host (not timed)."""
+    from oracle import oracle
+
+    b = oracle.mallows_ballots(512, args.cpu_sample, args.phi, seed=args.seed + 7)
+    return oracle.tally(b, "positions")
+
+
+def cpu_closure_sample(args, d):
+    """Times the reference's CPU closure (its OpenMP path compiled unmodified into oracle/_ref;
+    the oracle's port if that is absent) on the sample matrix d. Returns
+    (cells_per_s, kind, cores, sample description, seconds)."""
+    from oracle import oracle
+
+    Cs = d.shape[0]
+    cores = os.cpu_count() or 1
+    ref = oracle.reference_cpu()
+    if ref is not None:
+        kind = "reference"
+        ref.compute_strongest_paths(d[:256, :256].copy(), allow_gpu=False, allow_tma=False, tile_size=16)
+        t0 = time.perf_counter()
+        ref.compute_strongest_paths(d, allow_gpu=False, allow_tma=False, tile_size=16)
+        t = time.perf_counter() - t0
+        what = "scaling_elections.cu OpenMP closure (tile 16), compiled unmodified"
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        oracle.strongest_paths(d, "blocked", tile=16, threads=cores)
+        t = time.perf_counter() - t0
+        what = "oracle blocked closure (tile 16, OpenMP)"
+    sample = (f"{what}, one C={Cs} Mallows(phi={args.phi}) election ({Cs}^3 cells, {t:.2f} s) "
+              f"standing in for the C={args.candidates} workload; {cores} host threads")
+    return Cs ** 3 / t, kind, cores, sample, t
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    cfg = config(args, world)
+    d = cpu_sample_matrix(args)
+    values = []
+    for i in range(args.warmup + args.steps):
+        cps, kind, cores, sample, t = cpu_closure_sample(args, d)
+        if i >= args.warmup:
+            values.append(cps)
+    v = statistics.median(values) / 1e9
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": args.cpu_sample ** 3 / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Mallows ballots)", "config": cfg,
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# Our arm
+# ------------------------------------------------------------------------------------------
+def load_traffic(lanes: int, C: int):
+    """DRAM bytes per remainder-kernel launch from the committed ncu summary, scaled to C."""
+    p = ROOT / "profiles" / "closure_tile_kernel_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        rec = json.loads(p.read_text())
+        r = rec[f"u{lanes}"]
+        tiles_ref = (r["C"] // 128 - 1) ** 2
+        tiles = (C // 128 - 1) ** 2 if C % 128 == 0 else ((C + 127) // 128 - 1) ** 2
+        return r["dram_bytes_per_launch"] * tiles / tiles_ref
+    except Exception:
+        return None
+
+
+def run_ours(args, world, rank, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from scalingelections_b200 import _lib, api
+    from scalingelections_b200.ballots import mallows_ballots_device
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    C, V = args.candidates, args.voters
+    lanes = args.lanes
+    L = _lib.lib()
+
+    # Input: ballots drawn and tallied on the device.
+    ballots = mallows_ballots_device(V, C, args.phi, seed=args.seed + 1000 * rank, device=dev)
+    offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
+    d = api.tally_device(ballots.view(-1), offs, C)
+    del ballots
+    torch.cuda.synchronize()
+
+    # Roofline denominator: the min/max issue microbenchmark at this moment's clock.
+    peak = [ctypes.c_double() for _ in range(4)]
+    recipe = 3 if lanes in (0, 16) else 1
+    _lib.check(L.se_minmax_peak(recipe, 65536, *[ctypes.byref(x) for x in peak]))
+    peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
+
+    need = api.closure_workspace_bytes(C, lanes)
+    work = torch.empty(need, dtype=torch.uint8, device=dev)
+    out = torch.empty((C, C), dtype=torch.uint32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        api.strongest_paths_device(d, lanes=lanes, out=out, workspace=work)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cells = float(C) ** 3 * args.steps * world
+    value = cells / (ms_max * 1e-3) / 1e9
+
+    # Per-phase device time (one extra, event-instrumented closure) for the roofline.
+    phase = (ctypes.c_double * 4)()
+    launches = ctypes.c_int(0)
+    _lib.check(L.se_closure_profiled(d.data_ptr(), C, C, out.data_ptr(), C, lanes, 0, work.data_ptr(), need,
+                                     stream.cuda_stream, phase, ctypes.byref(launches)))
+    R = (C + 127) // 128
+    tile_launches = R if R > 1 else 0  # one remainder launch per round when R > 1
+    relax_per_launch = float(R - 1) ** 2 * 128 ** 3
+    tile_ms_avg = phase[3] / max(tile_launches, 1)
+    achieved = relax_per_launch / (tile_ms_avg * 1e-3)
+    cell_bytes = 2 if lanes in (0, 16) else 4
+    algo_bytes = float(R - 1) ** 2 * 128 * 128 * cell_bytes * 2  # each remainder tile read + written once
+
+    # End to end through the public host API: pinned host in, pinned host out.
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.empty((C, C), dtype=torch.int32, pin_memory=True)
+        host_in.copy_(d.view(torch.int32))
+        host_in = host_in.view(torch.uint32)
+        api.compute_strongest_paths(host_in, allow_gpu=True, tile_size=32, lanes=lanes)  # warm
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res = api.compute_strongest_paths(host_in, allow_gpu=True, tile_size=32, lanes=lanes)
+            del res
+        t_e2e = time.perf_counter() - t0
+        te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": cells / float(te.item()) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": C * C * 4, "d2h_bytes_per_step": C * C * 4}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cps, kind, cores, sample, _ = cpu_closure_sample(args, cpu_sample_matrix(args))
+        cpu = {"value": cps / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        traffic = load_traffic(lanes if lanes else 16, C)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": f"u{lanes}" if lanes else "u16/u32",
+            "data": "synthetic (seeded Mallows ballots drawn and tallied on the GPU)",
+            "config": config(args, world),
+            "roofline": {
+                "bound": "int_minmax",
+                "kernel": f"closure remainder tile_kernel<u{lanes or 16}>",
+                "achieved": achieved / 1e12, "peak": peak_relax_per_s / 1e12, "unit": "Trelax/s",
+                "frac": achieved / peak_relax_per_s,
+                "peak_source": f"measured: se_minmax_peak recipe {recipe} in this run "
+                               f"({peak_relax_per_clk:.1f} relax/SM/clk at {peak_mhz:.0f} MHz)",
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": algo_bytes,
+                "hbm_gbs_achieved": algo_bytes / (tile_ms_avg * 1e-3) / 1e9,
+                "phase_ms": {"pivot": phase[0], "row_panel": phase[1], "col_panel": phase[2],
+                             "remainder": phase[3]},
+            },
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks.summary(),
+            "gpu_launches": int(L.se_closure_launch_count(C)) * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, world, rank, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,153 @@
+/*
+ * se.h - C ABI of the sm_100a Schulze hot path (ballot tally, widest-path closure, ranking).
+ *
+ * Conventions (all entry points):
+ *   - Pointers named d_* are DEVICE pointers owned by the caller. Nothing here allocates or
+ *     frees memory on the compute paths; scratch space is passed in as `d_work`, sized by the
+ *     matching *_workspace_bytes() query.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream). Calls are
+ *     stream-ordered and asynchronous unless the comment says otherwise.
+ *   - The return value is an se_status_t; on failure se_last_error() returns a message
+ *     (thread-local). Messages reuse the reference's wording where it has one.
+ *   - Matrices are row-major uint32 with a row stride `ld` counted in elements.
+ *
+ * Reference interfaces replaced (paths relative to ashvardanian/ScalingElections):
+ *   compute_strongest_paths      scaling_elections.cu:863-989, bound at :1034-1038
+ *   compute_strongest_paths_cuda scaling_elections.cu:490-578
+ *   log_gpus                     scaling_elections.cu:996-1016
+ *   build_pairwise_preferences   scaling_elections.py:51-88 (+ populate_... :37-48)
+ *   get_winner_and_ranking       scaling_elections.py:274-296
+ */
+#ifndef SE_H
+#define SE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SE_API __attribute__((visibility("default")))
+#else
+#define SE_API
+#endif
+
+typedef int se_status_t;
+
+#define SE_OK 0
+#define SE_ERR_INVALID 1     /* malformed argument (shape, range, null pointer) */
+#define SE_ERR_CUDA 2        /* a CUDA runtime call or a kernel launch failed */
+#define SE_ERR_UNSUPPORTED 3 /* e.g. a tile size this build does not provide */
+#define SE_ERR_DEVICE 4      /* a kernel raised its device-side error word */
+#define SE_ERR_OVERFLOW 5    /* a count does not fit the requested 16-bit lanes */
+#define SE_ERR_WORKSPACE 6   /* d_work missing or smaller than the *_workspace_bytes() query */
+
+/* Lane modes for the closure: 16 = two u16 cells per 32-bit word (every count < 65536),
+ * 32 = one u32 cell per word, 0 = choose on the device (u16 when max(d) < 65536; this costs
+ * one 4-byte device-to-host read and a stream synchronisation). */
+#define SE_LANES_AUTO 0
+#define SE_LANES_U16 16
+#define SE_LANES_U32 32
+
+/* Message of the last failed call on this thread ("" if none). */
+SE_API const char* se_last_error(void);
+
+/* ABI version, bumped on any signature change. */
+SE_API int se_version(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Device information. Replaces log_gpus (scaling_elections.cu:996-1016), which prints the
+ * name, SM count, global memory and compute capability of every device.
+ * ------------------------------------------------------------------------------------- */
+SE_API se_status_t se_device_count(int* count);
+SE_API se_status_t se_device_info(int device, char* name, int name_capacity, int* sm_count,
+                           double* global_mem_gib, int* cc_major, int* cc_minor);
+
+/* ---------------------------------------------------------------------------------------
+ * Widest-path closure. Replaces compute_strongest_paths(preferences, allow_gpu=True, ...)
+ * (scaling_elections.cu:863-989 -> compute_strongest_paths_cuda :490-578).
+ *
+ *   d_pref  C x C uint32 pairwise preference counts d[i][j], row stride ld_pref.
+ *   d_out   C x C uint32 strongest-path strengths, row stride ld_out. Diagonal is 0.
+ *           out[i][j] = widest path i->j in the graph with edge i->j of width d[i][j] when
+ *           d[i][j] > d[j][i] (else no edge), exactly as scaling_elections.py:91-125.
+ *   tile    pivot block edge; 0 picks the default. Unsupported values return
+ *           SE_ERR_UNSUPPORTED ("Unsupported tile size", as scaling_elections.cu:900).
+ *   d_work  scratch of at least se_closure_workspace_bytes(C, lane_bits, tile) bytes.
+ * Any C >= 1 is accepted (the reference's GPU path needs C % tile == 0).
+ * ------------------------------------------------------------------------------------- */
+SE_API int64_t se_closure_workspace_bytes(int C, int lane_bits, int tile);
+SE_API se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out,
+                       int64_t ld_out, int lane_bits, int tile, void* d_work,
+                       int64_t work_bytes, void* stream);
+
+/* Same as se_closure, and also fills phase_ms[4] with the summed device time of the four
+ * kernel kinds (pivot tile, pivot-row panel, pivot-column panel, remainder) from CUDA events
+ * recorded between the launches, and *launches with the number of kernels launched.
+ * Synchronous. For profiling: the events add a little time between launches. */
+SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out,
+                                       int64_t ld_out, int lane_bits, int tile, void* d_work,
+                                       int64_t work_bytes, void* stream, double* phase_ms, int* launches);
+
+/* Number of kernels one se_closure call launches for C candidates (with lane_bits 16 or 32;
+ * the automatic mode adds at most one more). */
+SE_API int se_closure_launch_count(int C);
+
+/* ---------------------------------------------------------------------------------------
+ * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).
+ *
+ *   Ballots are given in CSR form: ballot v is d_ids[d_offsets[v] .. d_offsets[v+1]), the
+ *   candidate ids from most to least preferred. A ballot that omits candidates is completed
+ *   by appending the missing ids in ascending order (scaling_elections.py:75-83). C must be
+ *   at least max(id) + 1 (the reference uses exactly max(id) + 1, :63-66).
+ *   d_out receives d[i][j] = #ballots ranking i above j (uint32, diagonal 0), row stride
+ *   ld_out. Ids outside [0, C) or repeated within a ballot return SE_ERR_DEVICE with a
+ *   message (the reference does not validate these).
+ * ------------------------------------------------------------------------------------- */
+SE_API int64_t se_tally_workspace_bytes(int64_t V, int C);
+SE_API se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
+                     uint32_t* d_out, int64_t ld_out, void* d_work, int64_t work_bytes,
+                     void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Ranking. Replaces get_winner_and_ranking (scaling_elections.py:274-296).
+ *
+ *   d_wins[i]    = #{j != i : S[i][j] > S[j][i]}
+ *   d_ranking[r] = candidate at place r: candidates sorted by wins, descending, ties in
+ *                  ascending index order (Python's stable `sorted(..., reverse=True)`).
+ *   The winner is d_ranking[0]. S is C x C uint32 with row stride ld.
+ * ------------------------------------------------------------------------------------- */
+SE_API se_status_t se_rank(const uint32_t* d_S, int64_t ld, int C, int32_t* d_wins,
+                    int32_t* d_ranking, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Seeded synthetic ballots on the device (no reference counterpart; the reference draws
+ * unseeded np.random.permutation ballots on the host, scaling_elections.py:477-481).
+ *   d_out[v*C .. v*C+C) = ballot v, a permutation of 0..C-1 drawn from the Mallows model
+ *   around d_reference (C ids; NULL = identity) with dispersion phi in (0, 1]; phi = 1 is
+ *   uniform. Deterministic in (seed, v). d_work: se_mallows_workspace_bytes(V, C) bytes.
+ * ------------------------------------------------------------------------------------- */
+SE_API int64_t se_mallows_workspace_bytes(int64_t V, int C);
+SE_API se_status_t se_mallows_ballots(int64_t V, int C, double phi, uint64_t seed,
+                                      const int32_t* d_reference, int32_t* d_out, void* d_work,
+                                      int64_t work_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Integer min/max issue-rate microbenchmark (no reference counterpart): measures the
+ * relaxations c = max(c, min(a, b)) per SM per clock that one instruction recipe reaches on
+ * this GPU, with operands read from shared memory by a register-blocked 8 x 8 micro-kernel.
+ * This is the denominator of the closure's roofline. Synchronous; allocates its own small
+ * buffers (diagnostic only).
+ *   recipe: 0 u32 min+max, 1 u32 min+min+max3, 2 u16x2 min+max, 3 u16x2 min+min+max3,
+ *           4 f16x2 min+max, 5 f32 min+max, 6 f32 min+min+max3,
+ *           7 half rows recipe 3 / half rows recipe 4, 8 half rows recipe 1 / half recipe 6
+ * ------------------------------------------------------------------------------------- */
+SE_API se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per_sm_clock,
+                           double* sm_mhz, double* kernel_ms, double* relax_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SE_H */

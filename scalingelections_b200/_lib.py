@@ -1,0 +1,89 @@
+"""ctypes binding of libse.so, the C ABI declared in include/se.h.
+
+The library must have been built (``python -m scalingelections_b200.build`` or
+``__graft_entry__.build()``); there is deliberately no fallback: importing a compute entry
+point without the CUDA library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libse.so"
+
+SE_OK = 0
+SE_ERR_INVALID = 1
+SE_ERR_CUDA = 2
+SE_ERR_UNSUPPORTED = 3
+SE_ERR_DEVICE = 4
+SE_ERR_OVERFLOW = 5
+SE_ERR_WORKSPACE = 6
+
+LANES_AUTO = 0
+LANES_U16 = 16
+LANES_U32 = 32
+
+_c_i64 = ctypes.c_int64
+_c_int = ctypes.c_int
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+# name -> (restype, argtypes); every symbol include/se.h declares.
+SIGNATURES: dict[str, tuple] = {
+    "se_last_error": (ctypes.c_char_p, []),
+    "se_version": (_c_int, []),
+    "se_device_count": (_c_int, [_ip]),
+    "se_device_info": (_c_int, [_c_int, ctypes.c_char_p, _c_int, _ip, _dp, _ip, _ip]),
+    "se_closure_workspace_bytes": (_c_i64, [_c_int, _c_int, _c_int]),
+    "se_closure": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp]),
+    "se_closure_profiled": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _dp, _ip]),
+    "se_closure_launch_count": (_c_int, [_c_int]),
+    "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
+    "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
+    "se_rank": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
+    "se_mallows_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
+    "se_mallows_ballots": (_c_int, [_c_i64, _c_int, ctypes.c_double, ctypes.c_uint64, _vp, _vp, _vp, _c_i64, _vp]),
+    "se_minmax_peak": (_c_int, [_c_int, _c_int, _dp, _dp, _dp, _dp]),
+}
+
+_lib: ctypes.CDLL | None = None
+_lock = threading.Lock()
+
+
+class SchulzeError(RuntimeError):
+    """A failed libse call. Subclasses RuntimeError, which is what the reference's native
+    module raises for every failure (scaling_elections.cu:868-931)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not LIB_PATH.exists():
+                    raise ImportError(
+                        f"{LIB_PATH} is missing: build the CUDA library first "
+                        "(python -m scalingelections_b200.build)")
+                L = ctypes.CDLL(str(LIB_PATH))
+                for name, (res, args) in SIGNATURES.items():
+                    fn = getattr(L, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    msg = lib().se_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int) -> None:
+    if status != SE_OK:
+        raise SchulzeError(status, last_error() or f"libse error {status}")

@@ -1,0 +1,322 @@
+"""Host-side API: the reference's entry points for the Schulze GPU path, over libse.
+
+Mirrors, name for name, what ``scaling_elections.py`` imports from the native module and the
+Python functions on its hot path:
+
+=============================  ============================================================
+``compute_strongest_paths``    scaling_elections.cu:863-989 (bound at :1034-1038)
+``log_gpus``                   scaling_elections.cu:996-1016
+``build_pairwise_preferences`` scaling_elections.py:51-88
+``get_winner_and_ranking``     scaling_elections.py:274-296
+=============================  ============================================================
+
+plus device-resident forms (``*_device``) that take and return CUDA tensors, for callers that
+keep matrices in HBM between steps. Every compute path runs the sm_100a kernels; there is no
+CPU fallback (``allow_gpu=False`` raises).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import LANES_AUTO, LANES_U16, LANES_U32, SchulzeError, check
+
+# Tile sizes the reference's GPU driver accepts (scaling_elections.cu:895-901). The value
+# only selects the reference's kernel template; the result does not depend on it, and this
+# implementation always runs its own 128-cell tiles.
+REFERENCE_GPU_TILES = (4, 8, 16, 32)
+
+
+def _require_cuda() -> None:
+    if not torch.cuda.is_available():
+        raise RuntimeError("No CUDA devices available")
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _workspace(nbytes: int, device) -> torch.Tensor:
+    # The caching allocator returns 512-byte aligned blocks and recycles them across calls.
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def _to_device_u32(a: np.ndarray | torch.Tensor, dev) -> torch.Tensor:
+    """Host uint32 array -> CUDA uint32 tensor, copied through an int32 view (torch's uint32
+    is a storage-only dtype)."""
+    t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
+    t = t.view(torch.int32)
+    return t.to(device=dev, non_blocking=t.is_pinned()).view(torch.uint32)
+
+
+def _to_host_u32(t: torch.Tensor, pinned: bool = False) -> np.ndarray:
+    if pinned:
+        host = torch.empty(t.shape, dtype=torch.int32, pin_memory=True)
+        host.copy_(t.view(torch.int32), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return host.numpy().view(np.uint32)
+    return t.view(torch.int32).cpu().numpy().view(np.uint32)
+
+
+def _check_matrix(t: torch.Tensor, name: str) -> tuple[int, int]:
+    if t.dim() != 2 or t.shape[0] != t.shape[1]:
+        raise ValueError(f"{name} must be a square matrix")
+    if t.dtype != torch.uint32:
+        raise TypeError(f"{name} must be uint32")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be on a CUDA device")
+    if t.shape[0] > 0 and t.stride(1) != 1:
+        raise ValueError(f"{name} rows must be contiguous")
+    return t.shape[0], (t.stride(0) if t.shape[0] > 0 else 1)
+
+
+# ------------------------------------------------------------------------------------------
+# Device-resident entry points
+# ------------------------------------------------------------------------------------------
+def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO) -> int:
+    n = _lib.lib().se_closure_workspace_bytes(int(num_candidates), int(lanes), 0)
+    if n < 0:
+        raise ValueError("invalid closure size")
+    return n
+
+
+def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO, out: torch.Tensor | None = None,
+                           workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """Widest-path closure of a CUDA uint32 [C, C] preference matrix; returns uint32 [C, C]
+    on the same device (diagonal 0), bit-identical to compute_strongest_paths_numba_serial.
+
+    lanes: LANES_U16 (every count < 65536), LANES_U32, or LANES_AUTO (checked on the device,
+    one 4-byte read back)."""
+    C, ld = _check_matrix(preferences, "preferences")
+    if out is None:
+        out = torch.empty((C, C), dtype=torch.uint32, device=preferences.device)
+    Co, ldo = _check_matrix(out, "out")
+    if Co != C:
+        raise ValueError("out has the wrong shape")
+    if C == 0:
+        return out
+    need = closure_workspace_bytes(C, lanes)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = _workspace(need, preferences.device)
+    with torch.cuda.device(preferences.device):
+        check(_lib.lib().se_closure(preferences.data_ptr(), ld, C, out.data_ptr(), ldo, int(lanes), 0,
+                                    workspace.data_ptr(), need, _stream()))
+    return out
+
+
+def tally_workspace_bytes(num_voters: int, num_candidates: int) -> int:
+    n = _lib.lib().se_tally_workspace_bytes(int(num_voters), int(num_candidates))
+    if n < 0:
+        raise ValueError("invalid tally size")
+    return n
+
+
+def tally_device(ids: torch.Tensor, offsets: torch.Tensor, num_candidates: int, *, out: torch.Tensor | None = None,
+                 workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """Pairwise preference counts from CSR ballots on the device: ids int32 (concatenated
+    ballots, most preferred first), offsets int64 [V + 1]. Returns uint32 [C, C]."""
+    if ids.dtype != torch.int32 or offsets.dtype != torch.int64 or not ids.is_cuda or not offsets.is_cuda:
+        raise TypeError("ids must be CUDA int32 and offsets CUDA int64")
+    C = int(num_candidates)
+    V = offsets.numel() - 1
+    if V < 0:
+        raise ValueError("offsets must hold V + 1 entries")
+    if V > 0:
+        # The kernels trust the CSR bounds; check them here (one small device-to-host read).
+        bad = (offsets[0] != 0) | (offsets[-1] != ids.numel()) | (offsets[1:] < offsets[:-1]).any()
+        if bool(bad):
+            raise ValueError("offsets must start at 0, never decrease and end at len(ids)")
+    if out is None:
+        out = torch.empty((C, C), dtype=torch.uint32, device=ids.device)
+    Co, ldo = _check_matrix(out, "out")
+    need = tally_workspace_bytes(V, C)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = _workspace(need, ids.device)
+    with torch.cuda.device(ids.device):
+        check(_lib.lib().se_tally(ids.data_ptr(), offsets.data_ptr(), V, C, out.data_ptr(), ldo,
+                                  workspace.data_ptr(), need, _stream()))
+    return out
+
+
+def rank_device(strongest_paths: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+    """(wins, ranking) int32 CUDA tensors: wins[i] = #{j: S[i][j] > S[j][i]}; ranking lists
+    candidates by wins descending, ties by ascending index."""
+    C, ld = _check_matrix(strongest_paths, "strongest_paths")
+    wins = torch.empty(C, dtype=torch.int32, device=strongest_paths.device)
+    ranking = torch.empty(C, dtype=torch.int32, device=strongest_paths.device)
+    if C:
+        with torch.cuda.device(strongest_paths.device):
+            check(_lib.lib().se_rank(strongest_paths.data_ptr(), ld, C, wins.data_ptr(), ranking.data_ptr(),
+                                     _stream()))
+    return wins, ranking
+
+
+# ------------------------------------------------------------------------------------------
+# Reference-compatible host entry points
+# ------------------------------------------------------------------------------------------
+def _host_u32_matrix(preferences) -> np.ndarray | torch.Tensor:
+    if isinstance(preferences, torch.Tensor):
+        t = preferences.detach()
+        if t.dim() != 2:
+            raise RuntimeError("Number of dimensions must be two")
+        if t.shape[0] != t.shape[1]:
+            raise RuntimeError("Preferences matrix must be square")
+        if t.dtype != torch.uint32:
+            t = torch.from_numpy(t.cpu().numpy().astype(np.uint32))
+        return t.contiguous()
+    a = np.asarray(preferences)
+    if a.ndim != 2:
+        raise RuntimeError("Number of dimensions must be two")
+    if a.shape[0] != a.shape[1]:
+        raise RuntimeError("Preferences matrix must be square")
+    # pybind11's array_t<uint32, c_style> force-casts any dtype and layout (cu:864).
+    return np.ascontiguousarray(a.astype(np.uint32, copy=False))
+
+
+def compute_strongest_paths(preferences, *, allow_tma: bool = False, allow_gpu: bool = False,
+                            tile_size: int = 0, lanes: int = LANES_AUTO) -> np.ndarray:
+    """Drop-in for the reference's native ``compute_strongest_paths``
+    (scaling_elections.cu:863-989): preferences (C x C, any dtype, cast to uint32) in, a new
+    C-contiguous uint32 strongest-path matrix out, diagonal 0.
+
+    Error behaviour follows the reference: RuntimeError("Number of dimensions must be two"),
+    RuntimeError("Preferences matrix must be square"), RuntimeError("Unsupported tile size")
+    for a GPU tile outside {4, 8, 16, 32}. ``allow_tma`` is accepted and has no effect (every
+    kernel here stages through TMA). ``allow_gpu=False`` selects the reference's OpenMP CPU
+    path, which this GPU-only library does not provide: it raises RuntimeError.
+
+    Unlike the reference's GPU path, any C works (no C % tile_size == 0 requirement)."""
+    P = _host_u32_matrix(preferences)
+    if not allow_gpu:
+        raise RuntimeError("CPU path not provided: this module runs the closure on the GPU only "
+                           "(pass allow_gpu=True)")
+    if int(tile_size) not in REFERENCE_GPU_TILES:
+        raise RuntimeError("Unsupported tile size")
+    _require_cuda()
+    C = P.shape[0]
+    if C == 0:
+        return np.zeros((0, 0), dtype=np.uint32)
+    d = _to_device_u32(P, torch.cuda.current_device())
+    out = strongest_paths_device(d, lanes=lanes)
+    return _to_host_u32(out, pinned=True)
+
+
+def log_gpus() -> None:
+    """Prints every CUDA device as scaling_elections.cu:996-1016 does."""
+    L = _lib.lib()
+    n = ctypes.c_int(0)
+    check(L.se_device_count(ctypes.byref(n)))
+    for i in range(n.value):
+        name = ctypes.create_string_buffer(256)
+        sms, major, minor = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        mem = ctypes.c_double()
+        check(L.se_device_info(i, name, 256, ctypes.byref(sms), ctypes.byref(mem), ctypes.byref(major),
+                               ctypes.byref(minor)))
+        print(f"Device {i}: {name.value.decode()}")
+        print(f"\tSMs: {sms.value}")
+        print(f"\tGlobal mem: {mem.value:.2f}GB")
+        print(f"\tCUDA Cap: {major.value}.{minor.value}")
+
+
+@dataclass
+class Ballots:
+    """Ballots in CSR form: ballot v is ids[offsets[v]:offsets[v+1]], most preferred first."""
+    ids: np.ndarray      # int32
+    offsets: np.ndarray  # int64, V + 1 entries
+    num_candidates: int  # max id + 1 (at least 1), as scaling_elections.py:63-66
+
+    @property
+    def num_voters(self) -> int:
+        return len(self.offsets) - 1
+
+    @classmethod
+    def from_rankings(cls, voter_rankings: Sequence[np.ndarray] | np.ndarray) -> "Ballots":
+        if isinstance(voter_rankings, np.ndarray) and voter_rankings.ndim == 2:
+            V, L = voter_rankings.shape
+            if L == 0 and V > 0:
+                raise ValueError("zero-size array to reduction operation maximum which has no identity")
+            ids = np.ascontiguousarray(voter_rankings, dtype=np.int32).reshape(-1)
+            offsets = np.arange(V + 1, dtype=np.int64) * L
+        else:
+            rankings = [np.asarray(r) for r in voter_rankings]
+            lens = np.fromiter((r.size for r in rankings), dtype=np.int64, count=len(rankings))
+            if (lens == 0).any():
+                # The reference calls np.max on every ballot (py:64-65).
+                raise ValueError("zero-size array to reduction operation maximum which has no identity")
+            offsets = np.zeros(len(rankings) + 1, dtype=np.int64)
+            np.cumsum(lens, out=offsets[1:])
+            ids = (np.concatenate(rankings).astype(np.int32, copy=False) if rankings
+                   else np.zeros(0, dtype=np.int32))
+        if ids.size and int(ids.min()) < 0:
+            raise ValueError("candidate ids must be non-negative")
+        C = max(1, int(ids.max()) + 1) if ids.size else 1
+        return cls(np.ascontiguousarray(ids), offsets, C)
+
+
+def _tally_host(ballots: Ballots, dev) -> torch.Tensor:
+    ids = torch.from_numpy(ballots.ids).to(dev, non_blocking=False)
+    offs = torch.from_numpy(ballots.offsets).to(dev, non_blocking=False)
+    try:
+        return tally_device(ids, offs, ballots.num_candidates)
+    except SchulzeError as e:
+        if e.status == _lib.SE_ERR_DEVICE and "candidate" in str(e):
+            raise ValueError(str(e)) from e
+        raise
+
+
+def build_pairwise_preferences(voter_rankings: Sequence[np.ndarray] | np.ndarray) -> np.ndarray:
+    """GPU form of scaling_elections.py:51-88: uint32 [C, C] with d[i][j] = number of voters
+    ranking i above j, C = max id + 1. Incomplete ballots get the missing ids appended in
+    ascending order (py:75-83). A ballot repeating an id raises ValueError (the reference
+    counts such ballots without complaint)."""
+    _require_cuda()
+    b = Ballots.from_rankings(voter_rankings)
+    d = _tally_host(b, torch.cuda.current_device())
+    return _to_host_u32(d)
+
+
+def get_winner_and_ranking(candidates: list, strongest_paths) -> tuple:
+    """GPU form of scaling_elections.py:274-296: (winner, ranked candidates), ranking by the
+    number of pairwise wins, descending, ties in candidate order."""
+    _require_cuda()
+    n = len(candidates)
+    if n == 0:
+        raise IndexError("list index out of range")
+    S = strongest_paths[:n, :n]
+    if isinstance(S, torch.Tensor):
+        S = _to_device_u32(_host_u32_matrix(S.cpu()), torch.cuda.current_device())
+    else:
+        S = _to_device_u32(np.ascontiguousarray(np.asarray(S).astype(np.uint32, copy=False)),
+                           torch.cuda.current_device())
+    _, ranking = rank_device(S)
+    order = ranking.cpu().numpy()
+    ranked = [candidates[i] for i in order]
+    return ranked[0], ranked
+
+
+@dataclass
+class SchulzeResult:
+    winner: int
+    ranking: np.ndarray            # int32 [C]
+    wins: np.ndarray               # int32 [C]
+    strongest_paths: np.ndarray | None
+
+
+def schulze(voter_rankings: Sequence[np.ndarray] | np.ndarray, *, return_paths: bool = False) -> SchulzeResult:
+    """Whole Schulze election on the GPU: tally -> closure -> ranking, matrices kept in HBM.
+    Uses 16-bit closure lanes when every count fits (fewer than 65536 voters)."""
+    _require_cuda()
+    b = Ballots.from_rankings(voter_rankings)
+    dev = torch.cuda.current_device()
+    d = _tally_host(b, dev)
+    lanes = LANES_U16 if b.num_voters < 65536 else LANES_U32
+    S = strongest_paths_device(d, lanes=lanes)
+    wins, ranking = rank_device(S)
+    ranking_h = ranking.cpu().numpy()
+    return SchulzeResult(int(ranking_h[0]), ranking_h, wins.cpu().numpy(),
+                         _to_host_u32(S) if return_paths else None)

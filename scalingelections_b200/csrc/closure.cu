@@ -1,0 +1,640 @@
+// Widest-path closure over the (max, min) semiring on sm_100a: the blocked Floyd-Warshall
+// that compute_strongest_paths_cuda (scaling_elections.cu:490-578) drives, redesigned.
+//
+// Layout in HBM (all inside the caller's workspace):
+//   S   Cp x Cp cells, Cp = C rounded up to the 128-cell tile, u16 or u32 per cell. Padding
+//       rows/columns are 0: a vertex with no edges, which no widest path can use.
+//   AT  128 x Cp words: the closed pivot column panel of the current round, transposed
+//       (k-major) and, in u16 mode, with every cell duplicated into both halves of its word
+//       so it is a ready-made `min.u16x2` operand.
+//   dT  128 x 128 words: the closed pivot tile, transposed and duplicated the same way.
+//
+// One round k (pivot block K = rows/cols [128k, 128k+128)):
+//   diag_kernel       1 CTA:       close D = S[K][K] in place, k by k (the only sequential
+//                                  step); emit dT.
+//   row_panel (tile)  R-1 CTAs:    S[K][J] = max(S[K][J], D (x) S[K][J]).
+//   col_panel_kernel  R-1 CTAs:    S[I][K] = max(S[I][K], S[I][K] (x) D); emit AT.
+//   tile_kernel       (R-1)^2 CTAs S[I][J] = max(S[I][J], S[I][K] (x) S[K][J]).
+// where (x) is the max-min product. Because D is closed, a panel needs no sequential k loop:
+// a path k1 ->...-> k2 -> j inside block K is worth min(D*[k1][k2], S[k2][j]). So the
+// panels and the remainder are the same register-blocked "semiring GEMM": operands staged
+// into shared memory by TMA (this GPU's memory only, never multicast), 8 x 8 words per
+// thread, c = max3(c, min(a0, b0), min(a1, b1)) per word and k-pair.
+//
+// The reference's masks (scaling_elections.py:118-121, cu:133-161) are dropped: the closure
+// runs unmasked and the diagonal is zeroed at the end. That is exact: a relaxation through
+// pivot i == j or i == k computes min(S[j][j], S[j][k]) <= S[j][k] or
+// min(S[j][k], S[k][k]) <= S[j][k] and never changes an off-diagonal cell, and diagonal
+// cells only feed such relaxations.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace se {
+namespace closure {
+
+constexpr int kT = 128;             // pivot block edge = tile edge, in cells
+constexpr int kKC = 32;             // k-rows per TMA chunk
+constexpr int kChunks = kT / kKC;   // chunks per tile
+constexpr uint32_t kErrTmaTimeout = 1;
+
+template <int LB> struct cfg {
+    static constexpr int CPW = 32 / LB;               // cells per 32-bit word
+    static constexpr int TW = kT / CPW;               // words per tile row: 64 (u16) / 128 (u32)
+    static constexpr int WN = TW / 64;                // warps across a tile row
+    static constexpr int THREADS = 32 * 4 * WN;       // 128 (u16) / 256 (u32)
+    static constexpr int A_CHUNK = kKC * kT;          // words of one A chunk (k-major, 128 rows)
+    static constexpr int B_CHUNK = kKC * TW;          // words of one B chunk
+    static constexpr uint32_t A_BYTES = A_CHUNK * 4;
+    static constexpr uint32_t B_BYTES = B_CHUNK * 4;
+    // tile_kernel: all of K resident (no ring), one mbarrier per chunk.
+    static constexpr size_t TILE_SMEM = size_t(kChunks) * (A_CHUNK + B_CHUNK) * 4 + kChunks * 8;
+    // col_panel_kernel: the panel tile, its transposed-duplicated copy, and D.
+    static constexpr size_t COL_SMEM = size_t(kT) * TW * 4 * 2 + size_t(kT) * kT * 4 + 2 * kChunks * 8;
+};
+
+// Thread geometry shared by every kernel of one lane mode: warp (wm, wn) of a 4 x WN grid,
+// lane (tr, tc) of a 4 x 8 grid. The thread owns rows row0 .. row0+7 and words
+// wbase .. wbase+3 and wbase+32 .. wbase+35 of the tile, so the 8 threads of a row group read
+// 128 contiguous bytes of B per shared load, and 4 row groups read 4 disjoint bank groups of A.
+struct geom {
+    int row0, wbase;
+    __device__ __forceinline__ explicit geom(int tid) {
+        const int warp = tid >> 5, lane = tid & 31;
+        row0 = (warp & 3) * 32 + (lane >> 3) * 8;
+        wbase = (warp >> 2) * 64 + (lane & 7) * 4;
+    }
+    __device__ __forceinline__ int word(int q) const { return wbase + (q < 4 ? q : 28 + q); }
+};
+
+__device__ __forceinline__ void ld4(uint32_t* dst, const uint32_t* src) {
+    const uint4 v = *reinterpret_cast<const uint4*>(src);
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+}
+__device__ __forceinline__ void st4(uint32_t* dst, const uint32_t* src) {
+    *reinterpret_cast<uint4*>(dst) = make_uint4(src[0], src[1], src[2], src[3]);
+}
+
+// Extract cell h (0 = low half) of a word and duplicate it across the word.
+template <int LB> __device__ __forceinline__ uint32_t cell_splat(uint32_t w, int h);
+template <> __device__ __forceinline__ uint32_t cell_splat<32>(uint32_t w, int) { return w; }
+template <> __device__ __forceinline__ uint32_t cell_splat<16>(uint32_t w, int h) {
+    return __byte_perm(w, 0, h ? 0x3232 : 0x1010);
+}
+
+template <int LB>
+__device__ __forceinline__ void load_tile_regs(uint32_t (&c)[8][8], const uint32_t* base, int64_t ldw,
+                                               const geom& g) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
+        ld4(&c[r][0], p);
+        ld4(&c[r][4], p + 32);
+    }
+}
+
+template <int LB>
+__device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][8], uint32_t* base, int64_t ldw,
+                                                const geom& g) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
+        st4(p, &c[r][0]);
+        st4(p + 32, &c[r][4]);
+    }
+}
+
+// One K-chunk of the semiring product: c = max(c, max_k min(A[k][row], B[k][word])).
+// A is k-major [kKC][kT] (duplicated cells in u16 mode), B is [kKC][TW].
+template <int LB>
+__device__ __forceinline__ void relax_chunk(uint32_t (&c)[8][8], const uint32_t* __restrict__ As,
+                                            const uint32_t* __restrict__ Bs, const geom& g) {
+    using L = lanes<LB>;
+    constexpr int TW = cfg<LB>::TW;
+#pragma unroll
+    for (int k = 0; k < kKC; k += 2) {
+        uint32_t a0[8], a1[8], b0[8], b1[8];
+        ld4(a0, As + k * kT + g.row0);
+        ld4(a0 + 4, As + k * kT + g.row0 + 4);
+        ld4(a1, As + (k + 1) * kT + g.row0);
+        ld4(a1 + 4, As + (k + 1) * kT + g.row0 + 4);
+        ld4(b0, Bs + k * TW + g.wbase);
+        ld4(b0 + 4, Bs + k * TW + g.wbase + 32);
+        ld4(b1, Bs + (k + 1) * TW + g.wbase);
+        ld4(b1 + 4, Bs + (k + 1) * TW + g.wbase + 32);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
+    }
+}
+
+// Poll limit for one mbarrier phase: a TMA chunk lands in microseconds; ~2^26 polls is
+// seconds. Hitting it means a lost completion, reported through the error word.
+constexpr uint32_t kMaxPolls = 1u << 26;
+
+// ------------------------------------------------------------------------------------------
+// Remainder tiles (phase 3) and pivot-row panel tiles (phase 2, rows of block K).
+//   phase3 = true : C = S[I][J], A = AT[:, I], B = S[K][J], grid (R-1, R-1), I, J != K.
+//   phase3 = false: C = S[K][J], A = dT,       B = S[K][J], grid (R-1),      J != K.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    tile_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
+                uint32_t* __restrict__ S, int64_t ldw, int K, int phase3, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem_raw);
+    uint32_t* Bs = As + kChunks * CF::A_CHUNK;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Bs + kChunks * CF::B_CHUNK);
+
+    const int bj = blockIdx.x, bi = blockIdx.y;
+    const int J = bj + (bj >= K);
+    const int I = phase3 ? bi + (bi >= K) : K;
+
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) mbar_init(&bars[c], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::A_BYTES + CF::B_BYTES);
+            tma_load_2d(As + c * CF::A_CHUNK, &mapA, &bars[c], phase3 ? I * kT : 0, c * kKC);
+            tma_load_2d(Bs + c * CF::B_CHUNK, &mapS, &bars[c], J * CF::TW, K * kT + c * kKC);
+        }
+    }
+    const geom g(threadIdx.x);
+    uint32_t c[8][8];
+    uint32_t* Ct = S + int64_t(I) * kT * ldw + int64_t(J) * CF::TW;
+    load_tile_regs<LB>(c, Ct, ldw, g);
+
+    bool ok = true;
+#pragma unroll 1
+    for (int ch = 0; ch < kChunks; ++ch) {
+        if (!mbar_wait_bounded(&bars[ch], 0, kMaxPolls)) {
+            ok = false;
+            break;
+        }
+        relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+    }
+    if (!ok) {
+        raise_device_error(err, kErrTmaTimeout);
+        return;
+    }
+    store_tile_regs<LB>(c, Ct, ldw, g);
+}
+
+// Writes the thread's cells transposed and duplicated: out[k][row] for every cell (row, k)
+// it holds; out is k-major with row stride ld_out words.
+template <int LB>
+__device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8], uint32_t* out,
+                                                       int64_t ld_out, const geom& g) {
+    constexpr int CPW = cfg<LB>::CPW;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int h = 0; h < CPW; ++h) {
+            const int k = g.word(q) * CPW + h;
+            uint32_t v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = cell_splat<LB>(c[r][q], h);
+            uint32_t* p = out + int64_t(k) * ld_out + g.row0;
+            st4(p, v);
+            st4(p + 4, v + 4);
+        }
+}
+
+// ------------------------------------------------------------------------------------------
+// Pivot-column panel tiles (phase 2, columns of block K): C = S[I][K], A = transposed copy of
+// the same tile (built here in shared memory), B = D = S[K][K] (already closed).
+// Writes S[I][K] and the transposed, duplicated panel AT[:, I] that phase 3 reads.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    col_panel_kernel(const __grid_constant__ CUtensorMap mapS, uint32_t* __restrict__ S, int64_t ldw,
+                     int K, uint32_t* __restrict__ AT, int64_t ld_at, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
+    constexpr int TW = CF::TW;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint32_t* tile = reinterpret_cast<uint32_t*>(smem_raw);  // [kT][TW]
+    uint32_t* Ds = tile + kT * TW;                            // [kT][TW]
+    uint32_t* As = Ds + kT * TW;                              // [kT][kT]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(As + kT * kT);
+
+    const int I = blockIdx.x + (int(blockIdx.x) >= K);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::B_BYTES);
+            tma_load_2d(tile + c * CF::B_CHUNK, &mapS, &bars[c], K * TW, I * kT + c * kKC);
+            mbar_arrive_expect_tx(&bars[kChunks + c], CF::B_BYTES);
+            tma_load_2d(Ds + c * CF::B_CHUNK, &mapS, &bars[kChunks + c], K * TW, K * kT + c * kKC);
+        }
+    }
+    bool ok = true;
+#pragma unroll 1
+    for (int c = 0; c < kChunks; ++c) ok = ok && mbar_wait_bounded(&bars[c], 0, kMaxPolls);
+
+    if (ok) {
+        // As[k][i] = splat(cell(i, k)). Each thread walks one half-row (u32) or row (u16) with
+        // a per-row rotation so the 32 lanes of a warp hit 32 different banks on both sides.
+        constexpr int HALVES = CF::THREADS / kT;  // 1 (u16) or 2 (u32)
+        constexpr int SPAN = TW / HALVES;         // 64 words either way
+        const int i = threadIdx.x % kT;
+        const int half = threadIdx.x / kT;
+#pragma unroll 4
+        for (int s = 0; s < SPAN; ++s) {
+            const int w = half * SPAN + ((s + i) & (SPAN - 1));
+            const uint32_t word = tile[i * TW + w];
+#pragma unroll
+            for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
+        }
+    }
+    const geom g(threadIdx.x);
+    uint32_t c[8][8];
+    if (ok) load_tile_regs<LB>(c, tile, TW, g);
+    __syncthreads();
+    if (ok) {
+#pragma unroll 1
+        for (int ch = 0; ch < kChunks; ++ch) {
+            if (!mbar_wait_bounded(&bars[kChunks + ch], 0, kMaxPolls)) {
+                ok = false;
+                break;
+            }
+            relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Ds + ch * CF::B_CHUNK, g);
+        }
+    }
+    if (!ok) {
+        raise_device_error(err, kErrTmaTimeout);
+        return;
+    }
+    store_tile_regs<LB>(c, S + int64_t(I) * kT * ldw + int64_t(K) * TW, ldw, g);
+    store_transposed_splat<LB>(c, AT + int64_t(I) * kT, ld_at, g);
+}
+
+// ------------------------------------------------------------------------------------------
+// Pivot tile (phase 1): close D = S[K][K] in place, one k at a time (k-th row and column are
+// broadcast through double-buffered shared rows, one barrier per k), then emit dT.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    diag_kernel(uint32_t* __restrict__ S, int64_t ldw, int K, uint32_t* __restrict__ dT) {
+    using CF = cfg<LB>;
+    using L = lanes<LB>;
+    constexpr int TW = CF::TW;
+    constexpr int CPW = CF::CPW;
+    __shared__ __align__(16) uint32_t rowbuf[2][TW];
+    __shared__ __align__(16) uint32_t colbuf[2][kT];
+
+    const geom g(threadIdx.x);
+    uint32_t c[8][8];
+    uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * TW;
+    load_tile_regs<LB>(c, D, ldw, g);
+
+    // Publish row 0 and column 0.
+    if (g.row0 == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) rowbuf[0][g.word(q)] = c[0][q];
+    }
+    if (g.wbase == 0) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) colbuf[0][g.row0 + r] = cell_splat<LB>(c[r][0], 0);
+    }
+    __syncthreads();
+
+#pragma unroll 1
+    for (int k = 0; k < kT; ++k) {
+        const int buf = k & 1;
+        uint32_t a[8], b[8];
+        ld4(a, &colbuf[buf][g.row0]);
+        ld4(a + 4, &colbuf[buf][g.row0 + 4]);
+        ld4(b, &rowbuf[buf][g.wbase]);
+        ld4(b + 4, &rowbuf[buf][g.wbase + 32]);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a[r], b[q]));
+        const int k1 = k + 1;
+        if (k1 < kT) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (g.row0 + r == k1) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) rowbuf[buf ^ 1][g.word(q)] = c[r][q];
+                }
+            const int wk = k1 / CPW, hk = k1 % CPW;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (g.word(q) == wk) {
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) colbuf[buf ^ 1][g.row0 + r] = cell_splat<LB>(c[r][q], hk);
+                }
+        }
+        __syncthreads();
+    }
+    store_tile_regs<LB>(c, D, ldw, g);
+    store_transposed_splat<LB>(c, dT, kT, g);
+}
+
+// ------------------------------------------------------------------------------------------
+// Defeat matrix into the padded working matrix (scaling_elections.py:105-112 /
+// cu:495-503): S[i][j] = d[i][j] if d[i][j] > d[j][i] else 0, zero on the diagonal and in
+// the padding. d[j][i] is read through a shared-memory transpose so both reads coalesce.
+// In u16 mode a kept value above 65535 sets the overflow flag.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(256)
+    init_kernel(const uint32_t* __restrict__ d, int64_t ld, int C, int Cp, void* __restrict__ Sv,
+                uint32_t* __restrict__ flags) {
+    __shared__ uint32_t t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // this block writes S[by.., bx..]
+    // Stage d[bx + y][by + x] (the transposed block) so t[x][y] = d[bx + y][by + x].
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = bx + y, cc = by + threadIdx.x;
+        t[threadIdx.x][y] = (r < C && cc < C) ? d[int64_t(r) * ld + cc] : 0u;
+    }
+    __syncthreads();
+    bool over = false;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int i = by + y, j = bx + threadIdx.x;
+        uint32_t v = 0;
+        if (i < C && j < C && i != j) {
+            const uint32_t dij = d[int64_t(i) * ld + j];
+            const uint32_t dji = t[y][threadIdx.x];
+            v = dij > dji ? dij : 0u;
+        }
+        if constexpr (LB == 16) {
+            if (v > 0xFFFFu) {
+                over = true;
+                v = 0xFFFFu;
+            }
+            static_cast<uint16_t*>(Sv)[int64_t(i) * Cp + j] = static_cast<uint16_t>(v);
+        } else {
+            static_cast<uint32_t*>(Sv)[int64_t(i) * Cp + j] = v;
+        }
+    }
+    if (over) atomicOr(&flags[1], 1u);
+}
+
+// out[i][j] = S[i][j] widened to u32, 0 on the diagonal (the reference's masks).
+template <int LB>
+__global__ void __launch_bounds__(256)
+    finalize_kernel(const void* __restrict__ Sv, int Cp, int C, uint32_t* __restrict__ out, int64_t ld_out) {
+    for (int i = blockIdx.y; i < C; i += gridDim.y)
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < C; j += gridDim.x * blockDim.x) {
+            uint32_t v;
+            if constexpr (LB == 16) v = static_cast<const uint16_t*>(Sv)[int64_t(i) * Cp + j];
+            else v = static_cast<const uint32_t*>(Sv)[int64_t(i) * Cp + j];
+            out[int64_t(i) * ld_out + j] = (i == j) ? 0u : v;
+        }
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side.
+// ------------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// 2-D u32 tensor map: dims {inner, outer} words, row pitch in bytes, box {box_x, box_y}.
+se_status_t make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint64_t pitch_bytes,
+                     uint32_t box_x, uint32_t box_y) {
+    auto fn = encode_fn();
+    SE_REQUIRE(fn != nullptr, SE_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {pitch_bytes};
+    cuuint32_t box[2] = {box_x, box_y};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SE_REQUIRE(r == CUDA_SUCCESS, SE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+    return SE_OK;
+}
+
+struct layout {
+    int64_t Cp = 0;
+    int64_t flags_off = 0, s_off = 0, at_off = 0, dt_off = 0, total = 0;
+};
+
+layout plan(int C, int lane_bits) {
+    layout L;
+    L.Cp = round_up(C, kT);
+    const int64_t cell = lane_bits == 16 ? 2 : 4;
+    L.flags_off = 0;
+    L.s_off = 256;
+    L.at_off = L.s_off + round_up(L.Cp * L.Cp * cell, 256);
+    L.dt_off = L.at_off + round_up(int64_t(kT) * L.Cp * 4, 256);
+    L.total = L.dt_off + int64_t(kT) * kT * 4;
+    return L;
+}
+
+template <int LB> se_status_t set_smem_limits() {
+    static se_status_t st = [] {
+        if (cudaFuncSetAttribute(tile_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(cfg<LB>::TILE_SMEM)) != cudaSuccess ||
+            cudaFuncSetAttribute(col_panel_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(cfg<LB>::COL_SMEM)) != cudaSuccess) {
+            cudaGetLastError();
+            return se_status_t(SE_ERR_CUDA);
+        }
+        return se_status_t(SE_OK);
+    }();
+    SE_REQUIRE(st == SE_OK, SE_ERR_CUDA, "cannot raise the shared-memory limit of the closure kernels");
+    return SE_OK;
+}
+
+// Rounds of the blocked closure on an initialised working matrix.
+// phase_ms (optional, 4 entries): accumulated device time of the diagonal, row-panel,
+// column-panel and remainder launches, from events recorded between launches.
+template <int LB>
+se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms) {
+    using CF = cfg<LB>;
+    if (se_status_t st = set_smem_limits<LB>(); st != SE_OK) return st;
+    uint32_t* S = reinterpret_cast<uint32_t*>(work + P.s_off);
+    uint32_t* AT = reinterpret_cast<uint32_t*>(work + P.at_off);
+    uint32_t* dT = reinterpret_cast<uint32_t*>(work + P.dt_off);
+    uint32_t* err = reinterpret_cast<uint32_t*>(work + P.flags_off);
+    const int64_t ldw = P.Cp / CF::CPW;
+    const int R = int(P.Cp / kT);
+
+    CUtensorMap mapS, mapAT, mapDT;
+    if (se_status_t st = make_map(&mapS, S, uint64_t(ldw), uint64_t(P.Cp), uint64_t(ldw) * 4, CF::TW, kKC); st)
+        return st;
+    if (se_status_t st = make_map(&mapAT, AT, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st) return st;
+    if (se_status_t st = make_map(&mapDT, dT, kT, kT, kT * 4, kT, kKC); st) return st;
+
+    std::vector<cudaEvent_t> ev;
+    if (phase_ms) {
+        ev.resize(size_t(R) * 4 + 1, nullptr);
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                for (auto& x : ev)
+                    if (x) cudaEventDestroy(x);
+                SE_CUDA_TRY(cudaGetLastError());
+            }
+        cudaEventRecord(ev[0], stream);
+    }
+    for (int K = 0; K < R; ++K) {
+        diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, K, dT);
+        if (phase_ms) cudaEventRecord(ev[4 * K + 1], stream);
+        if (R > 1) {
+            tile_kernel<LB><<<dim3(R - 1, 1), CF::THREADS, CF::TILE_SMEM, stream>>>(mapDT, mapS, S, ldw, K, 0, err);
+            if (phase_ms) cudaEventRecord(ev[4 * K + 2], stream);
+            col_panel_kernel<LB><<<R - 1, CF::THREADS, CF::COL_SMEM, stream>>>(mapS, S, ldw, K, AT, P.Cp, err);
+            if (phase_ms) cudaEventRecord(ev[4 * K + 3], stream);
+            tile_kernel<LB><<<dim3(R - 1, R - 1), CF::THREADS, CF::TILE_SMEM, stream>>>(mapAT, mapS, S, ldw, K, 1,
+                                                                                       err);
+        } else if (phase_ms) {
+            cudaEventRecord(ev[4 * K + 2], stream);
+            cudaEventRecord(ev[4 * K + 3], stream);
+        }
+        if (phase_ms) cudaEventRecord(ev[4 * K + 4], stream);
+        SE_CHECK_LAUNCH();
+    }
+    if (phase_ms) {
+        cudaError_t e = cudaEventSynchronize(ev.back());
+        for (int p = 0; p < 4; ++p) phase_ms[p] = 0.0;
+        for (int K = 0; K < R && e == cudaSuccess; ++K)
+            for (int p = 0; p < 4; ++p) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[4 * K + p], ev[4 * K + p + 1]);
+                phase_ms[p] += ms;
+            }
+        for (auto& x : ev) cudaEventDestroy(x);
+        SE_CUDA_TRY(e);
+    }
+    return SE_OK;
+}
+
+template <int LB>
+se_status_t launch_init(const uint32_t* d, int64_t ld, int C, const layout& P, uint8_t* work, cudaStream_t s) {
+    const int nb = int(P.Cp / 32);
+    init_kernel<LB><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d, ld, C, int(P.Cp), work + P.s_off,
+                                                       reinterpret_cast<uint32_t*>(work + P.flags_off));
+    SE_CHECK_LAUNCH();
+    return SE_OK;
+}
+
+template <int LB>
+se_status_t launch_finalize(const layout& P, uint8_t* work, int C, uint32_t* out, int64_t ld_out, cudaStream_t s) {
+    const int gx = int((C + 255) / 256);
+    const int gy = C < 65535 ? C : 65535;
+    finalize_kernel<LB><<<dim3(gx, gy), 256, 0, s>>>(work + P.s_off, int(P.Cp), C, out, ld_out);
+    SE_CHECK_LAUNCH();
+    return SE_OK;
+}
+
+}  // namespace closure
+}  // namespace se
+
+using namespace se;
+using namespace se::closure;
+
+extern "C" int64_t se_closure_workspace_bytes(int C, int lane_bits, int tile) {
+    if (C < 1 || (tile != 0 && tile != kT)) return -1;
+    return plan(C, lane_bits == 16 ? 16 : 32).total;
+}
+
+namespace {
+se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
+                         int lane_bits, int tile, void* d_work, int64_t work_bytes, void* stream_, double* phase_ms) {
+    clear_error();
+    SE_REQUIRE(C >= 1, SE_ERR_INVALID, "Number of candidates must be positive");
+    SE_REQUIRE(C <= (1 << 20), SE_ERR_INVALID, "Number of candidates too large (%d)", C);
+    SE_REQUIRE(d_pref && d_out, SE_ERR_INVALID, "null matrix pointer");
+    SE_REQUIRE(ld_pref >= C && ld_out >= C, SE_ERR_INVALID, "row stride smaller than the number of candidates");
+    SE_REQUIRE(lane_bits == 0 || lane_bits == 16 || lane_bits == 32, SE_ERR_INVALID, "lane_bits must be 0, 16 or 32");
+    SE_REQUIRE(tile == 0 || tile == kT, SE_ERR_UNSUPPORTED, "Unsupported tile size");
+    const int64_t need = se_closure_workspace_bytes(C, lane_bits, tile);
+    SE_REQUIRE(d_work != nullptr && work_bytes >= need, SE_ERR_WORKSPACE,
+               "workspace of %lld bytes is smaller than the %lld bytes required", (long long)work_bytes,
+               (long long)need);
+    SE_REQUIRE((reinterpret_cast<uintptr_t>(d_work) & 255) == 0, SE_ERR_INVALID, "workspace must be 256-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream_);
+    uint8_t* work = static_cast<uint8_t*>(d_work);
+
+    int lb = lane_bits == 0 ? 16 : lane_bits;
+    layout P = plan(C, lb);
+    SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
+    if (lb == 16) {
+        if (se_status_t st = launch_init<16>(d_pref, ld_pref, C, P, work, s)) return st;
+        if (lane_bits == 0) {
+            uint32_t over = 0;
+            SE_CUDA_TRY(cudaMemcpyAsync(&over, work + P.flags_off + 4, 4, cudaMemcpyDeviceToHost, s));
+            SE_CUDA_TRY(cudaStreamSynchronize(s));
+            if (over) {
+                lb = 32;
+                P = plan(C, 32);
+                SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
+            }
+        }
+    }
+    if (lb == 32) {
+        if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, s)) return st;
+    }
+    se_status_t st = lb == 16 ? run_rounds<16>(work, P, s, phase_ms) : run_rounds<32>(work, P, s, phase_ms);
+    if (st) return st;
+    st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, s) : launch_finalize<32>(P, work, C, d_out, ld_out, s);
+    if (st) return st;
+
+    uint32_t flags[2] = {0, 0};
+    SE_CUDA_TRY(cudaMemcpyAsync(flags, work + P.flags_off, 8, cudaMemcpyDeviceToHost, s));
+    SE_CUDA_TRY(cudaStreamSynchronize(s));
+    SE_REQUIRE(flags[1] == 0, SE_ERR_OVERFLOW,
+               "a preference count exceeds 65535, which 16-bit lanes cannot hold; use 32-bit lanes");
+    SE_REQUIRE(flags[0] == 0, SE_ERR_DEVICE, "closure kernel reported device error %u (TMA wait timed out)",
+               flags[0]);
+    return SE_OK;
+}
+}  // namespace
+
+extern "C" se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
+                                  int lane_bits, int tile, void* d_work, int64_t work_bytes, void* stream) {
+    return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, nullptr);
+}
+
+extern "C" se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out,
+                                           int64_t ld_out, int lane_bits, int tile, void* d_work, int64_t work_bytes,
+                                           void* stream, double* phase_ms, int* launches) {
+    se_status_t st =
+        closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
+    if (launches) {
+        const int R = int(round_up(C, kT) / kT);
+        *launches = 2 + R + 3 * (R - 1);
+    }
+    return st;
+}
+
+extern "C" int se_closure_launch_count(int C) {
+    if (C < 1) return 0;
+    const int R = int(round_up(C, kT) / kT);
+    return 2 + R + 3 * (R - 1);
+}

@@ -1,0 +1,109 @@
+"""Closure parity on the GPU, through the C ABI: bit-exact against the reference's outputs
+(golden fixtures) and against the CPU oracle on seeded inputs, in both lane modes."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_names, load_golden
+from scalingelections_b200 import LANES_AUTO, LANES_U16, LANES_U32, api
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_closure(P, lanes):
+    d = api._to_device_u32(np.ascontiguousarray(P, dtype=np.uint32), "cuda")
+    out = api.strongest_paths_device(d, lanes=lanes)
+    return api._to_host_u32(out)
+
+
+def lane_modes(P):
+    return [LANES_AUTO, LANES_U32] + ([LANES_U16] if P.max(initial=0) <= 0xFFFF else [])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_closure(name):
+    case = load_golden(name)
+    P = case["preferences"]
+    for lanes in lane_modes(P):
+        S = gpu_closure(P, lanes)
+        import hashlib
+        assert hashlib.sha256(S.tobytes()).hexdigest() == str(case["strongest_sha256"]), (name, lanes)
+
+
+@pytest.mark.parametrize("C", [1, 2, 3, 5, 37, 127, 128, 129, 255, 256, 257, 300, 383, 1000])
+def test_odd_sizes_against_oracle(orc, C):
+    rng = np.random.default_rng(C)
+    for hi in (2, 7, C + 1, 60000):
+        P = rng.integers(0, hi, size=(C, C), dtype=np.uint64).astype(np.uint32)
+        S_ref = orc.strongest_paths(P, "blocked", tile=16)
+        for lanes in lane_modes(P):
+            assert np.array_equal(gpu_closure(P, lanes), S_ref), (C, hi, lanes)
+
+
+def test_u32_values_beyond_16_bits(orc):
+    rng = np.random.default_rng(5)
+    P = rng.integers(0, 2**32 - 1, size=(300, 300), dtype=np.uint64).astype(np.uint32)
+    S_ref = orc.strongest_paths(P, "blocked", tile=16)
+    assert np.array_equal(gpu_closure(P, LANES_U32), S_ref)
+    assert np.array_equal(gpu_closure(P, LANES_AUTO), S_ref)
+    with pytest.raises(api.SchulzeError, match="65535"):
+        gpu_closure(P, LANES_U16)
+
+
+def test_strided_input_and_output(orc):
+    rng = np.random.default_rng(6)
+    C = 200
+    P = rng.integers(0, 500, size=(C, C)).astype(np.uint32)
+    big = torch.zeros((C, C + 13), dtype=torch.int32, device="cuda")
+    big[:, :C] = torch.from_numpy(P.view(np.int32)).cuda()
+    d = big.view(torch.uint32)[:, :C]
+    out_big = torch.full((C, C + 7), -1, dtype=torch.int32, device="cuda")
+    out = out_big.view(torch.uint32)[:, :C]
+    api.strongest_paths_device(d, lanes=LANES_U16, out=out)
+    got = out_big[:, :C].cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, orc.strongest_paths(P, "blocked", tile=16))
+    assert (out_big[:, C:] == -1).all()  # padding columns of the output untouched
+
+
+def test_mallows_c2048_against_oracle(orc):
+    b = orc.mallows_ballots(400, 2048, 0.8, seed=21)
+    d = orc.tally(b, "positions")
+    S_ref = orc.strongest_paths(d, "blocked", tile=32)
+    assert np.array_equal(gpu_closure(d, LANES_U16), S_ref)
+
+
+def test_uniform_c4096_against_oracle(orc):
+    """Single election at C=4096, V=4096, uniform ballots: full matrix equality."""
+    from scalingelections_b200.ballots import uniform_ballots
+
+    b = uniform_ballots(4096, 4096, seed=42)
+    ids = torch.from_numpy(b.reshape(-1)).cuda()
+    offs = torch.arange(4097, dtype=torch.int64, device="cuda") * 4096
+    d = api.tally_device(ids, offs, 4096)
+    d_h = api._to_host_u32(d)
+    S = api._to_host_u32(api.strongest_paths_device(d, lanes=LANES_U16))
+    S_ref = orc.strongest_paths(d_h, "blocked", tile=64)
+    assert np.array_equal(S, S_ref)
+
+
+def test_closure_c16384_rows_by_dijkstra(orc):
+    """Headline size C=16384 (Mallows phi=0.8, V=4096): whole-matrix properties on the GPU
+    plus exact rows from an independent bottleneck Dijkstra on the CPU."""
+    from scalingelections_b200.ballots import mallows_ballots_device
+
+    C, V = 16384, 4096
+    ids = mallows_ballots_device(V, C, 0.8, seed=7).view(-1)
+    offs = torch.arange(V + 1, dtype=torch.int64, device="cuda") * C
+    d = api.tally_device(ids, offs, C)
+    S = api.strongest_paths_device(d, lanes=LANES_U16)
+    S32 = api.strongest_paths_device(d, lanes=LANES_U32)
+    assert torch.equal(S.view(torch.int32), S32.view(torch.int32))
+    d_h = api._to_host_u32(d)
+    S_h = api._to_host_u32(S)
+    rows = [0, 1, 4095, 8191, C - 1]
+    exp = orc.widest_rows(d_h, rows)
+    assert np.array_equal(S_h[rows], exp)
+    # Dominance: S >= the defeat matrix it started from; the diagonal is 0.
+    S0 = orc.defeats(d_h)
+    assert (S_h >= S0).all()
+    assert not np.diagonal(S_h).any()

@@ -1,0 +1,65 @@
+"""Ranking parity (get_winner_and_ranking, scaling_elections.py:274-296) and the whole
+pipeline on the participation-paradox known answer."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import ballots_of, golden_names, load_golden
+from scalingelections_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_ranking(name):
+    case = load_golden(name)
+    if "strongest" not in case:
+        pytest.skip("hash-only fixture")
+    S = case["strongest"]
+    winner, ranking = api.get_winner_and_ranking(list(range(S.shape[0])), S)
+    assert winner == int(case["winner"])
+    assert ranking == list(case["ranking"])
+
+
+def test_ties_keep_index_order(orc):
+    rng = np.random.default_rng(0)
+    for C in (3, 31, 32, 33, 1000, 1025, 3000):
+        S = rng.integers(0, 3, size=(C, C)).astype(np.uint32)  # many equal pairs -> ties
+        wins_ref, rank_ref = orc.wins_and_ranking(S)
+        w, r = api.rank_device(api._to_device_u32(S, "cuda"))
+        assert np.array_equal(w.cpu().numpy(), wins_ref)
+        assert np.array_equal(r.cpu().numpy(), rank_ref)
+
+
+def test_candidate_labels():
+    S = np.array([[0, 2, 2], [1, 0, 1], [1, 2, 0]], np.uint32)
+    assert api.get_winner_and_ranking(["a", "b", "c"], S) == ("a", ["a", "c", "b"])
+
+
+def test_paradox_pipeline():
+    names = ["Python", "Rust", "Go", "Java"]
+    before = api.schulze(ballots_of(load_golden("paradox_before")))
+    after = api.schulze(ballots_of(load_golden("paradox_after")))
+    assert (names[before.winner], names[after.winner]) == ("Java", "Python")
+
+
+@pytest.mark.parametrize("name", ["uniform_c128_v2000", "mallows_c300_v500_phi08", "incomplete_c40_v151"])
+def test_pipeline_matches_reference(name):
+    case = load_golden(name)
+    r = api.schulze(ballots_of(case), return_paths=True)
+    assert r.winner == int(case["winner"])
+    assert list(r.ranking) == list(case["ranking"])
+    assert np.array_equal(r.strongest_paths, case["strongest"])
+
+
+def test_dropin_reference_calls():
+    """The calls scaling_elections.py makes (py:425-430) on the reference's default size."""
+    case = load_golden("uniform_c128_v2000")
+    P = case["preferences"]
+    for tma in (False, True):
+        out = api.compute_strongest_paths(P, allow_gpu=True, allow_tma=tma, tile_size=32)
+        assert out.dtype == np.uint32 and out.flags.c_contiguous
+        assert np.array_equal(out, case["strongest"])
+    out = api.compute_strongest_paths(P.astype(np.int64), allow_gpu=True, tile_size=16)
+    assert np.array_equal(out, case["strongest"])
+    api.log_gpus()
