@@ -181,18 +181,20 @@ def run_reference_arm(args, world, rank):
 # Our arm
 # ------------------------------------------------------------------------------------------
 def load_traffic(lanes: int, C: int):
-    """DRAM bytes per remainder-kernel launch from the committed ncu summary, scaled to C."""
-    p = ROOT / "profiles" / "closure_tile_kernel_traffic.json"
+    """DRAM bytes (read + write) per remainder-kernel launch, from the committed ncu summary
+    of a smaller case, scaled to this C by the number of remainder tiles per launch (the
+    kernel's traffic is proportional to the tiles it processes)."""
+    import re
+
+    p = ROOT / "profiles" / "closure_tile_kernel_u16_c12288.md"
     if not p.exists():
         return None
-    try:
-        rec = json.loads(p.read_text())
-        r = rec[f"u{lanes}"]
-        tiles_ref = (r["C"] // 128 - 1) ** 2
-        tiles = (C // 128 - 1) ** 2 if C % 128 == 0 else ((C + 127) // 128 - 1) ** 2
-        return r["dram_bytes_per_launch"] * tiles / tiles_ref
-    except Exception:
+    m = re.search(r"traffic_bytes_per_launch: u(\d+) C=(\d+) (\d+)", p.read_text())
+    if not m or int(m.group(1)) != lanes:
         return None
+    C_ref, b_ref = int(m.group(2)), int(m.group(3))
+    tiles = lambda c: ((c + 127) // 128 - 1) ** 2
+    return b_ref * tiles(C) / tiles(C_ref)
 
 
 def run_ours(args, world, rank, local_rank):
