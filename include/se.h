@@ -94,6 +94,23 @@ SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, 
  * the automatic mode adds at most one more). */
 SE_API int se_closure_launch_count(int C);
 
+/* Largest C that se_closure_noalloc accepts. */
+#define SE_NOALLOC_MAX_CANDIDATES 2048
+
+/* No counterpart in the reference. The same widest-path closure as se_closure for callers
+ * that cannot allocate device memory: plugins whose host application owns the GPU memory
+ * budget, and latency-critical code that cannot afford cudaMalloc/cudaFree (cudaFree
+ * synchronises the device). The scratch space is a static 18 MiB device array inside this
+ * library, held on every GPU that loads it until the process exits, so C is limited to
+ * 1..SE_NOALLOC_MAX_CANDIDATES; larger C returns SE_ERR_INVALID with a message. Nothing is
+ * allocated or freed. The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress): make that first call before any stream capture. All calls share
+ * the array; calls that overlap on the GPU (e.g. on different streams) race and must be
+ * serialised by the caller. Synchronises `stream` once at the end, like se_closure. */
+SE_API se_status_t se_closure_noalloc(const uint32_t* d_pref, int64_t ld_pref, int C,
+                                      uint32_t* d_out, int64_t ld_out, int lane_bits,
+                                      void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).
  *

@@ -40,6 +40,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp]),
     "se_closure_profiled": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _dp, _ip]),
     "se_closure_launch_count": (_c_int, [_c_int]),
+    "se_closure_noalloc": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_rank": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
