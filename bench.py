@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["closure", "batch"], default="closure",
+                    help="closure: the headline single election; batch: many mixed elections")
+    ap.add_argument("--elections", type=int, default=4096, help="batch: number of elections")
+    ap.add_argument("--max-candidates", type=int, default=2048, help="batch: largest C")
     return ap.parse_args()
 
 
@@ -323,6 +327,119 @@ def run_ours(args, world, rank, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------------------
+# Batched workload: many independent elections of uneven size
+# ------------------------------------------------------------------------------------------
+def batch_specs(n: int, seed: int, c_max: int = 2048):
+    """C log-uniform in [8, c_max], V uniform in [50, 100000], the first half uniform ballots
+    and the second half Mallows with phi uniform in [0.2, 1.0]; seeded."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    C = np.rint(np.exp(rng.uniform(np.log(8), np.log(c_max), size=n))).astype(int)
+    V = rng.integers(50, 100001, size=n)
+    phi = np.where(np.arange(n) < n // 2, 1.0, rng.uniform(0.2, 1.0, size=n))
+    return [(int(C[e]), int(V[e]), float(phi[e]), seed * 1_000_003 + e) for e in range(n)]
+
+
+def make_batch_inputs(specs, dev):
+    """Ballots drawn and tallied on the GPU one election at a time; only the C x C tallies are
+    kept (the ballots of the largest elections are 0.8 GB each)."""
+    import torch
+
+    from scalingelections_b200 import api
+    from scalingelections_b200.ballots import mallows_ballots_device
+
+    prefs = []
+    for (C, V, phi, sd) in specs:
+        b = mallows_ballots_device(V, C, phi, seed=sd, device=dev)
+        offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
+        prefs.append(api.tally_device(b.view(-1), offs, C))
+        del b, offs
+    torch.cuda.synchronize()
+    return prefs
+
+
+def run_batch(args, world, rank, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from scalingelections_b200 import api
+    from scalingelections_b200.batch import BatchedElections, lanes_for_voters
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    specs = batch_specs(args.elections, args.seed + 7919 * rank, args.max_candidates)
+    t0 = time.perf_counter()
+    prefs = make_batch_inputs(specs, dev)
+    prep_s = time.perf_counter() - t0
+    lanes = [lanes_for_voters(V) for (_, V, _, _) in specs]
+    cells = float(sum(C ** 3 for (C, _, _, _) in specs))
+    b = BatchedElections(prefs, lanes)
+    b.build_graph()
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        b.launch_graph()
+    b.check()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.launch_graph()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    b.check()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+
+    # The same batch through the plain single-election entry points, one election at a time,
+    # checked bit for bit against the batched results.
+    ws = torch.empty(max(api.closure_workspace_bytes(C, 0) for (C, _, _, _) in specs),
+                     dtype=torch.uint8, device=dev)
+    outs = [torch.empty_like(p) for p in prefs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ranks = []
+    for p, o in zip(prefs, outs):
+        api.strongest_paths_device(p, lanes=0, out=o, workspace=ws)
+        ranks.append(api.rank_device(o)[1])
+    torch.cuda.synchronize()
+    loop_s = time.perf_counter() - t0
+    identical = all(torch.equal(o.view(torch.int32), bo.view(torch.int32)) and torch.equal(r, br)
+                    for o, bo, r, br in zip(outs, b.outs, ranks, b.rankings))
+
+    n_total = args.elections * world
+    value = n_total / (ms_max * 1e-3)
+    if rank == 0:
+        tasks = b.task_counts()
+        line = {
+            "metric": "elections/s, batched closure + ranking of mixed-size elections", "value": value,
+            "unit": "elections/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u16/u32 per election", "data": "synthetic (seeded uniform and Mallows ballots, GPU-tallied)",
+            "config": {"workload": f"{args.elections} elections per GPU, C log-uniform [8, {args.max_candidates}], "
+                                   "V uniform [50, 100000], half uniform / half Mallows(phi~U[0.2,1])",
+                       "u16_elections": sum(1 for l in lanes if l[0] == 16),
+                       "u16_shifted_elections": sum(1 for l in lanes if l[0] == 16 and l[1] > 0),
+                       "u32_elections": sum(1 for l in lanes if l[0] == 32),
+                       "tasks": {"u16": tasks[0], "u32": tasks[1]}, "graph": True},
+            "batched_gcells_per_s": cells * world / (ms_max * 1e-3) / 1e9,
+            "loop_elections_per_s": args.elections / loop_s,
+            "loop_seconds": loop_s,
+            "speedup_vs_loop": value / world / (args.elections / loop_s),
+            "bit_identical_to_loop": identical,
+            "input_prep_seconds": prep_s,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -340,7 +457,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, world, rank, local_rank)
+        if args.workload == "batch":
+            run_batch(args, world, rank, local_rank)
+        else:
+            run_ours(args, world, rank, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -44,8 +44,10 @@ typedef int se_status_t;
 #define SE_ERR_WORKSPACE 6   /* d_work missing or smaller than the *_workspace_bytes() query */
 
 /* Lane modes for the closure: 16 = two u16 cells per 32-bit word (every count < 65536),
- * 32 = one u32 cell per word, 0 = choose on the device (u16 when max(d) < 65536; this costs
- * one 4-byte device-to-host read and a stream synchronisation). */
+ * 32 = one u32 cell per word, 0 = choose on the device: 16-bit lanes whenever the kept
+ * defeat values fit a window of 65535 (stored shifted by a base; the closure commutes with
+ * that shift), which holds for any tally of up to 131070 ballots; else 32-bit. The automatic
+ * choice costs one pass over d, an 8-byte device-to-host read and a stream synchronisation. */
 #define SE_LANES_AUTO 0
 #define SE_LANES_U16 16
 #define SE_LANES_U32 32
@@ -110,6 +112,59 @@ SE_API int se_closure_launch_count(int C);
 SE_API se_status_t se_closure_noalloc(const uint32_t* d_pref, int64_t ld_pref, int C,
                                       uint32_t* d_out, int64_t ld_out, int lane_bits,
                                       void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Batched closure (no reference counterpart; the reference closes one matrix per call,
+ * scaling_elections.cu:863-989): many independent elections of uneven size, all tasks in
+ * one persistent launch per lane mode, optionally replayed as a CUDA graph.
+ *
+ * Each election gives its preference matrix, output matrix and (optionally, both or
+ * neither) wins/ranking arrays, with the same meaning as se_closure and se_rank. Elections
+ * with C <= 128 run whole inside one CTA; larger ones are cut into 128 x 128 tile tasks
+ * scheduled by per-election round counters. lane_bits per election: 16 or 32 (0 means 32).
+ * 16-bit lanes hold every kept value v (d[i][j] > d[j][i]) as v - value_offset, which must
+ * lie in [1, 65535]; the closure commutes with that shift, so results stay exact. For counts
+ * from V ballots, value_offset = V / 2 (rounded down) works for every V <= 131070, and 0 for
+ * V < 65536. A value outside the window makes se_batch_check report SE_ERR_OVERFLOW.
+ *
+ *   se_batch_workspace_bytes   device bytes for the batch (host-only computation).
+ *   se_batch_prepare           builds the task queues and tensor maps and uploads them into
+ *                              d_work (synchronous copies); fills the caller's plan.
+ *                              order: 0 = small elections after the tiled ones, 1 = before.
+ *   se_batch_run               enqueues one whole batch on `stream` (asynchronous, no host
+ *                              synchronisation, capturable).
+ *   se_batch_graph_build       captures se_batch_run into a CUDA graph held by the plan;
+ *   se_batch_graph_launch      replays it on `stream`; se_batch_release frees the graph.
+ *   se_batch_check             reads the batch's device error word (synchronises `stream`).
+ * The plan refers to d_work and to the elections' buffers: keep them alive while it is used.
+ * ------------------------------------------------------------------------------------- */
+typedef struct se_election {
+    const uint32_t* d_pref;
+    int64_t ld_pref;
+    uint32_t* d_out;
+    int64_t ld_out;
+    int32_t* d_wins;    /* C entries, or NULL */
+    int32_t* d_ranking; /* C entries, or NULL */
+    int32_t C;
+    int32_t lane_bits;
+    uint32_t value_offset; /* 16-bit lanes only */
+    int32_t reserved;
+} se_election_t;
+
+typedef struct se_batch_plan {
+    int64_t opaque[40];
+} se_batch_plan_t;
+
+SE_API int64_t se_batch_workspace_bytes(int n, const se_election_t* elections);
+SE_API se_status_t se_batch_prepare(int n, const se_election_t* elections, void* d_work,
+                                    int64_t work_bytes, int order, se_batch_plan_t* plan);
+SE_API se_status_t se_batch_run(const se_batch_plan_t* plan, void* stream);
+SE_API se_status_t se_batch_graph_build(se_batch_plan_t* plan);
+SE_API se_status_t se_batch_graph_launch(const se_batch_plan_t* plan, void* stream);
+SE_API se_status_t se_batch_release(se_batch_plan_t* plan);
+SE_API se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream);
+/* Number of tasks in queue 0 (16-bit lanes) or 1 (32-bit lanes) of a prepared plan. */
+SE_API int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue);
 
 /* ---------------------------------------------------------------------------------------
  * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).

@@ -41,6 +41,14 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure_profiled": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _dp, _ip]),
     "se_closure_launch_count": (_c_int, [_c_int]),
     "se_closure_noalloc": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _vp]),
+    "se_batch_workspace_bytes": (_c_i64, [_c_int, _vp]),
+    "se_batch_prepare": (_c_int, [_c_int, _vp, _vp, _c_i64, _c_int, _vp]),
+    "se_batch_run": (_c_int, [_vp, _vp]),
+    "se_batch_graph_build": (_c_int, [_vp]),
+    "se_batch_graph_launch": (_c_int, [_vp, _vp]),
+    "se_batch_release": (_c_int, [_vp]),
+    "se_batch_check": (_c_int, [_vp, _vp]),
+    "se_batch_task_count": (_c_i64, [_vp, _c_int]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_rank": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
@@ -48,6 +56,19 @@ SIGNATURES: dict[str, tuple] = {
     "se_mallows_ballots": (_c_int, [_c_i64, _c_int, ctypes.c_double, ctypes.c_uint64, _vp, _vp, _vp, _c_i64, _vp]),
     "se_minmax_peak": (_c_int, [_c_int, _c_int, _dp, _dp, _dp, _dp]),
 }
+
+class Election(ctypes.Structure):
+    """se_election_t"""
+    _fields_ = [("d_pref", ctypes.c_void_p), ("ld_pref", ctypes.c_int64), ("d_out", ctypes.c_void_p),
+                ("ld_out", ctypes.c_int64), ("d_wins", ctypes.c_void_p), ("d_ranking", ctypes.c_void_p),
+                ("C", ctypes.c_int32), ("lane_bits", ctypes.c_int32), ("value_offset", ctypes.c_uint32),
+                ("reserved", ctypes.c_int32)]
+
+
+class BatchPlan(ctypes.Structure):
+    """se_batch_plan_t (opaque)"""
+    _fields_ = [("opaque", ctypes.c_int64 * 40)]
+
 
 _lib: ctypes.CDLL | None = None
 _lock = threading.Lock()

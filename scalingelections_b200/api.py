@@ -314,7 +314,9 @@ def schulze(voter_rankings: Sequence[np.ndarray] | np.ndarray, *, return_paths: 
     b = Ballots.from_rankings(voter_rankings)
     dev = torch.cuda.current_device()
     d = _tally_host(b, dev)
-    lanes = LANES_U16 if b.num_voters < 65536 else LANES_U32
+    # Below 65536 ballots every count fits 16 bits; above, the automatic mode still finds a
+    # shifted 16-bit window (kept counts lie in (V/2, V]) up to 131070 ballots.
+    lanes = LANES_U16 if b.num_voters < 65536 else LANES_AUTO
     S = strongest_paths_device(d, lanes=lanes)
     wins, ranking = rank_device(S)
     ranking_h = ranking.cpu().numpy()

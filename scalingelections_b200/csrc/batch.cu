@@ -1,0 +1,908 @@
+// Batched persistent widest-path closure: many independent elections of uneven size in one
+// launch per lane mode (no reference counterpart; the reference closes one matrix per call,
+// scaling_elections.cu:863-989, one host-synchronised round at a time).
+//
+// Work is cut into tasks, all on 128 x 128 tiles:
+//   SMALL      an election with C <= 128, whole in one CTA: defeat init from d, closure over
+//              its C pivots in registers, u32 output, wins and ranking. Nothing in HBM but d
+//              and the outputs.
+//   PIVOT k    close the pivot tile (k, k) of a larger election in registers; emit dT.
+//   ROW k, j   pivot-row panel tile (k, j)       = max(P, D (x) P)
+//   COL k, i   pivot-column panel tile (i, k)    = max(P, P (x) D); emit AT (transposed).
+//   REM k,i,j  remainder tile (i, j)             = max(S, AT (x) S[k][j])
+// using the same device routines as the single-election kernels (closure_core.cuh).
+//
+// Scheduling: one persistent grid (every CTA resident) pulls tasks from a queue with an atomic
+// counter. The queue is ordered so that every task comes after the tasks it depends on:
+// round-major across elections (all pivots of round k, then all panels, then all remainders,
+// largest elections first), then the SMALL tasks, which fill the tail. A task waits (thread 0,
+// bounded by %globaltimer) on its election's per-round counters:
+//   PIVOT k   needs REM k-1 complete ((R-1)^2 tiles)
+//   ROW/COL k needs PIVOT k
+//   REM k     needs all 2(R-1) panels of round k
+// Because a task's prerequisites were dequeued earlier by CTAs that are running, and those only
+// wait on even earlier tasks, the schedule cannot deadlock. A wait that times out sets the
+// error word and an abort flag that makes every CTA drain the queue and exit.
+//
+// Memory ordering: a finished task's threads fence (gpu scope), the CTA barriers, and thread 0
+// bumps the counter. A waiting task's thread 0 reads the counter with acquire semantics, then
+// fences the async proxy before its TMA loads; generic loads of tiles another CTA wrote go
+// through ld.global.cg (L2), never a possibly stale L1 line.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "closure_core.cuh"
+
+namespace se {
+namespace batch {
+using namespace se::closure;
+
+enum : uint32_t { kSmall = 0, kPivot = 1, kRow = 2, kCol = 3, kRem = 4 };
+constexpr uint64_t kNoTask = ~0ull;
+constexpr uint32_t kErrTimeout = 1;
+constexpr uint32_t kErrOverflow = 2;
+constexpr uint32_t kErrDepTimeout = 3;
+constexpr uint64_t kDepWaitNs = 5000000000ull;  // 5 s for one dependency
+
+struct alignas(64) Elec {
+    CUtensorMap mapS;   // working matrix, box {TW, 32}
+    CUtensorMap mapAT;  // transposed column panel, box {128, 32}
+    CUtensorMap mapDT;  // transposed pivot tile, box {128, 32}
+    const uint32_t* d;
+    int64_t ld;
+    uint32_t* out;
+    int64_t ld_out;
+    int32_t* wins;
+    int32_t* ranking;
+    uint32_t* S;
+    uint32_t* AT;
+    uint32_t* dT;
+    uint32_t* counters;  // [0, R): pivot done; [R, 2R): panels done; [2R, 3R): remainder done
+    int32_t C, Cp, R, lanes;
+    uint32_t base;  // u16 lanes store a kept value v as v - base (see init_kernel in closure.cu)
+};
+
+// Kept defeat value v -> stored u16 cell, or a flagged overflow outside [base+1, base+65535].
+__device__ __forceinline__ uint32_t to_lane16(uint32_t v, uint32_t base, bool& over) {
+    if (v == 0u) return 0u;
+    if (v <= base || v - base > 0xFFFFu) {
+        over = true;
+        return 0xFFFFu;
+    }
+    return v - base;
+}
+
+struct Header {
+    uint32_t err;
+    uint32_t abort;
+    uint32_t head[2];  // queue heads of the u16 and u32 persistent launches
+};
+
+__host__ __device__ inline uint64_t pack_task(uint32_t e, uint32_t type, uint32_t k, uint32_t i, uint32_t j) {
+    return (uint64_t(e) << 39) | (uint64_t(type) << 36) | (uint64_t(k) << 24) | (uint64_t(i) << 12) | uint64_t(j);
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_tensormap(const void* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// Thread 0 only: wait until *ctr >= target or the abort flag rises or time runs out.
+__device__ bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag) {
+    if (ld_acquire(ctr) >= target) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (ld_acquire(ctr) >= target) return true;
+        if ((it & 63) == 0) {
+            if (ld_acquire(abort_flag)) return false;
+            if (global_ns() - t0 > kDepWaitNs) return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <int LB> struct pcfg {
+    using CF = cfg<LB>;
+    static constexpr size_t A_REGION = size_t(kChunks) * CF::A_CHUNK * 4;  // 64 KiB
+    static constexpr size_t B_REGION = size_t(kChunks) * CF::B_CHUNK * 4;  // 32 / 64 KiB
+    static constexpr size_t SMALL_BYTES = size_t(kT) * (kT + 1) * 4;         // d tile, padded rows
+    static constexpr size_t DATA = (A_REGION + B_REGION) > SMALL_BYTES ? (A_REGION + B_REGION) : SMALL_BYTES;
+    static constexpr size_t SMEM = DATA + 8 * 8;                              // + 8 mbarriers
+};
+
+// ------------------------------------------------------------------------------------------
+// SMALL: whole election in this CTA.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__device__ void run_small(const Elec& E, uint8_t* smem, uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT],
+                          int32_t* s_wins, uint32_t* err) {
+    constexpr int CPW = cfg<LB>::CPW;
+    constexpr int P = kT + 1;  // padded row pitch: row and column walks are bank-conflict free
+    uint32_t* dt = reinterpret_cast<uint32_t*>(smem);
+    const int C = E.C;
+    const geom g(threadIdx.x);
+    for (int idx = threadIdx.x; idx < kT * kT; idx += blockDim.x) {
+        const int r = idx / kT, c = idx % kT;
+        dt[r * P + c] = (r < C && c < C) ? __ldcg(E.d + int64_t(r) * E.ld + c) : 0u;
+    }
+    __syncthreads();
+    uint32_t c[8][8];
+    bool over = false;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int i = g.row0 + r;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int h = 0; h < CPW; ++h) {
+                const int j = g.word(q) * CPW + h;
+                const uint32_t dij = dt[i * P + j], dji = dt[j * P + i];
+                uint32_t v = (i != j && dij > dji) ? dij : 0u;
+                if constexpr (LB == 16) {
+                    w |= to_lane16(v, E.base, over) << (16 * h);
+                } else {
+                    w = v;
+                }
+            }
+            c[r][q] = w;
+        }
+    }
+    if (over) raise_device_error(err, kErrOverflow);
+    close_tile_in_registers<LB>(c, g, C, rowbuf, colbuf);
+    // Output, and the u32 matrix again in shared memory for the ranking.
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int i = g.row0 + r;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+#pragma unroll
+            for (int h = 0; h < CPW; ++h) {
+                const int j = g.word(q) * CPW + h;
+                uint32_t v = LB == 16 ? (c[r][q] >> (16 * h)) & 0xFFFFu : c[r][q];
+                if (LB == 16 && v) v += E.base;
+                if (i == j) v = 0u;
+                dt[i * P + j] = v;
+                if (i < C && j < C) E.out[int64_t(i) * E.ld_out + j] = v;
+            }
+    }
+    if (E.wins == nullptr) return;
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < C) {
+        int w = 0;
+        for (int j = 0; j < C; ++j) w += dt[t * P + j] > dt[j * P + t];
+        s_wins[t] = w;
+        E.wins[t] = w;
+    }
+    __syncthreads();
+    if (t < C) {
+        const int wt = s_wins[t];
+        int place = 0;
+        for (int j = 0; j < C; ++j) {
+            const int wj = s_wins[j];
+            place += (wj > wt) | ((wj == wt) & (j < t));
+        }
+        E.ranking[place] = t;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Tile tasks of elections with R >= 2.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__device__ void run_pivot(const Elec& E, int k, uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT]) {
+    using CF = cfg<LB>;
+    const geom g(threadIdx.x);
+    const int64_t ldw = E.Cp / CF::CPW;
+    uint32_t* D = E.S + int64_t(k) * kT * ldw + int64_t(k) * CF::TW;
+    uint32_t c[8][8];
+    load_tile_regs<LB, true>(c, D, ldw, g);
+    const int kmax = E.C - k * kT < kT ? E.C - k * kT : kT;  // pivots past C are zero padding
+    close_tile_in_registers<LB>(c, g, kmax, rowbuf, colbuf);
+    store_tile_regs<LB>(c, D, ldw, g);
+    store_transposed_splat<LB>(c, E.dT, kT, g);
+}
+
+// REM (a_panel = true: A = AT[:, I], C = S[I][J]) or ROW (A = dT, C = S[K][J]); B = S[K][J].
+template <int LB>
+__device__ bool run_product(const Elec& E, int K, int I, int J, bool a_panel, uint8_t* smem, uint64_t* bars,
+                            uint32_t parity) {
+    using CF = cfg<LB>;
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
+    const CUtensorMap* mapA = a_panel ? &E.mapAT : &E.mapDT;
+    if (threadIdx.x == 0) {
+        fence_tensormap(mapA);
+        fence_tensormap(&E.mapS);
+        fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::A_BYTES + CF::B_BYTES);
+            tma_load_2d(As + c * CF::A_CHUNK, mapA, &bars[c], a_panel ? I * kT : 0, c * kKC);
+            tma_load_2d(Bs + c * CF::B_CHUNK, &E.mapS, &bars[c], J * CF::TW, K * kT + c * kKC);
+        }
+    }
+    const geom g(threadIdx.x);
+    const int64_t ldw = E.Cp / CF::CPW;
+    uint32_t* Ct = E.S + int64_t(I) * kT * ldw + int64_t(J) * CF::TW;
+    uint32_t c[8][8];
+    load_tile_regs<LB, true>(c, Ct, ldw, g);
+    bool ok = true;
+#pragma unroll 1
+    for (int ch = 0; ch < kChunks; ++ch) {
+        if (!mbar_wait_bounded(&bars[ch], parity, 1u << 26)) {
+            ok = false;
+            break;
+        }
+        relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+    }
+    if (ok) store_tile_regs<LB>(c, Ct, ldw, g);
+    return ok;
+}
+
+template <int LB>
+__device__ bool run_col(const Elec& E, int K, int I, uint8_t* smem, uint64_t* bars, uint32_t parity_a,
+                        uint32_t parity_b) {
+    using CF = cfg<LB>;
+    constexpr int TW = CF::TW;
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);                          // [kT][kT]
+    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);     // tile, then D
+    if (threadIdx.x == 0) {
+        fence_tensormap(&E.mapS);
+        fence_proxy_async();
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::B_BYTES);
+            tma_load_2d(Bs + c * CF::B_CHUNK, &E.mapS, &bars[c], K * TW, I * kT + c * kKC);
+        }
+    }
+    bool ok = true;
+#pragma unroll 1
+    for (int c = 0; c < kChunks; ++c) ok = ok && mbar_wait_bounded(&bars[c], parity_a, 1u << 26);
+    const geom g(threadIdx.x);
+    uint32_t c[8][8];
+    if (ok) {
+        constexpr int HALVES = CF::THREADS / kT;
+        constexpr int SPAN = TW / HALVES;
+        const int i = threadIdx.x % kT;
+        const int half = threadIdx.x / kT;
+#pragma unroll 4
+        for (int s = 0; s < SPAN; ++s) {
+            const int w = half * SPAN + ((s + i) & (SPAN - 1));
+            const uint32_t word = Bs[i * TW + w];
+#pragma unroll
+            for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
+        }
+        load_tile_regs<LB>(c, Bs, TW, g);
+    }
+    __syncthreads();  // the tile region is free again
+    if (threadIdx.x == 0 && ok) {
+        fence_proxy_async();
+#pragma unroll
+        for (int ch = 0; ch < kChunks; ++ch) {
+            mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
+            tma_load_2d(Bs + ch * CF::B_CHUNK, &E.mapS, &bars[kChunks + ch], K * TW, K * kT + ch * kKC);
+        }
+    }
+    if (ok) {
+#pragma unroll 1
+        for (int ch = 0; ch < kChunks; ++ch) {
+            if (!mbar_wait_bounded(&bars[kChunks + ch], parity_b, 1u << 26)) {
+                ok = false;
+                break;
+            }
+            relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+        }
+    }
+    if (ok) {
+        const int64_t ldw = E.Cp / CF::CPW;
+        store_tile_regs<LB>(c, E.S + int64_t(I) * kT * ldw + int64_t(K) * TW, ldw, g);
+        store_transposed_splat<LB>(c, E.AT + int64_t(I) * kT, E.Cp, g);
+    }
+    return ok;
+}
+
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    persistent_kernel(const Elec* __restrict__ elecs, const uint64_t* __restrict__ tasks, uint32_t ntasks,
+                      Header* __restrict__ hdr, int queue) {
+    using CF = cfg<LB>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ int32_t s_wins[kT];
+    __shared__ uint64_t s_task;
+    __shared__ uint32_t s_go;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + pcfg<LB>::DATA);
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2 * kChunks; ++b) mbar_init(&bars[b], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t par_a = 0, par_b = 0;  // phase parity of barriers [0, 4) and [4, 8)
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint64_t t = kNoTask;
+            if (!ld_acquire(&hdr->abort)) {
+                const uint32_t n = atomicAdd(&hdr->head[queue], 1u);
+                if (n < ntasks) t = tasks[n];
+            }
+            s_task = t;
+            s_go = 1;
+            if (t != kNoTask) {
+                const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u, k = uint32_t(t >> 24) & 0xFFFu;
+                const Elec& E = elecs[e];
+                const uint32_t R = uint32_t(E.R);
+                bool ok = true;
+                if (type == kPivot && k > 0) ok = wait_counter(&E.counters[2 * R + k - 1], (R - 1) * (R - 1), &hdr->abort);
+                else if (type == kRow || type == kCol) ok = wait_counter(&E.counters[k], 1u, &hdr->abort);
+                else if (type == kRem) ok = wait_counter(&E.counters[R + k], 2u * (R - 1), &hdr->abort);
+                if (!ok) {
+                    raise_device_error(&hdr->err, kErrDepTimeout);
+                    atomicExch(&hdr->abort, 1u);
+                    s_go = 0;
+                }
+                fence_proxy_async_global();
+            }
+        }
+        __syncthreads();
+        const uint64_t t = s_task;
+        if (t == kNoTask || !s_go) break;
+        const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u, k = uint32_t(t >> 24) & 0xFFFu;
+        const uint32_t i = uint32_t(t >> 12) & 0xFFFu, j = uint32_t(t) & 0xFFFu;
+        const Elec& E = elecs[e];
+        bool ok = true;
+        if (type == kSmall) {
+            run_small<LB>(E, smem, rowbuf, colbuf, s_wins, &hdr->err);
+        } else if (type == kPivot) {
+            run_pivot<LB>(E, int(k), rowbuf, colbuf);
+        } else if (type == kRow) {
+            ok = run_product<LB>(E, int(k), int(k), int(j), false, smem, bars, par_a);
+            par_a ^= 1u;
+        } else if (type == kCol) {
+            ok = run_col<LB>(E, int(k), int(i), smem, bars, par_a, par_b);
+            par_a ^= 1u;
+            par_b ^= 1u;
+        } else {
+            ok = run_product<LB>(E, int(k), int(i), int(j), true, smem, bars, par_a);
+            par_a ^= 1u;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (!ok) {
+                raise_device_error(&hdr->err, kErrTimeout);
+                atomicExch(&hdr->abort, 1u);
+            } else if (type != kSmall) {
+                fence_proxy_async_global();
+                const uint32_t R = uint32_t(E.R);
+                const uint32_t slot = type == kPivot ? k : (type == kRem ? 2 * R + k : R + k);
+                atomicAdd(&E.counters[slot], 1u);
+            }
+        }
+        if (!ok) break;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched elementwise kernels over the elections with R >= 2: block b belongs to the big
+// election m with prefix[m] <= b < prefix[m + 1].
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int find_owner(const int64_t* prefix, int n, int64_t b) {
+    int lo = 0, hi = n;  // prefix[lo] <= b < prefix[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Defeat matrix into the padded working matrix (see init_kernel in closure.cu); also zeroes
+// the election's wins.
+__global__ void __launch_bounds__(256)
+    batch_init_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big, const int64_t* __restrict__ prefix,
+                      int nbig, Header* __restrict__ hdr) {
+    __shared__ uint32_t t[32][33];
+    const int64_t b = blockIdx.x;
+    const int m = find_owner(prefix, nbig, b);
+    const Elec& E = elecs[big[m]];
+    const int64_t local = b - prefix[m];
+    const int nb = E.Cp / 32;
+    const int bx = int(local % nb) * 32, by = int(local / nb) * 32;
+    const int C = E.C;
+    if (local == 0 && E.wins)
+        for (int x = threadIdx.y * 32 + threadIdx.x; x < C; x += 256) E.wins[x] = 0;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = bx + y, cc = by + threadIdx.x;
+        t[threadIdx.x][y] = (r < C && cc < C) ? E.d[int64_t(r) * E.ld + cc] : 0u;
+    }
+    __syncthreads();
+    bool over = false;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int i = by + y, j = bx + threadIdx.x;
+        uint32_t v = 0;
+        if (i < C && j < C && i != j) {
+            const uint32_t dij = E.d[int64_t(i) * E.ld + j];
+            const uint32_t dji = t[y][threadIdx.x];
+            v = dij > dji ? dij : 0u;
+        }
+        if (E.lanes == 16) {
+            reinterpret_cast<uint16_t*>(E.S)[int64_t(i) * E.Cp + j] = uint16_t(to_lane16(v, E.base, over));
+        } else {
+            E.S[int64_t(i) * E.Cp + j] = v;
+        }
+    }
+    if (over) raise_device_error(&hdr->err, kErrOverflow);
+}
+
+// Output (u32, zero diagonal) and wins, one unordered pair of 32 x 32 blocks per CTA.
+__global__ void __launch_bounds__(256)
+    batch_finalize_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
+                          const int64_t* __restrict__ prefix, int nbig) {
+    __shared__ uint32_t tJI[32][33];
+    __shared__ int32_t wi[32], wj[32];
+    const int64_t b = blockIdx.x;
+    const int m = find_owner(prefix, nbig, b);
+    const Elec& E = elecs[big[m]];
+    int64_t local = b - prefix[m];
+    const int C = E.C, nb = (C + 31) / 32;
+    int bi = 0;
+    while (local >= nb - bi) {
+        local -= nb - bi;
+        ++bi;
+    }
+    const int bj = bi + int(local);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    auto cell = [&](int r, int c) -> uint32_t {
+        if (E.lanes == 16) {
+            const uint32_t v = reinterpret_cast<const uint16_t*>(E.S)[int64_t(r) * E.Cp + c];
+            return v ? v + E.base : 0u;
+        }
+        return E.S[int64_t(r) * E.Cp + c];
+    };
+    if (ty == 0) wi[tx] = 0, wj[tx] = 0;
+    for (int y = ty; y < 32; y += 8) {
+        const int r = bj * 32 + y, c = bi * 32 + tx;
+        const uint32_t v = (r < C && c < C) ? cell(r, c) : 0u;
+        tJI[tx][y] = v;
+        if (r < C && c < C && bi != bj) E.out[int64_t(r) * E.ld_out + c] = v;
+    }
+    __syncthreads();
+    for (int y = ty; y < 32; y += 8) {
+        const int i = bi * 32 + y, j = bj * 32 + tx;
+        if (i < C && j < C) {
+            const uint32_t sij = cell(i, j);
+            E.out[int64_t(i) * E.ld_out + j] = i == j ? 0u : sij;
+            if (E.wins && (bi != bj || j > i)) {
+                const uint32_t sji = tJI[y][tx];
+                if (sij > sji) atomicAdd(&wi[y], 1);
+                else if (sji > sij) atomicAdd(&wj[tx], 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (ty == 0 && E.wins) {
+        const int i = bi * 32 + tx, j = bj * 32 + tx;
+        if (i < C && wi[tx]) atomicAdd(&E.wins[i], wi[tx]);
+        if (j < C && wj[tx]) atomicAdd(&E.wins[j], wj[tx]);
+    }
+}
+
+// Ranking of the elections with R >= 2 (see place_kernel in rank.cu).
+__global__ void __launch_bounds__(256)
+    batch_place_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
+                       const int64_t* __restrict__ prefix, int nbig) {
+    __shared__ int32_t w[1024];
+    const int64_t b = blockIdx.x;
+    const int m = find_owner(prefix, nbig, b);
+    const Elec& E = elecs[big[m]];
+    if (!E.wins) return;
+    const int C = E.C;
+    const int i = int(b - prefix[m]) * 256 + threadIdx.x;
+    const int wi = i < C ? E.wins[i] : 0;
+    int place = 0;
+    for (int j0 = 0; j0 < C; j0 += 1024) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < 1024; t += 256) w[t] = j0 + t < C ? E.wins[j0 + t] : -1;
+        __syncthreads();
+        const int n = C - j0 < 1024 ? C - j0 : 1024;
+        for (int t = 0; t < n; ++t) {
+            const int wj = w[t];
+            place += (wj > wi) | ((wj == wi) & (j0 + t < i));
+        }
+    }
+    if (i < C) E.ranking[place] = i;
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side: the plan lives in the caller's se_batch_plan_t; everything else in d_work.
+// ------------------------------------------------------------------------------------------
+struct Plan {
+    uint8_t* work;
+    int64_t work_bytes;
+    int32_t n, nbig, nsmall;
+    int64_t elec_off, big_off, init_prefix_off, fin_prefix_off, place_prefix_off, counters_off, counters_bytes;
+    int64_t tasks_off[2];
+    uint32_t ntasks[2];
+    int64_t init_blocks, fin_blocks, place_blocks;
+    int32_t grid[2];
+    cudaGraphExec_t graph;
+};
+static_assert(sizeof(Plan) <= sizeof(se_batch_plan_t), "se_batch_plan_t too small");
+
+int64_t align256(int64_t x) { return round_up(x, 256); }
+
+struct Sizes {
+    int64_t total = 0, elec_off, big_off, init_prefix_off, fin_prefix_off, place_prefix_off, counters_off,
+            counters_bytes, tasks_off[2];
+    std::vector<int64_t> s_off, at_off, dt_off, ctr_off;
+    std::vector<int> lanes, R, Cp;
+    int nbig = 0, nsmall = 0;
+    uint32_t ntasks[2] = {0, 0};
+};
+
+se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
+    SE_REQUIRE(n >= 0, SE_ERR_INVALID, "negative election count");
+    SE_REQUIRE(n < (1 << 24), SE_ERR_INVALID, "too many elections in one batch (%d)", n);
+    z.s_off.assign(n, -1);
+    z.at_off.assign(n, -1);
+    z.dt_off.assign(n, -1);
+    z.ctr_off.assign(n, -1);
+    z.lanes.resize(n);
+    z.R.resize(n);
+    z.Cp.resize(n);
+    int64_t off = 256;  // header
+    z.elec_off = off;
+    off = align256(off + int64_t(n) * int64_t(sizeof(Elec)));
+    for (int e = 0; e < n; ++e) {
+        SE_REQUIRE(el[e].C >= 1 && el[e].C <= (1 << 19), SE_ERR_INVALID, "election %d: bad candidate count %d", e,
+                   el[e].C);
+        SE_REQUIRE(el[e].lane_bits == 0 || el[e].lane_bits == 16 || el[e].lane_bits == 32, SE_ERR_INVALID,
+                   "election %d: lane_bits must be 0, 16 or 32", e);
+        z.lanes[e] = el[e].lane_bits == 16 ? 16 : 32;
+        z.Cp[e] = int(round_up(el[e].C, kT));
+        z.R[e] = z.Cp[e] / kT;
+        SE_REQUIRE(z.R[e] <= 4095, SE_ERR_INVALID, "election %d too large for a batch", e);
+        if (z.R[e] == 1) {
+            ++z.nsmall;
+            z.ntasks[z.lanes[e] == 16 ? 0 : 1] += 1;
+            continue;
+        }
+        ++z.nbig;
+        const int64_t cell = z.lanes[e] == 16 ? 2 : 4;
+        z.s_off[e] = off;
+        off = align256(off + int64_t(z.Cp[e]) * z.Cp[e] * cell);
+        z.at_off[e] = off;
+        off = align256(off + int64_t(kT) * z.Cp[e] * 4);
+        z.dt_off[e] = off;
+        off = align256(off + int64_t(kT) * kT * 4);
+        const uint64_t R = uint64_t(z.R[e]);
+        z.ntasks[z.lanes[e] == 16 ? 0 : 1] += uint32_t(R * R * R);
+    }
+    z.counters_off = off;
+    int64_t ctr = 0;
+    for (int e = 0; e < n; ++e)
+        if (z.R[e] > 1) {
+            z.ctr_off[e] = z.counters_off + ctr;
+            ctr += int64_t(3) * z.R[e] * 4;
+        }
+    z.counters_bytes = align256(ctr);
+    off = z.counters_off + z.counters_bytes;
+    z.big_off = off;
+    off = align256(off + int64_t(z.nbig) * 4);
+    z.init_prefix_off = off;
+    off = align256(off + int64_t(z.nbig + 1) * 8);
+    z.fin_prefix_off = off;
+    off = align256(off + int64_t(z.nbig + 1) * 8);
+    z.place_prefix_off = off;
+    off = align256(off + int64_t(z.nbig + 1) * 8);
+    for (int q = 0; q < 2; ++q) {
+        z.tasks_off[q] = off;
+        off = align256(off + int64_t(z.ntasks[q]) * 8);
+    }
+    z.total = off;
+    return SE_OK;
+}
+
+template <int LB> int occupancy() {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<LB>, cfg<LB>::THREADS, pcfg<LB>::SMEM);
+    cudaGetLastError();
+    return per_sm;
+}
+
+template <int LB> se_status_t set_persistent_smem() {
+    static const cudaError_t e = cudaFuncSetAttribute(persistent_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      int(pcfg<LB>::SMEM));
+    SE_REQUIRE(e == cudaSuccess, SE_ERR_CUDA, "cannot raise the shared-memory limit of the batched closure");
+    return SE_OK;
+}
+
+se_status_t enqueue(const Plan& P, cudaStream_t s) {
+    Header* hdr = reinterpret_cast<Header*>(P.work);
+    const Elec* elecs = reinterpret_cast<const Elec*>(P.work + P.elec_off);
+    const int32_t* big = reinterpret_cast<const int32_t*>(P.work + P.big_off);
+    SE_CUDA_TRY(cudaMemsetAsync(P.work, 0, 256, s));
+    if (P.counters_bytes) SE_CUDA_TRY(cudaMemsetAsync(P.work + P.counters_off, 0, size_t(P.counters_bytes), s));
+    if (P.nbig) {
+        batch_init_kernel<<<unsigned(P.init_blocks), dim3(32, 8), 0, s>>>(
+            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.init_prefix_off), P.nbig, hdr);
+        SE_CHECK_LAUNCH();
+    }
+    if (P.ntasks[0]) {
+        persistent_kernel<16><<<P.grid[0], cfg<16>::THREADS, pcfg<16>::SMEM, s>>>(
+            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[0]), P.ntasks[0], hdr, 0);
+        SE_CHECK_LAUNCH();
+    }
+    if (P.ntasks[1]) {
+        persistent_kernel<32><<<P.grid[1], cfg<32>::THREADS, pcfg<32>::SMEM, s>>>(
+            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[1]), P.ntasks[1], hdr, 1);
+        SE_CHECK_LAUNCH();
+    }
+    if (P.nbig) {
+        batch_finalize_kernel<<<unsigned(P.fin_blocks), dim3(32, 8), 0, s>>>(
+            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.fin_prefix_off), P.nbig);
+        SE_CHECK_LAUNCH();
+        batch_place_kernel<<<unsigned(P.place_blocks), 256, 0, s>>>(
+            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.place_prefix_off), P.nbig);
+        SE_CHECK_LAUNCH();
+    }
+    return SE_OK;
+}
+
+}  // namespace batch
+}  // namespace se
+
+using namespace se;
+using namespace se::batch;
+
+extern "C" int64_t se_batch_workspace_bytes(int n, const se_election_t* elections) {
+    clear_error();
+    if (n > 0 && elections == nullptr) return -1;
+    Sizes z;
+    if (size_batch(n, elections, z) != SE_OK) return -1;
+    return z.total;
+}
+
+extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_work, int64_t work_bytes, int order,
+                                        se_batch_plan_t* plan_out) {
+    clear_error();
+    SE_REQUIRE(plan_out != nullptr, SE_ERR_INVALID, "null plan");
+    SE_REQUIRE(n == 0 || el != nullptr, SE_ERR_INVALID, "null election array");
+    Sizes z;
+    if (se_status_t st = size_batch(n, el, z)) return st;
+    SE_REQUIRE(d_work != nullptr && work_bytes >= z.total, SE_ERR_WORKSPACE,
+               "workspace of %lld bytes is smaller than the %lld bytes required", (long long)work_bytes,
+               (long long)z.total);
+    SE_REQUIRE((reinterpret_cast<uintptr_t>(d_work) & 255) == 0, SE_ERR_INVALID, "workspace must be 256-byte aligned");
+    for (int e = 0; e < n; ++e) {
+        SE_REQUIRE(el[e].d_pref && el[e].d_out, SE_ERR_INVALID, "election %d: null matrix pointer", e);
+        SE_REQUIRE(el[e].ld_pref >= el[e].C && el[e].ld_out >= el[e].C, SE_ERR_INVALID,
+                   "election %d: row stride smaller than the number of candidates", e);
+        SE_REQUIRE((el[e].d_wins == nullptr) == (el[e].d_ranking == nullptr), SE_ERR_INVALID,
+                   "election %d: wins and ranking must both be given or both be null", e);
+    }
+    if (se_status_t st = set_persistent_smem<16>()) return st;
+    if (se_status_t st = set_persistent_smem<32>()) return st;
+    uint8_t* work = static_cast<uint8_t*>(d_work);
+
+    std::vector<Elec> host(n);
+    std::vector<int32_t> big;
+    for (int e = 0; e < n; ++e) {
+        Elec& E = host[e];
+        std::memset(&E, 0, sizeof(Elec));
+        E.d = el[e].d_pref;
+        E.ld = el[e].ld_pref;
+        E.out = el[e].d_out;
+        E.ld_out = el[e].ld_out;
+        E.wins = el[e].d_wins;
+        E.ranking = el[e].d_ranking;
+        E.C = el[e].C;
+        E.Cp = z.Cp[e];
+        E.R = z.R[e];
+        E.lanes = z.lanes[e];
+        E.base = E.lanes == 16 ? el[e].value_offset : 0u;
+        if (E.R > 1) {
+            big.push_back(e);
+            const int cpw = E.lanes == 16 ? 2 : 1;
+            const int64_t ldw = E.Cp / cpw;
+            E.S = reinterpret_cast<uint32_t*>(work + z.s_off[e]);
+            E.AT = reinterpret_cast<uint32_t*>(work + z.at_off[e]);
+            E.dT = reinterpret_cast<uint32_t*>(work + z.dt_off[e]);
+            E.counters = reinterpret_cast<uint32_t*>(work + z.ctr_off[e]);
+            if (se_status_t st = make_map(&E.mapS, E.S, uint64_t(ldw), uint64_t(E.Cp), uint64_t(ldw) * 4,
+                                          uint32_t(kT / cpw), kKC))
+                return st;
+            if (se_status_t st = make_map(&E.mapAT, E.AT, uint64_t(E.Cp), kT, uint64_t(E.Cp) * 4, kT, kKC)) return st;
+            if (se_status_t st = make_map(&E.mapDT, E.dT, kT, kT, kT * 4, kT, kKC)) return st;
+        }
+    }
+    // Task queues. Largest elections first inside every step.
+    std::vector<int32_t> order_big(big);
+    std::stable_sort(order_big.begin(), order_big.end(), [&](int a, int b) { return host[a].R > host[b].R; });
+    int Rmax = 1;
+    for (int e : big) Rmax = std::max(Rmax, host[e].R);
+    std::vector<uint64_t> q[2];
+    std::vector<uint64_t> small[2];
+    for (int e = 0; e < n; ++e)
+        if (host[e].R == 1) small[host[e].lanes == 16 ? 0 : 1].push_back(pack_task(e, kSmall, 0, 0, 0));
+    if (order == 1)  // small elections first
+        for (int l = 0; l < 2; ++l) q[l].insert(q[l].end(), small[l].begin(), small[l].end());
+    for (int k = 0; k < Rmax; ++k) {
+        for (int e : order_big)
+            if (host[e].R > k) q[host[e].lanes == 16 ? 0 : 1].push_back(pack_task(e, kPivot, k, k, k));
+        for (int e : order_big)
+            if (host[e].R > k) {
+                auto& Q = q[host[e].lanes == 16 ? 0 : 1];
+                for (int x = 0; x < host[e].R; ++x)
+                    if (x != k) {
+                        Q.push_back(pack_task(e, kRow, k, k, x));
+                        Q.push_back(pack_task(e, kCol, k, x, k));
+                    }
+            }
+        for (int e : order_big)
+            if (host[e].R > k) {
+                auto& Q = q[host[e].lanes == 16 ? 0 : 1];
+                for (int i = 0; i < host[e].R; ++i)
+                    if (i != k)
+                        for (int j = 0; j < host[e].R; ++j)
+                            if (j != k) Q.push_back(pack_task(e, kRem, k, i, j));
+            }
+    }
+    if (order != 1)
+        for (int l = 0; l < 2; ++l) q[l].insert(q[l].end(), small[l].begin(), small[l].end());
+    for (int l = 0; l < 2; ++l)
+        SE_REQUIRE(q[l].size() == z.ntasks[l], SE_ERR_INVALID, "internal: task count mismatch");
+
+    // Block prefixes of the batched elementwise kernels.
+    std::vector<int64_t> ip(big.size() + 1, 0), fp(big.size() + 1, 0), pp(big.size() + 1, 0);
+    for (size_t m = 0; m < big.size(); ++m) {
+        const Elec& E = host[big[m]];
+        const int64_t nb32 = E.Cp / 32, nbc = (E.C + 31) / 32;
+        ip[m + 1] = ip[m] + nb32 * nb32;
+        fp[m + 1] = fp[m] + nbc * (nbc + 1) / 2;
+        pp[m + 1] = pp[m] + (E.C + 255) / 256;
+    }
+    // Upload (synchronous).
+    SE_CUDA_TRY(cudaMemset(work, 0, 256));
+    if (n) SE_CUDA_TRY(cudaMemcpy(work + z.elec_off, host.data(), sizeof(Elec) * size_t(n), cudaMemcpyHostToDevice));
+    if (!big.empty()) {
+        SE_CUDA_TRY(cudaMemcpy(work + z.big_off, big.data(), 4 * big.size(), cudaMemcpyHostToDevice));
+        SE_CUDA_TRY(cudaMemcpy(work + z.init_prefix_off, ip.data(), 8 * ip.size(), cudaMemcpyHostToDevice));
+        SE_CUDA_TRY(cudaMemcpy(work + z.fin_prefix_off, fp.data(), 8 * fp.size(), cudaMemcpyHostToDevice));
+        SE_CUDA_TRY(cudaMemcpy(work + z.place_prefix_off, pp.data(), 8 * pp.size(), cudaMemcpyHostToDevice));
+    }
+    for (int l = 0; l < 2; ++l)
+        if (!q[l].empty())
+            SE_CUDA_TRY(cudaMemcpy(work + z.tasks_off[l], q[l].data(), 8 * q[l].size(), cudaMemcpyHostToDevice));
+
+    int device = 0, sms = 0;
+    SE_CUDA_TRY(cudaGetDevice(&device));
+    SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    Plan P;
+    std::memset(&P, 0, sizeof(P));
+    P.work = work;
+    P.work_bytes = work_bytes;
+    P.n = n;
+    P.nbig = int32_t(big.size());
+    P.nsmall = z.nsmall;
+    P.elec_off = z.elec_off;
+    P.big_off = z.big_off;
+    P.init_prefix_off = z.init_prefix_off;
+    P.fin_prefix_off = z.fin_prefix_off;
+    P.place_prefix_off = z.place_prefix_off;
+    P.counters_off = z.counters_off;
+    P.counters_bytes = z.counters_bytes;
+    for (int l = 0; l < 2; ++l) {
+        P.tasks_off[l] = z.tasks_off[l];
+        P.ntasks[l] = z.ntasks[l];
+    }
+    P.init_blocks = ip.back();
+    P.fin_blocks = fp.back();
+    P.place_blocks = pp.back();
+    const int occ16 = occupancy<16>(), occ32 = occupancy<32>();
+    SE_REQUIRE(occ16 >= 1 && occ32 >= 1, SE_ERR_CUDA, "batched closure kernel cannot be resident");
+    P.grid[0] = int(std::min<int64_t>(P.ntasks[0], int64_t(sms) * occ16));
+    P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * occ32));
+    P.graph = nullptr;
+    std::memcpy(plan_out, &P, sizeof(P));
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_run(const se_batch_plan_t* plan, void* stream) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    return enqueue(P, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" se_status_t se_batch_graph_build(se_batch_plan_t* plan) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    if (P.graph) {
+        cudaGraphExecDestroy(P.graph);
+        P.graph = nullptr;
+    }
+    cudaStream_t s;
+    SE_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    se_status_t st = SE_OK;
+    if (e == cudaSuccess) {
+        st = enqueue(P, s);
+        cudaError_t e2 = cudaStreamEndCapture(s, &g);
+        if (st == SE_OK && e2 != cudaSuccess) e = e2;
+    }
+    if (st == SE_OK && e == cudaSuccess) e = cudaGraphInstantiate(&P.graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(s);
+    if (st != SE_OK) return st;
+    SE_CUDA_TRY(e);
+    std::memcpy(plan, &P, sizeof(P));
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_graph_launch(const se_batch_plan_t* plan, void* stream) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    SE_REQUIRE(P.graph != nullptr, SE_ERR_INVALID, "plan has no graph; call se_batch_graph_build first");
+    SE_CUDA_TRY(cudaGraphLaunch(P.graph, static_cast<cudaStream_t>(stream)));
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_release(se_batch_plan_t* plan) {
+    clear_error();
+    if (!plan) return SE_OK;
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    if (P.graph) cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+    std::memcpy(plan, &P, sizeof(P));
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    Header h;
+    SE_CUDA_TRY(cudaMemcpyAsync(&h, P.work, sizeof(h), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    SE_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    SE_REQUIRE(h.err != kErrOverflow, SE_ERR_OVERFLOW,
+               "a kept preference count falls outside [value_offset + 1, value_offset + 65535] in an election "
+               "run with 16-bit lanes");
+    SE_REQUIRE(h.err == 0, SE_ERR_DEVICE, "batched closure reported device error %u (%s)", h.err,
+               h.err == kErrDepTimeout ? "dependency wait timed out" : "TMA wait timed out");
+    return SE_OK;
+}
+
+extern "C" int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue) {
+    if (!plan || queue < 0 || queue > 1) return -1;
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    return P.ntasks[queue];
+}

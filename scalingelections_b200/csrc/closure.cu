@@ -34,107 +34,10 @@
 #include <mutex>
 #include <vector>
 
-#include "common.cuh"
+#include "closure_core.cuh"
 
 namespace se {
 namespace closure {
-
-constexpr int kT = 128;             // pivot block edge = tile edge, in cells
-constexpr int kKC = 32;             // k-rows per TMA chunk
-constexpr int kChunks = kT / kKC;   // chunks per tile
-constexpr uint32_t kErrTmaTimeout = 1;
-
-template <int LB> struct cfg {
-    static constexpr int CPW = 32 / LB;               // cells per 32-bit word
-    static constexpr int TW = kT / CPW;               // words per tile row: 64 (u16) / 128 (u32)
-    static constexpr int WN = TW / 64;                // warps across a tile row
-    static constexpr int THREADS = 32 * 4 * WN;       // 128 (u16) / 256 (u32)
-    static constexpr int A_CHUNK = kKC * kT;          // words of one A chunk (k-major, 128 rows)
-    static constexpr int B_CHUNK = kKC * TW;          // words of one B chunk
-    static constexpr uint32_t A_BYTES = A_CHUNK * 4;
-    static constexpr uint32_t B_BYTES = B_CHUNK * 4;
-    // tile_kernel: all of K resident (no ring), one mbarrier per chunk.
-    static constexpr size_t TILE_SMEM = size_t(kChunks) * (A_CHUNK + B_CHUNK) * 4 + kChunks * 8;
-    // col_panel_kernel: the panel tile, its transposed-duplicated copy, and D.
-    static constexpr size_t COL_SMEM = size_t(kT) * TW * 4 * 2 + size_t(kT) * kT * 4 + 2 * kChunks * 8;
-};
-
-// Thread geometry shared by every kernel of one lane mode: warp (wm, wn) of a 4 x WN grid,
-// lane (tr, tc) of a 4 x 8 grid. The thread owns rows row0 .. row0+7 and words
-// wbase .. wbase+3 and wbase+32 .. wbase+35 of the tile, so the 8 threads of a row group read
-// 128 contiguous bytes of B per shared load, and 4 row groups read 4 disjoint bank groups of A.
-struct geom {
-    int row0, wbase;
-    __device__ __forceinline__ explicit geom(int tid) {
-        const int warp = tid >> 5, lane = tid & 31;
-        row0 = (warp & 3) * 32 + (lane >> 3) * 8;
-        wbase = (warp >> 2) * 64 + (lane & 7) * 4;
-    }
-    __device__ __forceinline__ int word(int q) const { return wbase + (q < 4 ? q : 28 + q); }
-};
-
-__device__ __forceinline__ void ld4(uint32_t* dst, const uint32_t* src) {
-    const uint4 v = *reinterpret_cast<const uint4*>(src);
-    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
-}
-__device__ __forceinline__ void st4(uint32_t* dst, const uint32_t* src) {
-    *reinterpret_cast<uint4*>(dst) = make_uint4(src[0], src[1], src[2], src[3]);
-}
-
-// Extract cell h (0 = low half) of a word and duplicate it across the word.
-template <int LB> __device__ __forceinline__ uint32_t cell_splat(uint32_t w, int h);
-template <> __device__ __forceinline__ uint32_t cell_splat<32>(uint32_t w, int) { return w; }
-template <> __device__ __forceinline__ uint32_t cell_splat<16>(uint32_t w, int h) {
-    return __byte_perm(w, 0, h ? 0x3232 : 0x1010);
-}
-
-template <int LB>
-__device__ __forceinline__ void load_tile_regs(uint32_t (&c)[8][8], const uint32_t* base, int64_t ldw,
-                                               const geom& g) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
-        ld4(&c[r][0], p);
-        ld4(&c[r][4], p + 32);
-    }
-}
-
-template <int LB>
-__device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][8], uint32_t* base, int64_t ldw,
-                                                const geom& g) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
-        st4(p, &c[r][0]);
-        st4(p + 32, &c[r][4]);
-    }
-}
-
-// One K-chunk of the semiring product: c = max(c, max_k min(A[k][row], B[k][word])).
-// A is k-major [kKC][kT] (duplicated cells in u16 mode), B is [kKC][TW].
-template <int LB>
-__device__ __forceinline__ void relax_chunk(uint32_t (&c)[8][8], const uint32_t* __restrict__ As,
-                                            const uint32_t* __restrict__ Bs, const geom& g) {
-    using L = lanes<LB>;
-    constexpr int TW = cfg<LB>::TW;
-#pragma unroll
-    for (int k = 0; k < kKC; k += 2) {
-        uint32_t a0[8], a1[8], b0[8], b1[8];
-        ld4(a0, As + k * kT + g.row0);
-        ld4(a0 + 4, As + k * kT + g.row0 + 4);
-        ld4(a1, As + (k + 1) * kT + g.row0);
-        ld4(a1 + 4, As + (k + 1) * kT + g.row0 + 4);
-        ld4(b0, Bs + k * TW + g.wbase);
-        ld4(b0 + 4, Bs + k * TW + g.wbase + 32);
-        ld4(b1, Bs + (k + 1) * TW + g.wbase);
-        ld4(b1 + 4, Bs + (k + 1) * TW + g.wbase + 32);
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
-    }
-}
 
 // Poll limit for one mbarrier phase: a TMA chunk lands in microseconds; ~2^26 polls is
 // seconds. Hitting it means a lost completion, reported through the error word.
@@ -192,26 +95,6 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         return;
     }
     store_tile_regs<LB>(c, Ct, ldw, g);
-}
-
-// Writes the thread's cells transposed and duplicated: out[k][row] for every cell (row, k)
-// it holds; out is k-major with row stride ld_out words.
-template <int LB>
-__device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8], uint32_t* out,
-                                                       int64_t ld_out, const geom& g) {
-    constexpr int CPW = cfg<LB>::CPW;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-#pragma unroll
-        for (int h = 0; h < CPW; ++h) {
-            const int k = g.word(q) * CPW + h;
-            uint32_t v[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = cell_splat<LB>(c[r][q], h);
-            uint32_t* p = out + int64_t(k) * ld_out + g.row0;
-            st4(p, v);
-            st4(p + 4, v + 4);
-        }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -289,65 +172,19 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// Pivot tile (phase 1): close D = S[K][K] in place, one k at a time (k-th row and column are
-// broadcast through double-buffered shared rows, one barrier per k), then emit dT.
+// Pivot tile (phase 1): close D = S[K][K] in place, one k at a time, then emit dT.
 // ------------------------------------------------------------------------------------------
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     diag_kernel(uint32_t* __restrict__ S, int64_t ldw, int K, uint32_t* __restrict__ dT) {
     using CF = cfg<LB>;
-    using L = lanes<LB>;
-    constexpr int TW = CF::TW;
-    constexpr int CPW = CF::CPW;
-    __shared__ __align__(16) uint32_t rowbuf[2][TW];
+    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
     __shared__ __align__(16) uint32_t colbuf[2][kT];
-
     const geom g(threadIdx.x);
     uint32_t c[8][8];
-    uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * TW;
+    uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * CF::TW;
     load_tile_regs<LB>(c, D, ldw, g);
-
-    // Publish row 0 and column 0.
-    if (g.row0 == 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) rowbuf[0][g.word(q)] = c[0][q];
-    }
-    if (g.wbase == 0) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) colbuf[0][g.row0 + r] = cell_splat<LB>(c[r][0], 0);
-    }
-    __syncthreads();
-
-#pragma unroll 1
-    for (int k = 0; k < kT; ++k) {
-        const int buf = k & 1;
-        uint32_t a[8], b[8];
-        ld4(a, &colbuf[buf][g.row0]);
-        ld4(a + 4, &colbuf[buf][g.row0 + 4]);
-        ld4(b, &rowbuf[buf][g.wbase]);
-        ld4(b + 4, &rowbuf[buf][g.wbase + 32]);
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-#pragma unroll
-            for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a[r], b[q]));
-        const int k1 = k + 1;
-        if (k1 < kT) {
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-                if (g.row0 + r == k1) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) rowbuf[buf ^ 1][g.word(q)] = c[r][q];
-                }
-            const int wk = k1 / CPW, hk = k1 % CPW;
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (g.word(q) == wk) {
-#pragma unroll
-                    for (int r = 0; r < 8; ++r) colbuf[buf ^ 1][g.row0 + r] = cell_splat<LB>(c[r][q], hk);
-                }
-        }
-        __syncthreads();
-    }
+    close_tile_in_registers<LB>(c, g, kT, rowbuf, colbuf);
     store_tile_regs<LB>(c, D, ldw, g);
     store_transposed_splat<LB>(c, dT, kT, g);
 }
@@ -356,11 +193,17 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 // Defeat matrix into the padded working matrix (scaling_elections.py:105-112 /
 // cu:495-503): S[i][j] = d[i][j] if d[i][j] > d[j][i] else 0, zero on the diagonal and in
 // the padding. d[j][i] is read through a shared-memory transpose so both reads coalesce.
-// In u16 mode a kept value above 65535 sets the overflow flag.
+//
+// In u16 mode every kept value v is stored as v - base. The widest-path closure only compares
+// values: (max, min) commute with any strictly increasing map, and v -> v - base (0 -> 0) is
+// one on {0} and [base + 1, inf). So the closure of the shifted matrix, shifted back, is the
+// closure of the original, exactly, provided every kept value lies in [base + 1, base + 65535].
+// Ballot counts from V voters always do for base = floor(V / 2): a kept d[i][j] > d[j][i]
+// with d[i][j] + d[j][i] = V is in (V/2, V]. A value outside the window sets the overflow flag.
 // ------------------------------------------------------------------------------------------
 template <int LB>
 __global__ void __launch_bounds__(256)
-    init_kernel(const uint32_t* __restrict__ d, int64_t ld, int C, int Cp, void* __restrict__ Sv,
+    init_kernel(const uint32_t* __restrict__ d, int64_t ld, int C, int Cp, void* __restrict__ Sv, uint32_t base,
                 uint32_t* __restrict__ flags) {
     __shared__ uint32_t t[32][33];
     const int bx = blockIdx.x * 32, by = blockIdx.y * 32;  // this block writes S[by.., bx..]
@@ -380,9 +223,13 @@ __global__ void __launch_bounds__(256)
             v = dij > dji ? dij : 0u;
         }
         if constexpr (LB == 16) {
-            if (v > 0xFFFFu) {
-                over = true;
-                v = 0xFFFFu;
+            if (v != 0u) {
+                if (v <= base || v - base > 0xFFFFu) {
+                    over = true;
+                    v = 0xFFFFu;
+                } else {
+                    v -= base;
+                }
             }
             static_cast<uint16_t*>(Sv)[int64_t(i) * Cp + j] = static_cast<uint16_t>(v);
         } else {
@@ -392,15 +239,53 @@ __global__ void __launch_bounds__(256)
     if (over) atomicOr(&flags[1], 1u);
 }
 
-// out[i][j] = S[i][j] widened to u32, 0 on the diagonal (the reference's masks).
+// Smallest and largest kept value of the defeat matrix (flags[2], flags[3]): decides whether
+// 16-bit lanes, possibly shifted by a base, can hold the closure exactly.
+__global__ void __launch_bounds__(256)
+    kept_range_kernel(const uint32_t* __restrict__ d, int64_t ld, int C, uint32_t* __restrict__ flags) {
+    __shared__ uint32_t t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = bx + y, cc = by + threadIdx.x;
+        t[threadIdx.x][y] = (r < C && cc < C) ? d[int64_t(r) * ld + cc] : 0u;
+    }
+    __syncthreads();
+    uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int i = by + y, j = bx + threadIdx.x;
+        if (i < C && j < C && i != j) {
+            const uint32_t dij = d[int64_t(i) * ld + j];
+            if (dij > t[y][threadIdx.x]) {
+                lo = dij < lo ? dij : lo;
+                hi = dij > hi ? dij : hi;
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (threadIdx.x == 0 && hi != 0u) {
+        atomicMin(&flags[2], lo);
+        atomicMax(&flags[3], hi);
+    }
+}
+
+// out[i][j] = S[i][j] widened to u32 (and shifted back by base), 0 on the diagonal (the
+// reference's masks).
 template <int LB>
 __global__ void __launch_bounds__(256)
-    finalize_kernel(const void* __restrict__ Sv, int Cp, int C, uint32_t* __restrict__ out, int64_t ld_out) {
+    finalize_kernel(const void* __restrict__ Sv, int Cp, int C, uint32_t* __restrict__ out, int64_t ld_out,
+                    uint32_t base) {
     for (int i = blockIdx.y; i < C; i += gridDim.y)
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < C; j += gridDim.x * blockDim.x) {
             uint32_t v;
-            if constexpr (LB == 16) v = static_cast<const uint16_t*>(Sv)[int64_t(i) * Cp + j];
-            else v = static_cast<const uint32_t*>(Sv)[int64_t(i) * Cp + j];
+            if constexpr (LB == 16) {
+                v = static_cast<const uint16_t*>(Sv)[int64_t(i) * Cp + j];
+                v = v ? v + base : 0u;
+            } else {
+                v = static_cast<const uint32_t*>(Sv)[int64_t(i) * Cp + j];
+            }
             out[int64_t(i) * ld_out + j] = (i == j) ? 0u : v;
         }
 }
@@ -535,19 +420,21 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
 }
 
 template <int LB>
-se_status_t launch_init(const uint32_t* d, int64_t ld, int C, const layout& P, uint8_t* work, cudaStream_t s) {
+se_status_t launch_init(const uint32_t* d, int64_t ld, int C, const layout& P, uint8_t* work, uint32_t base,
+                        cudaStream_t s) {
     const int nb = int(P.Cp / 32);
-    init_kernel<LB><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d, ld, C, int(P.Cp), work + P.s_off,
+    init_kernel<LB><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d, ld, C, int(P.Cp), work + P.s_off, base,
                                                        reinterpret_cast<uint32_t*>(work + P.flags_off));
     SE_CHECK_LAUNCH();
     return SE_OK;
 }
 
 template <int LB>
-se_status_t launch_finalize(const layout& P, uint8_t* work, int C, uint32_t* out, int64_t ld_out, cudaStream_t s) {
+se_status_t launch_finalize(const layout& P, uint8_t* work, int C, uint32_t* out, int64_t ld_out, uint32_t base,
+                            cudaStream_t s) {
     const int gx = int((C + 255) / 256);
     const int gy = C < 65535 ? C : 65535;
-    finalize_kernel<LB><<<dim3(gx, gy), 256, 0, s>>>(work + P.s_off, int(P.Cp), C, out, ld_out);
+    finalize_kernel<LB><<<dim3(gx, gy), 256, 0, s>>>(work + P.s_off, int(P.Cp), C, out, ld_out, base);
     SE_CHECK_LAUNCH();
     return SE_OK;
 }
@@ -582,27 +469,39 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
     uint8_t* work = static_cast<uint8_t*>(d_work);
 
     int lb = lane_bits == 0 ? 16 : lane_bits;
-    layout P = plan(C, lb);
+    uint32_t base = 0;
     SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
-    if (lb == 16) {
-        if (se_status_t st = launch_init<16>(d_pref, ld_pref, C, P, work, s)) return st;
-        if (lane_bits == 0) {
-            uint32_t over = 0;
-            SE_CUDA_TRY(cudaMemcpyAsync(&over, work + P.flags_off + 4, 4, cudaMemcpyDeviceToHost, s));
-            SE_CUDA_TRY(cudaStreamSynchronize(s));
-            if (over) {
-                lb = 32;
-                P = plan(C, 32);
-                SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
-            }
+    if (lane_bits == 0) {
+        // Automatic lanes: 16-bit (shifted by a base if need be) whenever the kept values fit
+        // a 65535-wide window, else 32-bit. One 8-byte read back.
+        SE_CUDA_TRY(cudaMemsetAsync(work + 8, 0xFF, 4, s));
+        const int nb = int(round_up(C, 32) / 32);
+        kept_range_kernel<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d_pref, ld_pref, C,
+                                                              reinterpret_cast<uint32_t*>(work));
+        SE_CHECK_LAUNCH();
+        uint32_t range[2] = {0, 0};
+        SE_CUDA_TRY(cudaMemcpyAsync(range, work + 8, 8, cudaMemcpyDeviceToHost, s));
+        SE_CUDA_TRY(cudaStreamSynchronize(s));
+        const uint32_t lo = range[0], hi = range[1];
+        if (hi <= 0xFFFFu) {
+            lb = 16;
+        } else if (hi - lo < 0xFFFFu) {
+            lb = 16;
+            base = lo - 1u;
+        } else {
+            lb = 32;
         }
     }
-    if (lb == 32) {
-        if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, s)) return st;
+    const layout P = plan(C, lb);
+    if (lb == 16) {
+        if (se_status_t st = launch_init<16>(d_pref, ld_pref, C, P, work, base, s)) return st;
+    } else {
+        if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
     se_status_t st = lb == 16 ? run_rounds<16>(work, P, s, phase_ms) : run_rounds<32>(work, P, s, phase_ms);
     if (st) return st;
-    st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, s) : launch_finalize<32>(P, work, C, d_out, ld_out, s);
+    st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, base, s)
+                  : launch_finalize<32>(P, work, C, d_out, ld_out, 0, s);
     if (st) return st;
 
     uint32_t flags[2] = {0, 0};

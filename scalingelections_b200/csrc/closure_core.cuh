@@ -1,0 +1,202 @@
+// Device building blocks shared by the single-election closure (closure.cu) and the batched
+// persistent closure (batch.cu): tile geometry, the register-blocked (max, min) product over
+// TMA-staged shared operands, the in-register pivot-tile closure, and tile load/store.
+#pragma once
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace se {
+namespace closure {
+
+constexpr int kT = 128;             // pivot block edge = tile edge, in cells
+constexpr int kKC = 32;             // k-rows per TMA chunk
+constexpr int kChunks = kT / kKC;   // chunks per tile
+constexpr uint32_t kErrTmaTimeout = 1;
+
+template <int LB> struct cfg {
+    static constexpr int CPW = 32 / LB;               // cells per 32-bit word
+    static constexpr int TW = kT / CPW;               // words per tile row: 64 (u16) / 128 (u32)
+    static constexpr int WN = TW / 64;                // warps across a tile row
+    static constexpr int THREADS = 32 * 4 * WN;       // 128 (u16) / 256 (u32)
+    static constexpr int A_CHUNK = kKC * kT;          // words of one A chunk (k-major, 128 rows)
+    static constexpr int B_CHUNK = kKC * TW;          // words of one B chunk
+    static constexpr uint32_t A_BYTES = A_CHUNK * 4;
+    static constexpr uint32_t B_BYTES = B_CHUNK * 4;
+    // tile_kernel: all of K resident (no ring), one mbarrier per chunk.
+    static constexpr size_t TILE_SMEM = size_t(kChunks) * (A_CHUNK + B_CHUNK) * 4 + kChunks * 8;
+    // col_panel_kernel: the panel tile, its transposed-duplicated copy, and D.
+    static constexpr size_t COL_SMEM = size_t(kT) * TW * 4 * 2 + size_t(kT) * kT * 4 + 2 * kChunks * 8;
+};
+
+// Thread geometry shared by every kernel of one lane mode: warp (wm, wn) of a 4 x WN grid,
+// lane (tr, tc) of a 4 x 8 grid. The thread owns rows row0 .. row0+7 and words
+// wbase .. wbase+3 and wbase+32 .. wbase+35 of the tile, so the 8 threads of a row group read
+// 128 contiguous bytes of B per shared load, and 4 row groups read 4 disjoint bank groups of A.
+struct geom {
+    int row0, wbase;
+    __device__ __forceinline__ explicit geom(int tid) {
+        const int warp = tid >> 5, lane = tid & 31;
+        row0 = (warp & 3) * 32 + (lane >> 3) * 8;
+        wbase = (warp >> 2) * 64 + (lane & 7) * 4;
+    }
+    __device__ __forceinline__ int word(int q) const { return wbase + (q < 4 ? q : 28 + q); }
+};
+
+__device__ __forceinline__ void ld4(uint32_t* dst, const uint32_t* src) {
+    const uint4 v = *reinterpret_cast<const uint4*>(src);
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+}
+__device__ __forceinline__ void st4(uint32_t* dst, const uint32_t* src) {
+    *reinterpret_cast<uint4*>(dst) = make_uint4(src[0], src[1], src[2], src[3]);
+}
+
+// Extract cell h (0 = low half) of a word and duplicate it across the word.
+template <int LB> __device__ __forceinline__ uint32_t cell_splat(uint32_t w, int h);
+template <> __device__ __forceinline__ uint32_t cell_splat<32>(uint32_t w, int) { return w; }
+template <> __device__ __forceinline__ uint32_t cell_splat<16>(uint32_t w, int h) {
+    return __byte_perm(w, 0, h ? 0x3232 : 0x1010);
+}
+
+// 128-bit global load that bypasses L1: for data another CTA of the same launch wrote.
+__device__ __forceinline__ void ld4_cg(uint32_t* dst, const uint32_t* src) {
+    const uint4 v = __ldcg(reinterpret_cast<const uint4*>(src));
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+}
+
+template <int LB, bool COHERENT = false>
+__device__ __forceinline__ void load_tile_regs(uint32_t (&c)[8][8], const uint32_t* base, int64_t ldw,
+                                               const geom& g) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
+        if constexpr (COHERENT) {
+            ld4_cg(&c[r][0], p);
+            ld4_cg(&c[r][4], p + 32);
+        } else {
+            ld4(&c[r][0], p);
+            ld4(&c[r][4], p + 32);
+        }
+    }
+}
+
+template <int LB>
+__device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][8], uint32_t* base, int64_t ldw,
+                                                const geom& g) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
+        st4(p, &c[r][0]);
+        st4(p + 32, &c[r][4]);
+    }
+}
+
+// One K-chunk of the semiring product: c = max(c, max_k min(A[k][row], B[k][word])).
+// A is k-major [kKC][kT] (duplicated cells in u16 mode), B is [kKC][TW].
+template <int LB>
+__device__ __forceinline__ void relax_chunk(uint32_t (&c)[8][8], const uint32_t* __restrict__ As,
+                                            const uint32_t* __restrict__ Bs, const geom& g) {
+    using L = lanes<LB>;
+    constexpr int TW = cfg<LB>::TW;
+#pragma unroll
+    for (int k = 0; k < kKC; k += 2) {
+        uint32_t a0[8], a1[8], b0[8], b1[8];
+        ld4(a0, As + k * kT + g.row0);
+        ld4(a0 + 4, As + k * kT + g.row0 + 4);
+        ld4(a1, As + (k + 1) * kT + g.row0);
+        ld4(a1 + 4, As + (k + 1) * kT + g.row0 + 4);
+        ld4(b0, Bs + k * TW + g.wbase);
+        ld4(b0 + 4, Bs + k * TW + g.wbase + 32);
+        ld4(b1, Bs + (k + 1) * TW + g.wbase);
+        ld4(b1 + 4, Bs + (k + 1) * TW + g.wbase + 32);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
+    }
+}
+
+// Writes the thread's cells transposed and duplicated: out[k][row] for every cell (row, k)
+// it holds; out is k-major with row stride ld_out words.
+template <int LB>
+__device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8], uint32_t* out,
+                                                       int64_t ld_out, const geom& g) {
+    constexpr int CPW = cfg<LB>::CPW;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+#pragma unroll
+        for (int h = 0; h < CPW; ++h) {
+            const int k = g.word(q) * CPW + h;
+            uint32_t v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = cell_splat<LB>(c[r][q], h);
+            uint32_t* p = out + int64_t(k) * ld_out + g.row0;
+            st4(p, v);
+            st4(p + 4, v + 4);
+        }
+}
+
+// Closes the 128 x 128 tile held in registers (the thread's 8 x 8 words) in place over
+// pivots k = 0 .. kmax-1, one k at a time: the k-th row and column are broadcast through
+// double-buffered shared rows, one barrier per k. Every thread of the block must call it.
+// Pivots >= kmax are skipped, which is exact when those rows/columns are zero padding.
+template <int LB>
+__device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][8], const geom& g, int kmax,
+                                                        uint32_t (*rowbuf)[cfg<LB>::TW],
+                                                        uint32_t (*colbuf)[kT]) {
+    using L = lanes<LB>;
+    constexpr int CPW = cfg<LB>::CPW;
+    // Publish row 0 and column 0.
+    if (g.row0 == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) rowbuf[0][g.word(q)] = c[0][q];
+    }
+    if (g.wbase == 0) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) colbuf[0][g.row0 + r] = cell_splat<LB>(c[r][0], 0);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int k = 0; k < kmax; ++k) {
+        const int buf = k & 1;
+        uint32_t a[8], b[8];
+        ld4(a, &colbuf[buf][g.row0]);
+        ld4(a + 4, &colbuf[buf][g.row0 + 4]);
+        ld4(b, &rowbuf[buf][g.wbase]);
+        ld4(b + 4, &rowbuf[buf][g.wbase + 32]);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a[r], b[q]));
+        const int k1 = k + 1;
+        if (k1 < kmax) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                if (g.row0 + r == k1) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) rowbuf[buf ^ 1][g.word(q)] = c[r][q];
+                }
+            const int wk = k1 / CPW, hk = k1 % CPW;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (g.word(q) == wk) {
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) colbuf[buf ^ 1][g.row0 + r] = cell_splat<LB>(c[r][q], hk);
+                }
+        }
+        __syncthreads();
+    }
+}
+
+// 2-D u32 tensor map over this GPU's memory: dims {inner, outer} words, row pitch in bytes,
+// box {box_x, box_y}. Defined in closure.cu.
+se_status_t make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint64_t pitch_bytes,
+                     uint32_t box_x, uint32_t box_y);
+
+}  // namespace closure
+}  // namespace se

@@ -107,3 +107,16 @@ def test_closure_c16384_rows_by_dijkstra(orc):
     S0 = orc.defeats(d_h)
     assert (S_h >= S0).all()
     assert not np.diagonal(S_h).any()
+
+
+def test_shifted_16_bit_lanes_for_large_counts(orc):
+    """Kept values in a window [70001, 130000] exceed 16 bits but span less than 65535: the
+    automatic mode closes them in shifted 16-bit lanes, bit-identical to 32-bit lanes."""
+    rng = np.random.default_rng(11)
+    C = 333
+    base = rng.integers(70001, 130000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    P = base.copy()
+    S_ref = orc.strongest_paths(P, "blocked", tile=16)
+    assert orc.defeats(P).max() > 65535
+    assert np.array_equal(gpu_closure(P, LANES_AUTO), S_ref)
+    assert np.array_equal(gpu_closure(P, LANES_U32), S_ref)
