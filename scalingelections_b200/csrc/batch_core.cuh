@@ -1,0 +1,296 @@
+// Task routines of the persistent closure schedulers (batch.cu: a fixed batch; serve.cu: a
+// queue fed while the kernel runs). Every task works on 128 x 128 tiles of one election:
+//   SMALL      an election with C <= 128, whole in one CTA: defeat init from d, closure over
+//              its C pivots in registers, u32 output, wins and ranking.
+//   PIVOT k    close the pivot tile (k, k) in registers; emit dT.
+//   ROW k, j   pivot-row panel tile (k, j)       = max(P, D (x) P)
+//   COL k, i   pivot-column panel tile (i, k)    = max(P, P (x) D); emit AT (transposed).
+//   REM k,i,j  remainder tile (i, j)             = max(S, AT (x) S[k][j])
+// Tiles another CTA wrote are read through L2 (ld.global.cg) or TMA, never through L1.
+#pragma once
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "closure_core.cuh"
+
+namespace se {
+namespace batch {
+using namespace se::closure;
+
+enum : uint32_t { kSmall = 0, kPivot = 1, kRow = 2, kCol = 3, kRem = 4 };
+constexpr uint64_t kNoTask = ~0ull;
+constexpr uint32_t kErrTimeout = 1;
+constexpr uint32_t kErrOverflow = 2;
+constexpr uint32_t kErrDepTimeout = 3;
+constexpr uint64_t kDepWaitNs = 5000000000ull;  // 5 s for one dependency
+
+struct alignas(64) Elec {
+    CUtensorMap mapS;   // working matrix, box {TW, 32}
+    CUtensorMap mapAT;  // transposed column panel, box {128, 32}
+    CUtensorMap mapDT;  // transposed pivot tile, box {128, 32}
+    const uint32_t* d;
+    int64_t ld;
+    uint32_t* out;
+    int64_t ld_out;
+    int32_t* wins;
+    int32_t* ranking;
+    uint32_t* S;
+    uint32_t* AT;
+    uint32_t* dT;
+    uint32_t* counters;  // [0, R): pivot done; [R, 2R): panels done; [2R, 3R): remainder done
+    int32_t C, Cp, R, lanes;
+    uint32_t base;  // u16 lanes store a kept value v as v - base (see init_kernel in closure.cu)
+};
+
+// Kept defeat value v -> stored u16 cell, or a flagged overflow outside [base+1, base+65535].
+__device__ __forceinline__ uint32_t to_lane16(uint32_t v, uint32_t base, bool& over) {
+    if (v == 0u) return 0u;
+    if (v <= base || v - base > 0xFFFFu) {
+        over = true;
+        return 0xFFFFu;
+    }
+    return v - base;
+}
+
+
+__host__ __device__ inline uint64_t pack_task(uint32_t e, uint32_t type, uint32_t k, uint32_t i, uint32_t j) {
+    return (uint64_t(e) << 39) | (uint64_t(type) << 36) | (uint64_t(k) << 24) | (uint64_t(i) << 12) | uint64_t(j);
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_tensormap(const void* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// Thread 0 only: wait until *ctr >= target or the abort flag rises or time runs out.
+__device__ bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag) {
+    if (ld_acquire(ctr) >= target) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (ld_acquire(ctr) >= target) return true;
+        if ((it & 63) == 0) {
+            if (ld_acquire(abort_flag)) return false;
+            if (global_ns() - t0 > kDepWaitNs) return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <int LB> struct pcfg {
+    using CF = cfg<LB>;
+    static constexpr size_t A_REGION = size_t(kChunks) * CF::A_CHUNK * 4;  // 64 KiB
+    static constexpr size_t B_REGION = size_t(kChunks) * CF::B_CHUNK * 4;  // 32 / 64 KiB
+    static constexpr size_t SMALL_BYTES = size_t(kT) * (kT + 1) * 4;         // d tile, padded rows
+    static constexpr size_t DATA = (A_REGION + B_REGION) > SMALL_BYTES ? (A_REGION + B_REGION) : SMALL_BYTES;
+    static constexpr size_t SMEM = DATA + 8 * 8;                              // + 8 mbarriers
+};
+
+// ------------------------------------------------------------------------------------------
+// SMALL: whole election in this CTA.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__device__ void run_small(const Elec& E, uint8_t* smem, uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT],
+                          int32_t* s_wins, uint32_t* err) {
+    constexpr int CPW = cfg<LB>::CPW;
+    constexpr int P = kT + 1;  // padded row pitch: row and column walks are bank-conflict free
+    uint32_t* dt = reinterpret_cast<uint32_t*>(smem);
+    const int C = E.C;
+    const geom g(threadIdx.x);
+    for (int idx = threadIdx.x; idx < kT * kT; idx += blockDim.x) {
+        const int r = idx / kT, c = idx % kT;
+        dt[r * P + c] = (r < C && c < C) ? __ldcg(E.d + int64_t(r) * E.ld + c) : 0u;
+    }
+    __syncthreads();
+    uint32_t c[8][8];
+    bool over = false;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int i = g.row0 + r;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int h = 0; h < CPW; ++h) {
+                const int j = g.word(q) * CPW + h;
+                const uint32_t dij = dt[i * P + j], dji = dt[j * P + i];
+                uint32_t v = (i != j && dij > dji) ? dij : 0u;
+                if constexpr (LB == 16) {
+                    w |= to_lane16(v, E.base, over) << (16 * h);
+                } else {
+                    w = v;
+                }
+            }
+            c[r][q] = w;
+        }
+    }
+    if (over) raise_device_error(err, kErrOverflow);
+    close_tile_in_registers<LB>(c, g, C, rowbuf, colbuf);
+    // Output, and the u32 matrix again in shared memory for the ranking.
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int i = g.row0 + r;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+#pragma unroll
+            for (int h = 0; h < CPW; ++h) {
+                const int j = g.word(q) * CPW + h;
+                uint32_t v = LB == 16 ? (c[r][q] >> (16 * h)) & 0xFFFFu : c[r][q];
+                if (LB == 16 && v) v += E.base;
+                if (i == j) v = 0u;
+                dt[i * P + j] = v;
+                if (i < C && j < C) E.out[int64_t(i) * E.ld_out + j] = v;
+            }
+    }
+    if (E.wins == nullptr) return;
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < C) {
+        int w = 0;
+        for (int j = 0; j < C; ++j) w += dt[t * P + j] > dt[j * P + t];
+        s_wins[t] = w;
+        E.wins[t] = w;
+    }
+    __syncthreads();
+    if (t < C) {
+        const int wt = s_wins[t];
+        int place = 0;
+        for (int j = 0; j < C; ++j) {
+            const int wj = s_wins[j];
+            place += (wj > wt) | ((wj == wt) & (j < t));
+        }
+        E.ranking[place] = t;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Tile tasks of elections with R >= 2.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__device__ void run_pivot(const Elec& E, int k, uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT]) {
+    using CF = cfg<LB>;
+    const geom g(threadIdx.x);
+    const int64_t ldw = E.Cp / CF::CPW;
+    uint32_t* D = E.S + int64_t(k) * kT * ldw + int64_t(k) * CF::TW;
+    uint32_t c[8][8];
+    load_tile_regs<LB, true>(c, D, ldw, g);
+    const int kmax = E.C - k * kT < kT ? E.C - k * kT : kT;  // pivots past C are zero padding
+    close_tile_in_registers<LB>(c, g, kmax, rowbuf, colbuf);
+    store_tile_regs<LB>(c, D, ldw, g);
+    store_transposed_splat<LB>(c, E.dT, kT, g);
+}
+
+// REM (a_panel = true: A = AT[:, I], C = S[I][J]) or ROW (A = dT, C = S[K][J]); B = S[K][J].
+// E holds the election's scalars (it may be a shared-memory copy); G is the descriptor in
+// global memory, whose tensor maps the TMA unit reads.
+template <int LB>
+__device__ bool run_product(const Elec& E, const Elec* G, int K, int I, int J, bool a_panel, uint8_t* smem,
+                            uint64_t* bars, uint32_t parity) {
+    using CF = cfg<LB>;
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
+    const CUtensorMap* mapA = a_panel ? &G->mapAT : &G->mapDT;
+    if (threadIdx.x == 0) {
+        fence_tensormap(mapA);
+        fence_tensormap(&G->mapS);
+        fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::A_BYTES + CF::B_BYTES);
+            tma_load_2d(As + c * CF::A_CHUNK, mapA, &bars[c], a_panel ? I * kT : 0, c * kKC);
+            tma_load_2d(Bs + c * CF::B_CHUNK, &G->mapS, &bars[c], J * CF::TW, K * kT + c * kKC);
+        }
+    }
+    const geom g(threadIdx.x);
+    const int64_t ldw = E.Cp / CF::CPW;
+    uint32_t* Ct = E.S + int64_t(I) * kT * ldw + int64_t(J) * CF::TW;
+    uint32_t c[8][8];
+    load_tile_regs<LB, true>(c, Ct, ldw, g);
+    bool ok = true;
+#pragma unroll 1
+    for (int ch = 0; ch < kChunks; ++ch) {
+        if (!mbar_wait_bounded(&bars[ch], parity, 1u << 26)) {
+            ok = false;
+            break;
+        }
+        relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+    }
+    if (ok) store_tile_regs<LB>(c, Ct, ldw, g);
+    return ok;
+}
+
+template <int LB>
+__device__ bool run_col(const Elec& E, const Elec* G, int K, int I, uint8_t* smem, uint64_t* bars,
+                        uint32_t parity_a, uint32_t parity_b) {
+    using CF = cfg<LB>;
+    constexpr int TW = CF::TW;
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);                          // [kT][kT]
+    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);     // tile, then D
+    if (threadIdx.x == 0) {
+        fence_tensormap(&G->mapS);
+        fence_proxy_async();
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            mbar_arrive_expect_tx(&bars[c], CF::B_BYTES);
+            tma_load_2d(Bs + c * CF::B_CHUNK, &G->mapS, &bars[c], K * TW, I * kT + c * kKC);
+        }
+    }
+    bool ok = true;
+#pragma unroll 1
+    for (int c = 0; c < kChunks; ++c) ok = ok && mbar_wait_bounded(&bars[c], parity_a, 1u << 26);
+    const geom g(threadIdx.x);
+    uint32_t c[8][8];
+    if (ok) {
+        constexpr int HALVES = CF::THREADS / kT;
+        constexpr int SPAN = TW / HALVES;
+        const int i = threadIdx.x % kT;
+        const int half = threadIdx.x / kT;
+#pragma unroll 4
+        for (int s = 0; s < SPAN; ++s) {
+            const int w = half * SPAN + ((s + i) & (SPAN - 1));
+            const uint32_t word = Bs[i * TW + w];
+#pragma unroll
+            for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
+        }
+        load_tile_regs<LB>(c, Bs, TW, g);
+    }
+    __syncthreads();  // the tile region is free again
+    if (threadIdx.x == 0 && ok) {
+        fence_proxy_async();
+#pragma unroll
+        for (int ch = 0; ch < kChunks; ++ch) {
+            mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
+            tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[kChunks + ch], K * TW, K * kT + ch * kKC);
+        }
+    }
+    if (ok) {
+#pragma unroll 1
+        for (int ch = 0; ch < kChunks; ++ch) {
+            if (!mbar_wait_bounded(&bars[kChunks + ch], parity_b, 1u << 26)) {
+                ok = false;
+                break;
+            }
+            relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+        }
+    }
+    if (ok) {
+        const int64_t ldw = E.Cp / CF::CPW;
+        store_tile_regs<LB>(c, E.S + int64_t(I) * kT * ldw + int64_t(K) * TW, ldw, g);
+        store_transposed_splat<LB>(c, E.AT + int64_t(I) * kT, E.Cp, g);
+    }
+    return ok;
+}
+
+}  // namespace batch
+}  // namespace se
