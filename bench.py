@@ -53,8 +53,12 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["closure", "batch"], default="closure",
-                    help="closure: the headline single election; batch: many mixed elections")
+    ap.add_argument("--workload", choices=["closure", "batch", "serve"], default="closure",
+                    help="closure: the headline single election; batch: many mixed elections; "
+                         "serve: Poisson arrivals on the continuous-batching server")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests per offered load")
+    ap.add_argument("--loads", default="0.3,0.6,0.9", help="serve: offered loads as fractions of capacity")
+    ap.add_argument("--budget-gb", type=float, default=40.0, help="serve: HBM admission budget")
     ap.add_argument("--elections", type=int, default=4096, help="batch: number of elections")
     ap.add_argument("--max-candidates", type=int, default=2048, help="batch: largest C")
     return ap.parse_args()
@@ -316,8 +320,8 @@ def run_ours(args, world, rank, local_rank):
                 "traffic": traffic,
                 "algorithmic_bytes_per_launch": algo_bytes,
                 "hbm_gbs_achieved": algo_bytes / (tile_ms_avg * 1e-3) / 1e9,
-                "phase_ms": {"pivot": phase[0], "row_panel": phase[1], "col_panel": phase[2],
-                             "remainder": phase[3]},
+                "phase_ms": {"pivot_round0": phase[0], "panels": phase[1],
+                             "remainder_with_fused_pivot": phase[3]},
             },
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -367,14 +371,20 @@ def run_batch(args, world, rank, local_rank):
     from scalingelections_b200 import api
     from scalingelections_b200.batch import BatchedElections, lanes_for_voters
 
+    from scalingelections_b200.shard import election_cost, partition_by_work
+
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    specs = batch_specs(args.elections, args.seed + 7919 * rank, args.max_candidates)
+    # One global batch of elections x world, split by closure work; no collective on the
+    # data path (weak scaling: the global batch grows with the number of GPUs).
+    all_specs = batch_specs(args.elections * world, args.seed, args.max_candidates)
+    mine = partition_by_work([election_cost(C) for (C, _, _, _) in all_specs], world)[rank]
+    specs = [all_specs[i] for i in mine]
     t0 = time.perf_counter()
     prefs = make_batch_inputs(specs, dev)
     prep_s = time.perf_counter() - t0
     lanes = [lanes_for_voters(V) for (_, V, _, _) in specs]
-    cells = float(sum(C ** 3 for (C, _, _, _) in specs))
+    cells = float(sum(C ** 3 for (C, _, _, _) in all_specs))
     b = BatchedElections(prefs, lanes)
     b.build_graph()
     stream = torch.cuda.current_stream()
@@ -414,7 +424,7 @@ def run_batch(args, world, rank, local_rank):
     identical = all(torch.equal(o.view(torch.int32), bo.view(torch.int32)) and torch.equal(r, br)
                     for o, bo, r, br in zip(outs, b.outs, ranks, b.rankings))
 
-    n_total = args.elections * world
+    n_total = len(all_specs)
     value = n_total / (ms_max * 1e-3)
     if rank == 0:
         tasks = b.task_counts()
@@ -429,11 +439,77 @@ def run_batch(args, world, rank, local_rank):
                        "u16_shifted_elections": sum(1 for l in lanes if l[0] == 16 and l[1] > 0),
                        "u32_elections": sum(1 for l in lanes if l[0] == 32),
                        "tasks": {"u16": tasks[0], "u32": tasks[1]}, "graph": True},
-            "batched_gcells_per_s": cells * world / (ms_max * 1e-3) / 1e9,
-            "loop_elections_per_s": args.elections / loop_s,
+            "batched_gcells_per_s": cells / (ms_max * 1e-3) / 1e9,
+            "loop_elections_per_s": len(specs) / loop_s,
             "loop_seconds": loop_s,
-            "speedup_vs_loop": value / world / (args.elections / loop_s),
+            "speedup_vs_loop": (len(specs) / (ms * 1e-3)) / (len(specs) / loop_s),
             "bit_identical_to_loop": identical,
+            "input_prep_seconds": prep_s,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# Serving workload: Poisson arrivals on the continuous-batching server
+# ------------------------------------------------------------------------------------------
+def serve_specs(n: int, seed: int):
+    """C log-uniform in [8, 8192], V log-uniform in [100, 100000], Mallows phi ~ U[0.2, 1]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    C = np.rint(np.exp(rng.uniform(np.log(8), np.log(8192), size=n))).astype(int)
+    V = np.rint(np.exp(rng.uniform(np.log(100), np.log(100000), size=n))).astype(int)
+    phi = rng.uniform(0.2, 1.0, size=n)
+    return [(int(V[i]), int(C[i]), float(phi[i]), seed * 7_000_003 + i) for i in range(n)]
+
+
+def run_serve(args, world, rank, local_rank):
+    import numpy as np
+    import torch
+
+    from scalingelections_b200.ballots import mallows_ballots_device
+    from scalingelections_b200.serve import Server, run_arrivals, summarize
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    specs = serve_specs(args.requests, args.seed + 104729 * rank)
+    t0 = time.perf_counter()
+    reqs = [(V, C, mallows_ballots_device(V, C, phi, seed=sd, device=dev)) for (V, C, phi, sd) in specs]
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
+    server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=20)
+    # Warm-up, then capacity: every request arrives at once (closed loop, admission-bound).
+    run_arrivals(server, reqs[: min(8, len(reqs))], [0.0] * min(8, len(reqs)))
+    done, makespan = run_arrivals(server, reqs, [0.0] * len(reqs))
+    capacity = len(done) / makespan
+    sat = summarize(done, float("inf"), makespan)
+    rng = np.random.default_rng(args.seed + 17)
+    loads = []
+    with ClockSampler(local_rank) as clocks:
+        for frac in [float(x) for x in args.loads.split(",")]:
+            rate = frac * capacity
+            gaps = rng.exponential(1.0 / rate, size=len(reqs))
+            arrivals = list(np.cumsum(gaps) - gaps[0])
+            done, span = run_arrivals(server, reqs, arrivals)
+            r = summarize(done, rate, span)
+            loads.append({"offered_fraction": frac, "offered_per_s": rate, "achieved_per_s": r.achieved_rate,
+                          "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms, "n": r.n})
+    server.close()
+    if rank == 0:
+        V = np.array([s[0] for s in specs], float)
+        C = np.array([s[1] for s in specs], float)
+        line = {
+            "metric": "served elections/s at saturation, and p50/p99 latency under Poisson load",
+            "value": capacity * world, "unit": "elections/s", "n_gpus": world, "steps": len(loads),
+            "warmup": 1, "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16 (shifted lanes above 65535 ballots)",
+            "data": "synthetic (seeded Mallows ballots resident on the GPU before arrival)",
+            "config": {"workload": f"{args.requests} requests, C log-uniform [8, 8192], V log-uniform [100, 100000], "
+                                   f"Mallows phi ~ U[0.2, 1]; HBM budget {args.budget_gb:g} GB",
+                       "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum())},
+            "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan},
+            "loads": loads,
             "input_prep_seconds": prep_s,
             "clocks": clocks.summary(),
         }
@@ -459,6 +535,8 @@ def main():
     try:
         if args.workload == "batch":
             run_batch(args, world, rank, local_rank)
+        elif args.workload == "serve":
+            run_serve(args, world, rank, local_rank)
         else:
             run_ours(args, world, rank, local_rank)
     finally:

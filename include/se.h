@@ -167,6 +167,52 @@ SE_API se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream);
 SE_API int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue);
 
 /* ---------------------------------------------------------------------------------------
+ * Serving engine (no reference counterpart): continuous batching of whole elections (tally,
+ * closure, ranking) on one persistent kernel that keeps running while requests are added.
+ * Each request's work is split into phases of independent tasks; the kernel's CTAs take
+ * claimable tasks from the oldest requests first, so new requests join the running kernel.
+ *
+ *   se_engine_workspace_bytes        device bytes for an engine with max_slots request slots.
+ *   se_engine_create                 ctas_per_sm in {1, 2}; idle_ms: the kernel exits after
+ *                                    that long without work, and the next submit or poll
+ *                                    relaunches it.
+ *   se_engine_request_scratch_bytes  per-request scratch (ballot places, working matrix,
+ *                                    panels) for V ballots and C candidates.
+ *   se_engine_submit                 publishes a request on `stream` (a few small copies and
+ *                                    memsets; asynchronous). Returns its slot and generation.
+ *   se_engine_poll                   requests finished since the last poll: slot and status
+ *                                    (0 ok, 4 = a kept count outside the 16-bit window,
+ *                                    8|2 = ballot id out of range, 8|3 = repeated id).
+ *   se_engine_stop / destroy         stop the kernel (waits for it) / also free host state.
+ * Every buffer of a request must stay alive until poll reports it.
+ * ------------------------------------------------------------------------------------- */
+typedef struct se_request {
+    const int32_t* d_ids;      /* ballots, most preferred first (see se_tally) */
+    const int64_t* d_offsets;  /* V + 1 CSR offsets, or NULL: every ballot lists exactly C ids */
+    int64_t V;
+    int32_t C;
+    uint32_t value_offset;     /* 16-bit lane shift, as in se_election_t (V / 2 above 65535) */
+    uint32_t* d_prefs;         /* out: C x C preference counts, row stride C */
+    uint32_t* d_out;           /* out: C x C strongest paths, row stride C */
+    int32_t* d_wins;           /* out: C */
+    int32_t* d_ranking;        /* out: C */
+    void* d_scratch;           /* se_engine_request_scratch_bytes(V, C), 256-byte aligned */
+    int64_t scratch_bytes;
+} se_request_t;
+
+typedef struct se_engine se_engine_t;
+SE_API int64_t se_engine_workspace_bytes(int max_slots);
+SE_API se_status_t se_engine_create(void* d_work, int64_t work_bytes, int max_slots, int ctas_per_sm,
+                                    int idle_ms, se_engine_t** engine);
+SE_API int64_t se_engine_request_scratch_bytes(int64_t V, int C);
+SE_API se_status_t se_engine_submit(se_engine_t* engine, const se_request_t* request, void* stream,
+                                    int* slot, uint32_t* generation);
+SE_API se_status_t se_engine_poll(se_engine_t* engine, int* slots, uint32_t* statuses, int max,
+                                  int* n_finished);
+SE_API se_status_t se_engine_stop(se_engine_t* engine);
+SE_API se_status_t se_engine_destroy(se_engine_t* engine);
+
+/* ---------------------------------------------------------------------------------------
  * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).
  *
  *   Ballots are given in CSR form: ballot v is d_ids[d_offsets[v] .. d_offsets[v+1]), the
@@ -181,6 +227,13 @@ SE_API int64_t se_tally_workspace_bytes(int64_t V, int C);
 SE_API se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
                      uint32_t* d_out, int64_t ld_out, void* d_work, int64_t work_bytes,
                      void* stream);
+
+/* se_tally without the final synchronisation: fully stream-ordered. Malformed ballots are
+ * reported in the first 4 bytes of d_work (0 = fine, 2 = id out of range, 3 = repeated id,
+ * 1 = lost TMA completion), which the caller reads after the stream reaches that point. */
+SE_API se_status_t se_tally_enqueue(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
+                                    uint32_t* d_out, int64_t ld_out, void* d_work,
+                                    int64_t work_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Ranking. Replaces get_winner_and_ranking (scaling_elections.py:274-296).

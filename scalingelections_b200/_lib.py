@@ -49,8 +49,16 @@ SIGNATURES: dict[str, tuple] = {
     "se_batch_release": (_c_int, [_vp]),
     "se_batch_check": (_c_int, [_vp, _vp]),
     "se_batch_task_count": (_c_i64, [_vp, _c_int]),
+    "se_engine_workspace_bytes": (_c_i64, [_c_int]),
+    "se_engine_create": (_c_int, [_vp, _c_i64, _c_int, _c_int, _c_int, _vp]),
+    "se_engine_request_scratch_bytes": (_c_i64, [_c_i64, _c_int]),
+    "se_engine_submit": (_c_int, [_vp, _vp, _vp, _ip, ctypes.POINTER(ctypes.c_uint32)]),
+    "se_engine_poll": (_c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_uint32), _c_int, _ip]),
+    "se_engine_stop": (_c_int, [_vp]),
+    "se_engine_destroy": (_c_int, [_vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
+    "se_tally_enqueue": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_rank": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
     "se_mallows_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_mallows_ballots": (_c_int, [_c_i64, _c_int, ctypes.c_double, ctypes.c_uint64, _vp, _vp, _vp, _c_i64, _vp]),
@@ -63,6 +71,14 @@ class Election(ctypes.Structure):
                 ("ld_out", ctypes.c_int64), ("d_wins", ctypes.c_void_p), ("d_ranking", ctypes.c_void_p),
                 ("C", ctypes.c_int32), ("lane_bits", ctypes.c_int32), ("value_offset", ctypes.c_uint32),
                 ("reserved", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    """se_request_t"""
+    _fields_ = [("d_ids", ctypes.c_void_p), ("d_offsets", ctypes.c_void_p), ("V", ctypes.c_int64),
+                ("C", ctypes.c_int32), ("value_offset", ctypes.c_uint32), ("d_prefs", ctypes.c_void_p),
+                ("d_out", ctypes.c_void_p), ("d_wins", ctypes.c_void_p), ("d_ranking", ctypes.c_void_p),
+                ("d_scratch", ctypes.c_void_p), ("scratch_bytes", ctypes.c_int64)]
 
 
 class BatchPlan(ctypes.Structure):

@@ -75,7 +75,7 @@ __device__ __forceinline__ void fence_tensormap(const void* map) {
 }
 
 // Thread 0 only: wait until *ctr >= target or the abort flag rises or time runs out.
-__device__ bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag) {
+__device__ inline bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag) {
     if (ld_acquire(ctr) >= target) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t it = 0;; ++it) {
@@ -192,9 +192,11 @@ __device__ void run_pivot(const Elec& E, int k, uint32_t (*rowbuf)[cfg<LB>::TW],
 }
 
 // REM (a_panel = true: A = AT[:, I], C = S[I][J]) or ROW (A = dT, C = S[K][J]); B = S[K][J].
-// E holds the election's scalars (it may be a shared-memory copy); G is the descriptor in
-// global memory, whose tensor maps the TMA unit reads.
-template <int LB>
+// E holds the election's scalars (it may be a shared-memory copy); G is the descriptor whose
+// tensor maps the TMA unit reads. GLOBAL_MAPS: G lives in global memory and may have been
+// rewritten since the last launch (batch and serving queues), so each use first acquires the
+// tensor maps; false for a descriptor passed as a kernel parameter.
+template <int LB, bool GLOBAL_MAPS = true>
 __device__ bool run_product(const Elec& E, const Elec* G, int K, int I, int J, bool a_panel, uint8_t* smem,
                             uint64_t* bars, uint32_t parity) {
     using CF = cfg<LB>;
@@ -202,8 +204,10 @@ __device__ bool run_product(const Elec& E, const Elec* G, int K, int I, int J, b
     uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
     const CUtensorMap* mapA = a_panel ? &G->mapAT : &G->mapDT;
     if (threadIdx.x == 0) {
-        fence_tensormap(mapA);
-        fence_tensormap(&G->mapS);
+        if constexpr (GLOBAL_MAPS) {
+            fence_tensormap(mapA);
+            fence_tensormap(&G->mapS);
+        }
         fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
 #pragma unroll
         for (int c = 0; c < kChunks; ++c) {
@@ -230,7 +234,7 @@ __device__ bool run_product(const Elec& E, const Elec* G, int K, int I, int J, b
     return ok;
 }
 
-template <int LB>
+template <int LB, bool GLOBAL_MAPS = true>
 __device__ bool run_col(const Elec& E, const Elec* G, int K, int I, uint8_t* smem, uint64_t* bars,
                         uint32_t parity_a, uint32_t parity_b) {
     using CF = cfg<LB>;
@@ -238,7 +242,7 @@ __device__ bool run_col(const Elec& E, const Elec* G, int K, int I, uint8_t* sme
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);                          // [kT][kT]
     uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);     // tile, then D
     if (threadIdx.x == 0) {
-        fence_tensormap(&G->mapS);
+        if constexpr (GLOBAL_MAPS) fence_tensormap(&G->mapS);
         fence_proxy_async();
 #pragma unroll
         for (int c = 0; c < kChunks; ++c) {

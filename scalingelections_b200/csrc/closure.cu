@@ -10,16 +10,17 @@
 //   dT  128 x 128 words: the closed pivot tile, transposed and duplicated the same way.
 //
 // One round k (pivot block K = rows/cols [128k, 128k+128)):
-//   diag_kernel       1 CTA:       close D = S[K][K] in place, k by k (the only sequential
-//                                  step); emit dT.
-//   row_panel (tile)  R-1 CTAs:    S[K][J] = max(S[K][J], D (x) S[K][J]).
-//   col_panel_kernel  R-1 CTAs:    S[I][K] = max(S[I][K], S[I][K] (x) D); emit AT.
-//   tile_kernel       (R-1)^2 CTAs S[I][J] = max(S[I][J], S[I][K] (x) S[K][J]).
+//   pivot     close D = S[K][K] in place, k by k (the only sequential step); emit dT. Round
+//             0 runs it as its own 1-CTA launch (diag_kernel); for round k+1 the first CTA of
+//             round k's remainder launch does it right after updating that tile.
+//   panels    one launch, 2(R-1) CTAs: S[K][J] = max(S[K][J], D (x) S[K][J]) and
+//             S[I][K] = max(S[I][K], S[I][K] (x) D), the latter emitting AT.
+//   remainder (R-1)^2 CTAs: S[I][J] = max(S[I][J], S[I][K] (x) S[K][J]).
 // where (x) is the max-min product. Because D is closed, a panel needs no sequential k loop:
 // a path k1 ->...-> k2 -> j inside block K is worth min(D*[k1][k2], S[k2][j]). So the
-// panels and the remainder are the same register-blocked "semiring GEMM": operands staged
-// into shared memory by TMA (this GPU's memory only, never multicast), 8 x 8 words per
-// thread, c = max3(c, min(a0, b0), min(a1, b1)) per word and k-pair.
+// panels and the remainder are the same register-blocked "semiring GEMM" (batch_core.cuh):
+// operands staged into shared memory by TMA (this GPU's memory only, never multicast),
+// 8 x 8 words per thread, c = max3(c, min(a0, b0), min(a1, b1)) per word and k-pair.
 //
 // The reference's masks (scaling_elections.py:118-121, cu:133-161) are dropped: the closure
 // runs unmasked and the diagonal is zeroed at the end. That is exact: a relaxation through
@@ -31,10 +32,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstring>
 #include <mutex>
 #include <vector>
 
-#include "closure_core.cuh"
+#include "batch_core.cuh"
 
 namespace se {
 namespace closure {
@@ -44,131 +46,64 @@ namespace closure {
 constexpr uint32_t kMaxPolls = 1u << 26;
 
 // ------------------------------------------------------------------------------------------
-// Remainder tiles (phase 3) and pivot-row panel tiles (phase 2, rows of block K).
-//   phase3 = true : C = S[I][J], A = AT[:, I], B = S[K][J], grid (R-1, R-1), I, J != K.
-//   phase3 = false: C = S[K][J], A = dT,       B = S[K][J], grid (R-1),      J != K.
+// One round's panels in one launch: blocks [0, R-1) the pivot-row tiles S[K][J] =
+// max(S[K][J], D (x) S[K][J]); blocks [R-1, 2(R-1)) the pivot-column tiles S[I][K] =
+// max(S[I][K], S[I][K] (x) D), which also emit the transposed panel AT. 96 KiB of shared
+// memory per CTA, so both sets are resident at once.
 // ------------------------------------------------------------------------------------------
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
-    tile_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapS,
-                uint32_t* __restrict__ S, int64_t ldw, int K, int phase3, uint32_t* __restrict__ err) {
-    using CF = cfg<LB>;
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint32_t* As = reinterpret_cast<uint32_t*>(smem_raw);
-    uint32_t* Bs = As + kChunks * CF::A_CHUNK;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(Bs + kChunks * CF::B_CHUNK);
-
-    const int bj = blockIdx.x, bi = blockIdx.y;
-    const int J = bj + (bj >= K);
-    const int I = phase3 ? bi + (bi >= K) : K;
-
+    panels_kernel(const __grid_constant__ batch::Elec E, int K, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < kChunks; ++c) mbar_init(&bars[c], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < kChunks; ++c) {
-            mbar_arrive_expect_tx(&bars[c], CF::A_BYTES + CF::B_BYTES);
-            tma_load_2d(As + c * CF::A_CHUNK, &mapA, &bars[c], phase3 ? I * kT : 0, c * kKC);
-            tma_load_2d(Bs + c * CF::B_CHUNK, &mapS, &bars[c], J * CF::TW, K * kT + c * kKC);
-        }
-    }
-    const geom g(threadIdx.x);
-    uint32_t c[8][8];
-    uint32_t* Ct = S + int64_t(I) * kT * ldw + int64_t(J) * CF::TW;
-    load_tile_regs<LB>(c, Ct, ldw, g);
-
-    bool ok = true;
-#pragma unroll 1
-    for (int ch = 0; ch < kChunks; ++ch) {
-        if (!mbar_wait_bounded(&bars[ch], 0, kMaxPolls)) {
-            ok = false;
-            break;
-        }
-        relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
-    }
-    if (!ok) {
-        raise_device_error(err, kErrTmaTimeout);
-        return;
-    }
-    store_tile_regs<LB>(c, Ct, ldw, g);
-}
-
-// ------------------------------------------------------------------------------------------
-// Pivot-column panel tiles (phase 2, columns of block K): C = S[I][K], A = transposed copy of
-// the same tile (built here in shared memory), B = D = S[K][K] (already closed).
-// Writes S[I][K] and the transposed, duplicated panel AT[:, I] that phase 3 reads.
-// ------------------------------------------------------------------------------------------
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
-    col_panel_kernel(const __grid_constant__ CUtensorMap mapS, uint32_t* __restrict__ S, int64_t ldw,
-                     int K, uint32_t* __restrict__ AT, int64_t ld_at, uint32_t* __restrict__ err) {
-    using CF = cfg<LB>;
-    constexpr int TW = CF::TW;
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint32_t* tile = reinterpret_cast<uint32_t*>(smem_raw);  // [kT][TW]
-    uint32_t* Ds = tile + kT * TW;                            // [kT][TW]
-    uint32_t* As = Ds + kT * TW;                              // [kT][kT]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(As + kT * kT);
-
-    const int I = blockIdx.x + (int(blockIdx.x) >= K);
-    if (threadIdx.x == 0) {
-#pragma unroll
         for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
         fence_barrier_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int c = 0; c < kChunks; ++c) {
-            mbar_arrive_expect_tx(&bars[c], CF::B_BYTES);
-            tma_load_2d(tile + c * CF::B_CHUNK, &mapS, &bars[c], K * TW, I * kT + c * kKC);
-            mbar_arrive_expect_tx(&bars[kChunks + c], CF::B_BYTES);
-            tma_load_2d(Ds + c * CF::B_CHUNK, &mapS, &bars[kChunks + c], K * TW, K * kT + c * kKC);
-        }
-    }
-    bool ok = true;
-#pragma unroll 1
-    for (int c = 0; c < kChunks; ++c) ok = ok && mbar_wait_bounded(&bars[c], 0, kMaxPolls);
+    const int R1 = E.R - 1;
+    const int b = blockIdx.x;
+    bool ok;
+    if (b < R1) ok = batch::run_product<LB, false>(E, &E, K, K, b + (b >= K), false, smem, bars, 0);
+    else ok = batch::run_col<LB, false>(E, &E, K, (b - R1) + ((b - R1) >= K), smem, bars, 0, 0);
+    if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
+}
 
-    if (ok) {
-        // As[k][i] = splat(cell(i, k)). Each thread walks one half-row (u32) or row (u16) with
-        // a per-row rotation so the 32 lanes of a warp hit 32 different banks on both sides.
-        constexpr int HALVES = CF::THREADS / kT;  // 1 (u16) or 2 (u32)
-        constexpr int SPAN = TW / HALVES;         // 64 words either way
-        const int i = threadIdx.x % kT;
-        const int half = threadIdx.x / kT;
-#pragma unroll 4
-        for (int s = 0; s < SPAN; ++s) {
-            const int w = half * SPAN + ((s + i) & (SPAN - 1));
-            const uint32_t word = tile[i * TW + w];
-#pragma unroll
-            for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
-        }
+// ------------------------------------------------------------------------------------------
+// One round's remainder tiles S[I][J] = max(S[I][J], AT (x) S[K][J]), I, J != K. With
+// fuse_pivot, block 0 takes tile (K+1, K+1) and, after its update, closes it as the next
+// round's pivot tile (and emits dT) while the other blocks continue: the next round needs no
+// separate pivot launch. Nothing else in this launch reads that tile or dT.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < kChunks; ++c) mbar_init(&bars[c], 1);
+        fence_barrier_init();
     }
-    const geom g(threadIdx.x);
-    uint32_t c[8][8];
-    if (ok) load_tile_regs<LB>(c, tile, TW, g);
     __syncthreads();
-    if (ok) {
-#pragma unroll 1
-        for (int ch = 0; ch < kChunks; ++ch) {
-            if (!mbar_wait_bounded(&bars[kChunks + ch], 0, kMaxPolls)) {
-                ok = false;
-                break;
-            }
-            relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Ds + ch * CF::B_CHUNK, g);
-        }
+    const int R1 = E.R - 1;
+    int t = blockIdx.x;
+    if (fuse_pivot) {
+        const int p = K * R1 + K;  // reduced coordinates of tile (K+1, K+1)
+        t = t == 0 ? p : (t == p ? 0 : t);
     }
+    const int ii = t / R1, jj = t % R1;
+    const bool ok = batch::run_product<LB, false>(E, &E, K, ii + (ii >= K), jj + (jj >= K), true, smem, bars, 0);
     if (!ok) {
-        raise_device_error(err, kErrTmaTimeout);
+        if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
     }
-    store_tile_regs<LB>(c, S + int64_t(I) * kT * ldw + int64_t(K) * TW, ldw, g);
-    store_transposed_splat<LB>(c, AT + int64_t(I) * kT, ld_at, g);
+    if (fuse_pivot && blockIdx.x == 0) {
+        __syncthreads();  // the tile's stores are visible to the whole CTA
+        batch::run_pivot<LB>(E, K + 1, rowbuf, colbuf);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -325,12 +260,14 @@ se_status_t make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_
 }
 
 struct layout {
+    int64_t C = 0;
     int64_t Cp = 0;
     int64_t flags_off = 0, s_off = 0, at_off = 0, dt_off = 0, total = 0;
 };
 
 layout plan(int C, int lane_bits) {
     layout L;
+    L.C = C;
     L.Cp = round_up(C, kT);
     const int64_t cell = lane_bits == 16 ? 2 : 4;
     L.flags_off = 0;
@@ -343,10 +280,9 @@ layout plan(int C, int lane_bits) {
 
 template <int LB> se_status_t set_smem_limits() {
     static se_status_t st = [] {
-        if (cudaFuncSetAttribute(tile_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(cfg<LB>::TILE_SMEM)) != cudaSuccess ||
-            cudaFuncSetAttribute(col_panel_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(cfg<LB>::COL_SMEM)) != cudaSuccess) {
+        const int bytes = int(batch::pcfg<LB>::SMEM);
+        if (cudaFuncSetAttribute(panels_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(rem_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
             cudaGetLastError();
             return se_status_t(SE_ERR_CUDA);
         }
@@ -370,15 +306,25 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     const int64_t ldw = P.Cp / CF::CPW;
     const int R = int(P.Cp / kT);
 
-    CUtensorMap mapS, mapAT, mapDT;
-    if (se_status_t st = make_map(&mapS, S, uint64_t(ldw), uint64_t(P.Cp), uint64_t(ldw) * 4, CF::TW, kKC); st)
+    batch::Elec E;
+    std::memset(&E, 0, sizeof(E));
+    if (se_status_t st = make_map(&E.mapS, S, uint64_t(ldw), uint64_t(P.Cp), uint64_t(ldw) * 4, CF::TW, kKC); st)
         return st;
-    if (se_status_t st = make_map(&mapAT, AT, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st) return st;
-    if (se_status_t st = make_map(&mapDT, dT, kT, kT, kT * 4, kT, kKC); st) return st;
+    if (se_status_t st = make_map(&E.mapAT, AT, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st) return st;
+    if (se_status_t st = make_map(&E.mapDT, dT, kT, kT, kT * 4, kT, kKC); st) return st;
+    E.S = S;
+    E.AT = AT;
+    E.dT = dT;
+    E.C = int(P.C);
+    E.Cp = int(P.Cp);
+    E.R = R;
+    E.lanes = LB;
+    const size_t smem = batch::pcfg<LB>::SMEM;
 
+    // Events bracket the pivot (round 0), panel and remainder launches when profiling.
     std::vector<cudaEvent_t> ev;
     if (phase_ms) {
-        ev.resize(size_t(R) * 4 + 1, nullptr);
+        ev.resize(size_t(R) * 2 + 2, nullptr);
         for (auto& e : ev)
             if (cudaEventCreate(&e) != cudaSuccess) {
                 for (auto& x : ev)
@@ -387,32 +333,31 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             }
         cudaEventRecord(ev[0], stream);
     }
-    for (int K = 0; K < R; ++K) {
-        diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, K, dT);
-        if (phase_ms) cudaEventRecord(ev[4 * K + 1], stream);
-        if (R > 1) {
-            tile_kernel<LB><<<dim3(R - 1, 1), CF::THREADS, CF::TILE_SMEM, stream>>>(mapDT, mapS, S, ldw, K, 0, err);
-            if (phase_ms) cudaEventRecord(ev[4 * K + 2], stream);
-            col_panel_kernel<LB><<<R - 1, CF::THREADS, CF::COL_SMEM, stream>>>(mapS, S, ldw, K, AT, P.Cp, err);
-            if (phase_ms) cudaEventRecord(ev[4 * K + 3], stream);
-            tile_kernel<LB><<<dim3(R - 1, R - 1), CF::THREADS, CF::TILE_SMEM, stream>>>(mapAT, mapS, S, ldw, K, 1,
-                                                                                       err);
-        } else if (phase_ms) {
-            cudaEventRecord(ev[4 * K + 2], stream);
-            cudaEventRecord(ev[4 * K + 3], stream);
-        }
-        if (phase_ms) cudaEventRecord(ev[4 * K + 4], stream);
+    diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
+    if (phase_ms) cudaEventRecord(ev[1], stream);
+    SE_CHECK_LAUNCH();
+    for (int K = 0; K < R && R > 1; ++K) {
+        panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
+        if (phase_ms) cudaEventRecord(ev[2 + 2 * K], stream);
+        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, K + 1 < R ? 1 : 0, err);
+        if (phase_ms) cudaEventRecord(ev[3 + 2 * K], stream);
         SE_CHECK_LAUNCH();
     }
     if (phase_ms) {
-        cudaError_t e = cudaEventSynchronize(ev.back());
+        const cudaEvent_t last = R > 1 ? ev[2 * R + 1] : ev[1];
+        cudaError_t e = cudaEventSynchronize(last);
         for (int p = 0; p < 4; ++p) phase_ms[p] = 0.0;
-        for (int K = 0; K < R && e == cudaSuccess; ++K)
-            for (int p = 0; p < 4; ++p) {
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, ev[4 * K + p], ev[4 * K + p + 1]);
-                phase_ms[p] += ms;
+        float ms = 0.f;
+        if (e == cudaSuccess) {
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            phase_ms[0] += ms;
+            for (int K = 0; K < R && R > 1; ++K) {
+                cudaEventElapsedTime(&ms, K == 0 ? ev[1] : ev[1 + 2 * K], ev[2 + 2 * K]);
+                phase_ms[1] += ms;
+                cudaEventElapsedTime(&ms, ev[2 + 2 * K], ev[3 + 2 * K]);
+                phase_ms[3] += ms;
             }
+        }
         for (auto& x : ev) cudaEventDestroy(x);
         SE_CUDA_TRY(e);
     }
@@ -435,6 +380,19 @@ se_status_t launch_finalize(const layout& P, uint8_t* work, int C, uint32_t* out
     const int gx = int((C + 255) / 256);
     const int gy = C < 65535 ? C : 65535;
     finalize_kernel<LB><<<dim3(gx, gy), 256, 0, s>>>(work + P.s_off, int(P.Cp), C, out, ld_out, base);
+    SE_CHECK_LAUNCH();
+    return SE_OK;
+}
+
+// Defeat init of one election into a padded working matrix (u16 lanes shifted by base, or
+// u32), for callers outside this file (the serving engine).
+se_status_t launch_defeat_init(const uint32_t* d, int64_t ld, int C, int Cp, void* S, int lane_bits, uint32_t base,
+                               uint32_t* flags, cudaStream_t s) {
+    const int nb = Cp / 32;
+    if (lane_bits == 16)
+        init_kernel<16><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d, ld, C, Cp, S, base, flags);
+    else
+        init_kernel<32><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(d, ld, C, Cp, S, 0, flags);
     SE_CHECK_LAUNCH();
     return SE_OK;
 }
@@ -525,15 +483,12 @@ extern "C" se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pr
                                            void* stream, double* phase_ms, int* launches) {
     se_status_t st =
         closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
-    if (launches) {
-        const int R = int(round_up(C, kT) / kT);
-        *launches = 2 + R + 3 * (R - 1);
-    }
+    if (launches) *launches = se_closure_launch_count(C);
     return st;
 }
 
 extern "C" int se_closure_launch_count(int C) {
     if (C < 1) return 0;
     const int R = int(round_up(C, kT) / kT);
-    return 2 + R + 3 * (R - 1);
+    return R == 1 ? 3 : 3 + 2 * R;  // init, pivot of round 0, R x (panels, remainder), finalize
 }

@@ -198,5 +198,9 @@ __device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][8], con
 se_status_t make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint64_t pitch_bytes,
                      uint32_t box_x, uint32_t box_y);
 
+// Defeat init of one election into a padded working matrix; defined in closure.cu.
+se_status_t launch_defeat_init(const uint32_t* d, int64_t ld, int C, int Cp, void* S, int lane_bits, uint32_t base,
+                               uint32_t* flags, cudaStream_t s);
+
 }  // namespace closure
 }  // namespace se

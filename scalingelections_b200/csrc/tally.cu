@@ -33,7 +33,7 @@ namespace tally {
 
 constexpr int kTile = 128;     // candidates per tile edge
 constexpr int kVC = 32;        // voters per TMA chunk
-constexpr int kStages = 4;     // chunk ring depth
+constexpr int kStages = 3;     // chunk ring depth (3 x 32 KiB: fits beside a serving-engine CTA on one SM)
 constexpr int kThreads = 256;  // 8 x 8 cells per thread
 constexpr uint32_t kChunkBytes = kVC * kTile * 4;
 constexpr size_t kSmem = size_t(kStages) * 2 * kVC * kTile * 4 + kStages * 8;
@@ -218,8 +218,9 @@ extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
     return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256);
 }
 
-extern "C" se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C, uint32_t* d_out,
-                                int64_t ld_out, void* d_work, int64_t work_bytes, void* stream_) {
+namespace {
+se_status_t tally_impl(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C, uint32_t* d_out,
+                       int64_t ld_out, void* d_work, int64_t work_bytes, void* stream_, bool check) {
     clear_error();
     SE_REQUIRE(C >= 1 && C <= (1 << 20), SE_ERR_INVALID, "Number of candidates out of range (%d)", C);
     SE_REQUIRE(V >= 0 && V < (int64_t(1) << 24), SE_ERR_INVALID, "Number of voters out of range (%lld)",
@@ -256,6 +257,7 @@ extern "C" se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, 
     const int64_t tiles = int64_t(R) * (R + 1) / 2;
     count_kernel<<<unsigned(tiles), kThreads, kSmem, s>>>(map, V, C, R, d_out, ld_out, err);
     SE_CHECK_LAUNCH();
+    if (!check) return SE_OK;
 
     uint32_t code = 0;
     SE_CUDA_TRY(cudaMemcpyAsync(&code, err, 4, cudaMemcpyDeviceToHost, s));
@@ -264,4 +266,16 @@ extern "C" se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, 
     SE_REQUIRE(code != kErrRepeat, SE_ERR_DEVICE, "a ballot names the same candidate twice");
     SE_REQUIRE(code == 0, SE_ERR_DEVICE, "tally kernel reported device error %u (TMA wait timed out)", code);
     return SE_OK;
+}
+}  // namespace
+
+extern "C" se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C, uint32_t* d_out,
+                                int64_t ld_out, void* d_work, int64_t work_bytes, void* stream) {
+    return tally_impl(d_ids, d_offsets, V, C, d_out, ld_out, d_work, work_bytes, stream, true);
+}
+
+extern "C" se_status_t se_tally_enqueue(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
+                                        uint32_t* d_out, int64_t ld_out, void* d_work, int64_t work_bytes,
+                                        void* stream) {
+    return tally_impl(d_ids, d_offsets, V, C, d_out, ld_out, d_work, work_bytes, stream, false);
 }

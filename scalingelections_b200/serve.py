@@ -1,0 +1,275 @@
+"""Continuous-batching Schulze server on one GPU.
+
+Requests are ballot sets already in device memory (V ballots of C candidates, int32 [V, C]).
+The server admits a request when its working memory fits the HBM budget (an arena carved
+from one preallocated block) and hands it to the serving engine (include/se.h, se_engine_*):
+one persistent kernel that tallies, closes and ranks every admitted election, task by task,
+and keeps running while requests join, so requests that arrive while others are on the GPU
+are processed alongside them. Completion is observed through host-mapped memory; latency is
+measured from a request's arrival to the poll that sees it finished.
+
+No reference counterpart: the reference runs one election per call on the host's thread.
+"""
+from __future__ import annotations
+
+import bisect
+import ctypes
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+from .batch import lanes_for_voters
+
+ALIGN = 256
+
+
+class Arena:
+    """First-fit allocator over [0, capacity) with coalescing frees; offsets are ALIGN-aligned.
+    Pure host bookkeeping: it hands out offsets into one device block."""
+
+    def __init__(self, capacity: int):
+        self.capacity = int(capacity) // ALIGN * ALIGN
+        self._starts = [0]               # free extents, sorted by start
+        self._sizes = {0: self.capacity}
+        self.used = 0
+
+    def alloc(self, nbytes: int) -> int | None:
+        n = (int(nbytes) + ALIGN - 1) // ALIGN * ALIGN
+        for idx, start in enumerate(self._starts):
+            size = self._sizes[start]
+            if size >= n:
+                del self._sizes[start]
+                self._starts.pop(idx)
+                if size > n:
+                    self._starts.insert(idx, start + n)
+                    self._sizes[start + n] = size - n
+                self.used += n
+                return start
+        return None
+
+    def free(self, offset: int, nbytes: int) -> None:
+        n = (int(nbytes) + ALIGN - 1) // ALIGN * ALIGN
+        self.used -= n
+        idx = bisect.bisect_left(self._starts, offset)
+        start, size = offset, n
+        # merge with the following extent
+        if idx < len(self._starts) and self._starts[idx] == start + size:
+            nxt = self._starts.pop(idx)
+            size += self._sizes.pop(nxt)
+        # merge with the preceding extent
+        if idx > 0:
+            prev = self._starts[idx - 1]
+            if prev + self._sizes[prev] == start:
+                self._sizes[prev] += size
+                return
+        self._starts.insert(idx, start)
+        self._sizes[start] = size
+
+    @property
+    def free_bytes(self) -> int:
+        return self.capacity - self.used
+
+
+def request_bytes(V: int, C: int) -> dict:
+    """Device bytes of one request's buffers, each ALIGN-aligned."""
+
+    def al(x):
+        return (int(x) + ALIGN - 1) // ALIGN * ALIGN
+
+    scratch = _lib.lib().se_engine_request_scratch_bytes(int(V), int(C))
+    if scratch < 0:
+        raise ValueError("invalid request shape")
+    parts = {
+        "prefs": al(4 * C * C),
+        "out": al(4 * C * C),
+        "wins": al(4 * C),
+        "ranking": al(4 * C),
+        "scratch": al(scratch),
+    }
+    parts["total"] = sum(parts.values())
+    return parts
+
+
+@dataclass
+class Ticket:
+    rid: int
+    V: int
+    C: int
+    arrival: float
+    offset: int = -1
+    nbytes: int = 0
+    slot: int = -1
+    gen: int = 0
+    admitted: float = 0.0
+    finished: float = 0.0
+    status: int = -1
+    ranking: np.ndarray | None = None
+    strongest_paths: np.ndarray | None = None
+    keep_paths: bool = False
+    views: dict = field(default_factory=dict)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class Server:
+    """budget_bytes: HBM admission budget for the requests' working memory (ballots are the
+    caller's). ctas_per_sm: engine CTAs per SM. idle_ms: the engine kernel exits after this
+    long without work and is relaunched by the next submit or poll."""
+
+    def __init__(self, budget_bytes: int = 40 << 30, max_slots: int = 1024, ctas_per_sm: int = 2,
+                 idle_ms: int = 20, device: int | None = None):
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        L = _lib.lib()
+        self.L = L
+        with torch.cuda.device(self.device):
+            self.block = torch.empty(int(budget_bytes), dtype=torch.uint8, device=self.device)
+            self.arena = Arena(budget_bytes)
+            nbytes = L.se_engine_workspace_bytes(max_slots)
+            if nbytes < 0:
+                raise ValueError("bad max_slots")
+            self.engine_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self.engine = ctypes.c_void_p()
+            check(L.se_engine_create(self.engine_ws.data_ptr(), nbytes, max_slots, ctas_per_sm, idle_ms,
+                                     ctypes.byref(self.engine)))
+            self.stream = torch.cuda.Stream(device=self.device)
+        self.max_slots = max_slots
+        self.by_slot: dict[int, Ticket] = {}
+        self._poll_slots = (ctypes.c_int * max_slots)()
+        self._poll_status = (ctypes.c_uint32 * max_slots)()
+        self.base_ptr = self.block.data_ptr()
+
+    # -- admission -------------------------------------------------------------------------
+    def try_submit(self, ticket: Ticket, ballots: torch.Tensor) -> bool:
+        """Admit and publish one request if its memory fits and a slot is free; else False.
+        ballots: CUDA int32 [V, C], one ballot per row listing each of the C candidates once,
+        most preferred first."""
+        if len(self.by_slot) >= self.max_slots:
+            return False
+        V, C = ticket.V, ticket.C
+        if ballots.shape != (V, C) or ballots.dtype != torch.int32 or not ballots.is_cuda:
+            raise ValueError("ballots must be a CUDA int32 [V, C] tensor")
+        lanes, offset = lanes_for_voters(V)
+        if lanes != 16:
+            raise ValueError("the server handles up to 131070 ballots per request")
+        parts = request_bytes(V, C)
+        off = self.arena.alloc(parts["total"])
+        if off is None:
+            return False
+        ticket.offset, ticket.nbytes = off, parts["total"]
+        pos = off
+        ptrs = {}
+        for name in ("prefs", "out", "wins", "ranking", "scratch"):
+            ptrs[name] = self.base_ptr + pos
+            ticket.views[name] = (pos, parts[name])
+            pos += parts[name]
+        rq = _lib.Request(ballots.data_ptr(), None, V, C, offset, ptrs["prefs"], ptrs["out"], ptrs["wins"],
+                          ptrs["ranking"], ptrs["scratch"], parts["scratch"])
+        slot, gen = ctypes.c_int(), ctypes.c_uint32()
+        with torch.cuda.device(self.device):
+            check(self.L.se_engine_submit(self.engine, ctypes.byref(rq), self.stream.cuda_stream, ctypes.byref(slot),
+                                          ctypes.byref(gen)))
+        ticket.slot, ticket.gen = slot.value, gen.value
+        ticket.admitted = time.perf_counter()
+        self.by_slot[ticket.slot] = ticket
+        ticket._ballots = ballots  # keep alive until done
+        return True
+
+    # -- completion ------------------------------------------------------------------------
+    def poll(self) -> list[Ticket]:
+        n = ctypes.c_int(0)
+        check(self.L.se_engine_poll(self.engine, self._poll_slots, self._poll_status, self.max_slots, ctypes.byref(n)))
+        now = time.perf_counter()
+        done = []
+        for x in range(n.value):
+            t = self.by_slot.pop(self._poll_slots[x])
+            t.finished = now
+            t.status = int(self._poll_status[x])
+            self._collect(t)
+            done.append(t)
+        return done
+
+    def _view(self, t: Ticket, name: str, shape, dtype) -> torch.Tensor:
+        pos, _ = t.views[name]
+        n = int(np.prod(shape)) * torch.empty(0, dtype=dtype).element_size()
+        return self.block[pos:pos + n].view(dtype).view(*shape)
+
+    def _collect(self, t: Ticket) -> None:
+        with torch.cuda.device(self.device):
+            t.ranking = self._view(t, "ranking", (t.C,), torch.int32).cpu().numpy()
+            if t.keep_paths:
+                S = self._view(t, "out", (t.C, t.C), torch.int32)
+                t.strongest_paths = S.cpu().numpy().view(np.uint32)
+        self.arena.free(t.offset, t.nbytes)
+        t._ballots = None
+
+    @property
+    def in_flight(self) -> int:
+        return len(self.by_slot)
+
+    def close(self) -> None:
+        if self.engine:
+            self.L.se_engine_destroy(self.engine)
+            self.engine = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class LoadResult:
+    offered_rate: float
+    achieved_rate: float
+    p50_ms: float
+    p99_ms: float
+    mean_ms: float
+    n: int
+    makespan_s: float
+
+
+def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], arrival_times: list[float],
+                 keep_paths: bool = False, stall_s: float = 60.0) -> tuple[list[Ticket], float]:
+    """Drives the server with requests (V, C, ballots) arriving at the given offsets (seconds
+    from start): admits each as soon as it has arrived and fits, polls completions, and
+    returns the finished tickets and the makespan. Raises if nothing completes for stall_s
+    seconds while requests are in flight."""
+    order = np.argsort(arrival_times, kind="stable")
+    pending: list[Ticket] = []
+    done: list[Ticket] = []
+    nxt = 0
+    t0 = time.perf_counter()
+    n = len(requests)
+    last_progress = t0
+    while len(done) < n:
+        now_abs = time.perf_counter()
+        if server.in_flight and now_abs - last_progress > stall_s:
+            raise RuntimeError(f"no request finished for {stall_s:.0f} s ({server.in_flight} in flight)")
+        now = now_abs - t0
+        while nxt < n and arrival_times[order[nxt]] <= now:
+            i = int(order[nxt])
+            V, C, _ = requests[i]
+            pending.append(Ticket(rid=i, V=V, C=C, arrival=t0 + arrival_times[i], keep_paths=keep_paths))
+            nxt += 1
+        while pending and server.try_submit(pending[0], requests[pending[0].rid][2]):
+            pending.pop(0)
+        finished = server.poll()
+        if finished or not server.in_flight:
+            last_progress = time.perf_counter()
+        done.extend(finished)
+        if not pending and nxt < n and server.in_flight == 0:
+            time.sleep(max(0.0, min(0.001, arrival_times[order[nxt]] - (time.perf_counter() - t0))))
+    return done, time.perf_counter() - t0
+
+
+def summarize(tickets: list[Ticket], offered_rate: float, makespan: float) -> LoadResult:
+    lat = np.array([t.latency for t in tickets]) * 1e3
+    return LoadResult(offered_rate, len(tickets) / makespan, float(np.percentile(lat, 50)),
+                      float(np.percentile(lat, 99)), float(lat.mean()), len(tickets), makespan)

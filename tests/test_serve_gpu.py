@@ -1,0 +1,77 @@
+"""Serving engine: requests arriving while others run are closed in the same persistent
+kernel; every result is bit-identical to the same election run alone."""
+import numpy as np
+import pytest
+import torch
+
+from scalingelections_b200 import api
+from scalingelections_b200.ballots import mallows_ballots_device
+from scalingelections_b200.serve import Server, run_arrivals
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(seed, n):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        C = int(rng.integers(2, 700))
+        V = int(rng.integers(5, 2500))
+        if i % 7 == 3:
+            C, V = int(rng.integers(3, 40)), int(rng.integers(66000, 90000))  # shifted 16-bit lanes
+        b = mallows_ballots_device(V, C, float(rng.uniform(0.2, 1.0)), seed=seed * 1000 + i)
+        reqs.append((V, C, b))
+    torch.cuda.synchronize()
+    return reqs
+
+
+def alone(V, C, b):
+    ids = b.reshape(-1)
+    offs = torch.arange(V + 1, dtype=torch.int64, device=b.device) * C
+    d = api.tally_device(ids, offs, C)
+    S = api.strongest_paths_device(d, lanes=api.LANES_AUTO)
+    wins, ranking = api.rank_device(S)
+    return api._to_host_u32(S), ranking.cpu().numpy()
+
+
+def test_in_mix_equals_alone():
+    reqs = make_requests(1, 24)
+    server = Server(budget_bytes=2 << 30, max_slots=64, idle_ms=20)
+    # Arrivals in three bursts, so requests join while earlier ones are on the GPU.
+    times = [0.0] * 8 + [0.002] * 8 + [0.004] * 8
+    done, _ = run_arrivals(server, reqs, times, keep_paths=True)
+    server.close()
+    assert len(done) == len(reqs)
+    for t in done:
+        V, C, b = reqs[t.rid]
+        assert t.status == 0, (t.rid, t.status)
+        S, ranking = alone(V, C, b)
+        assert np.array_equal(t.strongest_paths, S), t.rid
+        assert np.array_equal(t.ranking, ranking), t.rid
+
+
+def test_admission_under_a_tight_budget(orc):
+    """A budget too small for all requests at once: they queue on the host and are admitted
+    as memory frees up; results stay exact."""
+    reqs = make_requests(2, 10)
+    server = Server(budget_bytes=64 << 20, max_slots=8, idle_ms=5)
+    done, _ = run_arrivals(server, reqs, [0.0] * len(reqs), keep_paths=True)
+    server.close()
+    assert len(done) == len(reqs)
+    for t in done:
+        V, C, b = reqs[t.rid]
+        d = orc.tally(b.cpu().numpy(), "positions")
+        S_ref = orc.strongest_paths(d, "blocked", tile=32)
+        assert np.array_equal(t.strongest_paths, S_ref), t.rid
+        _, rank_ref = orc.wins_and_ranking(S_ref)
+        assert np.array_equal(t.ranking, rank_ref), t.rid
+
+
+def test_malformed_ballots_reported_in_status():
+    V, C = 10, 6
+    b = torch.arange(C, dtype=torch.int32, device="cuda").repeat(V, 1)
+    b[3, 2] = 0  # repeated id in ballot 3
+    server = Server(budget_bytes=64 << 20, max_slots=4, idle_ms=5)
+    done, _ = run_arrivals(server, [(V, C, b)], [0.0])
+    server.close()
+    assert done[0].status & 8 and (done[0].status & 3) == 3
