@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=40.0, help="serve: HBM admission budget")
     ap.add_argument("--elections", type=int, default=4096, help="batch: number of elections")
     ap.add_argument("--max-candidates", type=int, default=2048, help="batch: largest C")
+    ap.add_argument("--no-autotune", action="store_true", help="batch: skip the autotuner (use defaults)")
     return ap.parse_args()
 
 
@@ -383,9 +384,20 @@ def run_batch(args, world, rank, local_rank):
     t0 = time.perf_counter()
     prefs = make_batch_inputs(specs, dev)
     prep_s = time.perf_counter() - t0
-    lanes = [lanes_for_voters(V) for (_, V, _, _) in specs]
+    tuned = None
+    tune_s = 0.0
+    if args.no_autotune:
+        lanes, order, ctas = [lanes_for_voters(V) for (_, V, _, _) in specs], 0, 0
+    else:
+        from scalingelections_b200 import autotune
+
+        t0 = time.perf_counter()
+        tuned = autotune.tune(V=100000, per_bucket=24, reps=2, path=Path("gpurun_out") / "autotune.json"
+                              if Path("gpurun_out").exists() else None)
+        tune_s = time.perf_counter() - t0
+        lanes, order, ctas = autotune.choose(tuned, [C for (C, _, _, _) in specs], [V for (_, V, _, _) in specs])
     cells = float(sum(C ** 3 for (C, _, _, _) in all_specs))
-    b = BatchedElections(prefs, lanes)
+    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas)
     b.build_graph()
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -445,6 +457,10 @@ def run_batch(args, world, rank, local_rank):
             "speedup_vs_loop": (len(specs) / (ms * 1e-3)) / (len(specs) / loop_s),
             "bit_identical_to_loop": identical,
             "input_prep_seconds": prep_s,
+            "autotune": None if tuned is None else {
+                "seconds": tune_s, "order": order, "ctas_per_sm": ctas,
+                "buckets": {k: {"C": v["range"], "lanes": v["lanes"], "ctas_per_sm": v["ctas_per_sm"]}
+                            for k, v in tuned["buckets"].items()}},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -481,9 +497,11 @@ def run_serve(args, world, rank, local_rank):
     server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=20)
     # Warm-up, then capacity: every request arrives at once (closed loop, admission-bound).
     run_arrivals(server, reqs[: min(8, len(reqs))], [0.0] * min(8, len(reqs)))
+    launches0 = server.stats()["engine_launches"]
     done, makespan = run_arrivals(server, reqs, [0.0] * len(reqs))
     capacity = len(done) / makespan
     sat = summarize(done, float("inf"), makespan)
+    sat_launches = server.stats()["engine_launches"] - launches0
     rng = np.random.default_rng(args.seed + 17)
     loads = []
     with ClockSampler(local_rank) as clocks:
@@ -491,10 +509,12 @@ def run_serve(args, world, rank, local_rank):
             rate = frac * capacity
             gaps = rng.exponential(1.0 / rate, size=len(reqs))
             arrivals = list(np.cumsum(gaps) - gaps[0])
+            l0 = server.stats()["engine_launches"]
             done, span = run_arrivals(server, reqs, arrivals)
             r = summarize(done, rate, span)
             loads.append({"offered_fraction": frac, "offered_per_s": rate, "achieved_per_s": r.achieved_rate,
-                          "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms, "n": r.n})
+                          "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms, "n": r.n,
+                          "engine_launches": server.stats()["engine_launches"] - l0})
     server.close()
     if rank == 0:
         V = np.array([s[0] for s in specs], float)
@@ -508,7 +528,8 @@ def run_serve(args, world, rank, local_rank):
             "config": {"workload": f"{args.requests} requests, C log-uniform [8, 8192], V log-uniform [100, 100000], "
                                    f"Mallows phi ~ U[0.2, 1]; HBM budget {args.budget_gb:g} GB",
                        "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum())},
-            "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan},
+            "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan,
+                           "engine_launches": sat_launches, "grid": server.stats()["grid"]},
             "loads": loads,
             "input_prep_seconds": prep_s,
             "clocks": clocks.summary(),

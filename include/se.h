@@ -131,6 +131,7 @@ SE_API se_status_t se_closure_noalloc(const uint32_t* d_pref, int64_t ld_pref, i
  *   se_batch_prepare           builds the task queues and tensor maps and uploads them into
  *                              d_work (synchronous copies); fills the caller's plan.
  *                              order: 0 = small elections after the tiled ones, 1 = before.
+ *                              ctas_per_sm: persistent CTAs per SM (0 = as many as fit).
  *   se_batch_run               enqueues one whole batch on `stream` (asynchronous, no host
  *                              synchronisation, capturable).
  *   se_batch_graph_build       captures se_batch_run into a CUDA graph held by the plan;
@@ -157,7 +158,8 @@ typedef struct se_batch_plan {
 
 SE_API int64_t se_batch_workspace_bytes(int n, const se_election_t* elections);
 SE_API se_status_t se_batch_prepare(int n, const se_election_t* elections, void* d_work,
-                                    int64_t work_bytes, int order, se_batch_plan_t* plan);
+                                    int64_t work_bytes, int order, int ctas_per_sm,
+                                    se_batch_plan_t* plan);
 SE_API se_status_t se_batch_run(const se_batch_plan_t* plan, void* stream);
 SE_API se_status_t se_batch_graph_build(se_batch_plan_t* plan);
 SE_API se_status_t se_batch_graph_launch(const se_batch_plan_t* plan, void* stream);
@@ -209,6 +211,8 @@ SE_API se_status_t se_engine_submit(se_engine_t* engine, const se_request_t* req
                                     int* slot, uint32_t* generation);
 SE_API se_status_t se_engine_poll(se_engine_t* engine, int* slots, uint32_t* statuses, int max,
                                   int* n_finished);
+/* Kernel launches so far, the engine's grid size, and requests in flight. */
+SE_API se_status_t se_engine_stats(se_engine_t* engine, int64_t* launches, int* grid, int* in_flight);
 SE_API se_status_t se_engine_stop(se_engine_t* engine);
 SE_API se_status_t se_engine_destroy(se_engine_t* engine);
 

@@ -42,7 +42,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure_launch_count": (_c_int, [_c_int]),
     "se_closure_noalloc": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _vp]),
     "se_batch_workspace_bytes": (_c_i64, [_c_int, _vp]),
-    "se_batch_prepare": (_c_int, [_c_int, _vp, _vp, _c_i64, _c_int, _vp]),
+    "se_batch_prepare": (_c_int, [_c_int, _vp, _vp, _c_i64, _c_int, _c_int, _vp]),
     "se_batch_run": (_c_int, [_vp, _vp]),
     "se_batch_graph_build": (_c_int, [_vp]),
     "se_batch_graph_launch": (_c_int, [_vp, _vp]),
@@ -54,6 +54,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_engine_request_scratch_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_engine_submit": (_c_int, [_vp, _vp, _vp, _ip, ctypes.POINTER(ctypes.c_uint32)]),
     "se_engine_poll": (_c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_uint32), _c_int, _ip]),
+    "se_engine_stats": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _ip, _ip]),
     "se_engine_stop": (_c_int, [_vp]),
     "se_engine_destroy": (_c_int, [_vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),

@@ -1,0 +1,125 @@
+"""Autotuner for the batched closure.
+
+For each election-size bucket it times, on the GPU, the batched persistent closure of a
+sample batch under every candidate configuration and keeps the fastest:
+  lanes        16-bit (shifted by V // 2 when counts exceed 16 bits) or 32-bit;
+  ctas_per_sm  persistent CTAs per SM (1 or 2 where both fit);
+and, over a mixed sample of all buckets, the queue order (elections of at most 128
+candidates after the tiled ones, or before). The tile (128 x 128 cells) and the register
+micro-tile (8 x 8 words) are fixed: they come from the register and shared-memory budget and
+the measured min/max issue rate. Results are stored as JSON and looked up per election.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from ._lib import LANES_U16, LANES_U32
+from .batch import BatchedElections, lanes_for_voters
+
+BUCKETS = [(1, 32), (33, 64), (65, 128), (129, 256), (257, 512), (513, 1024), (1025, 2048), (2049, 4096)]
+
+
+def default_path() -> Path:
+    env = os.environ.get("SE_AUTOTUNE_PATH")
+    return Path(env) if env else Path.home() / ".cache" / "scalingelections_b200" / "autotune.json"
+
+
+def bucket_of(C: int) -> int:
+    for b, (lo, hi) in enumerate(BUCKETS):
+        if lo <= C <= hi:
+            return b
+    return len(BUCKETS) - 1
+
+
+def _sample_batch(lo: int, hi: int, n: int, V: int, seed: int, device) -> list[torch.Tensor]:
+    """Random tallies of V ballots (complete ballots: d[i][j] + d[j][i] = V)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        C = int(rng.integers(lo, hi + 1))
+        up = rng.integers(0, V + 1, size=(C, C), dtype=np.int64)
+        d = np.triu(up, 1)
+        d = d + np.triu(V - up, 1).T
+        out.append(torch.from_numpy(d.astype(np.uint32).view(np.int32)).to(device).view(torch.uint32))
+    return out
+
+
+def _time(prefs, lanes, order, ctas, reps: int) -> float:
+    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas)
+    b.build_graph()
+    b.launch_graph()
+    b.check()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        b.launch_graph()
+    e1.record(s)
+    torch.cuda.synchronize()
+    b.check()
+    ms = e0.elapsed_time(e1) / reps
+    b.close()
+    return ms
+
+
+def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, path: Path | None = None,
+         device=None) -> dict:
+    """Runs the search and writes the table; returns it. V is the ballot count of the sample
+    tallies (above 65535 so both lane modes are legal only through the shifted 16-bit window)."""
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    table = {"V_sample": V, "buckets": {}}
+    for b, (lo, hi) in enumerate(BUCKETS):
+        n = per_bucket if hi <= 1024 else max(4, per_bucket // 8)
+        prefs = _sample_batch(lo, hi, n, V, seed + b, device)
+        results = {}
+        for lanes in (LANES_U16, LANES_U32):
+            lane_pair = lanes_for_voters(V) if lanes == LANES_U16 else (LANES_U32, 0)
+            if lane_pair[0] != lanes:
+                continue
+            for ctas in (1, 2):
+                ms = _time(prefs, [lane_pair] * len(prefs), 0, ctas, reps)
+                results[f"u{lanes}/ctas{ctas}"] = ms
+        best = min(results, key=results.get)
+        table["buckets"][str(b)] = {"range": [lo, hi], "lanes": int(best.split("/")[0][1:]),
+                                    "ctas_per_sm": int(best.split("ctas")[1]), "ms": results}
+        del prefs
+    mixed = []
+    for b, (lo, hi) in enumerate(BUCKETS[:-1]):
+        mixed += _sample_batch(lo, hi, max(2, per_bucket // (1 + b)), V, seed + 100 + b, device)
+    lanes = [lanes_for_voters(V)] * len(mixed)
+    orders = {o: _time(mixed, lanes, o, 0, reps) for o in (0, 1)}
+    table["order"] = int(min(orders, key=orders.get))
+    table["order_ms"] = {str(k): v for k, v in orders.items()}
+    p = Path(path) if path else default_path()
+    p.parent.mkdir(parents=True, exist_ok=True)
+    p.write_text(json.dumps(table, indent=1) + "\n")
+    return table
+
+
+def load(path: Path | None = None) -> dict | None:
+    p = Path(path) if path else default_path()
+    return json.loads(p.read_text()) if p.exists() else None
+
+
+def choose(table: dict | None, Cs: Sequence[int], Vs: Sequence[int]) -> tuple[list, int, int]:
+    """(lanes per election, order, ctas_per_sm) for a batch: per-bucket lane modes from the
+    table (falling back to the widest legal 16-bit window), the table's order, and the CTA
+    count most of the batch's work prefers."""
+    lanes, votes = [], {}
+    for C, V in zip(Cs, Vs):
+        entry = (table or {}).get("buckets", {}).get(str(bucket_of(int(C))))
+        pair = lanes_for_voters(int(V))
+        if entry and entry["lanes"] == 32:
+            pair = (LANES_U32, 0)
+        lanes.append(pair)
+        if entry:
+            votes[entry["ctas_per_sm"]] = votes.get(entry["ctas_per_sm"], 0.0) + float(C) ** 3
+    ctas = max(votes, key=votes.get) if votes else 0
+    order = int((table or {}).get("order", 0))
+    return lanes, order, ctas

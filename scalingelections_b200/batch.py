@@ -34,10 +34,12 @@ class BatchedElections:
     lanes: per election, LANES_U16 or LANES_U32, or (lanes, value_offset) pairs such as
     lanes_for_voters() returns; None picks from each matrix's maximum (one device-to-host
     read for the whole batch). order: 0 runs small elections (C <= 128) after the tiled ones,
-    1 before them. The batch keeps references to every buffer it uses."""
+    1 before them. ctas_per_sm: persistent CTAs per SM (0 = as many as fit). An autotuned
+    table (scalingelections_b200.autotune) supplies lanes, order and ctas_per_sm per size
+    bucket. The batch keeps references to every buffer it uses."""
 
     def __init__(self, preferences: Sequence[torch.Tensor], lanes: Sequence | None = None, *,
-                 ranking: bool = True, order: int = 0):
+                 ranking: bool = True, order: int = 0, ctas_per_sm: int = 0):
         if not preferences:
             raise ValueError("empty batch")
         self.device = preferences[0].device
@@ -81,7 +83,7 @@ class BatchedElections:
         self.plan = _lib.BatchPlan()
         with torch.cuda.device(self.device):
             check(L.se_batch_prepare(len(self.prefs), ctypes.cast(arr, ctypes.c_void_p), self.workspace.data_ptr(),
-                                     need, int(order), ctypes.byref(self.plan)))
+                                     need, int(order), int(ctas_per_sm), ctypes.byref(self.plan)))
         self._graph = False
 
     @property

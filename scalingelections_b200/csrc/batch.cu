@@ -414,7 +414,7 @@ extern "C" int64_t se_batch_workspace_bytes(int n, const se_election_t* election
 }
 
 extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_work, int64_t work_bytes, int order,
-                                        se_batch_plan_t* plan_out) {
+                                        int ctas_per_sm, se_batch_plan_t* plan_out) {
     clear_error();
     SE_REQUIRE(plan_out != nullptr, SE_ERR_INVALID, "null plan");
     SE_REQUIRE(n == 0 || el != nullptr, SE_ERR_INVALID, "null election array");
@@ -551,8 +551,11 @@ extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_
     P.place_blocks = pp.back();
     const int occ16 = occupancy<16>(), occ32 = occupancy<32>();
     SE_REQUIRE(occ16 >= 1 && occ32 >= 1, SE_ERR_CUDA, "batched closure kernel cannot be resident");
-    P.grid[0] = int(std::min<int64_t>(P.ntasks[0], int64_t(sms) * occ16));
-    P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * occ32));
+    SE_REQUIRE(ctas_per_sm >= 0, SE_ERR_INVALID, "ctas_per_sm must be >= 0");
+    const int per16 = ctas_per_sm > 0 ? std::min(occ16, ctas_per_sm) : occ16;
+    const int per32 = ctas_per_sm > 0 ? std::min(occ32, ctas_per_sm) : occ32;
+    P.grid[0] = int(std::min<int64_t>(P.ntasks[0], int64_t(sms) * per16));
+    P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * per32));
     P.graph = nullptr;
     std::memcpy(plan_out, &P, sizeof(P));
     return SE_OK;

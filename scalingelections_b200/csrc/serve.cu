@@ -23,9 +23,10 @@
 // becomes visible only when the host's last write for it (active = 1) lands.
 //
 // Completion: the CTA finishing a request's last task writes (generation << 8 | status) to
-// host-mapped memory; the host polls it without any CUDA call. All waits are bounded: an idle
-// CTA exits after idle_ms without claimable work (the host relaunches the engine when new
-// work arrives), every mbarrier wait has a time limit, and the host can raise a stop flag.
+// host-mapped memory; the host polls it without any CUDA call. All waits are bounded: after
+// idle_ms with no active request the whole grid retires together (the host relaunches the
+// engine when new work arrives); while requests are active a CTA waits at most 10 s for a
+// claimable task; every mbarrier wait has a time limit; the host can raise a stop flag.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -70,7 +71,7 @@ struct EngineHeader {
     uint32_t err;
     uint32_t stop;
     uint32_t slot_hi;
-    uint32_t pad;
+    uint32_t retire;  // raised by the first CTA to time out idle: the whole grid leaves together
 };
 
 __host__ __device__ inline int phases_of(int R) { return R == 1 ? 3 : 3 * R + 4; }
@@ -360,6 +361,7 @@ __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8
 }
 
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+constexpr uint64_t kStallNs = 10000000000ull;  // 10 s without a claim while requests are active
 
 __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
     engine_kernel(Req* __restrict__ slots, uint64_t* __restrict__ claims, uint32_t* __restrict__ dones,
@@ -383,12 +385,14 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
     for (;;) {
         if (threadIdx.x == 0) {
             uint32_t got = kNoSlot;
-            const uint64_t t0 = global_ns();
+            uint64_t t0 = global_ns();
             while (got == kNoSlot) {
-                if (ld_acquire(&hdr->stop) || ld_acquire(&hdr->err)) break;
+                if (ld_acquire(&hdr->stop) || ld_acquire(&hdr->err) || ld_acquire(&hdr->retire)) break;
                 const uint32_t hi = ld_acquire(&hdr->slot_hi);
+                bool any_active = false;
                 for (uint32_t s = 0; s < hi && got == kNoSlot; ++s) {  // oldest slots first
                     if (!ld_acquire(&slots[s].active)) continue;
+                    any_active = true;
                     const uint32_t gen = __ldcg(&slots[s].gen);
                     const int R = __ldcg(&slots[s].e.R);
                     const int64_t V = __ldcg(&slots[s].V);
@@ -402,8 +406,22 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                     }
                 }
                 if (got == kNoSlot) {
-                    if (global_ns() - t0 > idle_ns) break;
-                    __nanosleep(500);
+                    // With no active request the CTA leaves after idle_ns (the host relaunches
+                    // the engine for the next one). While requests are active but have nothing
+                    // claimable (their current phase's last tasks are still running) it keeps
+                    // looking, up to kStallNs without any claim, which no task comes close to.
+                    const uint64_t waited = global_ns() - t0;
+                    if (!any_active && waited > idle_ns) {
+                        // Retire the whole grid, never part of it: a partial grid would keep
+                        // serving the next request with a fraction of the SMs.
+                        atomicExch(&hdr->retire, 1u);
+                        break;
+                    }
+                    if (waited > kStallNs) {
+                        atomicCAS(&hdr->err, 0u, 2u);
+                        break;
+                    }
+                    __nanosleep(any_active ? 200 : 1000);
                 }
             }
             s_slot = got;
@@ -522,6 +540,7 @@ struct Engine {
     cudaStream_t stream = nullptr;   // the engine kernel's stream
     cudaEvent_t finished = nullptr;  // recorded after each engine launch
     bool launched = false;
+    int64_t launches = 0;
     int grid = 0;
     uint64_t idle_ns = 0;
     int in_flight = 0;
@@ -541,11 +560,13 @@ int64_t offsets(int max_slots, int64_t* slots_off, int64_t* claims_off, int64_t*
 }
 
 se_status_t launch_engine(Engine& E) {
+    SE_CUDA_TRY(cudaMemsetAsync(&E.hdr->retire, 0, 4, E.stream));
     engine_kernel<<<E.grid, cfg<16>::THREADS, kEngineSmem, E.stream>>>(E.slots, E.claims, E.dones, E.hdr,
                                                                            E.idle_ns);
     SE_CHECK_LAUNCH();
     SE_CUDA_TRY(cudaEventRecord(E.finished, E.stream));
     E.launched = true;
+    ++E.launches;
     return SE_OK;
 }
 
@@ -559,7 +580,8 @@ se_status_t ensure_running(Engine& E) {
         EngineHeader h;
         SE_CUDA_TRY(cudaMemcpyAsync(&h, E.hdr, sizeof(h), cudaMemcpyDeviceToHost, E.stream));
         SE_CUDA_TRY(cudaStreamSynchronize(E.stream));
-        SE_REQUIRE(h.err == 0, SE_ERR_DEVICE, "serving engine stopped on a device error (%u)", h.err);
+        SE_REQUIRE(h.err == 0, SE_ERR_DEVICE, "serving engine stopped on a device error (%u: %s)", h.err,
+                   h.err == 2 ? "no task could be claimed for 10 s" : "lost TMA completion");
     }
     return launch_engine(E);
 }
@@ -772,6 +794,16 @@ extern "C" se_status_t se_engine_poll(se_engine_t* h, int* slots_out, uint32_t* 
     }
     *n_out = n;
     return ensure_running(E);
+}
+
+extern "C" se_status_t se_engine_stats(se_engine_t* h, int64_t* launches, int* grid, int* in_flight) {
+    clear_error();
+    SE_REQUIRE(h != nullptr, SE_ERR_INVALID, "null engine");
+    std::lock_guard<std::mutex> lock(h->e.mu);
+    if (launches) *launches = h->e.launches;
+    if (grid) *grid = h->e.grid;
+    if (in_flight) *in_flight = h->e.in_flight;
+    return SE_OK;
 }
 
 extern "C" se_status_t se_engine_stop(se_engine_t* h) {

@@ -212,6 +212,11 @@ class Server:
     def in_flight(self) -> int:
         return len(self.by_slot)
 
+    def stats(self) -> dict:
+        launches, grid, fl = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
+        check(self.L.se_engine_stats(self.engine, ctypes.byref(launches), ctypes.byref(grid), ctypes.byref(fl)))
+        return {"engine_launches": launches.value, "grid": grid.value, "in_flight": fl.value}
+
     def close(self) -> None:
         if self.engine:
             self.L.se_engine_destroy(self.engine)
