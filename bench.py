@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--phi", type=float, default=0.8)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
+    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="0: dataflow when the workspace allows, 1: round by round, 2: dataflow")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -73,6 +75,7 @@ def config(args, world):
         "voters": args.voters,
         "phi": args.phi,
         "lanes": f"u{args.lanes}" if args.lanes else "auto",
+        "closure_mode": ["auto (dataflow)", "round by round", "dataflow"][args.closure_mode],
         "tile": 128,
         "parallelism": f"replicas{world}" if world > 1 else "single",
         "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
@@ -233,6 +236,7 @@ def run_ours(args, world, rank, local_rank):
     _lib.check(L.se_minmax_peak(recipe, 65536, *[ctypes.byref(x) for x in peak]))
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
+    api.set_closure_mode(args.closure_mode)
     need = api.closure_workspace_bytes(C, lanes)
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
@@ -494,14 +498,21 @@ def run_serve(args, world, rank, local_rank):
     reqs = [(V, C, mallows_ballots_device(V, C, phi, seed=sd, device=dev)) for (V, C, phi, sd) in specs]
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
-    server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=20)
+    server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=5)
     # Warm-up, then capacity: every request arrives at once (closed loop, admission-bound).
     run_arrivals(server, reqs[: min(8, len(reqs))], [0.0] * min(8, len(reqs)))
-    launches0 = server.stats()["engine_launches"]
+    p0 = server.stats(profile=True)
     done, makespan = run_arrivals(server, reqs, [0.0] * len(reqs))
     capacity = len(done) / makespan
     sat = summarize(done, float("inf"), makespan)
-    sat_launches = server.stats()["engine_launches"] - launches0
+    p1 = server.stats(profile=True)
+    sat_launches = p1["engine_launches"] - p0["engine_launches"]
+    sat_profile = {
+        "busy_cta_ms": {k: p1["busy_cta_ms"][k] - p0["busy_cta_ms"][k] for k in p1["busy_cta_ms"]},
+        "tasks": {k: p1["tasks"][k] - p0["tasks"][k] for k in p1["tasks"]},
+        "search_cta_ms": p1["search_cta_ms"] - p0["search_cta_ms"],
+        "grid_cta_ms": p1["grid"] * makespan * 1e3,
+    }
     rng = np.random.default_rng(args.seed + 17)
     loads = []
     with ClockSampler(local_rank) as clocks:
@@ -515,6 +526,7 @@ def run_serve(args, world, rank, local_rank):
             loads.append({"offered_fraction": frac, "offered_per_s": rate, "achieved_per_s": r.achieved_rate,
                           "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms, "n": r.n,
                           "engine_launches": server.stats()["engine_launches"] - l0})
+    grid = server.stats()["grid"]
     server.close()
     if rank == 0:
         V = np.array([s[0] for s in specs], float)
@@ -529,7 +541,8 @@ def run_serve(args, world, rank, local_rank):
                                    f"Mallows phi ~ U[0.2, 1]; HBM budget {args.budget_gb:g} GB",
                        "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum())},
             "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan,
-                           "engine_launches": sat_launches, "grid": server.stats()["grid"]},
+                           "engine_launches": sat_launches, "grid": grid,
+                           "engine_profile": sat_profile},
             "loads": loads,
             "input_prep_seconds": prep_s,
             "clocks": clocks.summary(),

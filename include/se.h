@@ -92,6 +92,22 @@ SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, 
                                        int64_t ld_out, int lane_bits, int tile, void* d_work,
                                        int64_t work_bytes, void* stream, double* phase_ms, int* launches);
 
+/* Workspace for the dataflow form of the closure (no barrier between pivot rounds): one
+ * persistent launch that overlaps each round's panels and the start of the next round with
+ * the end of the current one. se_closure uses it whenever d_work is at least this large (and
+ * C > 128); with the smaller se_closure_workspace_bytes() it runs round by round. Results are
+ * identical either way. */
+SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
+
+/* Task t (< R^3) of the dataflow closure's fixed order for R = ceil(C / 128) pivot blocks:
+ * kind 0 pivot, 1 pivot-row panel, 2 pivot-column panel, 3 remainder; round k; tile (i, j).
+ * Host-only (no GPU needed): lets tests check the order against the dependency rules. */
+SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, int* i, int* j);
+
+/* Process-wide choice for se_closure: 0 = dataflow when the workspace allows (default),
+ * 1 = always round by round, 2 = dataflow only. For benchmarking and tests. */
+SE_API se_status_t se_closure_set_mode(int mode);
+
 /* Number of kernels one se_closure call launches for C candidates (with lane_bits 16 or 32;
  * the automatic mode adds at most one more). */
 SE_API int se_closure_launch_count(int C);
@@ -178,8 +194,9 @@ SE_API int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue);
  *   se_engine_create                 ctas_per_sm in {1, 2}; idle_ms: the kernel exits after
  *                                    that long without work, and the next submit or poll
  *                                    relaunches it.
- *   se_engine_request_scratch_bytes  per-request scratch (ballot places, working matrix,
- *                                    panels) for V ballots and C candidates.
+ *   se_engine_request_scratch_bytes  per-request scratch (working matrix, panels) for C
+ *                                    candidates; se_engine_request_positions_bytes the ballot
+ *                                    places, which are released early (se_engine_poll_tallied).
  *   se_engine_submit                 publishes a request on `stream` (a few small copies and
  *                                    memsets; asynchronous). Returns its slot and generation.
  *   se_engine_poll                   requests finished since the last poll: slot and status
@@ -200,6 +217,9 @@ typedef struct se_request {
     int32_t* d_ranking;        /* out: C */
     void* d_scratch;           /* se_engine_request_scratch_bytes(V, C), 256-byte aligned */
     int64_t scratch_bytes;
+    void* d_positions;         /* ballot places: se_engine_request_positions_bytes(V, C), 256-byte
+                                  aligned; free for reuse once se_engine_poll_tallied reports it */
+    int64_t positions_bytes;
 } se_request_t;
 
 typedef struct se_engine se_engine_t;
@@ -207,12 +227,20 @@ SE_API int64_t se_engine_workspace_bytes(int max_slots);
 SE_API se_status_t se_engine_create(void* d_work, int64_t work_bytes, int max_slots, int ctas_per_sm,
                                     int idle_ms, se_engine_t** engine);
 SE_API int64_t se_engine_request_scratch_bytes(int64_t V, int C);
+SE_API int64_t se_engine_request_positions_bytes(int64_t V, int C);
 SE_API se_status_t se_engine_submit(se_engine_t* engine, const se_request_t* request, void* stream,
                                     int* slot, uint32_t* generation);
 SE_API se_status_t se_engine_poll(se_engine_t* engine, int* slots, uint32_t* statuses, int max,
                                   int* n_finished);
-/* Kernel launches so far, the engine's grid size, and requests in flight. */
-SE_API se_status_t se_engine_stats(se_engine_t* engine, int64_t* launches, int* grid, int* in_flight);
+/* Requests whose tally finished since the last call: their ballot-place buffer (usually the
+ * largest part of a request's memory) may be reused from now on. */
+SE_API se_status_t se_engine_poll_tallied(se_engine_t* engine, int* slots, int max, int* n);
+/* Kernel launches so far, the engine's grid size, requests in flight and, when the arrays
+ * are given, a profile snapshot: busy_ms[8] / tasks[8] per task kind (positions, tally,
+ * small election, pivot, panels, remainder, output + wins, ranking), summed over CTAs, and
+ * the CTA-milliseconds spent looking for work (any pointer may be NULL). */
+SE_API se_status_t se_engine_stats(se_engine_t* engine, int64_t* launches, int* grid, int* in_flight,
+                                   double* busy_ms, int64_t* tasks, double* search_ms);
 SE_API se_status_t se_engine_stop(se_engine_t* engine);
 SE_API se_status_t se_engine_destroy(se_engine_t* engine);
 

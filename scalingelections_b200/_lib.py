@@ -40,6 +40,9 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp]),
     "se_closure_profiled": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _dp, _ip]),
     "se_closure_launch_count": (_c_int, [_c_int]),
+    "se_closure_workspace_bytes_flow": (_c_i64, [_c_int, _c_int, _c_int]),
+    "se_closure_set_mode": (_c_int, [_c_int]),
+    "se_closure_flow_task": (_c_int, [ctypes.c_uint32, _c_int, _ip, _ip, _ip, _ip]),
     "se_closure_noalloc": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _vp]),
     "se_batch_workspace_bytes": (_c_i64, [_c_int, _vp]),
     "se_batch_prepare": (_c_int, [_c_int, _vp, _vp, _c_i64, _c_int, _c_int, _vp]),
@@ -52,9 +55,11 @@ SIGNATURES: dict[str, tuple] = {
     "se_engine_workspace_bytes": (_c_i64, [_c_int]),
     "se_engine_create": (_c_int, [_vp, _c_i64, _c_int, _c_int, _c_int, _vp]),
     "se_engine_request_scratch_bytes": (_c_i64, [_c_i64, _c_int]),
+    "se_engine_request_positions_bytes": (_c_i64, [_c_i64, _c_int]),
+    "se_engine_poll_tallied": (_c_int, [_vp, _ip, _c_int, _ip]),
     "se_engine_submit": (_c_int, [_vp, _vp, _vp, _ip, ctypes.POINTER(ctypes.c_uint32)]),
     "se_engine_poll": (_c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_uint32), _c_int, _ip]),
-    "se_engine_stats": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _ip, _ip]),
+    "se_engine_stats": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _ip, _ip, _dp, ctypes.POINTER(ctypes.c_int64), _dp]),
     "se_engine_stop": (_c_int, [_vp]),
     "se_engine_destroy": (_c_int, [_vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
@@ -79,7 +84,8 @@ class Request(ctypes.Structure):
     _fields_ = [("d_ids", ctypes.c_void_p), ("d_offsets", ctypes.c_void_p), ("V", ctypes.c_int64),
                 ("C", ctypes.c_int32), ("value_offset", ctypes.c_uint32), ("d_prefs", ctypes.c_void_p),
                 ("d_out", ctypes.c_void_p), ("d_wins", ctypes.c_void_p), ("d_ranking", ctypes.c_void_p),
-                ("d_scratch", ctypes.c_void_p), ("scratch_bytes", ctypes.c_int64)]
+                ("d_scratch", ctypes.c_void_p), ("scratch_bytes", ctypes.c_int64),
+                ("d_positions", ctypes.c_void_p), ("positions_bytes", ctypes.c_int64)]
 
 
 class BatchPlan(ctypes.Structure):

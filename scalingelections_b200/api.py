@@ -78,11 +78,19 @@ def _check_matrix(t: torch.Tensor, name: str) -> tuple[int, int]:
 # ------------------------------------------------------------------------------------------
 # Device-resident entry points
 # ------------------------------------------------------------------------------------------
-def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO) -> int:
-    n = _lib.lib().se_closure_workspace_bytes(int(num_candidates), int(lanes), 0)
+def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, dataflow: bool = True) -> int:
+    """Workspace bytes of the closure; dataflow=True sizes it for the barrier-free form."""
+    L = _lib.lib()
+    fn = L.se_closure_workspace_bytes_flow if dataflow else L.se_closure_workspace_bytes
+    n = fn(int(num_candidates), int(lanes), 0)
     if n < 0:
         raise ValueError("invalid closure size")
     return n
+
+
+def set_closure_mode(mode: int) -> None:
+    """0: dataflow when the workspace allows (default); 1: round by round; 2: dataflow only."""
+    check(_lib.lib().se_closure_set_mode(int(mode)))
 
 
 def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO, out: torch.Tensor | None = None,
@@ -101,11 +109,12 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
     if C == 0:
         return out
     need = closure_workspace_bytes(C, lanes)
-    if workspace is None or workspace.numel() * workspace.element_size() < need:
+    if workspace is None or workspace.numel() * workspace.element_size() < closure_workspace_bytes(C, lanes, False):
         workspace = _workspace(need, preferences.device)
+    have = workspace.numel() * workspace.element_size()
     with torch.cuda.device(preferences.device):
         check(_lib.lib().se_closure(preferences.data_ptr(), ld, C, out.data_ptr(), ldo, int(lanes), 0,
-                                    workspace.data_ptr(), need, _stream()))
+                                    workspace.data_ptr(), have, _stream()))
     return out
 
 

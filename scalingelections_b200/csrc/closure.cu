@@ -33,6 +33,7 @@
 #include <stdint.h>
 
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -103,6 +104,259 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     if (fuse_pivot && blockIdx.x == 0) {
         __syncthreads();  // the tile's stores are visible to the whole CTA
         batch::run_pivot<LB>(E, K + 1, rowbuf, colbuf);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Dataflow closure: the same tasks as the round-by-round launches (pivot, panels, remainder),
+// run by one persistent grid that walks a fixed task order with no barrier between rounds.
+// Each task waits only for what it reads and for the readers of what it overwrites:
+//   ver[i][j]   rounds applied to tile (i, j); a task of round k on a tile needs ver == k and
+//               sets k + 1 (panels also need the pivot, the remainder needs both panels)
+//   pdone[k]    panel tasks of round k done: the readers of the pivot tile (column panels read
+//               it) and of dT[k % 2]
+//   rdone[k]    remainder tasks of round k done: the readers of the row-panel tiles S[k][*]
+//               and of AT[k % 2]
+// so a round-k task that writes a tile of row k-1 also waits for pdone[k-1] and rdone[k-1],
+// the column panels of round k wait for rdone[k-2] (AT is double-buffered), and the pivot of
+// round k for pdone[k-2] (so is dT). The order (flow_decode) puts the next round's pivot and
+// panels right after the tiles they need, ahead of the current round's bulk. Every task's
+// prerequisites come earlier in the order and were taken by running CTAs, so the
+// schedule cannot deadlock; waits are bounded and a timeout aborts the grid.
+//
+// A task's round picks the AT/dT buffer pair (k % 2). se_closure_flow_task exposes the order
+// to the host; tests/test_flow_order.py checks it against these rules for every task, small R.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void fence_proxy_async_global_flow() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t flow_ld(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// n-th value of [0, count) without the excluded values a and b (either may be -1).
+__host__ __device__ __forceinline__ int skip2(int n, int a, int b) {
+    int lo = a < b ? a : b, hi = a < b ? b : a;
+    if (lo < 0) {
+        lo = hi;
+        hi = -1;
+    }
+    if (lo >= 0 && n >= lo) ++n;
+    if (hi >= 0 && n >= hi) ++n;
+    return n;
+}
+
+struct FlowTask {
+    int kind;  // 0 pivot, 1 row panel, 2 column panel, 3 remainder
+    int k, i, j;
+};
+
+// Task t of the order. After [pivot 0][panels 0], round k's block is
+//   A  remainder tiles of round k that round k+1 needs first: (k+1, k+1), row k+1, column k+1
+//   B  pivot of round k+1
+//   C  panels of round k+1 except the column tile (k, k+1)
+//   D  the other remainder tiles of round k (rows other than k+1 and k-1)
+//   E  remainder row k-1 (waits for round k-1 to finish)
+//   F  column tile (k, k+1) of round k+1 (it overwrites a row-k tile: waits for round k)
+// so the next round's pivot and panels run while round k's bulk is still in flight. Round
+// R-1 has only D and E. Reduced coordinates of round k skip k; p = reduced k+1, q = reduced
+// k-1.
+__host__ __device__ FlowTask flow_decode(uint32_t t_in, int R) {
+    const int R1 = R - 1;
+    FlowTask T;
+    const uint32_t head = uint32_t(1 + 2 * R1);
+    if (t_in < head) {
+        T.k = 0;
+        if (t_in == 0) {
+            T.kind = 0;
+            T.i = T.j = 0;
+        } else if (int(t_in) - 1 < R1) {
+            T.kind = 1;
+            T.i = 0;
+            T.j = int(t_in);
+        } else {
+            T.kind = 2;
+            T.i = int(t_in) - R1;
+            T.j = 0;
+        }
+        return T;
+    }
+    const uint32_t t = t_in - head;
+    const uint32_t B = uint32_t(R1 * R1) + head;
+    int k = int(t / B);
+    int r;
+    if (k >= R - 1) {
+        k = R - 1;
+        r = int(t - uint32_t(R - 1) * B);
+    } else {
+        r = int(t % B);
+    }
+    const bool last = k + 1 >= R;
+    const int p = last ? -1 : k;
+    const int q = k >= 1 ? k - 1 : -1;
+    auto full = [&](int red) { return red + (red >= k); };
+    const int nA = last ? 0 : 1 + 2 * (R1 - 1);
+    T.k = k;
+    T.kind = 3;
+    if (r < nA) {
+        int ii, jj;
+        if (r == 0) ii = jj = p;
+        else if (r < R1) ii = p, jj = skip2(r - 1, p, -1);
+        else ii = skip2(r - R1, p, -1), jj = p;
+        T.i = full(ii);
+        T.j = full(jj);
+        return T;
+    }
+    r -= nA;
+    if (!last) {
+        const int k1 = k + 1;
+        if (r == 0) {
+            T.kind = 0;
+            T.k = k1;
+            T.i = T.j = k1;
+            return T;
+        }
+        r -= 1;
+        if (r < R1) {
+            T.kind = 1;
+            T.k = k1;
+            T.i = k1;
+            T.j = r + (r >= k1);
+            return T;
+        }
+        r -= R1;
+        if (r < R1 - 1) {
+            T.kind = 2;
+            T.k = k1;
+            T.i = skip2(r, k, k1);
+            T.j = k1;
+            return T;
+        }
+        r -= R1 - 1;
+    }
+    const int ncols = R1 - (last ? 0 : 1);
+    const int nmid = R1 - (last ? 0 : 1) - ((q >= 0 && q != p) ? 1 : 0);
+    if (r < nmid * ncols) {
+        T.i = full(skip2(r / ncols, p, q));
+        T.j = full(skip2(r % ncols, p, -1));
+        return T;
+    }
+    r -= nmid * ncols;
+    if (q >= 0 && q != p && r < ncols) {
+        T.i = full(q);
+        T.j = full(skip2(r, p, -1));
+        return T;
+    }
+    // F: column tile (k, k+1) of round k+1.
+    T.kind = 2;
+    T.k = k + 1;
+    T.i = k;
+    T.j = k + 1;
+    return T;
+}
+
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    flow_kernel(const __grid_constant__ batch::Elec E0, const __grid_constant__ batch::Elec E1,
+                uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ uint32_t s_t;
+    __shared__ int s_go;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int R = E0.R, R1 = R - 1;
+    uint32_t* head = state;
+    uint32_t* abort_flag = state + 1;
+    uint32_t* ver = state + 4;
+    uint32_t* pdone = ver + R * R;
+    uint32_t* rdone = pdone + R;
+    const uint32_t total = uint32_t(R) * uint32_t(R) * uint32_t(R);
+    uint32_t par_a = 0, par_b = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t t = total;
+            if (!flow_ld(abort_flag)) t = atomicAdd(head, 1u);
+            s_t = t;
+            s_go = 1;
+            if (t < total) {
+                const FlowTask T = flow_decode(t, R);
+                const int k = T.k;
+                const uint64_t t0 = global_ns();
+                auto ready = [&]() -> bool {
+                    const uint32_t kk = uint32_t(k);
+                    if (T.kind == 0) {
+                        if (flow_ld(&ver[k * R + k]) < kk) return false;
+                        if (k >= 2 && flow_ld(&pdone[k - 2]) < uint32_t(2 * R1)) return false;
+                        return true;
+                    }
+                    if (flow_ld(&ver[k * R + k]) < kk + 1) return false;  // the pivot of round k
+                    if (flow_ld(&ver[T.i * R + T.j]) < kk) return false;
+                    if (T.kind == 2 && k >= 2 && flow_ld(&rdone[k - 2]) < uint32_t(R1 * R1)) return false;
+                    if (T.kind == 3) {
+                        if (flow_ld(&ver[k * R + T.j]) < kk + 1) return false;
+                        if (flow_ld(&ver[T.i * R + k]) < kk + 1) return false;
+                    }
+                    if (T.i == k - 1 && T.kind >= 2) {
+                        if (flow_ld(&pdone[k - 1]) < uint32_t(2 * R1)) return false;
+                        if (flow_ld(&rdone[k - 1]) < uint32_t(R1 * R1)) return false;
+                    }
+                    return true;
+                };
+                for (uint32_t it = 0; !ready(); ++it) {
+                    if ((it & 31) == 0 && (flow_ld(abort_flag) || global_ns() - t0 > 2000000000ull)) {
+                        atomicExch(abort_flag, 1u);
+                        raise_device_error(err, kErrTmaTimeout + 2);
+                        s_go = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                fence_proxy_async_global_flow();
+            }
+        }
+        __syncthreads();
+        const uint32_t t = s_t;
+        if (t >= total || !s_go) break;
+        const FlowTask T = flow_decode(t, R);
+        const batch::Elec& E = (T.k & 1) ? E1 : E0;
+        bool ok = true;
+        if (T.kind == 0) {
+            batch::run_pivot<LB>(E, T.k, rowbuf, colbuf);
+        } else if (T.kind == 1) {
+            ok = batch::run_product<LB, false>(E, &E, T.k, T.k, T.j, false, smem, bars, par_a);
+            par_a ^= 1u;
+        } else if (T.kind == 2) {
+            ok = batch::run_col<LB, false>(E, &E, T.k, T.i, smem, bars, par_a, par_b);
+            par_a ^= 1u;
+            par_b ^= 1u;
+        } else {
+            ok = batch::run_product<LB, false>(E, &E, T.k, T.i, T.j, true, smem, bars, par_a);
+            par_a ^= 1u;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (!ok) {
+                atomicExch(abort_flag, 1u);
+                raise_device_error(err, kErrTmaTimeout);
+            } else {
+                fence_proxy_async_global_flow();
+                atomicExch(&ver[T.i * R + T.j], uint32_t(T.k + 1));
+                if (T.kind == 1 || T.kind == 2) atomicAdd(&pdone[T.k], 1u);
+                if (T.kind == 3) atomicAdd(&rdone[T.k], 1u);
+            }
+        }
+        if (!ok) break;
     }
 }
 
@@ -263,6 +517,8 @@ struct layout {
     int64_t C = 0;
     int64_t Cp = 0;
     int64_t flags_off = 0, s_off = 0, at_off = 0, dt_off = 0, total = 0;
+    // Dataflow extras: second AT and dT buffers and the task state.
+    int64_t at2_off = 0, dt2_off = 0, state_off = 0, flow_total = 0;
 };
 
 layout plan(int C, int lane_bits) {
@@ -275,14 +531,24 @@ layout plan(int C, int lane_bits) {
     L.at_off = L.s_off + round_up(L.Cp * L.Cp * cell, 256);
     L.dt_off = L.at_off + round_up(int64_t(kT) * L.Cp * 4, 256);
     L.total = L.dt_off + int64_t(kT) * kT * 4;
+    const int64_t R = L.Cp / kT;
+    L.at2_off = round_up(L.total, 256);
+    L.dt2_off = L.at2_off + round_up(int64_t(kT) * L.Cp * 4, 256);
+    L.state_off = L.dt2_off + round_up(int64_t(kT) * kT * 4, 256);
+    L.flow_total = L.state_off + (4 + R * R + 2 * R) * 4;
     return L;
 }
+
+// 0: dataflow when the workspace has room for it, else round by round; 1: always round by
+// round; 2: dataflow only (too small a workspace is an error).
+std::atomic<int> g_closure_mode{0};
 
 template <int LB> se_status_t set_smem_limits() {
     static se_status_t st = [] {
         const int bytes = int(batch::pcfg<LB>::SMEM);
         if (cudaFuncSetAttribute(panels_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-            cudaFuncSetAttribute(rem_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+            cudaFuncSetAttribute(rem_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+            cudaFuncSetAttribute(flow_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
             cudaGetLastError();
             return se_status_t(SE_ERR_CUDA);
         }
@@ -359,6 +625,64 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             }
         }
         for (auto& x : ev) cudaEventDestroy(x);
+        SE_CUDA_TRY(e);
+    }
+    return SE_OK;
+}
+
+// The dataflow closure on an initialised working matrix (pivot of round 0 included).
+template <int LB>
+se_status_t run_flow(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms) {
+    using CF = cfg<LB>;
+    if (se_status_t st = set_smem_limits<LB>(); st != SE_OK) return st;
+    uint32_t* S = reinterpret_cast<uint32_t*>(work + P.s_off);
+    uint32_t* err = reinterpret_cast<uint32_t*>(work + P.flags_off);
+    const int64_t ldw = P.Cp / CF::CPW;
+    const int R = int(P.Cp / kT);
+    batch::Elec E[2];
+    for (int b = 0; b < 2; ++b) {
+        std::memset(&E[b], 0, sizeof(E[b]));
+        uint32_t* AT = reinterpret_cast<uint32_t*>(work + (b ? P.at2_off : P.at_off));
+        uint32_t* dT = reinterpret_cast<uint32_t*>(work + (b ? P.dt2_off : P.dt_off));
+        if (se_status_t st = make_map(&E[b].mapS, S, uint64_t(ldw), uint64_t(P.Cp), uint64_t(ldw) * 4, CF::TW, kKC))
+            return st;
+        if (se_status_t st = make_map(&E[b].mapAT, AT, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC)) return st;
+        if (se_status_t st = make_map(&E[b].mapDT, dT, kT, kT, kT * 4, kT, kKC)) return st;
+        E[b].S = S;
+        E[b].AT = AT;
+        E[b].dT = dT;
+        E[b].C = int(P.C);
+        E[b].Cp = int(P.Cp);
+        E[b].R = R;
+        E[b].lanes = LB;
+    }
+    uint32_t* state = reinterpret_cast<uint32_t*>(work + P.state_off);
+    SE_CUDA_TRY(cudaMemsetAsync(state, 0, size_t(4 + R * R + 2 * R) * 4, stream));
+    int device = 0, sms = 0, occ = 0;
+    SE_CUDA_TRY(cudaGetDevice(&device));
+    SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    SE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, flow_kernel<LB>, CF::THREADS,
+                                                              batch::pcfg<LB>::SMEM));
+    SE_REQUIRE(occ >= 1, SE_ERR_CUDA, "dataflow closure kernel cannot be resident");
+    const int64_t total = int64_t(R) * R * R;
+    const int grid = int(std::min<int64_t>(total, int64_t(sms) * occ));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (phase_ms) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+    }
+    flow_kernel<LB><<<grid, CF::THREADS, batch::pcfg<LB>::SMEM, stream>>>(E[0], E[1], state, err);
+    SE_CHECK_LAUNCH();
+    if (phase_ms) {
+        cudaEventRecord(e1, stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        for (int q = 0; q < 4; ++q) phase_ms[q] = 0.0;
+        phase_ms[3] = ms;  // one launch: pivots, panels and remainders together
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
         SE_CUDA_TRY(e);
     }
     return SE_OK;
@@ -456,7 +780,12 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
     } else {
         if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
-    se_status_t st = lb == 16 ? run_rounds<16>(work, P, s, phase_ms) : run_rounds<32>(work, P, s, phase_ms);
+    const int mode = g_closure_mode.load();
+    const bool flow = mode != 1 && work_bytes >= P.flow_total && P.Cp > kT;
+    SE_REQUIRE(mode != 2 || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
+               "the dataflow closure needs a workspace of %lld bytes", (long long)P.flow_total);
+    se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
+                          : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms) : run_rounds<32>(work, P, s, phase_ms));
     if (st) return st;
     st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, base, s)
                   : launch_finalize<32>(P, work, C, d_out, ld_out, 0, s);
@@ -485,6 +814,29 @@ extern "C" se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pr
         closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
     if (launches) *launches = se_closure_launch_count(C);
     return st;
+}
+
+extern "C" int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile) {
+    if (C < 1 || (tile != 0 && tile != kT)) return -1;
+    return plan(C, lane_bits == 16 ? 16 : 32).flow_total;
+}
+
+extern "C" se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, int* i, int* j) {
+    clear_error();
+    SE_REQUIRE(R >= 2 && R <= 1024 && uint64_t(t) < uint64_t(R) * R * R, SE_ERR_INVALID, "task out of range");
+    const FlowTask T = flow_decode(t, R);
+    if (kind) *kind = T.kind;
+    if (k) *k = T.k;
+    if (i) *i = T.i;
+    if (j) *j = T.j;
+    return SE_OK;
+}
+
+extern "C" se_status_t se_closure_set_mode(int mode) {
+    clear_error();
+    SE_REQUIRE(mode >= 0 && mode <= 2, SE_ERR_INVALID, "closure mode must be 0, 1 or 2");
+    g_closure_mode.store(mode);
+    return SE_OK;
 }
 
 extern "C" int se_closure_launch_count(int C) {

@@ -61,6 +61,7 @@ struct alignas(64) Req {
     const int64_t* offsets;      // V + 1 CSR offsets, or null when every ballot has exactly C ids
     float* pos;                  // [V][Cq]
     uint64_t* done_host;         // host-mapped completion word of this slot
+    uint32_t* tally_host;        // host-mapped: the generation, once the TALLY phase is done
     uint32_t* flags;             // [0] ballot error (2 range, 3 repeat), [1] 16-bit lane overflow
     int64_t V;
     uint32_t gen;
@@ -72,7 +73,13 @@ struct EngineHeader {
     uint32_t stop;
     uint32_t slot_hi;
     uint32_t retire;  // raised by the first CTA to time out idle: the whole grid leaves together
+    // Profile: per task kind, CTA-nanoseconds busy and tasks run; CTA-nanoseconds spent
+    // looking for work. Kinds: POS, TALLY, SMALL, PIVOT, PANELS, REM, FIN, PLACE.
+    unsigned long long busy_ns[8];
+    unsigned long long tasks[8];
+    unsigned long long search_ns;
 };
+constexpr int kKindCount = 8;
 
 __host__ __device__ inline int phases_of(int R) { return R == 1 ? 3 : 3 * R + 4; }
 
@@ -383,6 +390,7 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
     uint32_t par_a = 0, par_b = 0, tpar = 0;
 
     for (;;) {
+        uint64_t t_task = 0;
         if (threadIdx.x == 0) {
             uint32_t got = kNoSlot;
             uint64_t t0 = global_ns();
@@ -425,6 +433,8 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                 }
             }
             s_slot = got;
+            t_task = global_ns();
+            atomicAdd(&hdr->search_ns, (unsigned long long)(t_task - t0));
             if (got != kNoSlot) {
                 // The slot's descriptor may have been rewritten since this SM last read it:
                 // copy it through L2.
@@ -498,11 +508,19 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
+            const int kind = f == 0 ? 0 : f == 1 ? 1 : R == 1 ? 2 : (f - 2 < 3 * R ? 3 + (f - 2) % 3 : (f - 2 == 3 * R ? 6 : 7));
+            atomicAdd(&hdr->busy_ns[kind], (unsigned long long)(global_ns() - t_task));
+            atomicAdd(&hdr->tasks[kind], 1ull);
             if (!ok) {
                 atomicCAS(&hdr->err, 0u, 1u);
             } else {
                 fence_proxy_async_global();
                 const uint32_t prev = atomicAdd(&dones[size_t(s) * kMaxPhases + f], 1u);
+                if (f == 1 && prev + 1 == phase_size(R, Q.V, f)) {
+                    // The ballot places are no longer needed: tell the host it may reuse them.
+                    __threadfence_system();
+                    asm volatile("st.release.sys.u32 [%0], %1;" ::"l"(Q.tally_host), "r"(Q.gen) : "memory");
+                }
                 if (last && prev + 1 == phase_size(R, Q.V, f)) {
                     uint32_t status = 0;
                     const uint32_t ballot_err = __ldcg(Q.flags);
@@ -532,6 +550,9 @@ struct Engine {
     uint32_t* dones = nullptr;
     uint64_t* done_host = nullptr;  // host-mapped
     uint64_t* done_dev = nullptr;   // its device address
+    uint32_t* tally_host = nullptr; // host-mapped: per slot, generation whose tally finished
+    uint32_t* tally_dev = nullptr;
+    std::vector<uint8_t> tally_reported;
     uint8_t* staging = nullptr;     // pinned, one region per slot: its H2D sources stay valid
                                     // until the slot is reused, i.e. long after the copies ran
     std::vector<uint32_t> gen;
@@ -632,6 +653,7 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
         set_error("%s failed: %s", what, cudaGetErrorString(err));
         if (E.done_host) cudaFreeHost(E.done_host);
         if (E.staging) cudaFreeHost(E.staging);
+        if (E.tally_host) cudaFreeHost(E.tally_host);
         if (E.stream) cudaStreamDestroy(E.stream);
         if (E.finished) cudaEventDestroy(E.finished);
         delete h;
@@ -643,6 +665,12 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
     std::memset(E.done_host, 0, sizeof(uint64_t) * size_t(max_slots));
     if ((err = cudaHostAlloc(&E.staging, kStagingPerSlot * size_t(max_slots), cudaHostAllocDefault)) != cudaSuccess)
         return fail(err, "cudaHostAlloc");
+    if ((err = cudaHostAlloc(&E.tally_host, sizeof(uint32_t) * size_t(max_slots), cudaHostAllocMapped)) != cudaSuccess)
+        return fail(err, "cudaHostAlloc");
+    std::memset(E.tally_host, 0, sizeof(uint32_t) * size_t(max_slots));
+    if ((err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&E.tally_dev), E.tally_host, 0)) != cudaSuccess)
+        return fail(err, "cudaHostGetDevicePointer");
+    E.tally_reported.assign(max_slots, 0);
     if ((err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&E.done_dev), E.done_host, 0)) != cudaSuccess)
         return fail(err, "cudaHostGetDevicePointer");
     if ((err = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -663,14 +691,13 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
 
 namespace {
 struct ScratchLayout {
-    int64_t Cq, flags, pos, S, AT, dT, total;
+    int64_t Cq, flags, S, AT, dT, total;
 };
-ScratchLayout scratch_layout(int64_t V, int C) {
+ScratchLayout scratch_layout(int C) {
     ScratchLayout L;
     L.Cq = round_up(C, kT);
     L.flags = 0;
-    L.pos = 256;
-    L.S = round_up(L.pos + std::max<int64_t>(V, 1) * L.Cq * 4, 256);
+    L.S = 256;
     L.AT = round_up(L.S + L.Cq * L.Cq * 2, 256);
     L.dT = round_up(L.AT + int64_t(kT) * L.Cq * 4, 256);
     L.total = L.dT + int64_t(kT) * kT * 4;
@@ -680,7 +707,12 @@ ScratchLayout scratch_layout(int64_t V, int C) {
 
 extern "C" int64_t se_engine_request_scratch_bytes(int64_t V, int C) {
     if (V < 1 || C < 1) return -1;
-    return scratch_layout(V, C).total;
+    return scratch_layout(C).total;
+}
+
+extern "C" int64_t se_engine_request_positions_bytes(int64_t V, int C) {
+    if (V < 1 || C < 1) return -1;
+    return V * round_up(C, kT) * 4;
 }
 
 extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, void* stream_, int* slot_out,
@@ -695,9 +727,14 @@ extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, 
     SE_REQUIRE(V >= 1 && V < (int64_t(1) << 24), SE_ERR_INVALID, "the engine serves 1 to 2^24 - 1 ballots");
     SE_REQUIRE(rq->d_ids && rq->d_prefs && rq->d_out && rq->d_wins && rq->d_ranking, SE_ERR_INVALID,
                "a request needs ballots, preference, output, wins and ranking buffers");
-    const ScratchLayout L = scratch_layout(V, C);
+    const ScratchLayout L = scratch_layout(C);
     SE_REQUIRE(rq->d_scratch && rq->scratch_bytes >= L.total, SE_ERR_WORKSPACE,
                "request scratch of %lld bytes is below %lld", (long long)rq->scratch_bytes, (long long)L.total);
+    const int64_t pos_need = V * L.Cq * 4;
+    SE_REQUIRE(rq->d_positions && rq->positions_bytes >= pos_need, SE_ERR_WORKSPACE,
+               "ballot-place buffer of %lld bytes is below %lld", (long long)rq->positions_bytes, (long long)pos_need);
+    SE_REQUIRE((reinterpret_cast<uintptr_t>(rq->d_positions) & 255) == 0, SE_ERR_INVALID,
+               "the ballot-place buffer must be 256-byte aligned");
     SE_REQUIRE((reinterpret_cast<uintptr_t>(rq->d_scratch) & 255) == 0, SE_ERR_INVALID,
                "scratch must be 256-byte aligned");
     int slot = -1;
@@ -734,7 +771,7 @@ extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, 
         if (se_status_t st = make_map(&e.mapAT, e.AT, uint64_t(L.Cq), kT, uint64_t(L.Cq) * 4, kT, kKC)) return st;
         if (se_status_t st = make_map(&e.mapDT, e.dT, kT, kT, kT * 4, kT, kKC)) return st;
     }
-    q.pos = reinterpret_cast<float*>(sc + L.pos);
+    q.pos = static_cast<float*>(rq->d_positions);
     if (se_status_t st = make_map(&q.mapPos, q.pos, uint64_t(L.Cq), uint64_t(V), uint64_t(L.Cq) * 4, 64, kVC))
         return st;
     q.ids = rq->d_ids;
@@ -743,6 +780,8 @@ extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, 
     q.V = V;
     const uint32_t gen = ++E.gen[slot];
     q.done_host = E.done_dev + slot;
+    q.tally_host = E.tally_dev + slot;
+    E.tally_reported[slot] = 0;
     q.gen = gen;
     q.active = 0;
     E.done_host[slot] = 0;
@@ -796,13 +835,49 @@ extern "C" se_status_t se_engine_poll(se_engine_t* h, int* slots_out, uint32_t* 
     return ensure_running(E);
 }
 
-extern "C" se_status_t se_engine_stats(se_engine_t* h, int64_t* launches, int* grid, int* in_flight) {
+extern "C" se_status_t se_engine_poll_tallied(se_engine_t* h, int* slots_out, int max, int* n_out) {
+    clear_error();
+    SE_REQUIRE(h && n_out, SE_ERR_INVALID, "null argument");
+    Engine& E = h->e;
+    std::lock_guard<std::mutex> lock(E.mu);
+    int n = 0;
+    for (int s = 0; s < E.max_slots && n < max; ++s) {
+        if (!E.busy[s] || E.tally_reported[s]) continue;
+        if (reinterpret_cast<volatile uint32_t*>(E.tally_host)[s] == E.gen[s]) {
+            E.tally_reported[s] = 1;
+            if (slots_out) slots_out[n] = s;
+            ++n;
+        }
+    }
+    *n_out = n;
+    return SE_OK;
+}
+
+extern "C" se_status_t se_engine_stats(se_engine_t* h, int64_t* launches, int* grid, int* in_flight,
+                                       double* busy_ms, int64_t* tasks, double* search_ms) {
     clear_error();
     SE_REQUIRE(h != nullptr, SE_ERR_INVALID, "null engine");
-    std::lock_guard<std::mutex> lock(h->e.mu);
-    if (launches) *launches = h->e.launches;
-    if (grid) *grid = h->e.grid;
-    if (in_flight) *in_flight = h->e.in_flight;
+    Engine& E = h->e;
+    std::lock_guard<std::mutex> lock(E.mu);
+    if (launches) *launches = E.launches;
+    if (grid) *grid = E.grid;
+    if (in_flight) *in_flight = E.in_flight;
+    if (busy_ms || tasks || search_ms) {
+        // The counters are read while the kernel may run: a snapshot, not a barrier.
+        EngineHeader hd;
+        cudaStream_t side;
+        SE_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        cudaError_t e1 = cudaMemcpyAsync(&hd, E.hdr, sizeof(hd), cudaMemcpyDeviceToHost, side);
+        cudaError_t e2 = cudaStreamSynchronize(side);
+        cudaStreamDestroy(side);
+        SE_CUDA_TRY(e1);
+        SE_CUDA_TRY(e2);
+        for (int k = 0; k < kKindCount; ++k) {
+            if (busy_ms) busy_ms[k] = double(hd.busy_ns[k]) * 1e-6;
+            if (tasks) tasks[k] = int64_t(hd.tasks[k]);
+        }
+        if (search_ms) *search_ms = double(hd.search_ns) * 1e-6;
+    }
     return SE_OK;
 }
 
@@ -837,6 +912,7 @@ extern "C" se_status_t se_engine_destroy(se_engine_t* h) {
     Engine& E = h->e;
     if (E.done_host) cudaFreeHost(E.done_host);
     if (E.staging) cudaFreeHost(E.staging);
+    if (E.tally_host) cudaFreeHost(E.tally_host);
     if (E.stream) cudaStreamDestroy(E.stream);
     if (E.finished) cudaEventDestroy(E.finished);
     delete h;

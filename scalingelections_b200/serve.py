@@ -75,13 +75,16 @@ class Arena:
 
 
 def request_bytes(V: int, C: int) -> dict:
-    """Device bytes of one request's buffers, each ALIGN-aligned."""
+    """Device bytes of one request's buffers, each ALIGN-aligned. "positions" (the ballot
+    places, usually the largest part) is a separate block, released when the tally is done."""
 
     def al(x):
         return (int(x) + ALIGN - 1) // ALIGN * ALIGN
 
-    scratch = _lib.lib().se_engine_request_scratch_bytes(int(V), int(C))
-    if scratch < 0:
+    L = _lib.lib()
+    scratch = L.se_engine_request_scratch_bytes(int(V), int(C))
+    positions = L.se_engine_request_positions_bytes(int(V), int(C))
+    if scratch < 0 or positions < 0:
         raise ValueError("invalid request shape")
     parts = {
         "prefs": al(4 * C * C),
@@ -90,7 +93,9 @@ def request_bytes(V: int, C: int) -> dict:
         "ranking": al(4 * C),
         "scratch": al(scratch),
     }
-    parts["total"] = sum(parts.values())
+    parts["main"] = sum(parts.values())
+    parts["positions"] = al(positions)
+    parts["total"] = parts["main"] + parts["positions"]
     return parts
 
 
@@ -102,6 +107,8 @@ class Ticket:
     arrival: float
     offset: int = -1
     nbytes: int = 0
+    pos_offset: int = -1
+    pos_nbytes: int = 0
     slot: int = -1
     gen: int = 0
     admitted: float = 0.0
@@ -158,10 +165,15 @@ class Server:
         if lanes != 16:
             raise ValueError("the server handles up to 131070 ballots per request")
         parts = request_bytes(V, C)
-        off = self.arena.alloc(parts["total"])
+        off = self.arena.alloc(parts["main"])
         if off is None:
             return False
-        ticket.offset, ticket.nbytes = off, parts["total"]
+        pos_off = self.arena.alloc(parts["positions"])
+        if pos_off is None:
+            self.arena.free(off, parts["main"])
+            return False
+        ticket.offset, ticket.nbytes = off, parts["main"]
+        ticket.pos_offset, ticket.pos_nbytes = pos_off, parts["positions"]
         pos = off
         ptrs = {}
         for name in ("prefs", "out", "wins", "ranking", "scratch"):
@@ -169,7 +181,8 @@ class Server:
             ticket.views[name] = (pos, parts[name])
             pos += parts[name]
         rq = _lib.Request(ballots.data_ptr(), None, V, C, offset, ptrs["prefs"], ptrs["out"], ptrs["wins"],
-                          ptrs["ranking"], ptrs["scratch"], parts["scratch"])
+                          ptrs["ranking"], ptrs["scratch"], parts["scratch"], self.base_ptr + pos_off,
+                          parts["positions"])
         slot, gen = ctypes.c_int(), ctypes.c_uint32()
         with torch.cuda.device(self.device):
             check(self.L.se_engine_submit(self.engine, ctypes.byref(rq), self.stream.cuda_stream, ctypes.byref(slot),
@@ -181,8 +194,32 @@ class Server:
         return True
 
     # -- completion ------------------------------------------------------------------------
+    def admit(self, pending: list[Ticket], ballots_of, now: float, max_bypass_s: float = 0.25) -> int:
+        """Admits pending requests in arrival order. A request that does not fit yet may be
+        passed by later ones that do, unless the oldest has waited longer than max_bypass_s:
+        then nothing passes it (no starvation). Returns how many were admitted."""
+        admitted = 0
+        strict = bool(pending) and now - pending[0].arrival > max_bypass_s
+        x = 0
+        while x < len(pending):
+            t = pending[x]
+            if self.try_submit(t, ballots_of(t)):
+                pending.pop(x)
+                admitted += 1
+                continue
+            if strict or len(self.by_slot) >= self.max_slots:
+                break
+            x += 1
+        return admitted
+
     def poll(self) -> list[Ticket]:
         n = ctypes.c_int(0)
+        check(self.L.se_engine_poll_tallied(self.engine, self._poll_slots, self.max_slots, ctypes.byref(n)))
+        for x in range(n.value):
+            t = self.by_slot.get(self._poll_slots[x])
+            if t is not None and t.pos_offset >= 0:
+                self.arena.free(t.pos_offset, t.pos_nbytes)
+                t.pos_offset = -1
         check(self.L.se_engine_poll(self.engine, self._poll_slots, self._poll_status, self.max_slots, ctypes.byref(n)))
         now = time.perf_counter()
         done = []
@@ -206,16 +243,31 @@ class Server:
                 S = self._view(t, "out", (t.C, t.C), torch.int32)
                 t.strongest_paths = S.cpu().numpy().view(np.uint32)
         self.arena.free(t.offset, t.nbytes)
+        if t.pos_offset >= 0:
+            self.arena.free(t.pos_offset, t.pos_nbytes)
+            t.pos_offset = -1
         t._ballots = None
 
     @property
     def in_flight(self) -> int:
         return len(self.by_slot)
 
-    def stats(self) -> dict:
+    KINDS = ("positions", "tally", "small", "pivot", "panels", "remainder", "output_wins", "ranking")
+
+    def stats(self, profile: bool = False) -> dict:
         launches, grid, fl = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
-        check(self.L.se_engine_stats(self.engine, ctypes.byref(launches), ctypes.byref(grid), ctypes.byref(fl)))
-        return {"engine_launches": launches.value, "grid": grid.value, "in_flight": fl.value}
+        busy = (ctypes.c_double * 8)()
+        tasks = (ctypes.c_int64 * 8)()
+        search = ctypes.c_double()
+        check(self.L.se_engine_stats(self.engine, ctypes.byref(launches), ctypes.byref(grid), ctypes.byref(fl),
+                                     busy if profile else None, tasks if profile else None,
+                                     ctypes.byref(search) if profile else None))
+        out = {"engine_launches": launches.value, "grid": grid.value, "in_flight": fl.value}
+        if profile:
+            out["busy_cta_ms"] = {k: busy[i] for i, k in enumerate(self.KINDS)}
+            out["tasks"] = {k: tasks[i] for i, k in enumerate(self.KINDS)}
+            out["search_cta_ms"] = search.value
+        return out
 
     def close(self) -> None:
         if self.engine:
@@ -263,8 +315,8 @@ def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], 
             V, C, _ = requests[i]
             pending.append(Ticket(rid=i, V=V, C=C, arrival=t0 + arrival_times[i], keep_paths=keep_paths))
             nxt += 1
-        while pending and server.try_submit(pending[0], requests[pending[0].rid][2]):
-            pending.pop(0)
+        if pending:
+            server.admit(pending, lambda t: requests[t.rid][2], time.perf_counter())
         finished = server.poll()
         if finished or not server.in_flight:
             last_progress = time.perf_counter()

@@ -120,3 +120,19 @@ def test_shifted_16_bit_lanes_for_large_counts(orc):
     assert orc.defeats(P).max() > 65535
     assert np.array_equal(gpu_closure(P, LANES_AUTO), S_ref)
     assert np.array_equal(gpu_closure(P, LANES_U32), S_ref)
+
+
+@pytest.mark.parametrize("C", [129, 300, 640, 1000, 1700])
+def test_dataflow_equals_round_by_round(orc, C):
+    """The barrier-free dataflow closure and the round-by-round launches give the same
+    matrix (and the oracle's), in both lane modes."""
+    rng = np.random.default_rng(C + 1)
+    P = rng.integers(0, 5000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    S_ref = orc.strongest_paths(P, "blocked", tile=32)
+    try:
+        for mode in (1, 2):
+            api.set_closure_mode(mode)
+            for lanes in (LANES_U16, LANES_U32):
+                assert np.array_equal(gpu_closure(P, lanes), S_ref), (mode, lanes)
+    finally:
+        api.set_closure_mode(0)
