@@ -50,8 +50,8 @@ def parse():
     ap.add_argument("--phi", type=float, default=0.8)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
-    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2],
-                    help="0: dataflow when the workspace allows, 1: round by round, 2: dataflow")
+    ap.add_argument("--closure-mode", type=int, default=1, choices=[1, 2],
+                    help="1: round by round (default), 2: dataflow")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -75,7 +75,7 @@ def config(args, world):
         "voters": args.voters,
         "phi": args.phi,
         "lanes": f"u{args.lanes}" if args.lanes else "auto",
-        "closure_mode": ["auto (dataflow)", "round by round", "dataflow"][args.closure_mode],
+        "closure_mode": {1: "round by round", 2: "dataflow"}[args.closure_mode],
         "tile": 128,
         "parallelism": f"replicas{world}" if world > 1 else "single",
         "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
@@ -237,7 +237,7 @@ def run_ours(args, world, rank, local_rank):
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
     api.set_closure_mode(args.closure_mode)
-    need = api.closure_workspace_bytes(C, lanes)
+    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode == 2)
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()
@@ -419,6 +419,14 @@ def run_batch(args, world, rank, local_rank):
         torch.cuda.synchronize()
     b.check()
     ms = e0.elapsed_time(e1) / args.steps
+    # One more run, timed alone, for the engine profile (the counters reset every run).
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    b.launch_graph()
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    prof = b.profile()
+    prof["run_ms"] = pe0.elapsed_time(pe1)
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -461,6 +469,7 @@ def run_batch(args, world, rank, local_rank):
             "speedup_vs_loop": (len(specs) / (ms * 1e-3)) / (len(specs) / loop_s),
             "bit_identical_to_loop": identical,
             "input_prep_seconds": prep_s,
+            "engine_profile": prof,
             "autotune": None if tuned is None else {
                 "seconds": tune_s, "order": order, "ctas_per_sm": ctas,
                 "buckets": {k: {"C": v["range"], "lanes": v["lanes"], "ctas_per_sm": v["ctas_per_sm"]}
@@ -512,6 +521,7 @@ def run_serve(args, world, rank, local_rank):
         "tasks": {k: p1["tasks"][k] - p0["tasks"][k] for k in p1["tasks"]},
         "search_cta_ms": p1["search_cta_ms"] - p0["search_cta_ms"],
         "grid_cta_ms": p1["grid"] * makespan * 1e3,
+        "host": dict(getattr(server, "last_host_stats", {})),
     }
     rng = np.random.default_rng(args.seed + 17)
     loads = []

@@ -93,10 +93,10 @@ SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, 
                                        int64_t work_bytes, void* stream, double* phase_ms, int* launches);
 
 /* Workspace for the dataflow form of the closure (no barrier between pivot rounds): one
- * persistent launch that overlaps each round's panels and the start of the next round with
- * the end of the current one. se_closure uses it whenever d_work is at least this large (and
- * C > 128); with the smaller se_closure_workspace_bytes() it runs round by round. Results are
- * identical either way. */
+ * persistent launch whose task order runs the next round's pivot and panels ahead of the
+ * current round's bulk. se_closure runs it only after se_closure_set_mode(2). Results are
+ * identical to the default round-by-round form, which is faster on B200 at every size
+ * measured (hardware block scheduling costs less than the persistent grid's claim and poll). */
 SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
 
 /* Task t (< R^3) of the dataflow closure's fixed order for R = ceil(C / 128) pivot blocks:
@@ -104,8 +104,8 @@ SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
  * Host-only (no GPU needed): lets tests check the order against the dependency rules. */
 SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, int* i, int* j);
 
-/* Process-wide choice for se_closure: 0 = dataflow when the workspace allows (default),
- * 1 = always round by round, 2 = dataflow only. For benchmarking and tests. */
+/* Process-wide choice for se_closure: 0 or 1 = round by round (default), 2 = dataflow (needs
+ * se_closure_workspace_bytes_flow() of workspace). For benchmarking and tests. */
 SE_API se_status_t se_closure_set_mode(int mode);
 
 /* Number of kernels one se_closure call launches for C candidates (with lane_bits 16 or 32;
@@ -181,6 +181,11 @@ SE_API se_status_t se_batch_graph_build(se_batch_plan_t* plan);
 SE_API se_status_t se_batch_graph_launch(const se_batch_plan_t* plan, void* stream);
 SE_API se_status_t se_batch_release(se_batch_plan_t* plan);
 SE_API se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream);
+/* Profile of the last run (synchronises `stream`): per task kind (small election, pivot,
+ * row panel, column panel, remainder) CTA-milliseconds busy and tasks run, and the
+ * CTA-milliseconds spent waiting for dependencies. Any pointer may be NULL. */
+SE_API se_status_t se_batch_profile(const se_batch_plan_t* plan, double* busy_ms, int64_t* tasks,
+                                    double* wait_ms, void* stream);
 /* Number of tasks in queue 0 (16-bit lanes) or 1 (32-bit lanes) of a prepared plan. */
 SE_API int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue);
 

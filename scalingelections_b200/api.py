@@ -78,8 +78,8 @@ def _check_matrix(t: torch.Tensor, name: str) -> tuple[int, int]:
 # ------------------------------------------------------------------------------------------
 # Device-resident entry points
 # ------------------------------------------------------------------------------------------
-def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, dataflow: bool = True) -> int:
-    """Workspace bytes of the closure; dataflow=True sizes it for the barrier-free form."""
+def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, dataflow: bool = False) -> int:
+    """Workspace bytes of the closure; dataflow=True sizes it for the barrier-free form (mode 2)."""
     L = _lib.lib()
     fn = L.se_closure_workspace_bytes_flow if dataflow else L.se_closure_workspace_bytes
     n = fn(int(num_candidates), int(lanes), 0)
@@ -88,9 +88,14 @@ def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, datafl
     return n
 
 
+_closure_mode = 1
+
+
 def set_closure_mode(mode: int) -> None:
-    """0: dataflow when the workspace allows (default); 1: round by round; 2: dataflow only."""
+    """0 or 1: round by round (default); 2: the dataflow form (same results)."""
+    global _closure_mode
     check(_lib.lib().se_closure_set_mode(int(mode)))
+    _closure_mode = int(mode)
 
 
 def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO, out: torch.Tensor | None = None,
@@ -108,8 +113,8 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         raise ValueError("out has the wrong shape")
     if C == 0:
         return out
-    need = closure_workspace_bytes(C, lanes)
-    if workspace is None or workspace.numel() * workspace.element_size() < closure_workspace_bytes(C, lanes, False):
+    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode == 2)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = _workspace(need, preferences.device)
     have = workspace.numel() * workspace.element_size()
     with torch.cuda.device(preferences.device):

@@ -110,6 +110,20 @@ class BatchedElections:
         with torch.cuda.device(self.device):
             check(_lib.lib().se_batch_graph_launch(ctypes.byref(self.plan), torch.cuda.current_stream().cuda_stream))
 
+    KINDS = ("small", "pivot", "row_panel", "col_panel", "remainder")
+
+    def profile(self) -> dict:
+        """CTA-milliseconds busy per task kind, tasks run and CTA-milliseconds spent waiting on
+        dependencies, accumulated over the runs since the plan's last reset (each run resets)."""
+        busy = (ctypes.c_double * 5)()
+        tasks = (ctypes.c_int64 * 5)()
+        wait = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().se_batch_profile(ctypes.byref(self.plan), busy, tasks, ctypes.byref(wait),
+                                              torch.cuda.current_stream().cuda_stream))
+        return {"busy_cta_ms": dict(zip(self.KINDS, busy)), "tasks": dict(zip(self.KINDS, tasks)),
+                "wait_cta_ms": wait.value}
+
     def check(self) -> None:
         """Raise if a kernel of the last run reported an error (synchronises the stream)."""
         with torch.cuda.device(self.device):

@@ -47,6 +47,11 @@ struct Header {
     uint32_t err;
     uint32_t abort;
     uint32_t head[2];  // queue heads of the u16 and u32 persistent launches
+    // Profile: per task kind (SMALL, PIVOT, ROW, COL, REM) CTA-nanoseconds busy and tasks run;
+    // CTA-nanoseconds waiting for dependencies.
+    unsigned long long busy_ns[5];
+    unsigned long long tasks[5];
+    unsigned long long wait_ns;
 };
 
 template <int LB>
@@ -82,9 +87,11 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
                 const Elec& E = elecs[e];
                 const uint32_t R = uint32_t(E.R);
                 bool ok = true;
+                const uint64_t w0 = global_ns();
                 if (type == kPivot && k > 0) ok = wait_counter(&E.counters[2 * R + k - 1], (R - 1) * (R - 1), &hdr->abort);
                 else if (type == kRow || type == kCol) ok = wait_counter(&E.counters[k], 1u, &hdr->abort);
                 else if (type == kRem) ok = wait_counter(&E.counters[R + k], 2u * (R - 1), &hdr->abort);
+                atomicAdd(&hdr->wait_ns, (unsigned long long)(global_ns() - w0));
                 if (!ok) {
                     raise_device_error(&hdr->err, kErrDepTimeout);
                     atomicExch(&hdr->abort, 1u);
@@ -100,6 +107,7 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         const uint32_t i = uint32_t(t >> 12) & 0xFFFu, j = uint32_t(t) & 0xFFFu;
         const Elec& E = elecs[e];
         bool ok = true;
+        const uint64_t tb = threadIdx.x == 0 ? global_ns() : 0;
         if (type == kSmall) {
             run_small<LB>(E, smem, rowbuf, colbuf, s_wins, &hdr->err);
         } else if (type == kPivot) {
@@ -118,6 +126,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
+            atomicAdd(&hdr->busy_ns[type], (unsigned long long)(global_ns() - tb));
+            atomicAdd(&hdr->tasks[type], 1ull);
             if (!ok) {
                 raise_device_error(&hdr->err, kErrTimeout);
                 atomicExch(&hdr->abort, 1u);
@@ -631,6 +641,23 @@ extern "C" se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream)
                "run with 16-bit lanes");
     SE_REQUIRE(h.err == 0, SE_ERR_DEVICE, "batched closure reported device error %u (%s)", h.err,
                h.err == kErrDepTimeout ? "dependency wait timed out" : "TMA wait timed out");
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_profile(const se_batch_plan_t* plan, double* busy_ms, int64_t* tasks, double* wait_ms,
+                                        void* stream) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    Header h;
+    SE_CUDA_TRY(cudaMemcpyAsync(&h, P.work, sizeof(h), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    SE_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    for (int k = 0; k < 5; ++k) {
+        if (busy_ms) busy_ms[k] = double(h.busy_ns[k]) * 1e-6;
+        if (tasks) tasks[k] = int64_t(h.tasks[k]);
+    }
+    if (wait_ms) *wait_ms = double(h.wait_ns) * 1e-6;
     return SE_OK;
 }
 

@@ -539,9 +539,10 @@ layout plan(int C, int lane_bits) {
     return L;
 }
 
-// 0: dataflow when the workspace has room for it, else round by round; 1: always round by
-// round; 2: dataflow only (too small a workspace is an error).
-std::atomic<int> g_closure_mode{0};
+// 0 or 1: round by round (the default: on B200 hardware block scheduling of one launch per
+// phase beats the persistent grid's claim-and-poll overhead at every size measured);
+// 2: dataflow, which then needs se_closure_workspace_bytes_flow() of workspace.
+std::atomic<int> g_closure_mode{1};
 
 template <int LB> se_status_t set_smem_limits() {
     static se_status_t st = [] {
@@ -781,7 +782,7 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
         if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
     const int mode = g_closure_mode.load();
-    const bool flow = mode != 1 && work_bytes >= P.flow_total && P.Cp > kT;
+    const bool flow = mode == 2 && P.Cp > kT;
     SE_REQUIRE(mode != 2 || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
                "the dataflow closure needs a workspace of %lld bytes", (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))

@@ -118,6 +118,7 @@ class Ticket:
     strongest_paths: np.ndarray | None = None
     keep_paths: bool = False
     views: dict = field(default_factory=dict)
+    parts: dict | None = None  # request_bytes(V, C), computed once
 
     @property
     def latency(self) -> float:
@@ -164,7 +165,11 @@ class Server:
         lanes, offset = lanes_for_voters(V)
         if lanes != 16:
             raise ValueError("the server handles up to 131070 ballots per request")
-        parts = request_bytes(V, C)
+        if ticket.parts is None:
+            ticket.parts = request_bytes(V, C)
+        parts = ticket.parts
+        if parts["total"] > self.arena.free_bytes:
+            return False
         off = self.arena.alloc(parts["main"])
         if off is None:
             return False
@@ -201,13 +206,20 @@ class Server:
         admitted = 0
         strict = bool(pending) and now - pending[0].arrival > max_bypass_s
         x = 0
+        smallest_failed = None
         while x < len(pending):
             t = pending[x]
-            if self.try_submit(t, ballots_of(t)):
-                pending.pop(x)
-                admitted += 1
-                continue
-            if strict or len(self.by_slot) >= self.max_slots:
+            if t.parts is None:
+                t.parts = request_bytes(t.V, t.C)
+            # A request at least as large as one that just failed cannot fit either.
+            if smallest_failed is None or t.parts["total"] < smallest_failed:
+                if self.try_submit(t, ballots_of(t)):
+                    pending.pop(x)
+                    admitted += 1
+                    continue
+                smallest_failed = t.parts["total"] if smallest_failed is None else min(smallest_failed,
+                                                                                       t.parts["total"])
+            if strict or len(self.by_slot) >= self.max_slots or self.arena.free_bytes < (1 << 20):
                 break
             x += 1
         return admitted
@@ -305,7 +317,9 @@ def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], 
     t0 = time.perf_counter()
     n = len(requests)
     last_progress = t0
+    host = {"admit_s": 0.0, "poll_s": 0.0, "iterations": 0}
     while len(done) < n:
+        host["iterations"] += 1
         now_abs = time.perf_counter()
         if server.in_flight and now_abs - last_progress > stall_s:
             raise RuntimeError(f"no request finished for {stall_s:.0f} s ({server.in_flight} in flight)")
@@ -316,13 +330,18 @@ def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], 
             pending.append(Ticket(rid=i, V=V, C=C, arrival=t0 + arrival_times[i], keep_paths=keep_paths))
             nxt += 1
         if pending:
-            server.admit(pending, lambda t: requests[t.rid][2], time.perf_counter())
+            ta = time.perf_counter()
+            server.admit(pending, lambda t: requests[t.rid][2], ta)
+            host["admit_s"] += time.perf_counter() - ta
+        tp = time.perf_counter()
         finished = server.poll()
+        host["poll_s"] += time.perf_counter() - tp
         if finished or not server.in_flight:
             last_progress = time.perf_counter()
         done.extend(finished)
         if not pending and nxt < n and server.in_flight == 0:
             time.sleep(max(0.0, min(0.001, arrival_times[order[nxt]] - (time.perf_counter() - t0))))
+    server.last_host_stats = host
     return done, time.perf_counter() - t0
 
 

@@ -135,4 +135,4 @@ def test_dataflow_equals_round_by_round(orc, C):
             for lanes in (LANES_U16, LANES_U32):
                 assert np.array_equal(gpu_closure(P, lanes), S_ref), (mode, lanes)
     finally:
-        api.set_closure_mode(0)
+        api.set_closure_mode(1)
