@@ -272,6 +272,25 @@ SE_API se_status_t se_tally_enqueue(const int32_t* d_ids, const int64_t* d_offse
                                     uint32_t* d_out, int64_t ld_out, void* d_work,
                                     int64_t work_bytes, void* stream);
 
+/* Tally of streamed or packed ballots, e.g. a ballot file read in chunks (no reference
+ * counterpart: the reference only tallies in-memory ballots, scaling_elections.py:51-88).
+ *   id_bytes   1, 2 or 4: ids are uint8, uint16 or int32 (d_ids aligned to that width).
+ *   d_offsets  V + 1 offsets: ballot v is d_ids[d_offsets[v] - id_base .. d_offsets[v+1] - id_base),
+ *              so a slice of a larger CSR index works with id_base = its first offset; or NULL:
+ *              every ballot lists exactly C ids (ballot v starts at v * C).
+ *   flags      SE_TALLY_ACCUMULATE adds this call's counts to d_out (the diagonal is left
+ *              as it is), so a tally over chunks equals the tally of all ballots at once;
+ *              SE_TALLY_NO_SYNC returns without synchronising, leaving the error code in the
+ *              first 4 bytes of d_work as se_tally_enqueue does; SE_TALLY_KEEP_ERROR does not
+ *              reset that code first, so a sequence of calls reports the first error of any.
+ * Workspace: se_tally_workspace_bytes(V, C). */
+#define SE_TALLY_ACCUMULATE 1u
+#define SE_TALLY_NO_SYNC 2u
+#define SE_TALLY_KEEP_ERROR 4u
+SE_API se_status_t se_tally_ex(const void* d_ids, int id_bytes, const int64_t* d_offsets, int64_t id_base,
+                               int64_t V, int C, unsigned flags, uint32_t* d_out, int64_t ld_out,
+                               void* d_work, int64_t work_bytes, void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Ranking. Replaces get_winner_and_ranking (scaling_elections.py:274-296).
  *

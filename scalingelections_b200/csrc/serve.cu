@@ -136,6 +136,65 @@ __device__ bool try_claim(uint64_t* claims, const uint32_t* dones, uint32_t gen,
     return false;
 }
 
+// Read-only look at slot state: true when the front phase of generation gen has an unclaimed
+// task and its predecessor is complete. A front phase with nothing left to claim is moved on
+// here (the same harmless CAS try_claim makes), so the next look sees the following phase.
+__device__ bool claimable(uint64_t* claims, const uint32_t* dones, uint32_t gen, int R, int64_t V) {
+    const uint64_t fr = ld_acquire64(&claims[0]);
+    if (uint32_t(fr >> 32) != gen) return false;
+    const int f = int(uint32_t(fr));
+    if (f >= phases_of(R)) return false;
+    if (f > 0 && ld_acquire(&dones[f - 1]) < phase_size(R, V, f - 1)) return false;
+    const uint64_t c = ld_acquire64(&claims[1 + f]);
+    if (uint32_t(c >> 32) != gen) return false;
+    if (uint32_t(c) < phase_size(R, V, f)) return true;
+    atomicCAS(reinterpret_cast<unsigned long long*>(&claims[0]), (unsigned long long)fr, (unsigned long long)(fr + 1));
+    return false;
+}
+
+// Warp-wide search for a task: the 32 lanes look at 32 slots at once (lowest slot first), so a
+// step costs a few L2 round trips however many requests are in flight; the candidates are then
+// claimed one at a time in slot order. Returns the slot or kNoSlot; any_active reports whether
+// any slot below hi holds a request.
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+
+__device__ uint32_t warp_find_task(Req* slots, uint64_t* claims, const uint32_t* dones, uint32_t hi, bool& any_active,
+                                   int& f_out, uint32_t& t_out) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s0 = 0; s0 < hi; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        bool active = false, cand = false;
+        uint32_t gen = 0;
+        int R = 0;
+        int64_t V = 0;
+        if (s < hi && ld_acquire(&slots[s].active)) {
+            active = true;
+            gen = __ldcg(&slots[s].gen);
+            R = __ldcg(&slots[s].e.R);
+            V = __ldcg(&slots[s].V);
+            cand = claimable(claims + size_t(s) * (kMaxPhases + 1), dones + size_t(s) * kMaxPhases, gen, R, V);
+        }
+        if (__any_sync(0xffffffffu, active)) any_active = true;
+        uint32_t mask = __ballot_sync(0xffffffffu, cand);
+        while (mask) {
+            const int l = __ffs(mask) - 1;
+            int f = 0;
+            uint32_t t = 0;
+            int got = 0;
+            if (lane == l)
+                got = try_claim(claims + size_t(s) * (kMaxPhases + 1), dones + size_t(s) * kMaxPhases, gen, R, V, f, t);
+            got = __shfl_sync(0xffffffffu, got, l);
+            if (got) {
+                f_out = __shfl_sync(0xffffffffu, f, l);
+                t_out = __shfl_sync(0xffffffffu, t, l);
+                return s0 + l;
+            }
+            mask &= mask - 1;
+        }
+    }
+    return kNoSlot;
+}
+
 // Output (u32, shifted back, zero diagonal) and wins for the 128-block pair (I, J), I <= J.
 __device__ void run_fin(const Elec& E, int I, int J, uint8_t* smem) {
     uint16_t* tJI = reinterpret_cast<uint16_t*>(smem);  // [128][130]: S[J-block][I-block], padded
@@ -367,7 +426,6 @@ __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8
     return true;
 }
 
-constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 constexpr uint64_t kStallNs = 10000000000ull;  // 10 s without a claim while requests are active
 
 __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
@@ -391,56 +449,58 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
 
     for (;;) {
         uint64_t t_task = 0;
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {
             uint32_t got = kNoSlot;
-            uint64_t t0 = global_ns();
+            const uint64_t t0 = global_ns();
             while (got == kNoSlot) {
-                if (ld_acquire(&hdr->stop) || ld_acquire(&hdr->err) || ld_acquire(&hdr->retire)) break;
-                const uint32_t hi = ld_acquire(&hdr->slot_hi);
+                int stop = 0;
+                if (threadIdx.x == 0)
+                    stop = ld_acquire(&hdr->stop) || ld_acquire(&hdr->err) || ld_acquire(&hdr->retire);
+                if (__shfl_sync(0xffffffffu, stop, 0)) break;
+                uint32_t hi = threadIdx.x == 0 ? ld_acquire(&hdr->slot_hi) : 0u;
+                hi = __shfl_sync(0xffffffffu, hi, 0);
                 bool any_active = false;
-                for (uint32_t s = 0; s < hi && got == kNoSlot; ++s) {  // oldest slots first
-                    if (!ld_acquire(&slots[s].active)) continue;
-                    any_active = true;
-                    const uint32_t gen = __ldcg(&slots[s].gen);
-                    const int R = __ldcg(&slots[s].e.R);
-                    const int64_t V = __ldcg(&slots[s].V);
-                    int f;
-                    uint32_t t;
-                    if (try_claim(claims + size_t(s) * (kMaxPhases + 1), dones + size_t(s) * kMaxPhases, gen, R, V,
-                                  f, t)) {
-                        got = s;
-                        s_f = f;
-                        s_t = t;
-                    }
+                int f = 0;
+                uint32_t t = 0;
+                got = warp_find_task(slots, claims, dones, hi, any_active, f, t);
+                if (got != kNoSlot && threadIdx.x == 0) {
+                    s_f = f;
+                    s_t = t;
                 }
                 if (got == kNoSlot) {
                     // With no active request the CTA leaves after idle_ns (the host relaunches
                     // the engine for the next one). While requests are active but have nothing
                     // claimable (their current phase's last tasks are still running) it keeps
                     // looking, up to kStallNs without any claim, which no task comes close to.
-                    const uint64_t waited = global_ns() - t0;
-                    if (!any_active && waited > idle_ns) {
-                        // Retire the whole grid, never part of it: a partial grid would keep
-                        // serving the next request with a fraction of the SMs.
-                        atomicExch(&hdr->retire, 1u);
-                        break;
+                    // Lane 0 decides for the warp.
+                    int leave = 0;
+                    if (threadIdx.x == 0) {
+                        const uint64_t waited = global_ns() - t0;
+                        if (!any_active && waited > idle_ns) {
+                            // Retire the whole grid, never part of it: a partial grid would
+                            // keep serving the next request with a fraction of the SMs.
+                            atomicExch(&hdr->retire, 1u);
+                            leave = 1;
+                        } else if (waited > kStallNs) {
+                            atomicCAS(&hdr->err, 0u, 2u);
+                            leave = 1;
+                        }
                     }
-                    if (waited > kStallNs) {
-                        atomicCAS(&hdr->err, 0u, 2u);
-                        break;
-                    }
+                    if (__shfl_sync(0xffffffffu, leave, 0)) break;
                     __nanosleep(any_active ? 200 : 1000);
                 }
             }
-            s_slot = got;
-            t_task = global_ns();
-            atomicAdd(&hdr->search_ns, (unsigned long long)(t_task - t0));
+            if (threadIdx.x == 0) {
+                s_slot = got;
+                t_task = global_ns();
+                atomicAdd(&hdr->search_ns, (unsigned long long)(t_task - t0));
+            }
             if (got != kNoSlot) {
                 // The slot's descriptor may have been rewritten since this SM last read it:
-                // copy it through L2.
+                // copy it through L2, one 16-byte piece per lane.
                 const uint4* src = reinterpret_cast<const uint4*>(&slots[got]);
                 uint4* dst = reinterpret_cast<uint4*>(&s_q);
-                for (int q = 0; q < int(sizeof(Req) / 16); ++q) dst[q] = __ldcg(src + q);
+                for (int q = threadIdx.x; q < int(sizeof(Req) / 16); q += 32) dst[q] = __ldcg(src + q);
                 fence_proxy_async_global();
             }
         }

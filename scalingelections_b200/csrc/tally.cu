@@ -46,21 +46,26 @@ int64_t padded(int C) { return round_up(C, kTile); }
 
 // ------------------------------------------------------------------------------------------
 // Positions of one ballot. pos[v][c] = place of candidate c on completed ballot v.
+// Id is int32_t, or uint16_t / uint8_t for packed ballots. Ballot v is
+// ids[offsets[v] - id_base, offsets[v + 1] - id_base), or ids[v * C, (v + 1) * C) when offsets
+// is null (complete ballots).
 // ------------------------------------------------------------------------------------------
+template <typename Id>
 __global__ void __launch_bounds__(256)
-    positions_kernel(const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets, int C, int64_t Cq,
-                     float* __restrict__ pos, uint32_t* __restrict__ err) {
+    positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int C,
+                     int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
     __shared__ uint32_t warp_sums[8];
     __shared__ int bad;
     const int64_t v = blockIdx.x;
     float* p = pos + v * Cq;
-    const int64_t beg = offsets[v], len = offsets[v + 1] - beg;
-    const int32_t* r = ids + beg;
+    const int64_t beg = offsets ? offsets[v] - id_base : v * C;
+    const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
+    const Id* r = ids + beg;
     if (threadIdx.x == 0) bad = 0;
     for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) p[c] = c < C ? -1.0f : 0.0f;
     __syncthreads();
     for (int64_t a = threadIdx.x; a < len; a += blockDim.x) {
-        const int32_t id = r[a];
+        const int64_t id = int64_t(r[a]);
         if (id < 0 || id >= C) {
             raise_device_error(err, kErrRange);
             bad = 1;
@@ -117,7 +122,7 @@ __device__ __forceinline__ void lds4f(float* dst, const float* src) {
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 1)
     count_kernel(const __grid_constant__ CUtensorMap mapPos, int64_t V, int C, int R, uint32_t* __restrict__ out,
-                 int64_t ld_out, uint32_t* __restrict__ err) {
+                 int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     float* sI = reinterpret_cast<float*>(smem_raw);           // [kStages][kVC][kTile]
     float* sJ = sI + kStages * kVC * kTile;                   // [kStages][kVC][kTile]
@@ -196,11 +201,20 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int j = J * kTile + col0 + (q < 4 ? q : 28 + q);
             const uint32_t n = uint32_t(acc[r][q]);
             if (i < C && j < C) {
-                if (I == J) {
-                    out[int64_t(i) * ld_out + j] = i == j ? 0u : n;
+                uint32_t* ij = out + int64_t(i) * ld_out + j;
+                uint32_t* ji = out + int64_t(j) * ld_out + i;
+                if (accumulate) {
+                    if (I != J) {
+                        *ij += n;
+                        *ji += Vu - n;
+                    } else if (i != j) {
+                        *ij += n;  // the (j, i) cell of a diagonal tile is some thread's (i, j)
+                    }
+                } else if (I == J) {
+                    *ij = i == j ? 0u : n;
                 } else {
-                    out[int64_t(i) * ld_out + j] = n;
-                    out[int64_t(j) * ld_out + i] = Vu - n;
+                    *ij = n;
+                    *ji = Vu - n;
                 }
             }
         }
@@ -219,14 +233,23 @@ extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
 }
 
 namespace {
-se_status_t tally_impl(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C, uint32_t* d_out,
-                       int64_t ld_out, void* d_work, int64_t work_bytes, void* stream_, bool check) {
+se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets, int64_t id_base, int64_t V, int C,
+                       unsigned flags, uint32_t* d_out, int64_t ld_out, void* d_work, int64_t work_bytes,
+                       void* stream_) {
     clear_error();
     SE_REQUIRE(C >= 1 && C <= (1 << 20), SE_ERR_INVALID, "Number of candidates out of range (%d)", C);
     SE_REQUIRE(V >= 0 && V < (int64_t(1) << 24), SE_ERR_INVALID, "Number of voters out of range (%lld)",
                (long long)V);
     SE_REQUIRE(d_out != nullptr && ld_out >= C, SE_ERR_INVALID, "bad output matrix");
-    SE_REQUIRE(V == 0 || (d_ids && d_offsets), SE_ERR_INVALID, "null ballot pointer");
+    SE_REQUIRE(id_bytes == 1 || id_bytes == 2 || id_bytes == 4, SE_ERR_INVALID, "id width must be 1, 2 or 4 bytes");
+    SE_REQUIRE((flags & ~unsigned(SE_TALLY_ACCUMULATE | SE_TALLY_NO_SYNC | SE_TALLY_KEEP_ERROR)) == 0,
+               SE_ERR_INVALID, "unknown tally flags %u", flags);
+    SE_REQUIRE(V == 0 || d_ids, SE_ERR_INVALID, "null ballot pointer");
+    SE_REQUIRE(d_offsets == nullptr || id_base >= 0, SE_ERR_INVALID, "negative id base");
+    SE_REQUIRE((reinterpret_cast<uintptr_t>(d_ids) % unsigned(id_bytes)) == 0, SE_ERR_INVALID,
+               "ballot ids are not aligned to their width");
+    const bool accumulate = flags & SE_TALLY_ACCUMULATE;
+    const bool check = !(flags & SE_TALLY_NO_SYNC);
     const int64_t need = se_tally_workspace_bytes(V, C);
     SE_REQUIRE(d_work != nullptr && work_bytes >= need, SE_ERR_WORKSPACE,
                "workspace of %lld bytes is smaller than the %lld bytes required", (long long)work_bytes,
@@ -239,13 +262,20 @@ se_status_t tally_impl(const int32_t* d_ids, const int64_t* d_offsets, int64_t V
     const int64_t Cq = padded(C);
     const int R = int(Cq / kTile);
 
-    SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
+    if (!(flags & SE_TALLY_KEEP_ERROR)) SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
     if (V == 0) {
-        SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
+        if (!accumulate) SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
         return SE_OK;
     }
-    SE_REQUIRE(V <= 0x7fffffff, SE_ERR_INVALID, "too many ballots");
-    positions_kernel<<<unsigned(V), 256, 0, s>>>(d_ids, d_offsets, C, Cq, pos, err);
+    if (id_bytes == 4)
+        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, C, Cq,
+                                                     pos, err);
+    else if (id_bytes == 2)
+        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, C, Cq,
+                                                     pos, err);
+    else
+        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, C, Cq,
+                                                     pos, err);
     SE_CHECK_LAUNCH();
 
     static bool smem_ok = cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -255,7 +285,7 @@ se_status_t tally_impl(const int32_t* d_ids, const int64_t* d_offsets, int64_t V
     if (se_status_t st = se::closure::make_map(&map, pos, uint64_t(Cq), uint64_t(V), uint64_t(Cq) * 4, kTile, kVC))
         return st;
     const int64_t tiles = int64_t(R) * (R + 1) / 2;
-    count_kernel<<<unsigned(tiles), kThreads, kSmem, s>>>(map, V, C, R, d_out, ld_out, err);
+    count_kernel<<<unsigned(tiles), kThreads, kSmem, s>>>(map, V, C, R, d_out, ld_out, accumulate, err);
     SE_CHECK_LAUNCH();
     if (!check) return SE_OK;
 
@@ -271,11 +301,21 @@ se_status_t tally_impl(const int32_t* d_ids, const int64_t* d_offsets, int64_t V
 
 extern "C" se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C, uint32_t* d_out,
                                 int64_t ld_out, void* d_work, int64_t work_bytes, void* stream) {
-    return tally_impl(d_ids, d_offsets, V, C, d_out, ld_out, d_work, work_bytes, stream, true);
+    clear_error();
+    SE_REQUIRE(V == 0 || d_offsets != nullptr, SE_ERR_INVALID, "null ballot pointer");
+    return tally_impl(d_ids, 4, d_offsets, 0, V, C, 0u, d_out, ld_out, d_work, work_bytes, stream);
 }
 
 extern "C" se_status_t se_tally_enqueue(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
                                         uint32_t* d_out, int64_t ld_out, void* d_work, int64_t work_bytes,
                                         void* stream) {
-    return tally_impl(d_ids, d_offsets, V, C, d_out, ld_out, d_work, work_bytes, stream, false);
+    clear_error();
+    SE_REQUIRE(V == 0 || d_offsets != nullptr, SE_ERR_INVALID, "null ballot pointer");
+    return tally_impl(d_ids, 4, d_offsets, 0, V, C, SE_TALLY_NO_SYNC, d_out, ld_out, d_work, work_bytes, stream);
+}
+
+extern "C" se_status_t se_tally_ex(const void* d_ids, int id_bytes, const int64_t* d_offsets, int64_t id_base,
+                                   int64_t V, int C, unsigned flags, uint32_t* d_out, int64_t ld_out, void* d_work,
+                                   int64_t work_bytes, void* stream) {
+    return tally_impl(d_ids, id_bytes, d_offsets, id_base, V, C, flags, d_out, ld_out, d_work, work_bytes, stream);
 }
