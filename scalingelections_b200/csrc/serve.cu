@@ -615,6 +615,7 @@ struct Engine {
     std::vector<uint8_t> tally_reported;
     uint8_t* staging = nullptr;     // pinned, one region per slot: its H2D sources stay valid
                                     // until the slot is reused, i.e. long after the copies ran
+    uint8_t* zeros = nullptr;       // pinned, kZeroBytes of zeros: the source of every clearing copy
     std::vector<uint32_t> gen;
     std::vector<uint8_t> busy;
     uint32_t slot_hi = 0;
@@ -628,6 +629,11 @@ struct Engine {
 };
 
 constexpr size_t kStagingPerSlot = round_up_const(sizeof(Req) + 16 + (kMaxPhases + 1) * 8, 256);
+// Submission clears a request's flags, wins and phase counters by copying from pinned zeros
+// rather than with cudaMemsetAsync: a memset is a kernel, and while the engine is resident
+// its CTAs hold every SM's registers, so a memset (and every copy queued behind it on the
+// submitting stream) would wait for the whole grid to retire.
+constexpr size_t kZeroBytes = std::max<size_t>(size_t(4) << 15, size_t(kMaxPhases) * 4);  // wins of C = 32768
 
 int64_t offsets(int max_slots, int64_t* slots_off, int64_t* claims_off, int64_t* dones_off) {
     int64_t off = 256;
@@ -713,6 +719,7 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
         set_error("%s failed: %s", what, cudaGetErrorString(err));
         if (E.done_host) cudaFreeHost(E.done_host);
         if (E.staging) cudaFreeHost(E.staging);
+        if (E.zeros) cudaFreeHost(E.zeros);
         if (E.tally_host) cudaFreeHost(E.tally_host);
         if (E.stream) cudaStreamDestroy(E.stream);
         if (E.finished) cudaEventDestroy(E.finished);
@@ -725,6 +732,9 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
     std::memset(E.done_host, 0, sizeof(uint64_t) * size_t(max_slots));
     if ((err = cudaHostAlloc(&E.staging, kStagingPerSlot * size_t(max_slots), cudaHostAllocDefault)) != cudaSuccess)
         return fail(err, "cudaHostAlloc");
+    if ((err = cudaHostAlloc(&E.zeros, kZeroBytes, cudaHostAllocDefault)) != cudaSuccess)
+        return fail(err, "cudaHostAlloc");
+    std::memset(E.zeros, 0, kZeroBytes);
     if ((err = cudaHostAlloc(&E.tally_host, sizeof(uint32_t) * size_t(max_slots), cudaHostAllocMapped)) != cudaSuccess)
         return fail(err, "cudaHostAlloc");
     std::memset(E.tally_host, 0, sizeof(uint32_t) * size_t(max_slots));
@@ -856,11 +866,14 @@ extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, 
     stg_words[1] = std::max(E.slot_hi, uint32_t(slot + 1));
     uint64_t* cl = reinterpret_cast<uint64_t*>(stg + sizeof(Req) + 16);
     for (int f = 0; f <= nph; ++f) cl[f] = uint64_t(gen) << 32;
-    SE_CUDA_TRY(cudaMemsetAsync(sc, 0, 256, s));
-    if (e.R > 1) SE_CUDA_TRY(cudaMemsetAsync(rq->d_wins, 0, sizeof(int32_t) * size_t(C), s));
+    // Copies only (copy engines), no kernels: see kZeroBytes.
+    SE_CUDA_TRY(cudaMemcpyAsync(sc, E.zeros, 256, cudaMemcpyHostToDevice, s));
+    if (e.R > 1)
+        SE_CUDA_TRY(cudaMemcpyAsync(rq->d_wins, E.zeros, sizeof(int32_t) * size_t(C), cudaMemcpyHostToDevice, s));
     SE_CUDA_TRY(cudaMemcpyAsync(E.claims + size_t(slot) * (kMaxPhases + 1), cl, size_t(nph + 1) * 8,
                                 cudaMemcpyHostToDevice, s));
-    SE_CUDA_TRY(cudaMemsetAsync(E.dones + size_t(slot) * kMaxPhases, 0, size_t(nph) * 4, s));
+    SE_CUDA_TRY(cudaMemcpyAsync(E.dones + size_t(slot) * kMaxPhases, E.zeros, size_t(nph) * 4,
+                                cudaMemcpyHostToDevice, s));
     SE_CUDA_TRY(cudaMemcpyAsync(&E.slots[slot], stg, sizeof(Req), cudaMemcpyHostToDevice, s));
     SE_CUDA_TRY(cudaMemcpyAsync(&E.slots[slot].active, &stg_words[0], 4, cudaMemcpyHostToDevice, s));
     if (uint32_t(slot + 1) > E.slot_hi) {
@@ -972,6 +985,7 @@ extern "C" se_status_t se_engine_destroy(se_engine_t* h) {
     Engine& E = h->e;
     if (E.done_host) cudaFreeHost(E.done_host);
     if (E.staging) cudaFreeHost(E.staging);
+    if (E.zeros) cudaFreeHost(E.zeros);
     if (E.tally_host) cudaFreeHost(E.tally_host);
     if (E.stream) cudaStreamDestroy(E.stream);
     if (E.finished) cudaEventDestroy(E.finished);
