@@ -234,11 +234,13 @@ class BallotFile:
             yield v0, min(v0 + step, self.num_voters)
 
 
-def _pread_into(fd: int, dst: np.ndarray, file_offset: int, pool: ThreadPoolExecutor, piece: int = 8 << 20) -> None:
-    """Fill the byte view dst from the file at file_offset with parallel pread calls."""
+def _pread_into(fd: int, dst: np.ndarray, file_offset: int, pool: ThreadPoolExecutor, threads: int) -> None:
+    """Fill the byte view dst from the file at file_offset with parallel pread calls, about two
+    pieces per thread (at least 1 MiB each)."""
     buf = dst.view(np.uint8).reshape(-1)
     n = buf.size
     mv = memoryview(buf)
+    piece = max(1 << 20, -(-n // (2 * threads)))
 
     def read(a: int) -> None:
         b = min(a + piece, n)
@@ -260,12 +262,14 @@ def default_chunk_ballots(num_candidates: int, positions_bytes: int = 1 << 30) -
 
 
 def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | None = None,
-               out: torch.Tensor | None = None, threads: int = 8, stats: dict | None = None) -> torch.Tensor:
+               out: torch.Tensor | None = None, threads: int | None = None,
+               stats: dict | None = None) -> torch.Tensor:
     """Pairwise preference counts (uint32 [C, C] on ``device``) of every ballot in the file,
     streamed through the GPU in chunks of ``chunk_ballots``. Equals ``build_pairwise_preferences``
     of the same ballots. Raises ValueError for an id outside [0, C) or repeated in a ballot."""
     bf = BallotFile(path)
     h = bf.header
+    threads = int(threads) if threads else min(32, os.cpu_count() or 1)
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     V, C = h.num_voters, h.num_candidates
     if out is None:
@@ -307,14 +311,15 @@ def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | Non
         fd = os.open(bf.path, os.O_RDONLY)
         read_s = 0.0
         try:
-            with ThreadPoolExecutor(max_workers=max(1, int(threads))) as pool:
+            with ThreadPoolExecutor(max_workers=max(1, threads)) as pool:
                 for n, (v0, v1) in enumerate(bf.chunks(nv)):
                     b = n & 1
                     if used[b]:
                         copied[b].synchronize()  # the pinned buffer's previous copy has finished
                     a, z = bf.span(v0, v1)
                     t0 = time.perf_counter()
-                    _pread_into(fd, host_ids[b][:z - a].numpy().view(np_dtype), h.ids_offset + a * width, pool)
+                    _pread_into(fd, host_ids[b][:z - a].numpy().view(np_dtype), h.ids_offset + a * width, pool,
+                                threads)
                     if ragged:
                         host_offs[b][:v1 - v0 + 1].copy_(torch.from_numpy(np.array(bf.offsets[v0:v1 + 1])))
                     read_s += time.perf_counter() - t0
@@ -336,7 +341,8 @@ def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | Non
             os.close(fd)
         code = int(work[:4].view(torch.int32).cpu().item())  # synchronises the compute stream
     if stats is not None:
-        stats.update(chunks=-(-V // nv), chunk_ballots=nv, read_s=read_s, file_bytes=os.path.getsize(bf.path))
+        stats.update(chunks=-(-V // nv), chunk_ballots=nv, read_s=read_s, file_bytes=os.path.getsize(bf.path),
+                     read_threads=threads)
     if code == 2:
         raise ValueError(f"a ballot names a candidate outside [0, {C})")
     if code == 3:

@@ -119,24 +119,34 @@ __device__ __forceinline__ void lds4f(float* dst, const float* src) {
 
 // ------------------------------------------------------------------------------------------
 // Counting over one upper tile (I <= J): d[I][J] and, for I < J, d[J][I] = V - d[I][J].
+// With splits > 1 the voters are cut into `splits` ranges of whole 32-voter chunks, one CTA per
+// (tile, range), and each CTA adds its range's counts (and, below the diagonal, the range's
+// voters minus them) to out with atomics: exact, since every count is an integer, and it keeps
+// the grid full when there are few tiles and many voters.
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 1)
-    count_kernel(const __grid_constant__ CUtensorMap mapPos, int64_t V, int C, int R, uint32_t* __restrict__ out,
-                 int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
+    count_kernel(const __grid_constant__ CUtensorMap mapPos, int64_t V, int C, int R, int splits,
+                 uint32_t* __restrict__ out, int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     float* sI = reinterpret_cast<float*>(smem_raw);           // [kStages][kVC][kTile]
     float* sJ = sI + kStages * kVC * kTile;                   // [kStages][kVC][kTile]
     uint64_t* bars = reinterpret_cast<uint64_t*>(sJ + kStages * kVC * kTile);
 
     // Upper-triangle tile index -> (I, J), row-major over I <= J.
-    int64_t t = blockIdx.x;
+    int64_t t = blockIdx.x / splits;
+    const int split = int(blockIdx.x % splits);
     int I = 0;
     while (t >= R - I) {
         t -= R - I;
         ++I;
     }
     const int J = I + int(t);
-    const int nch = int((V + kVC - 1) / kVC);
+    const int total_ch = int((V + kVC - 1) / kVC);
+    const int per = (total_ch + splits - 1) / splits;
+    const int ch0 = split * per < total_ch ? split * per : total_ch;
+    const int ch1 = ch0 + per < total_ch ? ch0 + per : total_ch;
+    const int nch = ch1 - ch0;
+    const int64_t vlo = int64_t(ch0) * kVC, vhi = int64_t(ch1) * kVC < V ? int64_t(ch1) * kVC : V;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
@@ -146,8 +156,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages && s < nch; ++s) {
             mbar_arrive_expect_tx(&bars[s], 2 * kChunkBytes);
-            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, s * kVC);
-            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, s * kVC);
+            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, (ch0 + s) * kVC);
+            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, (ch0 + s) * kVC);
         }
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -184,15 +194,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (threadIdx.x == 0 && ok && ch + kStages < nch) {
             fence_proxy_async();  // order this stage's shared reads before the TMA rewrite
             mbar_arrive_expect_tx(&bars[s], 2 * kChunkBytes);
-            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, (ch + kStages) * kVC);
-            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, (ch + kStages) * kVC);
+            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, (ch0 + ch + kStages) * kVC);
+            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, (ch0 + ch + kStages) * kVC);
         }
     }
     if (!ok) {
         raise_device_error(err, kErrTimeout);
         return;
     }
-    const uint32_t Vu = uint32_t(V);
+    const uint32_t Vu = uint32_t(vhi - vlo);
+    if (nch == 0) return;  // an empty trailing range (more splits than chunks)
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const int i = I * kTile + row0 + r;
@@ -203,7 +214,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (i < C && j < C) {
                 uint32_t* ij = out + int64_t(i) * ld_out + j;
                 uint32_t* ji = out + int64_t(j) * ld_out + i;
-                if (accumulate) {
+                if (splits > 1) {
+                    if (I != J) {
+                        atomicAdd(ij, n);
+                        atomicAdd(ji, Vu - n);
+                    } else if (i != j) {
+                        atomicAdd(ij, n);
+                    }
+                } else if (accumulate) {
                     if (I != J) {
                         *ij += n;
                         *ji += Vu - n;
@@ -285,7 +303,19 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     if (se_status_t st = se::closure::make_map(&map, pos, uint64_t(Cq), uint64_t(V), uint64_t(Cq) * 4, kTile, kVC))
         return st;
     const int64_t tiles = int64_t(R) * (R + 1) / 2;
-    count_kernel<<<unsigned(tiles), kThreads, kSmem, s>>>(map, V, C, R, d_out, ld_out, accumulate, err);
+    // Few tiles and many voters: split the voters so that the grid covers every SM about four
+    // times, keeping at least 32 chunks (1024 voters) per range.
+    int sms = 0, dev = 0;
+    SE_CUDA_TRY(cudaGetDevice(&dev));
+    SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t want = 4 * int64_t(sms);
+    const int64_t chunks = (V + kVC - 1) / kVC;
+    int splits = 1;
+    if (tiles < want) splits = int(std::max<int64_t>(1, std::min<int64_t>((want + tiles - 1) / tiles, chunks / 32)));
+    if (splits > 1 && !accumulate)
+        SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
+    count_kernel<<<unsigned(tiles * splits), kThreads, kSmem, s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
+                                                                   err);
     SE_CHECK_LAUNCH();
     if (!check) return SE_OK;
 

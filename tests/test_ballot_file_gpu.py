@@ -151,3 +151,30 @@ def test_tally_file_reports_bad_ids(tmp_path, where):
     p.write_bytes(bytes(raw))
     with pytest.raises(ValueError, match="twice"):
         bfm.tally_file(p, chunk_ballots=16)
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_tally_split_voters(orc, accumulate):
+    """Few tiles, many voters: the count kernel splits the voters across CTAs and adds the
+    partial counts with atomics; results stay exact, in overwrite and accumulate modes."""
+    C, V = 260, 20000
+    B = ragged(V, C, 123, min_len=C // 2)
+    lens = np.array([b.size for b in B])
+    offs = np.zeros(V + 1, dtype=np.int64)
+    np.cumsum(lens, out=offs[1:])
+    d_ids = torch.from_numpy(np.concatenate(B).astype(np.int16)).cuda()
+    d_offs = torch.from_numpy(offs).cuda()
+    L = _lib.lib()
+    need = L.se_tally_workspace_bytes(V, C)
+    work = torch.empty(need, dtype=torch.uint8, device="cuda")
+    seed = torch.randint(0, 1000, (C, C), dtype=torch.int32, device="cuda")
+    out = seed.clone().view(torch.uint32)
+    flags = bfm.SE_TALLY_ACCUMULATE if accumulate else 0
+    _lib.check(L.se_tally_ex(d_ids.data_ptr(), 2, d_offs.data_ptr(), 0, V, C, flags, out.data_ptr(), C,
+                             work.data_ptr(), need, torch.cuda.current_stream().cuda_stream))
+    expect = oracle_tally(orc, B, C).astype(np.int64)
+    if accumulate:
+        base = seed.cpu().numpy().astype(np.int64)
+        np.fill_diagonal(expect, 0)
+        expect = expect + base
+    assert np.array_equal(host_u32(out).astype(np.int64), expect)
