@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--candidates", type=int, default=16384)
     ap.add_argument("--voters", type=int, default=4096)
     ap.add_argument("--phi", type=float, default=0.8)
+    ap.add_argument("--input", choices=["mallows", "random"], default="mallows",
+                    help="closure input: tallied Mallows ballots, or the reference's random matrix mode")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
     ap.add_argument("--closure-mode", type=int, default=1, choices=[1, 2],
@@ -72,8 +74,11 @@ def parse():
 
 def config(args, world):
     return {
-        "workload": f"Schulze widest-path closure, one election per GPU: C={args.candidates} candidates, "
-                    f"V={args.voters} Mallows(phi={args.phi}) ballots",
+        "workload": (f"Schulze widest-path closure, one election per GPU: C={args.candidates} candidates, "
+                     f"V={args.voters} Mallows(phi={args.phi}) ballots" if args.input == "mallows" else
+                     f"Schulze widest-path closure, one election per GPU: C={args.candidates} candidates, "
+                     f"random preference matrix (values uniform in [0, C), the reference's benchmark mode)"),
+        "input": args.input,
         "candidates": args.candidates,
         "voters": args.voters,
         "phi": args.phi,
@@ -226,11 +231,17 @@ def run_ours(args, world, rank, local_rank):
     lanes = args.lanes
     L = _lib.lib()
 
-    # Input: ballots drawn and tallied on the device.
-    ballots = mallows_ballots_device(V, C, args.phi, seed=args.seed + 1000 * rank, device=dev)
-    offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
-    d = api.tally_device(ballots.view(-1), offs, C)
-    del ballots
+    # Input: ballots drawn and tallied on the device, or the reference's random benchmark matrix
+    # (values uniform in [0, C), scaling_elections.py:473-476) drawn on the device.
+    if args.input == "random":
+        from scalingelections_b200.ballots import random_preferences_device
+
+        d = random_preferences_device(C, seed=args.seed + 1000 * rank, device=dev)
+    else:
+        ballots = mallows_ballots_device(V, C, args.phi, seed=args.seed + 1000 * rank, device=dev)
+        offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
+        d = api.tally_device(ballots.view(-1), offs, C)
+        del ballots
     torch.cuda.synchronize()
 
     # Roofline denominator: the min/max issue microbenchmark at this moment's clock.
@@ -316,7 +327,8 @@ def run_ours(args, world, rank, local_rank):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"u{lanes}" if lanes else "u16/u32",
-            "data": "synthetic (seeded Mallows ballots drawn and tallied on the GPU)",
+            "data": ("synthetic (seeded Mallows ballots drawn and tallied on the GPU)" if args.input == "mallows"
+                     else "synthetic (seeded random matrix drawn on the GPU)"),
             "config": config(args, world),
             "roofline": {
                 "bound": "int_minmax",

@@ -314,6 +314,13 @@ SE_API se_status_t se_mallows_ballots(int64_t V, int C, double phi, uint64_t see
                                       const int32_t* d_reference, int32_t* d_out, void* d_work,
                                       int64_t work_bytes, void* stream);
 
+/* Random preference matrix on the device: the reference's benchmark input
+ * np.random.randint(0, C, (C, C)) (scaling_elections.py:473-476) as a seeded, counter-based
+ * draw. Cell (i, j) = (hi32(splitmix64(seed ^ splitmix64(i*C + j))) * high) >> 32, uniform in
+ * [0, high) up to a bias of high / 2^32; high = 0 means C. Deterministic in (seed, i, j). */
+SE_API se_status_t se_random_preferences(int C, uint32_t high, uint64_t seed, uint32_t* d_out,
+                                         int64_t ld_out, void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Integer min/max issue-rate microbenchmark (no reference counterpart): measures the
  * relaxations c = max(c, min(a, b)) per SM per clock that one instruction recipe reaches on

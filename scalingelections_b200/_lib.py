@@ -66,6 +66,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_tally_enqueue": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
+    "se_random_preferences": (_c_int, [_c_int, ctypes.c_uint32, ctypes.c_uint64, _vp, _c_i64, _vp]),
     "se_tally_ex": (_c_int, [_vp, _c_int, _vp, _c_i64, _c_i64, _c_int, ctypes.c_uint, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_rank": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
     "se_mallows_workspace_bytes": (_c_i64, [_c_i64, _c_int]),

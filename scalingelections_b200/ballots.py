@@ -125,3 +125,36 @@ def mallows_ballots_device(V: int, C: int, phi: float, seed: int, reference=None
                                         out.data_ptr(), work.data_ptr(), need,
                                         torch.cuda.current_stream().cuda_stream))
     return out
+
+
+def random_preferences_device(C: int, seed: int, high: int | None = None, device="cuda"):
+    """The reference's random benchmark matrix (scaling_elections.py:473-476: values uniform in
+    [0, C)) drawn on the GPU as a CUDA uint32 [C, C] tensor: a counter-based, seeded draw,
+    not NumPy's stream (``random_matrix_host`` restates it on the host)."""
+    import torch
+
+    from . import _lib
+
+    out = torch.empty((C, C), dtype=torch.uint32, device=device)
+    with torch.cuda.device(out.device):
+        _lib.check(_lib.lib().se_random_preferences(int(C), int(high or 0), int(seed) & (2**64 - 1), out.data_ptr(),
+                                                    max(int(C), 1), torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def random_matrix_host(C: int, seed: int, high: int | None = None) -> np.ndarray:
+    """Host restatement of random_preferences_device, bit for bit (for checking and for
+    callers without a GPU)."""
+    high = np.uint64(high or C)
+    with np.errstate(over="ignore"):
+        x = np.arange(C * C, dtype=np.uint64)
+        h = _splitmix64(np.uint64(int(seed) & (2**64 - 1)) ^ _splitmix64(x))
+        v = ((h >> np.uint64(32)) * high) >> np.uint64(32)
+    return v.astype(np.uint32).reshape(C, C)

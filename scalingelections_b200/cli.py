@@ -66,8 +66,8 @@ def parser() -> argparse.ArgumentParser:
     ap.add_argument("--seed", type=int, default=None, help="Seed of NumPy's global generator")
     ap.add_argument("--lanes", choices=["auto", "16", "32"], default="auto", help="Closure lane mode")
     ap.add_argument("--device-ballots", action="store_true",
-                    help="Draw uniform ballots on the GPU and tally them there (fast at large V x C; "
-                         "not NumPy's stream)")
+                    help="Draw the random matrix, or uniform ballots tallied in place, on the GPU "
+                         "(fast at large V x C; not NumPy's stream)")
     ap.add_argument("--reference-script", default=None,
                     help="Run this unmodified scaling_elections.py against the drop-in module instead")
     return ap
@@ -101,6 +101,10 @@ def draw_preferences(num_candidates: int, num_voters: int, device_ballots: bool)
     from .ballots import mallows_ballots_device
 
     C, V = num_candidates, num_voters
+    if V == 0 and device_ballots:
+        from .ballots import random_preferences_device
+
+        return api._to_host_u32(random_preferences_device(C, seed=int(np.random.randint(0, 2**31 - 1))))
     if V == 0:
         return np.random.randint(0, C, (C, C)).astype(np.uint32)
     if device_ballots:

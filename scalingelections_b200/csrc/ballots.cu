@@ -31,6 +31,21 @@ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t v, uint64_t 
     return double(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
+// Random preference matrix: the reference's benchmark input np.random.randint(0, C, (C, C))
+// (scaling_elections.py:473-476) drawn on the device. Cell (i, j) is
+// (hi32(splitmix64(seed ^ splitmix64(i * C + j))) * high) >> 32, a multiply-shift map of 32
+// random bits onto [0, high) (bias at most high / 2^32). The diagonal is filled too, as in
+// the reference; the closure ignores it.
+__global__ void __launch_bounds__(256)
+    random_matrix_kernel(int C, int64_t ld, uint32_t high, uint64_t seed, uint32_t* __restrict__ out) {
+    const int64_t n = int64_t(C) * C;
+    for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < n; x += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = x / C, j = x - i * C;
+        const uint64_t h = splitmix64(seed ^ splitmix64(uint64_t(x)));
+        out[i * ld + j] = uint32_t(((h >> 32) * uint64_t(high)) >> 32);
+    }
+}
+
 __global__ void __launch_bounds__(128)
     mallows_kernel(int64_t V, int C, int size, double phi, double log_phi, uint64_t seed,
                    const int32_t* __restrict__ pi0, int32_t* __restrict__ out, uint32_t* __restrict__ tree) {
@@ -112,6 +127,24 @@ extern "C" se_status_t se_mallows_ballots(int64_t V, int C, double phi, uint64_t
     SE_REQUIRE(blocks < (int64_t(1) << 31), SE_ERR_INVALID, "too many voters");
     ballots::mallows_kernel<<<unsigned(blocks), 128, 0, s>>>(V, C, size, phi, log_phi, seed, d_reference, d_out,
                                                              static_cast<uint32_t*>(d_work));
+    SE_CHECK_LAUNCH();
+    return SE_OK;
+}
+
+extern "C" se_status_t se_random_preferences(int C, uint32_t high, uint64_t seed, uint32_t* d_out, int64_t ld_out,
+                                             void* stream_) {
+    clear_error();
+    SE_REQUIRE(C >= 0 && C <= (1 << 20), SE_ERR_INVALID, "Number of candidates out of range (%d)", C);
+    SE_REQUIRE(C == 0 || (d_out && ld_out >= C), SE_ERR_INVALID, "bad output matrix");
+    if (C == 0) return SE_OK;
+    if (high == 0) high = uint32_t(C);
+    cudaStream_t s = static_cast<cudaStream_t>(stream_);
+    int sms = 0, dev = 0;
+    SE_CUDA_TRY(cudaGetDevice(&dev));
+    SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t cells = int64_t(C) * C;
+    const int64_t blocks = std::min<int64_t>((cells + 255) / 256, int64_t(sms) * 8);
+    ballots::random_matrix_kernel<<<unsigned(blocks), 256, 0, s>>>(C, ld_out, high, seed, d_out);
     SE_CHECK_LAUNCH();
     return SE_OK;
 }

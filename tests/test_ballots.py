@@ -42,3 +42,14 @@ def test_mallows_concentrates_near_reference():
 def test_random_preferences_match_reference_mode():
     P = ballots.random_preferences(9, seed=4)
     assert P.dtype == np.uint32 and P.shape == (9, 9) and P.max() < 9
+
+
+def test_random_matrix_host_restatement():
+    """Host restatement of the device generator: deterministic, in range, roughly uniform."""
+    from scalingelections_b200.ballots import random_matrix_host
+
+    a = random_matrix_host(200, 5)
+    assert a.dtype == np.uint32 and a.shape == (200, 200)
+    assert np.array_equal(a, random_matrix_host(200, 5)) and not np.array_equal(a, random_matrix_host(200, 6))
+    assert a.max() == 199 and abs(a.mean() - 99.5) < 2
+    assert random_matrix_host(50, 1, high=3).max() == 2

@@ -34,3 +34,20 @@ def test_device_mallows_concentration():
     assert tight < mid < loose
     # Uniform permutations of 40 items: E|pos - i| = (n^2 - 1) / (3n) = 13.3.
     assert abs(loose - (40 * 40 - 1) / (3 * 40)) < 0.5
+
+
+@pytest.mark.parametrize("C,high", [(1, None), (300, None), (1000, 7), (4096, 65535)])
+def test_random_preferences_device_bit_exact(C, high):
+    """The device's random benchmark matrix equals its host restatement bit for bit, and its
+    values cover [0, high)."""
+    from scalingelections_b200.ballots import random_matrix_host, random_preferences_device
+
+    d = random_preferences_device(C, seed=42, high=high)
+    got = d.view(torch.int32).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, random_matrix_host(C, 42, high))
+    hi = high or C
+    assert got.max() < hi and (C < 64 or got.max() == hi - 1)
+    if C >= 1000:
+        assert abs(got.mean() - (hi - 1) / 2) < 0.01 * hi
+    assert not np.array_equal(random_preferences_device(C, seed=43, high=high).view(torch.int32).cpu().numpy(),
+                              got.view(np.int32)) or C == 1
