@@ -35,7 +35,8 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "Gcells/s (C^3/t), single-election widest-path closure, C=16384"
+def metric_name(C: int) -> str:
+    return f"Gcells/s (C^3/t), single-election widest-path closure, C={C}"
 UNIT = "Gcells/s"
 
 
@@ -186,7 +187,7 @@ def run_reference_arm(args, world, rank):
             values.append(cps)
     v = statistics.median(values) / 1e9
     line = {
-        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": metric_name(args.candidates), "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": args.cpu_sample ** 3 / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Mallows ballots)", "config": cfg,
         "impl": "reference",
@@ -324,7 +325,7 @@ def run_ours(args, world, rank, local_rank):
     if rank == 0:
         traffic = load_traffic(lanes if lanes else 16, C)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": metric_name(args.candidates), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"u{lanes}" if lanes else "u16/u32",
             "data": ("synthetic (seeded Mallows ballots drawn and tallied on the GPU)" if args.input == "mallows"
