@@ -6,7 +6,8 @@ baseline. The product package ``scalingelections_b200`` never imports it.
 
 Wraps ``oracle.c`` (a C restatement of the reference's algorithm, each function citing the
 ``scaling_elections.py`` lines it follows) and, where it was built, the reference's own CPU
-closure compiled unmodified from ``scaling_elections.cu`` into ``oracle/_ref``.
+closure compiled unmodified from ``scaling_elections.cu`` into ``oracle/_ref``, and its CUDA
+build (the reference's own GPU kernels, for sm_100a) into ``oracle/_ref/gpu``.
 """
 from __future__ import annotations
 
@@ -23,9 +24,11 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "liboracle.so"
 REF_PATH = HERE / "_ref" / ("scaling_elections" + sysconfig.get_config_var("EXT_SUFFIX"))
+REF_GPU_PATH = HERE / "_ref" / "gpu" / ("scaling_elections" + sysconfig.get_config_var("EXT_SUFFIX"))
 
 _lib = None
 _ref = None
+_ref_gpu = None
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -37,6 +40,7 @@ def build(reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
     if reference and Path("/root/reference/scaling_elections.cu").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref_gpu"], check=True)
 
 
 def lib() -> ctypes.CDLL:
@@ -165,6 +169,19 @@ def mallows_ballots(V: int, C: int, phi: float, seed: int) -> np.ndarray:
     out = np.empty((V, C), dtype=np.int32)
     np.put_along_axis(out, final, np.broadcast_to(pi0, (V, C)), axis=1)
     return out
+
+
+def reference_gpu():
+    """The reference's own CUDA module (scaling_elections.cu built by `make ref_gpu` for
+    sm_100a), or None. Loaded like reference_cpu(), outside sys.modules."""
+    global _ref_gpu
+    if _ref_gpu is None and REF_GPU_PATH.exists():
+        loader = importlib.machinery.ExtensionFileLoader("scaling_elections", str(REF_GPU_PATH))
+        spec = importlib.util.spec_from_file_location("scaling_elections", str(REF_GPU_PATH), loader=loader)
+        mod = importlib.util.module_from_spec(spec)
+        loader.exec_module(mod)
+        _ref_gpu = mod
+    return _ref_gpu
 
 
 def reference_cpu():

@@ -1,0 +1,95 @@
+"""Against the reference's own GPU kernels: scaling_elections.cu compiled unmodified for sm_100a
+(oracle/_ref/gpu, built by `make -C oracle ref_gpu` where the reference sources are present).
+Its CUDA path (compute_strongest_paths with allow_gpu=True, allow_tma=False, tile 32;
+scaling_elections.cu:490-578) needs C % 32 == 0. Skipped when that build is absent.
+
+Besides parity, one test times both on the single-election C = 4096, V = 4096 uniform-ballot
+workload. Each side is timed by wall clock around its host API, the reference's own convention
+(scaling_elections.py:320-356). The line is written to $SE_REPORT_DIR/reference_gpu.json when
+that variable is set."""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+import torch
+
+from scalingelections_b200 import api
+from scalingelections_b200.ballots import mallows_ballots_device, random_preferences_device
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref_gpu():
+    from oracle import oracle
+
+    mod = oracle.reference_gpu()
+    if mod is None:
+        pytest.skip("the reference's CUDA build is not present")
+    return mod
+
+
+def tallied(C, V, phi, seed):
+    b = mallows_ballots_device(V, C, phi, seed=seed)
+    offs = torch.arange(V + 1, dtype=torch.int64, device=b.device) * C
+    return api._to_host_u32(api.tally_device(b.view(-1), offs, C))
+
+
+def reference_paths(ref_gpu, P):
+    return ref_gpu.compute_strongest_paths(P, allow_gpu=True, allow_tma=False, tile_size=32)
+
+
+@pytest.mark.parametrize("C,V,phi", [(256, 301, 0.8), (1024, 4096, 0.8), (2048, 999, 1.0)])
+def test_same_matrix_as_reference_kernels(ref_gpu, C, V, phi):
+    P = tallied(C, V, phi, seed=C + V)
+    ours = api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
+    assert np.array_equal(ours, reference_paths(ref_gpu, P))
+
+
+@pytest.mark.parametrize("C", [512, 2048])
+def test_same_matrix_as_reference_kernels_random_matrix(ref_gpu, C):
+    """The reference's benchmark input (values uniform in [0, C), py:473-476)."""
+    P = api._to_host_u32(random_preferences_device(C, seed=C))
+    ours = api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
+    assert np.array_equal(ours, reference_paths(ref_gpu, P))
+
+
+def test_speed_against_reference_kernels(ref_gpu):
+    C, V = 4096, 4096
+    P = tallied(C, V, 1.0, seed=11)  # phi = 1: uniform permutations
+    reference_paths(ref_gpu, P)  # warm-up (context, module load)
+    t0 = time.perf_counter()
+    ref_out = reference_paths(ref_gpu, P)
+    ref_s = time.perf_counter() - t0
+    api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ours = api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
+        runs.append(time.perf_counter() - t0)
+    ours_s = min(runs)
+    d = api._to_device_u32(P, torch.device("cuda"))
+    out = torch.empty_like(d)
+    api.strongest_paths_device(d, out=out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        api.strongest_paths_device(d, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    device_s = e0.elapsed_time(e1) / 5e3
+    assert np.array_equal(ours, ref_out)
+    line = {"workload": "C=4096, V=4096 uniform ballots, one election",
+            "reference_cuda_s": ref_s, "reference_cuda_gcells_s": C ** 3 / ref_s / 1e9,
+            "ours_host_api_s": ours_s, "ours_host_api_gcells_s": C ** 3 / ours_s / 1e9,
+            "ours_device_s": device_s, "ours_device_gcells_s": C ** 3 / device_s / 1e9,
+            "speedup_host_api": ref_s / ours_s, "bit_identical": True,
+            "reference_call": "compute_strongest_paths(P, allow_gpu=True, allow_tma=False, tile_size=32)"}
+    out_dir = os.environ.get("SE_REPORT_DIR")
+    if out_dir:
+        with open(os.path.join(out_dir, "reference_gpu.json"), "w") as f:
+            json.dump(line, f)
+    print(json.dumps(line))
+    assert ours_s < ref_s
