@@ -242,7 +242,6 @@ def run_ours(args, world, rank, local_rank):
         ballots = mallows_ballots_device(V, C, args.phi, seed=args.seed + 1000 * rank, device=dev)
         offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
         d = api.tally_device(ballots.view(-1), offs, C)
-        del ballots
     torch.cuda.synchronize()
 
     # Roofline denominator: the min/max issue microbenchmark at this moment's clock.
@@ -297,6 +296,31 @@ def run_ours(args, world, rank, local_rank):
     algo_bytes = float(R - 1) ** 2 * 128 * 128 * cell_bytes * 2  # each remainder tile read + written once
 
     # End to end through the public host API: pinned host in, pinned host out.
+    # The tally half of the path on the same ballots (device-resident), against the FP32 pipe:
+    # one sub.sat.f32 + add.f32 per voter and candidate pair of the upper block triangle.
+    tally = None
+    if args.input == "mallows":
+        tw = torch.empty(api.tally_workspace_bytes(V, C), dtype=torch.uint8, device=dev)
+        d2 = torch.empty_like(d)
+        for _ in range(2):
+            api.tally_device(ballots.view(-1), offs, C, out=d2, workspace=tw)
+        t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0e.record(stream)
+        for _ in range(3):
+            api.tally_device(ballots.view(-1), offs, C, out=d2, workspace=tw)
+        t1e.record(stream)
+        torch.cuda.synchronize()
+        tally_s = t0e.elapsed_time(t1e) / 3e3
+        Rt = (C + 127) // 128
+        executed = Rt * (Rt + 1) / 2 * 128 * 128 * V
+        fp32_peak = torch.cuda.get_device_properties(dev).multi_processor_count * 128 * peak_mhz * 1e6 / 2
+        tally = {"ms": tally_s * 1e3, "voters": V, "pairs_per_s": V * C * (C - 1) / 2 / tally_s,
+                 "roofline": {"bound": "fp32_pipe", "achieved": executed / tally_s / 1e12, "peak": fp32_peak / 1e12,
+                              "unit": "Tpairs/s", "frac": executed / tally_s / fp32_peak,
+                              "peak_source": "SMs x 128 FP32 lanes x the measured SM clock / 2 instructions"},
+                 "same_as_input": bool(torch.equal(d2.view(torch.int32), d.view(torch.int32)))}
+        del tw, d2, ballots
+
     e2e = None
     if not args.no_e2e:
         host_in = torch.empty((C, C), dtype=torch.int32, pin_memory=True)
@@ -346,6 +370,7 @@ def run_ours(args, world, rank, local_rank):
             },
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "tally": tally,
             "clocks": clocks.summary(),
             "gpu_launches": int(L.se_closure_launch_count(C)) * args.steps,
         }
