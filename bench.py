@@ -437,7 +437,7 @@ def run_batch(args, world, rank, local_rank):
         from scalingelections_b200 import autotune
 
         t0 = time.perf_counter()
-        tuned = autotune.tune(V=100000, per_bucket=24, reps=2, path=Path("gpurun_out") / "autotune.json"
+        tuned = autotune.tune(V=100000, per_bucket=32, reps=3, path=Path("gpurun_out") / "autotune.json"
                               if Path("gpurun_out").exists() else None)
         tune_s = time.perf_counter() - t0
         lanes, order, ctas = autotune.choose(tuned, [C for (C, _, _, _) in specs], [V for (_, V, _, _) in specs])
@@ -513,8 +513,8 @@ def run_batch(args, world, rank, local_rank):
             "engine_profile": prof,
             "autotune": None if tuned is None else {
                 "seconds": tune_s, "order": order, "ctas_per_sm": ctas,
-                "buckets": {k: {"C": v["range"], "lanes": v["lanes"], "ctas_per_sm": v["ctas_per_sm"]}
-                            for k, v in tuned["buckets"].items()}},
+                "launch_ms": tuned.get("launch_ms"),
+                "buckets": {k: {"C": v["range"], "lanes": v["lanes"]} for k, v in tuned["buckets"].items()}},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -1,11 +1,15 @@
 """Autotuner for the batched closure.
 
 For each election-size bucket it times, on the GPU, the batched persistent closure of a
-sample batch under every candidate configuration and keeps the fastest:
-  lanes        16-bit (shifted by V // 2 when counts exceed 16 bits) or 32-bit;
-  ctas_per_sm  persistent CTAs per SM (1 or 2 where both fit);
-and, over a mixed sample of all buckets, the queue order (elections of at most 128
-candidates after the tiled ones, or before). The tile (128 x 128 cells) and the register
+sample batch in both lane modes and keeps the faster:
+  lanes        16-bit (shifted by V // 2 when counts exceed 16 bits) or 32-bit.
+Then, over a mixed sample with the same number of elections in every bucket (a log-uniform
+spread of sizes, like a real batch), it times every pair of the settings that belong to the
+whole persistent launch rather than to one election:
+  ctas_per_sm  persistent CTAs per SM (1 or 2);
+  order        elections of at most 128 candidates after the tiled ones, or before.
+A per-bucket CTA count would be tuned on a few elections of one size, where one election's
+chain of pivot rounds dominates, and would not carry over to a mixed launch. The tile (128 x 128 cells) and the register
 micro-tile (8 x 8 words) are fixed: they come from the register and shared-memory budget and
 the measured min/max issue rate. Results are stored as JSON and looked up per election.
 """
@@ -82,20 +86,20 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
             lane_pair = lanes_for_voters(V) if lanes == LANES_U16 else (LANES_U32, 0)
             if lane_pair[0] != lanes:
                 continue
-            for ctas in (1, 2):
-                ms = _time(prefs, [lane_pair] * len(prefs), 0, ctas, reps)
-                results[f"u{lanes}/ctas{ctas}"] = ms
+            results[f"u{lanes}"] = _time(prefs, [lane_pair] * len(prefs), 0, 2, reps)
         best = min(results, key=results.get)
-        table["buckets"][str(b)] = {"range": [lo, hi], "lanes": int(best.split("/")[0][1:]),
-                                    "ctas_per_sm": int(best.split("ctas")[1]), "ms": results}
+        table["buckets"][str(b)] = {"range": [lo, hi], "lanes": int(best[1:]), "ms": results}
         del prefs
     mixed = []
     for b, (lo, hi) in enumerate(BUCKETS[:-1]):
-        mixed += _sample_batch(lo, hi, max(2, per_bucket // (1 + b)), V, seed + 100 + b, device)
-    lanes = [lanes_for_voters(V)] * len(mixed)
-    orders = {o: _time(mixed, lanes, o, 0, reps) for o in (0, 1)}
-    table["order"] = int(min(orders, key=orders.get))
-    table["order_ms"] = {str(k): v for k, v in orders.items()}
+        mixed += _sample_batch(lo, hi, max(2, per_bucket // 2), V, seed + 100 + b, device)
+    lanes = [(LANES_U32, 0) if table["buckets"][str(bucket_of(int(p.shape[0])))]["lanes"] == 32
+             else lanes_for_voters(V) for p in mixed]
+    launch = {(o, c): _time(mixed, lanes, o, c, reps) for o in (0, 1) for c in (1, 2)}
+    order, ctas = min(launch, key=launch.get)
+    table["order"] = int(order)
+    table["ctas_per_sm"] = int(ctas)
+    table["launch_ms"] = {f"order{o}/ctas{c}": v for (o, c), v in launch.items()}
     p = Path(path) if path else default_path()
     p.parent.mkdir(parents=True, exist_ok=True)
     p.write_text(json.dumps(table, indent=1) + "\n")
@@ -109,17 +113,15 @@ def load(path: Path | None = None) -> dict | None:
 
 def choose(table: dict | None, Cs: Sequence[int], Vs: Sequence[int]) -> tuple[list, int, int]:
     """(lanes per election, order, ctas_per_sm) for a batch: per-bucket lane modes from the
-    table (falling back to the widest legal 16-bit window), the table's order, and the CTA
-    count most of the batch's work prefers."""
-    lanes, votes = [], {}
+    table (falling back to the widest legal 16-bit window), and the table's launch settings
+    (0 CTAs per SM, i.e. as many as fit, without a table)."""
+    lanes = []
     for C, V in zip(Cs, Vs):
         entry = (table or {}).get("buckets", {}).get(str(bucket_of(int(C))))
         pair = lanes_for_voters(int(V))
         if entry and entry["lanes"] == 32:
             pair = (LANES_U32, 0)
         lanes.append(pair)
-        if entry:
-            votes[entry["ctas_per_sm"]] = votes.get(entry["ctas_per_sm"], 0.0) + float(C) ** 3
-    ctas = max(votes, key=votes.get) if votes else 0
     order = int((table or {}).get("order", 0))
+    ctas = int((table or {}).get("ctas_per_sm", 0))
     return lanes, order, ctas

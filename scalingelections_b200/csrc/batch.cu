@@ -112,16 +112,9 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
             run_small<LB>(E, smem, rowbuf, colbuf, s_wins, &hdr->err);
         } else if (type == kPivot) {
             run_pivot<LB>(E, int(k), rowbuf, colbuf);
-        } else if (type == kRow) {
-            ok = run_product<LB>(E, &E, int(k), int(k), int(j), false, smem, bars, par_a);
-            par_a ^= 1u;
-        } else if (type == kCol) {
-            ok = run_col<LB>(E, &E, int(k), int(i), smem, bars, par_a, par_b);
-            par_a ^= 1u;
-            par_b ^= 1u;
         } else {
-            ok = run_product<LB>(E, &E, int(k), int(i), int(j), true, smem, bars, par_a);
-            par_a ^= 1u;
+            const int kind = type == kRow ? kTileRow : (type == kCol ? kTileCol : kTileRem);
+            ok = run_tile<LB>(E, &E, kind, int(k), int(i), int(j), smem, bars, par_a, par_b);
         }
         __threadfence();
         __syncthreads();

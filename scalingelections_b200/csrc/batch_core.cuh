@@ -191,97 +191,102 @@ __device__ void run_pivot(const Elec& E, int k, uint32_t (*rowbuf)[cfg<LB>::TW],
     store_transposed_splat<LB>(c, E.dT, kT, g);
 }
 
-// REM (a_panel = true: A = AT[:, I], C = S[I][J]) or ROW (A = dT, C = S[K][J]); B = S[K][J].
+// Tile tasks of one pivot round K, all through one routine:
+//   kTileRow  S[K][J] = max(S[K][J], D (x) S[K][J]):  A = dT, B = S[K][J] (TMA), C = S[K][J]
+//   kTileCol  S[I][K] = max(S[I][K], S[I][K] (x) D):  A = the tile transposed in shared memory,
+//             B = D = S[K][K] (TMA), C = S[I][K]; also emits the transposed panel AT[:, I]
+//   kTileRem  S[I][J] = max(S[I][J], AT[:, I] (x) S[K][J]):  A = AT (TMA), B = S[K][J] (TMA)
+// The (max, min) product, a fully unrolled loop of about 27 KB of code, has a single call site
+// here, so every kind of tile task runs the same instructions: with a copy per kind, the rarely
+// run panel copies missed in the instruction cache and took about 1.5x a remainder tile.
 // E holds the election's scalars (it may be a shared-memory copy); G is the descriptor whose
 // tensor maps the TMA unit reads. GLOBAL_MAPS: G lives in global memory and may have been
 // rewritten since the last launch (batch and serving queues), so each use first acquires the
-// tensor maps; false for a descriptor passed as a kernel parameter.
-template <int LB, bool GLOBAL_MAPS = true>
-__device__ bool run_product(const Elec& E, const Elec* G, int K, int I, int J, bool a_panel, uint8_t* smem,
-                            uint64_t* bars, uint32_t parity) {
-    using CF = cfg<LB>;
-    uint32_t* As = reinterpret_cast<uint32_t*>(smem);
-    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
-    const CUtensorMap* mapA = a_panel ? &G->mapAT : &G->mapDT;
-    if (threadIdx.x == 0) {
-        if constexpr (GLOBAL_MAPS) {
-            fence_tensormap(mapA);
-            fence_tensormap(&G->mapS);
-        }
-        fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
-#pragma unroll
-        for (int c = 0; c < kChunks; ++c) {
-            mbar_arrive_expect_tx(&bars[c], CF::A_BYTES + CF::B_BYTES);
-            tma_load_2d(As + c * CF::A_CHUNK, mapA, &bars[c], a_panel ? I * kT : 0, c * kKC);
-            tma_load_2d(Bs + c * CF::B_CHUNK, &G->mapS, &bars[c], J * CF::TW, K * kT + c * kKC);
-        }
-    }
-    const geom g(threadIdx.x);
-    const int64_t ldw = E.Cp / CF::CPW;
-    uint32_t* Ct = E.S + int64_t(I) * kT * ldw + int64_t(J) * CF::TW;
-    uint32_t c[8][8];
-    load_tile_regs<LB, true>(c, Ct, ldw, g);
-    bool ok = true;
-#pragma unroll 1
-    for (int ch = 0; ch < kChunks; ++ch) {
-        if (!mbar_wait_bounded(&bars[ch], parity, 1u << 26)) {
-            ok = false;
-            break;
-        }
-        relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
-    }
-    if (ok) store_tile_regs<LB>(c, Ct, ldw, g);
-    return ok;
-}
+// tensor maps; false for a descriptor passed as a kernel parameter. bars[0, 4) use parity
+// par_a, bars[4, 8) par_b; both are advanced here.
+constexpr int kTileRow = 0;
+constexpr int kTileCol = 1;
+constexpr int kTileRem = 2;
 
 template <int LB, bool GLOBAL_MAPS = true>
-__device__ bool run_col(const Elec& E, const Elec* G, int K, int I, uint8_t* smem, uint64_t* bars,
-                        uint32_t parity_a, uint32_t parity_b) {
+__device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
+                         uint32_t& par_a, uint32_t& par_b) {
     using CF = cfg<LB>;
     constexpr int TW = CF::TW;
-    uint32_t* As = reinterpret_cast<uint32_t*>(smem);                          // [kT][kT]
-    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);     // tile, then D
-    if (threadIdx.x == 0) {
-        if constexpr (GLOBAL_MAPS) fence_tensormap(&G->mapS);
-        fence_proxy_async();
-#pragma unroll
-        for (int c = 0; c < kChunks; ++c) {
-            mbar_arrive_expect_tx(&bars[c], CF::B_BYTES);
-            tma_load_2d(Bs + c * CF::B_CHUNK, &G->mapS, &bars[c], K * TW, I * kT + c * kKC);
-        }
-    }
-    bool ok = true;
-#pragma unroll 1
-    for (int c = 0; c < kChunks; ++c) ok = ok && mbar_wait_bounded(&bars[c], parity_a, 1u << 26);
+    uint32_t* As = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
     const geom g(threadIdx.x);
+    const int64_t ldw = E.Cp / CF::CPW;
     uint32_t c[8][8];
-    if (ok) {
-        constexpr int HALVES = CF::THREADS / kT;
-        constexpr int SPAN = TW / HALVES;
-        const int i = threadIdx.x % kT;
-        const int half = threadIdx.x / kT;
+    bool ok = true;
+    uint64_t* wait_bars = bars;  // the product's chunk barriers and their parity
+    uint32_t wait_par = par_a;
+    uint32_t* Ct;
+    if (kind != kTileCol) {
+        const bool rem = kind == kTileRem;
+        const CUtensorMap* mapA = rem ? &G->mapAT : &G->mapDT;
+        if (threadIdx.x == 0) {
+            if constexpr (GLOBAL_MAPS) {
+                fence_tensormap(mapA);
+                fence_tensormap(&G->mapS);
+            }
+            fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
+#pragma unroll
+            for (int ch = 0; ch < kChunks; ++ch) {
+                mbar_arrive_expect_tx(&bars[ch], CF::A_BYTES + CF::B_BYTES);
+                tma_load_2d(As + ch * CF::A_CHUNK, mapA, &bars[ch], rem ? I * kT : 0, ch * kKC);
+                tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[ch], J * TW, K * kT + ch * kKC);
+            }
+        }
+        Ct = E.S + int64_t(rem ? I : K) * kT * ldw + int64_t(J) * TW;
+        load_tile_regs<LB, true>(c, Ct, ldw, g);
+        par_a ^= 1u;
+    } else {
+        // The tile itself into Bs, transposed and duplicated into As; then D into Bs.
+        if (threadIdx.x == 0) {
+            if constexpr (GLOBAL_MAPS) fence_tensormap(&G->mapS);
+            fence_proxy_async();
+#pragma unroll
+            for (int ch = 0; ch < kChunks; ++ch) {
+                mbar_arrive_expect_tx(&bars[ch], CF::B_BYTES);
+                tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[ch], K * TW, I * kT + ch * kKC);
+            }
+        }
+#pragma unroll 1
+        for (int ch = 0; ch < kChunks; ++ch) ok = ok && mbar_wait_bounded(&bars[ch], par_a, 1u << 26);
+        if (ok) {
+            constexpr int HALVES = CF::THREADS / kT;
+            constexpr int SPAN = TW / HALVES;
+            const int i = threadIdx.x % kT;
+            const int half = threadIdx.x / kT;
 #pragma unroll 4
-        for (int s = 0; s < SPAN; ++s) {
-            const int w = half * SPAN + ((s + i) & (SPAN - 1));
-            const uint32_t word = Bs[i * TW + w];
+            for (int s = 0; s < SPAN; ++s) {
+                const int w = half * SPAN + ((s + i) & (SPAN - 1));
+                const uint32_t word = Bs[i * TW + w];
 #pragma unroll
-            for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
+                for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
+            }
+            load_tile_regs<LB>(c, Bs, TW, g);
         }
-        load_tile_regs<LB>(c, Bs, TW, g);
-    }
-    __syncthreads();  // the tile region is free again
-    if (threadIdx.x == 0 && ok) {
-        fence_proxy_async();
+        __syncthreads();  // the tile region is free again
+        if (threadIdx.x == 0 && ok) {
+            fence_proxy_async();
 #pragma unroll
-        for (int ch = 0; ch < kChunks; ++ch) {
-            mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
-            tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[kChunks + ch], K * TW, K * kT + ch * kKC);
+            for (int ch = 0; ch < kChunks; ++ch) {
+                mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
+                tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[kChunks + ch], K * TW, K * kT + ch * kKC);
+            }
         }
+        Ct = E.S + int64_t(I) * kT * ldw + int64_t(K) * TW;
+        wait_bars = bars + kChunks;
+        wait_par = par_b;
+        par_a ^= 1u;
+        par_b ^= 1u;
     }
     if (ok) {
 #pragma unroll 1
         for (int ch = 0; ch < kChunks; ++ch) {
-            if (!mbar_wait_bounded(&bars[kChunks + ch], parity_b, 1u << 26)) {
+            if (!mbar_wait_bounded(&wait_bars[ch], wait_par, 1u << 26)) {
                 ok = false;
                 break;
             }
@@ -289,9 +294,8 @@ __device__ bool run_col(const Elec& E, const Elec* G, int K, int I, uint8_t* sme
         }
     }
     if (ok) {
-        const int64_t ldw = E.Cp / CF::CPW;
-        store_tile_regs<LB>(c, E.S + int64_t(I) * kT * ldw + int64_t(K) * TW, ldw, g);
-        store_transposed_splat<LB>(c, E.AT + int64_t(I) * kT, E.Cp, g);
+        store_tile_regs<LB>(c, Ct, ldw, g);
+        if (kind == kTileCol) store_transposed_splat<LB>(c, E.AT + int64_t(I) * kT, E.Cp, g);
     }
     return ok;
 }

@@ -65,8 +65,11 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     const int R1 = E.R - 1;
     const int b = blockIdx.x;
     bool ok;
-    if (b < R1) ok = batch::run_product<LB, false>(E, &E, K, K, b + (b >= K), false, smem, bars, 0);
-    else ok = batch::run_col<LB, false>(E, &E, K, (b - R1) + ((b - R1) >= K), smem, bars, 0, 0);
+    uint32_t par_a = 0, par_b = 0;
+    const bool row = b < R1;
+    const int x = row ? b : b - R1;
+    ok = batch::run_tile<LB, false>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K), x + (x >= K),
+                                    smem, bars, par_a, par_b);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -96,7 +99,9 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         t = t == 0 ? p : (t == p ? 0 : t);
     }
     const int ii = t / R1, jj = t % R1;
-    const bool ok = batch::run_product<LB, false>(E, &E, K, ii + (ii >= K), jj + (jj >= K), true, smem, bars, 0);
+    uint32_t par_a = 0, par_b = 0;
+    const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, ii + (ii >= K), jj + (jj >= K), smem, bars,
+                                               par_a, par_b);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
@@ -332,16 +337,9 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         bool ok = true;
         if (T.kind == 0) {
             batch::run_pivot<LB>(E, T.k, rowbuf, colbuf);
-        } else if (T.kind == 1) {
-            ok = batch::run_product<LB, false>(E, &E, T.k, T.k, T.j, false, smem, bars, par_a);
-            par_a ^= 1u;
-        } else if (T.kind == 2) {
-            ok = batch::run_col<LB, false>(E, &E, T.k, T.i, smem, bars, par_a, par_b);
-            par_a ^= 1u;
-            par_b ^= 1u;
         } else {
-            ok = batch::run_product<LB, false>(E, &E, T.k, T.i, T.j, true, smem, bars, par_a);
-            par_a ^= 1u;
+            const int kind = T.kind == 1 ? batch::kTileRow : (T.kind == 2 ? batch::kTileCol : batch::kTileRem);
+            ok = batch::run_tile<LB, false>(E, &E, kind, T.k, T.i, T.j, smem, bars, par_a, par_b);
         }
         __threadfence();
         __syncthreads();

@@ -536,22 +536,23 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                 const int k = g / 3, kind = g % 3;
                 if (kind == 0) {
                     run_pivot<16>(E, k, rowbuf, colbuf);
-                } else if (kind == 1) {
-                    const int R1 = R - 1;
-                    if (int(t) < R1) {
-                        ok = run_product<16>(E, G, k, k, int(t) + (int(t) >= k), false, smem, bars, par_a);
-                        par_a ^= 1u;
-                    } else {
-                        const int x = int(t) - R1;
-                        ok = run_col<16>(E, G, k, x + (x >= k), smem, bars, par_a, par_b);
-                        par_a ^= 1u;
-                        par_b ^= 1u;
-                    }
                 } else {
+                    // Panels (row panels first, then column panels) or remainder: one tile task.
                     const int R1 = R - 1;
-                    const int ii = int(t) / R1, jj = int(t) % R1;
-                    ok = run_product<16>(E, G, k, ii + (ii >= k), jj + (jj >= k), true, smem, bars, par_a);
-                    par_a ^= 1u;
+                    int tk, ii, jj;
+                    if (kind == 1) {
+                        const bool row = int(t) < R1;
+                        const int x = row ? int(t) : int(t) - R1;
+                        tk = row ? kTileRow : kTileCol;
+                        ii = jj = x + (x >= k);
+                    } else {
+                        tk = kTileRem;
+                        ii = int(t) / R1;
+                        jj = int(t) % R1;
+                        ii += ii >= k;
+                        jj += jj >= k;
+                    }
+                    ok = run_tile<16>(E, G, tk, k, ii, jj, smem, bars, par_a, par_b);
                 }
             } else if (g == 3 * R) {
                 int rem = int(t), I = 0;

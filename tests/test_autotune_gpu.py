@@ -1,5 +1,5 @@
-"""The batched-closure autotuner measures every candidate and its choices drive a batch that
-stays bit-exact."""
+"""The batched-closure autotuner measures every candidate (lane mode per size bucket; CTAs per
+SM and queue order for the whole launch) and its choices drive a batch that stays bit-exact."""
 import numpy as np
 import pytest
 import torch
@@ -15,8 +15,10 @@ def test_autotune_table_and_choice(tmp_path):
     assert autotune.load(tmp_path / "t.json") == table
     assert set(table["buckets"]) == {str(b) for b in range(len(autotune.BUCKETS))}
     for entry in table["buckets"].values():
-        assert entry["lanes"] in (16, 32) and entry["ctas_per_sm"] in (1, 2)
+        assert entry["lanes"] in (16, 32)
         assert all(ms > 0 for ms in entry["ms"].values())
+    assert table["ctas_per_sm"] in (1, 2) and table["order"] in (0, 1)
+    assert len(table["launch_ms"]) == 4 and all(ms > 0 for ms in table["launch_ms"].values())
     Cs, Vs = [5, 100, 300, 700], [40, 2000, 70000, 90000]
     lanes, order, ctas = autotune.choose(table, Cs, Vs)
     rng = np.random.default_rng(0)
