@@ -109,6 +109,35 @@ def test_closure_c16384_rows_by_dijkstra(orc):
     assert not np.diagonal(S_h).any()
 
 
+def test_closure_c32768_properties(orc):
+    """The largest headline size, C=32768 (Mallows phi=0.8, V=4096; a 4 GiB preference
+    matrix): 16-bit and 32-bit lanes agree bit for bit, two rows match the independent
+    bottleneck Dijkstra exactly, S dominates its defeat matrix, the diagonal is 0, and the
+    ranking from S equals the oracle's ranking rule applied to the same S."""
+    from scalingelections_b200.ballots import mallows_ballots_device
+
+    C, V = 32768, 4096
+    ids = mallows_ballots_device(V, C, 0.8, seed=3).view(-1)
+    offs = torch.arange(V + 1, dtype=torch.int64, device="cuda") * C
+    d = api.tally_device(ids, offs, C)
+    del ids
+    S = api.strongest_paths_device(d, lanes=LANES_U16)
+    S32 = api.strongest_paths_device(d, lanes=LANES_U32)
+    assert torch.equal(S.view(torch.int32), S32.view(torch.int32))
+    del S32
+    wins, ranking = api.rank_device(S)
+    d_h = api._to_host_u32(d)
+    del d
+    S_h = api._to_host_u32(S)
+    rows = [5, C - 2]
+    assert np.array_equal(S_h[rows], orc.widest_rows(d_h, rows))
+    assert (S_h >= orc.defeats(d_h)).all()
+    assert not np.diagonal(S_h).any()
+    w_ref, r_ref = orc.wins_and_ranking(S_h)
+    assert np.array_equal(wins.cpu().numpy(), w_ref)
+    assert np.array_equal(ranking.cpu().numpy(), r_ref)
+
+
 def test_shifted_16_bit_lanes_for_large_counts(orc):
     """Kept values in a window [70001, 130000] exceed 16 bits but span less than 65535: the
     automatic mode closes them in shifted 16-bit lanes, bit-identical to 32-bit lanes."""

@@ -70,6 +70,15 @@ def test_speed_against_reference_kernels(ref_gpu):
         ours = api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
         runs.append(time.perf_counter() - t0)
     ours_s = min(runs)
+    # The reference's own tile sweep on the same input (its GPU tiles are 4, 8, 16 or 32 cells;
+    # this closure always uses 128): one timed call each after the warm-up above.
+    sweep = {}
+    for tile in (8, 16):
+        t0 = time.perf_counter()
+        r = ref_gpu.compute_strongest_paths(P, allow_gpu=True, allow_tma=False, tile_size=tile)
+        sweep[tile] = time.perf_counter() - t0
+        assert np.array_equal(r, ref_out)
+    sweep[32] = ref_s
     d = api._to_device_u32(P, torch.device("cuda"))
     out = torch.empty_like(d)
     api.strongest_paths_device(d, out=out)
@@ -86,6 +95,7 @@ def test_speed_against_reference_kernels(ref_gpu):
             "ours_host_api_s": ours_s, "ours_host_api_gcells_s": C ** 3 / ours_s / 1e9,
             "ours_device_s": device_s, "ours_device_gcells_s": C ** 3 / device_s / 1e9,
             "speedup_host_api": ref_s / ours_s, "bit_identical": True,
+            "reference_tile_sweep_s": {str(k): v for k, v in sorted(sweep.items())},
             "reference_call": "compute_strongest_paths(P, allow_gpu=True, allow_tma=False, tile_size=32)"}
     out_dir = os.environ.get("SE_REPORT_DIR")
     if out_dir:
