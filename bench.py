@@ -207,7 +207,7 @@ def load_traffic(lanes: int, C: int):
     kernel's traffic is proportional to the tiles it processes)."""
     import re
 
-    p = ROOT / "profiles" / "closure_tile_kernel_u16_c12288.md"
+    p = ROOT / "profiles" / "closure_rem_kernel_u16_c12288.md"
     if not p.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch: u(\d+) C=(\d+) (\d+)", p.read_text())
@@ -357,7 +357,7 @@ def run_ours(args, world, rank, local_rank):
             "config": config(args, world),
             "roofline": {
                 "bound": "int_minmax",
-                "kernel": f"closure remainder tile_kernel<u{lanes or 16}>",
+                "kernel": f"closure remainder rem_kernel<u{lanes or 16}>",
                 "achieved": achieved / 1e12, "peak": peak_relax_per_s / 1e12, "unit": "Trelax/s",
                 "frac": achieved / peak_relax_per_s,
                 "peak_source": f"measured: se_minmax_peak recipe {recipe} in this run "
