@@ -150,7 +150,9 @@ __device__ __forceinline__ int find_owner(const int64_t* prefix, int n, int64_t 
 }
 
 // Defeat matrix into the padded working matrix (see init_kernel in closure.cu); also zeroes
-// the election's wins.
+// the election's wins. One CTA per 128 x 128 tile (I, J), walking its 16 blocks of 32 x 32:
+// the owner lookup (a binary search over the elections) is paid once per 16 blocks, which
+// with one CTA per block made the kernel latency-bound.
 __global__ void __launch_bounds__(256)
     batch_init_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big, const int64_t* __restrict__ prefix,
                       int nbig, Header* __restrict__ hdr) {
@@ -159,35 +161,43 @@ __global__ void __launch_bounds__(256)
     const int m = find_owner(prefix, nbig, b);
     const Elec& E = elecs[big[m]];
     const int64_t local = b - prefix[m];
-    const int nb = E.Cp / 32;
-    const int bx = int(local % nb) * 32, by = int(local / nb) * 32;
+    const int R = E.Cp / kT;
+    const int TI = int(local / R), TJ = int(local % R);
     const int C = E.C;
+    const bool u16 = E.lanes == 16;
     if (local == 0 && E.wins)
         for (int x = threadIdx.y * 32 + threadIdx.x; x < C; x += 256) E.wins[x] = 0;
-    for (int y = threadIdx.y; y < 32; y += 8) {
-        const int r = bx + y, cc = by + threadIdx.x;
-        t[threadIdx.x][y] = (r < C && cc < C) ? E.d[int64_t(r) * E.ld + cc] : 0u;
-    }
-    __syncthreads();
     bool over = false;
-    for (int y = threadIdx.y; y < 32; y += 8) {
-        const int i = by + y, j = bx + threadIdx.x;
-        uint32_t v = 0;
-        if (i < C && j < C && i != j) {
-            const uint32_t dij = E.d[int64_t(i) * E.ld + j];
-            const uint32_t dji = t[y][threadIdx.x];
-            v = dij > dji ? dij : 0u;
+#pragma unroll 1
+    for (int sub = 0; sub < 16; ++sub) {
+        const int by = TI * kT + (sub >> 2) * 32, bx = TJ * kT + (sub & 3) * 32;
+        if (sub) __syncthreads();  // t is free again
+        for (int y = threadIdx.y; y < 32; y += 8) {
+            const int r = bx + y, cc = by + threadIdx.x;
+            t[threadIdx.x][y] = (r < C && cc < C) ? E.d[int64_t(r) * E.ld + cc] : 0u;
         }
-        if (E.lanes == 16) {
-            reinterpret_cast<uint16_t*>(E.S)[int64_t(i) * E.Cp + j] = uint16_t(to_lane16(v, E.base, over));
-        } else {
-            E.S[int64_t(i) * E.Cp + j] = v;
+        __syncthreads();
+        for (int y = threadIdx.y; y < 32; y += 8) {
+            const int i = by + y, j = bx + threadIdx.x;
+            uint32_t v = 0;
+            if (i < C && j < C && i != j) {
+                const uint32_t dij = E.d[int64_t(i) * E.ld + j];
+                const uint32_t dji = t[y][threadIdx.x];
+                v = dij > dji ? dij : 0u;
+            }
+            if (u16) {
+                reinterpret_cast<uint16_t*>(E.S)[int64_t(i) * E.Cp + j] = uint16_t(to_lane16(v, E.base, over));
+            } else {
+                E.S[int64_t(i) * E.Cp + j] = v;
+            }
         }
     }
     if (over) raise_device_error(&hdr->err, kErrOverflow);
 }
 
-// Output (u32, zero diagonal) and wins, one unordered pair of 32 x 32 blocks per CTA.
+// Output (u32, zero diagonal) and wins. One CTA per unordered pair of 128 x 128 tiles
+// (I <= J), walking its pairs of 32 x 32 blocks (16, or 10 on the diagonal); blocks past C
+// are skipped.
 __global__ void __launch_bounds__(256)
     batch_finalize_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
                           const int64_t* __restrict__ prefix, int nbig) {
@@ -197,46 +207,53 @@ __global__ void __launch_bounds__(256)
     const int m = find_owner(prefix, nbig, b);
     const Elec& E = elecs[big[m]];
     int64_t local = b - prefix[m];
-    const int C = E.C, nb = (C + 31) / 32;
-    int bi = 0;
-    while (local >= nb - bi) {
-        local -= nb - bi;
-        ++bi;
+    const int C = E.C, R = E.Cp / kT;
+    int TI = 0;
+    while (local >= R - TI) {
+        local -= R - TI;
+        ++TI;
     }
-    const int bj = bi + int(local);
+    const int TJ = TI + int(local);
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool u16 = E.lanes == 16;
     auto cell = [&](int r, int c) -> uint32_t {
-        if (E.lanes == 16) {
+        if (u16) {
             const uint32_t v = reinterpret_cast<const uint16_t*>(E.S)[int64_t(r) * E.Cp + c];
             return v ? v + E.base : 0u;
         }
         return E.S[int64_t(r) * E.Cp + c];
     };
-    if (ty == 0) wi[tx] = 0, wj[tx] = 0;
-    for (int y = ty; y < 32; y += 8) {
-        const int r = bj * 32 + y, c = bi * 32 + tx;
-        const uint32_t v = (r < C && c < C) ? cell(r, c) : 0u;
-        tJI[tx][y] = v;
-        if (r < C && c < C && bi != bj) E.out[int64_t(r) * E.ld_out + c] = v;
-    }
-    __syncthreads();
-    for (int y = ty; y < 32; y += 8) {
-        const int i = bi * 32 + y, j = bj * 32 + tx;
-        if (i < C && j < C) {
-            const uint32_t sij = cell(i, j);
-            E.out[int64_t(i) * E.ld_out + j] = i == j ? 0u : sij;
-            if (E.wins && (bi != bj || j > i)) {
-                const uint32_t sji = tJI[y][tx];
-                if (sij > sji) atomicAdd(&wi[y], 1);
-                else if (sji > sij) atomicAdd(&wj[tx], 1);
+#pragma unroll 1
+    for (int sub = 0; sub < 16; ++sub) {
+        const int bi = TI * 4 + (sub >> 2), bj = TJ * 4 + (sub & 3);
+        if (bi > bj || bi * 32 >= C || bj * 32 >= C) continue;  // CTA-uniform
+        __syncthreads();  // tJI, wi and wj are free again
+        if (ty == 0) wi[tx] = 0, wj[tx] = 0;
+        for (int y = ty; y < 32; y += 8) {
+            const int r = bj * 32 + y, c = bi * 32 + tx;
+            const uint32_t v = (r < C && c < C) ? cell(r, c) : 0u;
+            tJI[tx][y] = v;
+            if (r < C && c < C && bi != bj) E.out[int64_t(r) * E.ld_out + c] = v;
+        }
+        __syncthreads();
+        for (int y = ty; y < 32; y += 8) {
+            const int i = bi * 32 + y, j = bj * 32 + tx;
+            if (i < C && j < C) {
+                const uint32_t sij = cell(i, j);
+                E.out[int64_t(i) * E.ld_out + j] = i == j ? 0u : sij;
+                if (E.wins && (bi != bj || j > i)) {
+                    const uint32_t sji = tJI[y][tx];
+                    if (sij > sji) atomicAdd(&wi[y], 1);
+                    else if (sji > sij) atomicAdd(&wj[tx], 1);
+                }
             }
         }
-    }
-    __syncthreads();
-    if (ty == 0 && E.wins) {
-        const int i = bi * 32 + tx, j = bj * 32 + tx;
-        if (i < C && wi[tx]) atomicAdd(&E.wins[i], wi[tx]);
-        if (j < C && wj[tx]) atomicAdd(&E.wins[j], wj[tx]);
+        __syncthreads();
+        if (ty == 0 && E.wins) {
+            const int i = bi * 32 + tx, j = bj * 32 + tx;
+            if (i < C && wi[tx]) atomicAdd(&E.wins[i], wi[tx]);
+            if (j < C && wj[tx]) atomicAdd(&E.wins[j], wj[tx]);
+        }
     }
 }
 
@@ -510,9 +527,9 @@ extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_
     std::vector<int64_t> ip(big.size() + 1, 0), fp(big.size() + 1, 0), pp(big.size() + 1, 0);
     for (size_t m = 0; m < big.size(); ++m) {
         const Elec& E = host[big[m]];
-        const int64_t nb32 = E.Cp / 32, nbc = (E.C + 31) / 32;
-        ip[m + 1] = ip[m] + nb32 * nb32;
-        fp[m + 1] = fp[m] + nbc * (nbc + 1) / 2;
+        const int64_t R = E.Cp / kT;  // tiles per side: init takes one CTA per tile, finalize one per pair
+        ip[m + 1] = ip[m] + R * R;
+        fp[m + 1] = fp[m] + R * (R + 1) / 2;
         pp[m + 1] = pp[m] + (E.C + 255) / 256;
     }
     // Upload (synchronous).
