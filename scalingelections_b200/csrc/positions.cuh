@@ -1,0 +1,64 @@
+// Places of the candidates on one ballot, computed by one warp: the first step of the tally
+// (build_pairwise_preferences, scaling_elections.py:51-88), shared by the tally kernels
+// (tally.cu) and the serving engine's POS tasks (serve.cu).
+//
+// p[c] = place of candidate c on ballot r[0 .. len), as f32 (exact integers), for c < C; the
+// padding p[C .. Cq) is 0. A ballot that omits candidates is completed by the reference's
+// rule: the missing ids take places len, len + 1, ... in ascending id order (py:75-83). Every
+// step is a warp-strided loop with warp barriers only, so a CTA works on several ballots at once
+// (one per warp) and keeps many loads in flight. A complete ballot (len == C) needs no
+// initialisation pass: its scatter writes every place once, and a repeated id (the only way a
+// valid-looking complete ballot can miss a candidate) is caught by the check.
+#pragma once
+
+#include <stdint.h>
+
+namespace se {
+
+constexpr int kPosOk = 0;
+constexpr int kPosRange = 2;   // an id outside [0, C)
+constexpr int kPosRepeat = 3;  // the same id twice
+
+// COHERENT: read the ballot and the places through L2 (ld.global.cg). A persistent kernel needs
+// this: its SM's L1 may still hold lines of an earlier request that used the same addresses.
+template <bool COHERENT, typename T>
+__device__ __forceinline__ T pos_load(const T* p) {
+    if constexpr (COHERENT) return __ldcg(p);
+    else return *p;
+}
+
+template <typename Id, bool COHERENT = false>
+__device__ __forceinline__ int warp_positions(const Id* __restrict__ r, int64_t len, int C, int64_t Cq,
+                                              float* __restrict__ p) {
+    const int lane = threadIdx.x & 31;
+    const bool complete = len >= C;
+    for (int64_t c = complete ? C + lane : lane; c < Cq; c += 32) p[c] = c < C ? -1.0f : 0.0f;
+    __syncwarp();
+    int bad = 0;
+#pragma unroll 4
+    for (int64_t a = lane; a < len; a += 32) {
+        const int64_t id = int64_t(pos_load<COHERENT>(r + a));
+        if (id < 0 || id >= C) bad = 1;
+        else p[id] = float(a);
+    }
+    if (__any_sync(0xffffffffu, bad)) return kPosRange;
+    __syncwarp();  // the scatter's stores are visible to the whole warp
+#pragma unroll 4
+    for (int64_t a = lane; a < len; a += 32)
+        if (pos_load<COHERENT>(p + int64_t(pos_load<COHERENT>(r + a))) != float(a))
+            bad = 1;  // a repeated id left at most one of its places
+    if (__any_sync(0xffffffffu, bad)) return kPosRepeat;
+    if (complete) return kPosOk;
+    // Missing ids (still -1) in ascending order: a ballot-and-popcount scan, 32 candidates a step.
+    int64_t base = len;
+    for (int64_t c0 = 0; c0 < C; c0 += 32) {
+        const int64_t c = c0 + lane;
+        const bool miss = c < C && pos_load<COHERENT>(p + c) < 0.0f;
+        const uint32_t m = __ballot_sync(0xffffffffu, miss);
+        if (miss) p[c] = float(base + __popc(m & ((1u << lane) - 1u)));
+        base += __popc(m);
+    }
+    return kPosOk;
+}
+
+}  // namespace se

@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "batch_core.cuh"
+#include "positions.cuh"
 
 namespace se {
 namespace serve {
@@ -101,10 +102,16 @@ __device__ __forceinline__ uint64_t ld_acquire64(const uint64_t* p) {
     return v;
 }
 
-// Claims the next task of slot s (generation gen); returns the phase and index, or false.
+__host__ __device__ inline bool is_remainder_phase(int R, int f) { return R > 1 && f >= 2 && f - 2 < 3 * R && (f - 2) % 3 == 2; }
+
+// Claims the next task of slot s (generation gen); returns the phase, the first index and how
+// many consecutive tasks were taken (two remainder tiles at a time while two are left: the
+// claim costs several L2 round trips, a remainder tile about 20 µs), or false.
 // claims[0] = front (gen << 32 | phase), claims[1 + f] = gen << 32 | next index of phase f.
+constexpr uint32_t kRemPerClaim = 2;
+
 __device__ bool try_claim(uint64_t* claims, const uint32_t* dones, uint32_t gen, int R, int64_t V, int& f_out,
-                          uint32_t& t_out) {
+                          uint32_t& t_out, uint32_t& cnt_out) {
     const int nph = phases_of(R);
     for (int attempt = 0; attempt < 8; ++attempt) {
         const uint64_t fr = ld_acquire64(&claims[0]);
@@ -123,13 +130,15 @@ __device__ bool try_claim(uint64_t* claims, const uint32_t* dones, uint32_t gen,
                       (unsigned long long)(fr + 1));
             continue;
         }
+        const uint32_t take = is_remainder_phase(R, f) && size - n >= kRemPerClaim ? kRemPerClaim : 1u;
         if (atomicCAS(reinterpret_cast<unsigned long long*>(&claims[1 + f]), (unsigned long long)c,
-                      (unsigned long long)(c + 1)) == (unsigned long long)c) {
-            if (n + 1 == size)
+                      (unsigned long long)(c + take)) == (unsigned long long)c) {
+            if (n + take == size)
                 atomicCAS(reinterpret_cast<unsigned long long*>(&claims[0]), (unsigned long long)fr,
                           (unsigned long long)(fr + 1));
             f_out = f;
             t_out = n;
+            cnt_out = take;
             return true;
         }
     }
@@ -159,7 +168,7 @@ __device__ bool claimable(uint64_t* claims, const uint32_t* dones, uint32_t gen,
 constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 
 __device__ uint32_t warp_find_task(Req* slots, uint64_t* claims, const uint32_t* dones, uint32_t hi, bool& any_active,
-                                   int& f_out, uint32_t& t_out) {
+                                   int& f_out, uint32_t& t_out, uint32_t& cnt_out) {
     const int lane = threadIdx.x & 31;
     for (uint32_t s0 = 0; s0 < hi; s0 += 32) {
         const uint32_t s = s0 + lane;
@@ -179,14 +188,16 @@ __device__ uint32_t warp_find_task(Req* slots, uint64_t* claims, const uint32_t*
         while (mask) {
             const int l = __ffs(mask) - 1;
             int f = 0;
-            uint32_t t = 0;
+            uint32_t t = 0, cnt = 0;
             int got = 0;
             if (lane == l)
-                got = try_claim(claims + size_t(s) * (kMaxPhases + 1), dones + size_t(s) * kMaxPhases, gen, R, V, f, t);
+                got = try_claim(claims + size_t(s) * (kMaxPhases + 1), dones + size_t(s) * kMaxPhases, gen, R, V, f, t,
+                                cnt);
             got = __shfl_sync(0xffffffffu, got, l);
             if (got) {
                 f_out = __shfl_sync(0xffffffffu, f, l);
                 t_out = __shfl_sync(0xffffffffu, t, l);
+                cnt_out = __shfl_sync(0xffffffffu, cnt, l);
                 return s0 + l;
             }
             mask &= mask - 1;
@@ -272,52 +283,13 @@ __device__ void run_place(const Elec& E, uint8_t* smem) {
 // order (the reference's completion rule, scaling_elections.py:75-83). Out-of-range or repeated
 // ids set the request's ballot error word.
 // ------------------------------------------------------------------------------------------
-__device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v1, uint8_t* smem) {
-    uint32_t* warp_sums = reinterpret_cast<uint32_t*>(smem);
-    int* bad = reinterpret_cast<int*>(smem + 64);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int64_t v = v0; v < v1; ++v) {
-        float* p = Q.pos + v * Cq;
+__device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v1) {
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int64_t v = v0 + warp; v < v1; v += nw) {  // one ballot per warp at a time
         const int64_t beg = Q.offsets ? __ldcg(Q.offsets + v) : v * C;
         const int64_t len = Q.offsets ? __ldcg(Q.offsets + v + 1) - beg : C;
-        const int32_t* r = Q.ids + beg;
-        if (threadIdx.x == 0) *bad = 0;
-        for (int c = threadIdx.x; c < Cq; c += blockDim.x) p[c] = c < C ? -1.0f : 0.0f;
-        __syncthreads();
-        for (int64_t x = threadIdx.x; x < len; x += blockDim.x) {
-            const int32_t id = __ldcg(r + x);
-            if (id < 0 || id >= C) {
-                atomicCAS(&Q.flags[0], 0u, 2u);
-                *bad = 1;
-            } else {
-                p[id] = float(x);
-            }
-        }
-        __syncthreads();
-        if (*bad) continue;
-        for (int64_t x = threadIdx.x; x < len; x += blockDim.x)
-            if (p[__ldcg(r + x)] != float(x)) {
-                atomicCAS(&Q.flags[0], 0u, 3u);
-                *bad = 1;
-            }
-        __syncthreads();
-        if (*bad || len >= C) continue;
-        int64_t base = len;
-        for (int c0 = 0; c0 < C; c0 += blockDim.x) {
-            const int c = c0 + threadIdx.x;
-            const bool miss = c < C && p[c] < 0.0f;
-            const uint32_t ballot = __ballot_sync(0xffffffffu, miss);
-            if (lane == 0) warp_sums[warp] = __popc(ballot);
-            __syncthreads();
-            uint32_t before = __popc(ballot & ((1u << lane) - 1u)), total = 0;
-            for (int w = 0; w < nw; ++w) {
-                before += w < warp ? warp_sums[w] : 0u;
-                total += warp_sums[w];
-            }
-            if (miss) p[c] = float(base + before);
-            base += total;
-            __syncthreads();
-        }
+        const int code = warp_positions<int32_t, true>(Q.ids + beg, len, C, Cq, Q.pos + v * Cq);
+        if (code != kPosOk && (threadIdx.x & 31) == 0) atomicCAS(&Q.flags[0], 0u, uint32_t(code));
     }
 }
 
@@ -437,7 +409,7 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
     __shared__ __align__(16) uint32_t colbuf[2][kT];
     __shared__ int32_t s_wins[kT];
     __shared__ __align__(64) Req s_q;
-    __shared__ uint32_t s_slot, s_t;
+    __shared__ uint32_t s_slot, s_t, s_cnt;
     __shared__ int s_f;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + pcfg<16>::DATA);  // [0,8) closure, [8,11) tally
     if (threadIdx.x == 0) {
@@ -446,12 +418,34 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
     }
     __syncthreads();
     uint32_t par_a = 0, par_b = 0, tpar = 0;
+    // The slot of the CTA's last task, whose descriptor is still in s_q: tried first, before
+    // the ordered scan, because a request in a bulk phase (places, tally, remainder) usually
+    // has more of it. Its claim counters carry the generation, so a slot reused by another
+    // request fails this claim and the scan takes over.
+    uint32_t last_slot = kNoSlot;
 
     for (;;) {
         uint64_t t_task = 0;
         if (threadIdx.x < 32) {
             uint32_t got = kNoSlot;
+            bool fresh = true;  // the claimed slot's descriptor must be (re)loaded
             const uint64_t t0 = global_ns();
+            if (last_slot != kNoSlot) {
+                int ok_claim = 0, f = 0;
+                uint32_t t = 0, cnt = 0;
+                if (threadIdx.x == 0 && !ld_acquire(&hdr->stop) && !ld_acquire(&hdr->err))
+                    ok_claim = try_claim(claims + size_t(last_slot) * (kMaxPhases + 1),
+                                         dones + size_t(last_slot) * kMaxPhases, s_q.gen, s_q.e.R, s_q.V, f, t, cnt);
+                if (__shfl_sync(0xffffffffu, ok_claim, 0)) {
+                    got = last_slot;
+                    fresh = false;
+                    if (threadIdx.x == 0) {
+                        s_f = f;
+                        s_t = t;
+                        s_cnt = cnt;
+                    }
+                }
+            }
             while (got == kNoSlot) {
                 int stop = 0;
                 if (threadIdx.x == 0)
@@ -461,11 +455,12 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                 hi = __shfl_sync(0xffffffffu, hi, 0);
                 bool any_active = false;
                 int f = 0;
-                uint32_t t = 0;
-                got = warp_find_task(slots, claims, dones, hi, any_active, f, t);
+                uint32_t t = 0, cnt = 0;
+                got = warp_find_task(slots, claims, dones, hi, any_active, f, t, cnt);
                 if (got != kNoSlot && threadIdx.x == 0) {
                     s_f = f;
                     s_t = t;
+                    s_cnt = cnt;
                 }
                 if (got == kNoSlot) {
                     // With no active request the CTA leaves after idle_ns (the host relaunches
@@ -495,12 +490,17 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                 t_task = global_ns();
                 atomicAdd(&hdr->search_ns, (unsigned long long)(t_task - t0));
             }
+            last_slot = got;
             if (got != kNoSlot) {
-                // The slot's descriptor may have been rewritten since this SM last read it:
-                // copy it through L2, one 16-byte piece per lane.
-                const uint4* src = reinterpret_cast<const uint4*>(&slots[got]);
-                uint4* dst = reinterpret_cast<uint4*>(&s_q);
-                for (int q = threadIdx.x; q < int(sizeof(Req) / 16); q += 32) dst[q] = __ldcg(src + q);
+                if (fresh) {
+                    // The slot's descriptor may have been rewritten since this SM last read
+                    // it: copy it through L2, one 16-byte piece per lane.
+                    const uint4* src = reinterpret_cast<const uint4*>(&slots[got]);
+                    uint4* dst = reinterpret_cast<uint4*>(&s_q);
+                    for (int q = threadIdx.x; q < int(sizeof(Req) / 16); q += 32) dst[q] = __ldcg(src + q);
+                }
+                // Other CTAs' results that this task's TMA loads read were published with a
+                // release after their own proxy fence; order the claim's acquire before them.
                 fence_proxy_async_global();
             }
         }
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         if (f == 0) {
             const int64_t v0 = int64_t(t) * kPosChunk;
             const int64_t v1 = v0 + kPosChunk < Q.V ? v0 + kPosChunk : Q.V;
-            run_positions(Q, E.C, E.Cp, v0, v1, smem);
+            run_positions(Q, E.C, E.Cp, v0, v1);
         } else if (f == 1) {
             int q = int(t) >> 1, I = 0;
             while (q >= R - I) {
@@ -537,22 +537,33 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                 if (kind == 0) {
                     run_pivot<16>(E, k, rowbuf, colbuf);
                 } else {
-                    // Panels (row panels first, then column panels) or remainder: one tile task.
+                    // Panels (row panels first, then column panels) or remainder tiles, one per
+                    // task; a remainder claim may hold two consecutive tiles.
                     const int R1 = R - 1;
-                    int tk, ii, jj;
-                    if (kind == 1) {
-                        const bool row = int(t) < R1;
-                        const int x = row ? int(t) : int(t) - R1;
-                        tk = row ? kTileRow : kTileCol;
-                        ii = jj = x + (x >= k);
-                    } else {
-                        tk = kTileRem;
-                        ii = int(t) / R1;
-                        jj = int(t) % R1;
-                        ii += ii >= k;
-                        jj += jj >= k;
+                    const uint32_t cnt = s_cnt;
+                    for (uint32_t x = 0; x < cnt; ++x) {
+                        // The previous tile's shared operands are read before the next TMA;
+                        // the reduction keeps every thread's view of ok the same.
+                        if (x > 0 && !__syncthreads_and(ok)) {
+                            ok = false;
+                            break;
+                        }
+                        const int tt = int(t + x);
+                        int tk, ii, jj;
+                        if (kind == 1) {
+                            const bool row = tt < R1;
+                            const int y = row ? tt : tt - R1;
+                            tk = row ? kTileRow : kTileCol;
+                            ii = jj = y + (y >= k);
+                        } else {
+                            tk = kTileRem;
+                            ii = tt / R1;
+                            jj = tt % R1;
+                            ii += ii >= k;
+                            jj += jj >= k;
+                        }
+                        ok = run_tile<16>(E, G, tk, k, ii, jj, smem, bars, par_a, par_b);
                     }
-                    ok = run_tile<16>(E, G, tk, k, ii, jj, smem, bars, par_a, par_b);
                 }
             } else if (g == 3 * R) {
                 int rem = int(t), I = 0;
@@ -570,19 +581,20 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         __syncthreads();
         if (threadIdx.x == 0) {
             const int kind = f == 0 ? 0 : f == 1 ? 1 : R == 1 ? 2 : (f - 2 < 3 * R ? 3 + (f - 2) % 3 : (f - 2 == 3 * R ? 6 : 7));
+            const uint32_t cnt = s_cnt;
             atomicAdd(&hdr->busy_ns[kind], (unsigned long long)(global_ns() - t_task));
-            atomicAdd(&hdr->tasks[kind], 1ull);
+            atomicAdd(&hdr->tasks[kind], (unsigned long long)cnt);
             if (!ok) {
                 atomicCAS(&hdr->err, 0u, 1u);
             } else {
                 fence_proxy_async_global();
-                const uint32_t prev = atomicAdd(&dones[size_t(s) * kMaxPhases + f], 1u);
-                if (f == 1 && prev + 1 == phase_size(R, Q.V, f)) {
+                const uint32_t prev = atomicAdd(&dones[size_t(s) * kMaxPhases + f], cnt);
+                if (f == 1 && prev + cnt == phase_size(R, Q.V, f)) {
                     // The ballot places are no longer needed: tell the host it may reuse them.
                     __threadfence_system();
                     asm volatile("st.release.sys.u32 [%0], %1;" ::"l"(Q.tally_host), "r"(Q.gen) : "memory");
                 }
-                if (last && prev + 1 == phase_size(R, Q.V, f)) {
+                if (last && prev + cnt == phase_size(R, Q.V, f)) {
                     uint32_t status = 0;
                     const uint32_t ballot_err = __ldcg(Q.flags);
                     if (__ldcg(Q.flags + 1)) status |= kStatusOverflow;

@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "positions.cuh"
 
 namespace se {
 namespace closure {
@@ -45,65 +46,23 @@ constexpr uint32_t kMaxPolls = 1u << 26;
 int64_t padded(int C) { return round_up(C, kTile); }
 
 // ------------------------------------------------------------------------------------------
-// Positions of one ballot. pos[v][c] = place of candidate c on completed ballot v.
-// Id is int32_t, or uint16_t / uint8_t for packed ballots. Ballot v is
-// ids[offsets[v] - id_base, offsets[v + 1] - id_base), or ids[v * C, (v + 1) * C) when offsets
-// is null (complete ballots).
+// Positions: pos[v][c] = place of candidate c on completed ballot v, one warp per ballot
+// (positions.cuh), 8 ballots per CTA. Id is int32_t, or uint16_t / uint8_t for packed ballots.
+// Ballot v is ids[offsets[v] - id_base, offsets[v + 1] - id_base), or ids[v * C, (v + 1) * C)
+// when offsets is null (complete ballots).
 // ------------------------------------------------------------------------------------------
+constexpr int kPosWarps = 8;
+
 template <typename Id>
-__global__ void __launch_bounds__(256)
-    positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int C,
-                     int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
-    __shared__ uint32_t warp_sums[8];
-    __shared__ int bad;
-    const int64_t v = blockIdx.x;
-    float* p = pos + v * Cq;
+__global__ void __launch_bounds__(32 * kPosWarps)
+    positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int64_t V,
+                     int C, int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
+    const int64_t v = int64_t(blockIdx.x) * kPosWarps + (threadIdx.x >> 5);
+    if (v >= V) return;  // warp-uniform
     const int64_t beg = offsets ? offsets[v] - id_base : v * C;
     const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
-    const Id* r = ids + beg;
-    if (threadIdx.x == 0) bad = 0;
-    for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) p[c] = c < C ? -1.0f : 0.0f;
-    __syncthreads();
-    for (int64_t a = threadIdx.x; a < len; a += blockDim.x) {
-        const int64_t id = int64_t(r[a]);
-        if (id < 0 || id >= C) {
-            raise_device_error(err, kErrRange);
-            bad = 1;
-        } else {
-            p[id] = float(a);
-        }
-    }
-    __syncthreads();
-    if (bad) return;
-    // A repeated id leaves at most one of its places in p; the others see a mismatch.
-    for (int64_t a = threadIdx.x; a < len; a += blockDim.x)
-        if (p[r[a]] != float(a)) {
-            raise_device_error(err, kErrRepeat);
-            bad = 1;
-        }
-    __syncthreads();
-    if (bad || len >= C) return;  // a complete, valid ballot has no missing ids
-    // Missing ids take places len, len+1, ... in ascending id order: exclusive block scan of
-    // the "missing" flags over c.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int64_t base = len;
-    for (int64_t c0 = 0; c0 < C; c0 += blockDim.x) {
-        const int64_t c = c0 + threadIdx.x;
-        const bool miss = c < C && p[c] < 0.0f;
-        const uint32_t ballot = __ballot_sync(0xffffffffu, miss);
-        if (lane == 0) warp_sums[warp] = __popc(ballot);
-        __syncthreads();
-        uint32_t before = __popc(ballot & ((1u << lane) - 1u));
-        uint32_t total = 0;
-        for (int w = 0; w < 8; ++w) {
-            const uint32_t s = warp_sums[w];
-            if (w < warp) before += s;
-            total += s;
-        }
-        if (miss) p[c] = float(base + before);
-        base += total;
-        __syncthreads();
-    }
+    const int code = warp_positions(ids + beg, len, C, Cq, pos + v * Cq);
+    if (code != kPosOk && (threadIdx.x & 31) == 0) raise_device_error(err, uint32_t(code));
 }
 
 __device__ __forceinline__ float sat_sub(float a, float b) {
@@ -285,15 +244,16 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         if (!accumulate) SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
         return SE_OK;
     }
+    const unsigned pos_blocks = unsigned((V + kPosWarps - 1) / kPosWarps);
     if (id_bytes == 4)
-        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, C, Cq,
-                                                     pos, err);
+        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base,
+                                                               V, C, Cq, pos, err);
     else if (id_bytes == 2)
-        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, C, Cq,
-                                                     pos, err);
+        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets,
+                                                               id_base, V, C, Cq, pos, err);
     else
-        positions_kernel<<<unsigned(V), 256, 0, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, C, Cq,
-                                                     pos, err);
+        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base,
+                                                               V, C, Cq, pos, err);
     SE_CHECK_LAUNCH();
 
     static bool smem_ok = cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
