@@ -61,4 +61,49 @@ __device__ __forceinline__ int warp_positions(const Id* __restrict__ r, int64_t 
     return kPosOk;
 }
 
+// The same for one ballot per CTA (all blockDim.x threads, a multiple of 32, at most 1024):
+// for long ballots, where one warp per ballot leaves too few warps in flight. Every thread of
+// the block must call it with the same ballot. scratch: 32 + 1 ints of shared memory.
+template <typename Id>
+__device__ __forceinline__ int block_positions(const Id* __restrict__ r, int64_t len, int C, int64_t Cq,
+                                               float* __restrict__ p, int* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool complete = len >= C;
+    for (int64_t c = complete ? C + threadIdx.x : threadIdx.x; c < Cq; c += blockDim.x) p[c] = c < C ? -1.0f : 0.0f;
+    __syncthreads();
+    int bad = 0;
+#pragma unroll 4
+    for (int64_t a = threadIdx.x; a < len; a += blockDim.x) {
+        const int64_t id = int64_t(r[a]);
+        if (id < 0 || id >= C) bad = 1;
+        else p[id] = float(a);
+    }
+    if (__syncthreads_or(bad)) return kPosRange;
+#pragma unroll 4
+    for (int64_t a = threadIdx.x; a < len; a += blockDim.x)
+        if (p[int64_t(r[a])] != float(a)) bad = 1;
+    if (__syncthreads_or(bad)) return kPosRepeat;
+    if (complete) return kPosOk;
+    // Missing ids in ascending order: a block-wide exclusive scan of the "missing" flags.
+    int* warp_sums = scratch;
+    int64_t base = len;
+    for (int64_t c0 = 0; c0 < C; c0 += blockDim.x) {
+        const int64_t c = c0 + threadIdx.x;
+        const bool miss = c < C && p[c] < 0.0f;
+        const uint32_t m = __ballot_sync(0xffffffffu, miss);
+        if (lane == 0) warp_sums[warp] = __popc(m);
+        __syncthreads();
+        int before = __popc(m & ((1u << lane) - 1u)), total = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int x = warp_sums[w];
+            before += w < warp ? x : 0;
+            total += x;
+        }
+        if (miss) p[c] = float(base + before);
+        base += total;
+        __syncthreads();
+    }
+    return kPosOk;
+}
+
 }  // namespace se

@@ -52,17 +52,36 @@ int64_t padded(int C) { return round_up(C, kTile); }
 // when offsets is null (complete ballots).
 // ------------------------------------------------------------------------------------------
 constexpr int kPosWarps = 8;
+constexpr int kPosBlockFromC = 2048;  // from this many candidates on, one CTA per ballot
 
-template <typename Id>
+// PER_WARP: one ballot per warp, kPosWarps ballots per CTA; else one ballot per CTA.
+template <typename Id, bool PER_WARP>
 __global__ void __launch_bounds__(32 * kPosWarps)
     positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int64_t V,
                      int C, int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
-    const int64_t v = int64_t(blockIdx.x) * kPosWarps + (threadIdx.x >> 5);
-    if (v >= V) return;  // warp-uniform
+    const int64_t v = PER_WARP ? int64_t(blockIdx.x) * kPosWarps + (threadIdx.x >> 5) : int64_t(blockIdx.x);
+    if (v >= V) return;  // warp-uniform (and CTA-uniform for one ballot per CTA)
     const int64_t beg = offsets ? offsets[v] - id_base : v * C;
     const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
-    const int code = warp_positions(ids + beg, len, C, Cq, pos + v * Cq);
-    if (code != kPosOk && (threadIdx.x & 31) == 0) raise_device_error(err, uint32_t(code));
+    int code;
+    if constexpr (PER_WARP) {
+        code = warp_positions(ids + beg, len, C, Cq, pos + v * Cq);
+        if (code != kPosOk && (threadIdx.x & 31) == 0) raise_device_error(err, uint32_t(code));
+    } else {
+        __shared__ int scratch[33];
+        code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
+        if (code != kPosOk && threadIdx.x == 0) raise_device_error(err, uint32_t(code));
+    }
+}
+
+template <typename Id>
+void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, int64_t V, int C, int64_t Cq,
+                      float* pos, uint32_t* err, cudaStream_t s) {
+    if (C >= kPosBlockFromC)
+        positions_kernel<Id, false><<<unsigned(V), 32 * kPosWarps, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
+    else
+        positions_kernel<Id, true><<<unsigned((V + kPosWarps - 1) / kPosWarps), 32 * kPosWarps, 0, s>>>(
+            ids, offsets, id_base, V, C, Cq, pos, err);
 }
 
 __device__ __forceinline__ float sat_sub(float a, float b) {
@@ -244,16 +263,12 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         if (!accumulate) SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
         return SE_OK;
     }
-    const unsigned pos_blocks = unsigned((V + kPosWarps - 1) / kPosWarps);
     if (id_bytes == 4)
-        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base,
-                                                               V, C, Cq, pos, err);
+        launch_positions(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
     else if (id_bytes == 2)
-        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets,
-                                                               id_base, V, C, Cq, pos, err);
+        launch_positions(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
     else
-        positions_kernel<<<pos_blocks, 32 * kPosWarps, 0, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base,
-                                                               V, C, Cq, pos, err);
+        launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
     SE_CHECK_LAUNCH();
 
     static bool smem_ok = cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -35,6 +35,21 @@ def test_incomplete_ballots(orc):
     assert np.array_equal(api.build_pairwise_preferences(ballots), orc.tally(ballots, "scatter"))
 
 
+@pytest.mark.parametrize("C,complete", [(2048, True), (2500, False), (4096, False)])
+def test_long_ballots_one_cta_per_ballot(orc, C, complete):
+    """From 2048 candidates on, one CTA places each ballot: complete and incomplete ballots,
+    and a repeated or out-of-range id in a long ballot, against the oracle."""
+    rng = np.random.default_rng(C)
+    V = 60
+    ballots = [rng.permutation(C) if complete else rng.permutation(C)[: rng.integers(1, C + 1)] for _ in range(V)]
+    ballots.append(np.array([C - 1]))
+    assert np.array_equal(api.build_pairwise_preferences(ballots), orc.tally(ballots, "scatter"))
+    bad = [b.copy() for b in ballots[:3]]
+    bad[1][len(bad[1]) // 2] = bad[1][0] if len(bad[1]) > 1 else C + 5
+    with pytest.raises(ValueError):
+        api.build_pairwise_preferences(bad + [np.array([C - 1])])
+
+
 def test_many_voters_beyond_16_bits(orc):
     """V = 70000 > 65535: counts need 32-bit lanes downstream; the tally itself is exact."""
     from scalingelections_b200.ballots import mallows_ballots
