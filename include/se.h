@@ -250,6 +250,38 @@ SE_API se_status_t se_engine_stop(se_engine_t* engine);
 SE_API se_status_t se_engine_destroy(se_engine_t* engine);
 
 /* ---------------------------------------------------------------------------------------
+ * One election's closure sharded across GPUs by row blocks (no reference counterpart: the
+ * reference closes one matrix on one GPU, scaling_elections.cu:490-578).
+ *
+ * With R = ceil(C / 128) row blocks of 128 candidates, each GPU (rank) holds a shard: the row
+ * blocks [b0, b1) of the working matrix. For every pivot round k = 0 .. R-1, in order:
+ *   1. the shard that holds block k calls se_shard_pivot(k): it closes the pivot tile and
+ *      updates its pivot-row panel;
+ *   2. the caller broadcasts that panel, se_shard_panel_bytes() bytes at byte offset
+ *      se_shard_panel_offset(k) of the owner's workspace, into the same offset of every other
+ *      shard's workspace (e.g. one NCCL broadcast; the offsets differ between owner and
+ *      receivers, so each rank asks its own shard);
+ *   3. every shard calls se_shard_update(k): column panels and remainder tiles of its rows.
+ * Before round 0 each shard calls se_shard_init with the whole C x C preference matrix on its
+ * GPU; after round R-1, se_shard_finalize writes its rows [128 b0, min(128 b1, C)) of the
+ * strongest-path matrix (u32, zero diagonal). Results equal se_closure's bit for bit.
+ * lane_bits 16 (value_offset as in se_election_t) or 32. All calls are stream-ordered;
+ * se_shard_check synchronises and reports device errors.
+ * ------------------------------------------------------------------------------------- */
+typedef struct se_shard se_shard_t;
+SE_API int64_t se_shard_workspace_bytes(int C, int b0, int b1, int lane_bits);
+SE_API se_status_t se_shard_create(int C, int b0, int b1, int lane_bits, uint32_t value_offset,
+                                   void* d_work, int64_t work_bytes, se_shard_t** shard);
+SE_API se_status_t se_shard_destroy(se_shard_t* shard);
+SE_API se_status_t se_shard_init(se_shard_t* shard, const uint32_t* d_pref, int64_t ld_pref, void* stream);
+SE_API se_status_t se_shard_pivot(se_shard_t* shard, int k, void* stream);
+SE_API int64_t se_shard_panel_offset(const se_shard_t* shard, int k);
+SE_API int64_t se_shard_panel_bytes(const se_shard_t* shard);
+SE_API se_status_t se_shard_update(se_shard_t* shard, int k, void* stream);
+SE_API se_status_t se_shard_finalize(se_shard_t* shard, uint32_t* d_out, int64_t ld_out, void* stream);
+SE_API se_status_t se_shard_check(se_shard_t* shard, void* stream);
+
+/* ---------------------------------------------------------------------------------------
  * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).
  *
  *   Ballots are given in CSR form: ballot v is d_ids[d_offsets[v] .. d_offsets[v+1]), the

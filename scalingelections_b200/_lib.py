@@ -63,6 +63,16 @@ SIGNATURES: dict[str, tuple] = {
     "se_engine_stats": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _ip, _ip, _dp, ctypes.POINTER(ctypes.c_int64), _dp]),
     "se_engine_stop": (_c_int, [_vp]),
     "se_engine_destroy": (_c_int, [_vp]),
+    "se_shard_workspace_bytes": (_c_i64, [_c_int, _c_int, _c_int, _c_int]),
+    "se_shard_create": (_c_int, [_c_int, _c_int, _c_int, _c_int, ctypes.c_uint32, _vp, _c_i64, _vp]),
+    "se_shard_destroy": (_c_int, [_vp]),
+    "se_shard_init": (_c_int, [_vp, _vp, _c_i64, _vp]),
+    "se_shard_pivot": (_c_int, [_vp, _c_int, _vp]),
+    "se_shard_panel_offset": (_c_i64, [_vp, _c_int]),
+    "se_shard_panel_bytes": (_c_i64, [_vp]),
+    "se_shard_update": (_c_int, [_vp, _c_int, _vp]),
+    "se_shard_finalize": (_c_int, [_vp, _vp, _c_i64, _vp]),
+    "se_shard_check": (_c_int, [_vp, _vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),
     "se_tally": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),
     "se_tally_enqueue": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _c_i64, _vp]),

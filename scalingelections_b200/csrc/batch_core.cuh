@@ -208,9 +208,12 @@ constexpr int kTileRow = 0;
 constexpr int kTileCol = 1;
 constexpr int kTileRem = 2;
 
+// mapB / kb: where the pivot rows S[K][*] (B of row and remainder tiles, D of column tiles)
+// are read: by default G->mapS at row block K; a sharded closure passes the map of a
+// received panel buffer (kb = 0) or of its own slab (kb = the local row block).
 template <int LB, bool GLOBAL_MAPS = true>
 __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
-                         uint32_t& par_a, uint32_t& par_b) {
+                         uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1) {
     using CF = cfg<LB>;
     constexpr int TW = CF::TW;
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);
@@ -222,20 +225,22 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     uint64_t* wait_bars = bars;  // the product's chunk barriers and their parity
     uint32_t wait_par = par_a;
     uint32_t* Ct;
+    if (mapB == nullptr) mapB = &G->mapS;
+    if (kb < 0) kb = K;
     if (kind != kTileCol) {
         const bool rem = kind == kTileRem;
         const CUtensorMap* mapA = rem ? &G->mapAT : &G->mapDT;
         if (threadIdx.x == 0) {
             if constexpr (GLOBAL_MAPS) {
                 fence_tensormap(mapA);
-                fence_tensormap(&G->mapS);
+                fence_tensormap(mapB);
             }
             fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
                 mbar_arrive_expect_tx(&bars[ch], CF::A_BYTES + CF::B_BYTES);
                 tma_load_2d(As + ch * CF::A_CHUNK, mapA, &bars[ch], rem ? I * kT : 0, ch * kKC);
-                tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[ch], J * TW, K * kT + ch * kKC);
+                tma_load_2d(Bs + ch * CF::B_CHUNK, mapB, &bars[ch], J * TW, kb * kT + ch * kKC);
             }
         }
         Ct = E.S + int64_t(rem ? I : K) * kT * ldw + int64_t(J) * TW;
@@ -270,11 +275,14 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
         }
         __syncthreads();  // the tile region is free again
         if (threadIdx.x == 0 && ok) {
+            if constexpr (GLOBAL_MAPS) {
+                if (mapB != &G->mapS) fence_tensormap(mapB);
+            }
             fence_proxy_async();
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
                 mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
-                tma_load_2d(Bs + ch * CF::B_CHUNK, &G->mapS, &bars[kChunks + ch], K * TW, K * kT + ch * kKC);
+                tma_load_2d(Bs + ch * CF::B_CHUNK, mapB, &bars[kChunks + ch], K * TW, kb * kT + ch * kKC);
             }
         }
         Ct = E.S + int64_t(I) * kT * ldw + int64_t(K) * TW;
