@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest"], default="closure",
+    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest", "sharded"], default="closure",
                     help="closure: the headline single election; batch: many mixed elections; "
                          "serve: Poisson arrivals on the continuous-batching server")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per offered load")
@@ -601,6 +601,76 @@ def run_serve(args, world, rank, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_sharded(args, world, rank, local_rank):
+    """One election closed by all ranks together (scalingelections_b200.sharded): row blocks
+    split across the ranks, one pivot-row panel broadcast (NCCL) per round. Every rank draws
+    and tallies the same ballots, so all hold the same preference matrix. Strong scaling: the
+    work is one C^3 closure whatever the number of GPUs."""
+    import torch
+    import torch.distributed as dist
+
+    from scalingelections_b200 import LANES_U16, api
+    from scalingelections_b200.ballots import mallows_ballots_device
+    from scalingelections_b200.sharded import strongest_paths_sharded
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    C, V = args.candidates, args.voters
+    if world == 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if "MASTER_PORT" not in os.environ:
+            import socket
+
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+        dist.init_process_group("nccl", rank=0, world_size=1)
+    ballots = mallows_ballots_device(V, C, args.phi, seed=args.seed, device=dev)
+    offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
+    d = api.tally_device(ballots.view(-1), offs, C)
+    del ballots
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        rows, _ = strongest_paths_sharded(d, lanes=LANES_U16)
+    torch.cuda.synchronize()
+    dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            rows, (r0, r1) = strongest_paths_sharded(d, lanes=LANES_U16)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    # Check this rank's rows against the single-GPU closure of the same matrix.
+    single = api.strongest_paths_device(d, lanes=LANES_U16)
+    identical = torch.equal(rows.view(torch.int32), single[r0:r1].view(torch.int32))
+    ok = torch.tensor([1 if identical else 0], device=dev)
+    dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+    R = (C + 127) // 128
+    if rank == 0:
+        line = {
+            "metric": f"Gcells/s (C^3/t), one election's closure sharded over the GPUs, C={C}",
+            "value": C ** 3 * args.steps / (ms_max / 1e3) / 1e9, "unit": "Gcells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u16", "data": "synthetic (seeded Mallows ballots)",
+            "config": {"workload": f"one election, C={C}, V={V} Mallows(phi={args.phi}) ballots, row blocks split "
+                                   f"over {world} GPU(s), one NCCL broadcast of the pivot-row panel per round",
+                       "rounds": R, "panel_bytes": 128 * ((C + 127) // 128 * 128) * 2},
+            "bit_identical_to_single_gpu": bool(ok.item()),
+            "gpu_launches": (R * 2 + R * 2 * world) * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world == 1:
+        dist.destroy_process_group()
+
+
 def run_ingest(args, world, rank, local_rank):
     """Ballot file -> preference matrix: 2^20 incomplete ballots over C = 1024 candidates
     (lengths uniform in [1, C], Mallows(0.8) orders) in a packed file of 16-bit ids, tallied
@@ -749,6 +819,8 @@ def main():
             run_serve(args, world, rank, local_rank)
         elif args.workload == "ingest":
             run_ingest(args, world, rank, local_rank)
+        elif args.workload == "sharded":
+            run_sharded(args, world, rank, local_rank)
         else:
             run_ours(args, world, rank, local_rank)
     finally:
