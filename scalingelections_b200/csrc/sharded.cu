@@ -79,11 +79,19 @@ constexpr int kPhaseRemainder = 2;
 // One phase of round k on the slab. E describes the slab: S is its first row, mapS covers its
 // rows, AT is indexed by local row block. own: this shard holds row block k (local kl), so the
 // pivot rows are read from its own slab; otherwise from the panel buffer (mapP, row block 0).
+// fuse_next >= 0 (remainder phase only): this shard also holds row block k + 1, at local index
+// fuse_next. Block 0 then takes tile (k+1, k+1) and, after updating it, closes it as round
+// k+1's pivot over kmax_next pivots and writes dT, while the other blocks go on: the next
+// round's se_shard_pivot needs only its row panel. Nothing else in this launch reads that
+// tile or dT.
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     shard_tiles_kernel(const __grid_constant__ Elec E, const __grid_constant__ CUtensorMap mapP, int phase, int k,
-                       int kl, int own, uint32_t* __restrict__ err) {
+                       int kl, int own, int fuse_next, int kmax_next, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[2][kT];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
         for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
@@ -92,7 +100,13 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     __syncthreads();
     const CUtensorMap* mapB = own ? &E.mapS : &mapP;
     const int kb = own ? kl : 0;
-    const int b = blockIdx.x;
+    int b = blockIdx.x;
+    const bool fuse = phase == kPhaseRemainder && fuse_next >= 0;
+    if (fuse) {
+        // Reduced coordinates of tile (k+1, k+1): local rows without kl, columns without k.
+        const int p = (own && fuse_next > kl ? fuse_next - 1 : fuse_next) * (E.R - 1) + k;
+        b = b == 0 ? p : (b == p ? 0 : b);
+    }
     int kind, K = k, I = 0, J = 0;
     if (phase == kPhaseRowPanel) {  // owner only: tiles (k, J != k) of its row block kl
         kind = kTileRow;
@@ -110,7 +124,21 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     }
     uint32_t pa = 0, pb = 0;
     const bool ok = run_tile<LB, false>(E, &E, kind, K, I, J, smem, bars, pa, pb, mapB, kb);
-    if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
+    if (!ok) {
+        if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
+        return;
+    }
+    if (fuse && blockIdx.x == 0) {
+        __syncthreads();  // the tile's stores are visible to the whole CTA
+        const geom g(threadIdx.x);
+        const int64_t ldw = E.Cp / CF::CPW;
+        uint32_t* D = E.S + int64_t(fuse_next) * kT * ldw + int64_t(k + 1) * CF::TW;
+        uint32_t c[8][8];
+        load_tile_regs<LB, true>(c, D, ldw, g);
+        close_tile_in_registers<LB>(c, g, kmax_next, rowbuf, colbuf);
+        store_tile_regs<LB>(c, D, ldw, g);
+        store_transposed_splat<LB>(c, E.dT, kT, g);
+    }
 }
 
 // out rows [0, nrows) = global rows row0.. of the closure as u32, zero on the diagonal.
@@ -169,6 +197,7 @@ struct se_shard {
     uint8_t* P;
     int64_t panel_bytes;
     int32_t b0, b1, nloc;
+    int32_t pivot_ready;  // a round whose pivot tile the previous update already closed, or -1
 };
 
 extern "C" int64_t se_shard_workspace_bytes(int C, int b0, int b1, int lane_bits) {
@@ -201,6 +230,7 @@ extern "C" se_status_t se_shard_create(int C, int b0, int b1, int lane_bits, uin
     h->b0 = b0;
     h->b1 = b1;
     h->nloc = b1 - b0;
+    h->pivot_ready = -1;
     Elec& E = h->E;
     E.C = C;
     E.Cp = int(round_up(int64_t(C), kT));
@@ -250,12 +280,15 @@ template <int LB> se_status_t pivot_impl(se_shard& h, int k, cudaStream_t s) {
     const Elec& E = h.E;
     if (se_status_t st = set_smem<LB>()) return st;
     const int kl = k - h.b0;
-    const int kmax = E.C - k * kT < kT ? E.C - k * kT : kT;  // pivots past C are zero padding
-    shard_pivot_kernel<LB><<<1, cfg<LB>::THREADS, 0, s>>>(E.S, int64_t(E.Cp) / (32 / LB), kl, k, kmax, E.dT);
-    SE_CHECK_LAUNCH();
+    if (h.pivot_ready != k) {  // not closed already by the previous round's remainder launch
+        const int kmax = E.C - k * kT < kT ? E.C - k * kT : kT;  // pivots past C are zero padding
+        shard_pivot_kernel<LB><<<1, cfg<LB>::THREADS, 0, s>>>(E.S, int64_t(E.Cp) / (32 / LB), kl, k, kmax, E.dT);
+        SE_CHECK_LAUNCH();
+    }
+    h.pivot_ready = -1;
     if (E.R > 1) {
         shard_tiles_kernel<LB><<<unsigned(E.R - 1), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseRowPanel, k,
-                                                                                         kl, 1, h.err);
+                                                                                         kl, 1, -1, 0, h.err);
         SE_CHECK_LAUNCH();
     }
     return SE_OK;
@@ -269,12 +302,17 @@ template <int LB> se_status_t update_impl(se_shard& h, int k, cudaStream_t s) {
     const int rows = own ? h.nloc - 1 : h.nloc;  // local row blocks other than k
     if (rows <= 0) return SE_OK;
     shard_tiles_kernel<LB><<<unsigned(rows), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseColPanel, k, kl,
-                                                                                  own ? 1 : 0, h.err);
+                                                                                  own ? 1 : 0, -1, 0, h.err);
     SE_CHECK_LAUNCH();
     if (E.R > 1) {
+        // Close round k+1's pivot inside this launch when this shard holds row block k+1.
+        const int next = k + 1;
+        const int fuse = next < E.R && next >= h.b0 && next < h.b1 ? next - h.b0 : -1;
+        const int kmax_next = fuse >= 0 ? (E.C - next * kT < kT ? E.C - next * kT : kT) : 0;
         shard_tiles_kernel<LB><<<unsigned(rows * (E.R - 1)), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(
-            E, h.mapP, kPhaseRemainder, k, kl, own ? 1 : 0, h.err);
+            E, h.mapP, kPhaseRemainder, k, kl, own ? 1 : 0, fuse, kmax_next, h.err);
         SE_CHECK_LAUNCH();
+        if (fuse >= 0) h.pivot_ready = next;
     }
     return SE_OK;
 }
