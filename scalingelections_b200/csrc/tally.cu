@@ -8,12 +8,11 @@
 // permutation, so for i != j exactly one of (i above j), (j above i) holds and
 // d[j][i] = V - d[i][j]: only the upper-triangle tiles are computed.
 //
-// Kernel 1 (positions_kernel, one CTA per ballot) writes pos as f32 [V][Cq] (exact integers),
-// validating ids (range, repeats). Kernel 2 (count_kernel, one CTA per upper tile) streams
-// 32-voter chunks of the two 128-candidate position strips into shared memory with TMA and
-// counts per 8 x 8 register micro-tile with `sub.sat.f32` (1.0 when pos_j > pos_i, the
-// positions differ by at least 1) plus `add.f32`: both on the FP32 pipe, leaving the
-// integer min/max pipe to the closure. Counts stay exact in f32 up to 2^24 voters.
+// Kernel 1 (positions_kernel) writes pos as f32 [V][Cq] (exact integers), validating ids
+// (range, repeats). Kernel 2 (pack_planes_kernel) packs each 32-voter chunk into bit planes.
+// Kernel 3 (count_bits_kernel, one CTA per upper tile) streams the planes of the two
+// 128-candidate strips into shared memory with TMA and counts per 8 x 8 register micro-tile
+// with a bit-serial borrow chain (one lop3 per plane) and a popc per 32 voters.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -34,10 +33,7 @@ namespace tally {
 
 constexpr int kTile = 128;     // candidates per tile edge
 constexpr int kVC = 32;        // voters per TMA chunk
-constexpr int kStages = 3;     // chunk ring depth (3 x 32 KiB: fits beside a serving-engine CTA on one SM)
 constexpr int kThreads = 256;  // 8 x 8 cells per thread
-constexpr uint32_t kChunkBytes = kVC * kTile * 4;
-constexpr size_t kSmem = size_t(kStages) * 2 * kVC * kTile * 4 + kStages * 8;
 constexpr uint32_t kErrRange = 2;
 constexpr uint32_t kErrRepeat = 3;
 constexpr uint32_t kErrTimeout = 1;
@@ -84,33 +80,69 @@ void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, in
             ids, offsets, id_base, V, C, Cq, pos, err);
 }
 
-__device__ __forceinline__ float sat_sub(float a, float b) {
-    float r;
-    asm("sub.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+// ------------------------------------------------------------------------------------------
+// Bit-sliced counting. For a chunk of 32 voters, bit k of every voter's place of candidate c is
+// gathered into one word: plane[ch][k][c] (bit v = bit k of pos_{32 ch + v}(c)). Then
+// pos(i) < pos(j) for all 32 voters at once is the borrow out of the bit-serial subtraction
+// pos(i) - pos(j): borrow' = MAJ(~a_k, b_k, borrow) over the planes from the least significant,
+// one `lop3.b32` (LUT 0x8E) per plane, and one `popc` adds the 32 answers. With B = bits of
+// C - 1 planes that is about (B + 2) / 32 ALU instructions per voter pair, against two FP32
+// instructions in the direct form.
+// ------------------------------------------------------------------------------------------
+constexpr int kMaxPlanes = 20;  // C <= 2^20
+constexpr int kBitStages = 4;
+
+__host__ __device__ inline int planes_for(int C) {
+    int b = 0;
+    for (uint32_t x = uint32_t(C > 1 ? C - 1 : 1); x; x >>= 1) ++b;
+    return b;
+}
+
+// planes[(ch * B + k) * Cq + c] for the chunks of voters [0, V); voters past V count as place 0.
+__global__ void __launch_bounds__(256)
+    pack_planes_kernel(const float* __restrict__ pos, int64_t V, int64_t Cq, int B, uint32_t* __restrict__ planes) {
+    const int64_t c = int64_t(blockIdx.y) * blockDim.x + threadIdx.x;  // grid: (chunks, ceil(Cq / 256))
+    const int64_t ch = blockIdx.x;
+    if (c >= Cq) return;
+    uint32_t pl[kMaxPlanes];
+#pragma unroll
+    for (int k = 0; k < kMaxPlanes; ++k) pl[k] = 0u;
+    for (int v = 0; v < 32; ++v) {
+        const int64_t voter = ch * 32 + v;
+        const uint32_t p = voter < V ? uint32_t(pos[voter * Cq + c]) : 0u;
+#pragma unroll
+        for (int k = 0; k < kMaxPlanes; ++k) pl[k] |= ((p >> k) & 1u) << v;
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxPlanes; ++k)
+        if (k < B) planes[(ch * B + k) * Cq + c] = pl[k];
+}
+
+__device__ __forceinline__ uint32_t borrow_step(uint32_t a, uint32_t b, uint32_t br) {
+    uint32_t r;
+    asm("lop3.b32 %0, %1, %2, %3, 0x8E;" : "=r"(r) : "r"(a), "r"(b), "r"(br));
     return r;
 }
 
-__device__ __forceinline__ void lds4f(float* dst, const float* src) {
-    const float4 v = *reinterpret_cast<const float4*>(src);
-    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
-}
+inline size_t bits_smem(int B) { return size_t(kBitStages) * 2 * B * kTile * 4 + kBitStages * 8; }
 
-// ------------------------------------------------------------------------------------------
-// Counting over one upper tile (I <= J): d[I][J] and, for I < J, d[J][I] = V - d[I][J].
-// With splits > 1 the voters are cut into `splits` ranges of whole 32-voter chunks, one CTA per
-// (tile, range), and each CTA adds its range's counts (and, below the diagonal, the range's
-// voters minus them) to out with atomics: exact, since every count is an integer, and it keeps
-// the grid full when there are few tiles and many voters.
-// ------------------------------------------------------------------------------------------
+// Counting over one upper tile (I <= J): d[I][J] and, for I < J, d[J][I] = V - d[I][J]. One
+// CTA per tile (and voter range): the two 128-candidate plane strips of each 32-voter chunk
+// are staged by TMA (box {128, B}) through a 4-stage ring. With splits > 1 the voters are cut
+// into `splits` ranges of whole chunks, one CTA per (tile, range), and each CTA adds its
+// range's counts (and, below the diagonal, the range's voters minus them) to out with atomics:
+// exact, since every count is an integer, and it keeps the grid full when there are few tiles
+// and many voters.
 __global__ void __launch_bounds__(kThreads, 1)
-    count_kernel(const __grid_constant__ CUtensorMap mapPos, int64_t V, int C, int R, int splits,
-                 uint32_t* __restrict__ out, int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
+    count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int B, int64_t V, int C, int R, int splits,
+                      uint32_t* __restrict__ out, int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    float* sI = reinterpret_cast<float*>(smem_raw);           // [kStages][kVC][kTile]
-    float* sJ = sI + kStages * kVC * kTile;                   // [kStages][kVC][kTile]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sJ + kStages * kVC * kTile);
+    uint32_t* sI = reinterpret_cast<uint32_t*>(smem_raw);  // [kBitStages][B][kTile]
+    uint32_t* sJ = sI + kBitStages * B * kTile;            // [kBitStages][B][kTile]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sJ + kBitStages * B * kTile);
+    const uint32_t stage_words = uint32_t(B) * kTile;
+    const uint32_t stage_bytes = 2u * stage_words * 4u;
 
-    // Upper-triangle tile index -> (I, J), row-major over I <= J.
     int64_t t = blockIdx.x / splits;
     const int split = int(blockIdx.x % splits);
     int I = 0;
@@ -127,53 +159,64 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int64_t vlo = int64_t(ch0) * kVC, vhi = int64_t(ch1) * kVC < V ? int64_t(ch1) * kVC : V;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < kBitStages; ++s) mbar_init(&bars[s], 1);
         fence_barrier_init();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages && s < nch; ++s) {
-            mbar_arrive_expect_tx(&bars[s], 2 * kChunkBytes);
-            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, (ch0 + s) * kVC);
-            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, (ch0 + s) * kVC);
+        for (int s = 0; s < kBitStages && s < nch; ++s) {
+            mbar_arrive_expect_tx(&bars[s], stage_bytes);
+            tma_load_2d(sI + s * stage_words, &mapPl, &bars[s], I * kTile, (ch0 + s) * B);
+            tma_load_2d(sJ + s * stage_words, &mapPl, &bars[s], J * kTile, (ch0 + s) * B);
         }
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row0 = (warp & 3) * 32 + (lane >> 3) * 8;
     const int col0 = (warp >> 2) * 64 + (lane & 7) * 4;  // cols col0..+3 and col0+32..+35
-    float acc[8][8];
+    uint32_t acc[8][8];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0u;
 
     bool ok = true;
 #pragma unroll 1
     for (int ch = 0; ch < nch; ++ch) {
-        const int s = ch % kStages;
-        if (ok && !mbar_wait_bounded(&bars[s], uint32_t(ch / kStages) & 1u, kMaxPolls)) ok = false;
+        const int s = ch % kBitStages;
+        if (ok && !mbar_wait_bounded(&bars[s], uint32_t(ch / kBitStages) & 1u, kMaxPolls)) ok = false;
         if (ok) {
-            const float* pI = sI + s * kVC * kTile;
-            const float* pJ = sJ + s * kVC * kTile;
-#pragma unroll 4
-            for (int v = 0; v < kVC; ++v) {
-                float a[8], b[8];
-                lds4f(a, pI + v * kTile + row0);
-                lds4f(a + 4, pI + v * kTile + row0 + 4);
-                lds4f(b, pJ + v * kTile + col0);
-                lds4f(b + 4, pJ + v * kTile + col0 + 32);
+            const uint32_t* pI = sI + s * stage_words;
+            const uint32_t* pJ = sJ + s * stage_words;
+            uint32_t br[8][8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i)
+            for (int r = 0; r < 8; ++r)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[i][j] += sat_sub(b[j], a[i]);
+                for (int q = 0; q < 8; ++q) br[r][q] = 0u;
+#pragma unroll 2
+            for (int k = 0; k < B; ++k) {
+                uint32_t a[8], b[8];
+                const uint4 a0 = *reinterpret_cast<const uint4*>(pI + k * kTile + row0);
+                const uint4 a1 = *reinterpret_cast<const uint4*>(pI + k * kTile + row0 + 4);
+                const uint4 b0 = *reinterpret_cast<const uint4*>(pJ + k * kTile + col0);
+                const uint4 b1 = *reinterpret_cast<const uint4*>(pJ + k * kTile + col0 + 32);
+                a[0] = a0.x, a[1] = a0.y, a[2] = a0.z, a[3] = a0.w, a[4] = a1.x, a[5] = a1.y, a[6] = a1.z, a[7] = a1.w;
+                b[0] = b0.x, b[1] = b0.y, b[2] = b0.z, b[3] = b0.w, b[4] = b1.x, b[5] = b1.y, b[6] = b1.z, b[7] = b1.w;
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) br[r][q] = borrow_step(a[r], b[q], br[r][q]);
             }
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[r][q] += __popc(br[r][q]);
         }
         __syncthreads();  // every thread is done with stage s
-        if (threadIdx.x == 0 && ok && ch + kStages < nch) {
-            fence_proxy_async();  // order this stage's shared reads before the TMA rewrite
-            mbar_arrive_expect_tx(&bars[s], 2 * kChunkBytes);
-            tma_load_2d(sI + s * kVC * kTile, &mapPos, &bars[s], I * kTile, (ch0 + ch + kStages) * kVC);
-            tma_load_2d(sJ + s * kVC * kTile, &mapPos, &bars[s], J * kTile, (ch0 + ch + kStages) * kVC);
+        if (threadIdx.x == 0 && ok && ch + kBitStages < nch) {
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&bars[s], stage_bytes);
+            tma_load_2d(sI + s * stage_words, &mapPl, &bars[s], I * kTile, (ch0 + ch + kBitStages) * B);
+            tma_load_2d(sJ + s * stage_words, &mapPl, &bars[s], J * kTile, (ch0 + ch + kBitStages) * B);
         }
     }
     if (!ok) {
@@ -181,14 +224,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         return;
     }
     const uint32_t Vu = uint32_t(vhi - vlo);
-    if (nch == 0) return;  // an empty trailing range (more splits than chunks)
+    if (nch == 0) return;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const int i = I * kTile + row0 + r;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int j = J * kTile + col0 + (q < 4 ? q : 28 + q);
-            const uint32_t n = uint32_t(acc[r][q]);
+            const uint32_t n = acc[r][q];
             if (i < C && j < C) {
                 uint32_t* ij = out + int64_t(i) * ld_out + j;
                 uint32_t* ji = out + int64_t(j) * ld_out + i;
@@ -204,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         *ij += n;
                         *ji += Vu - n;
                     } else if (i != j) {
-                        *ij += n;  // the (j, i) cell of a diagonal tile is some thread's (i, j)
+                        *ij += n;
                     }
                 } else if (I == J) {
                     *ij = i == j ? 0u : n;
@@ -223,9 +266,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 using namespace se;
 using namespace se::tally;
 
+// Error word (256 B), then the places f32 [V][Cq], then the bit planes u32 [ceil(V/32) * B][Cq].
+int64_t planes_offset(int64_t V, int C) { return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256); }
+
 extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
     if (V < 0 || C < 1) return -1;
-    return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256);
+    const int64_t nch = (std::max<int64_t>(V, 1) + kVC - 1) / kVC;
+    return planes_offset(V, C) + round_up(nch * planes_for(C) * padded(C) * 4, 256);
 }
 
 namespace {
@@ -271,11 +318,17 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
     SE_CHECK_LAUNCH();
 
-    static bool smem_ok = cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               int(kSmem)) == cudaSuccess;
+    static bool smem_ok = cudaFuncSetAttribute(count_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(bits_smem(kMaxPlanes))) == cudaSuccess;
     SE_REQUIRE(smem_ok, SE_ERR_CUDA, "cannot raise the shared-memory limit of the tally kernel");
+    const int B = planes_for(C);
+    const int64_t nch_all = (V + kVC - 1) / kVC;
+    uint32_t* planes = reinterpret_cast<uint32_t*>(work + planes_offset(V, C));
+    pack_planes_kernel<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, B, planes);
+    SE_CHECK_LAUNCH();
     CUtensorMap map;
-    if (se_status_t st = se::closure::make_map(&map, pos, uint64_t(Cq), uint64_t(V), uint64_t(Cq) * 4, kTile, kVC))
+    if (se_status_t st = se::closure::make_map(&map, planes, uint64_t(Cq), uint64_t(nch_all * B), uint64_t(Cq) * 4,
+                                               kTile, uint32_t(B)))
         return st;
     const int64_t tiles = int64_t(R) * (R + 1) / 2;
     // Few tiles and many voters: split the voters so that the grid covers every SM about four
@@ -289,8 +342,8 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     if (tiles < want) splits = int(std::max<int64_t>(1, std::min<int64_t>((want + tiles - 1) / tiles, chunks / 32)));
     if (splits > 1 && !accumulate)
         SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
-    count_kernel<<<unsigned(tiles * splits), kThreads, kSmem, s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
-                                                                   err);
+    count_bits_kernel<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, B, V, C, R, splits, d_out, ld_out,
+                                                                                accumulate, err);
     SE_CHECK_LAUNCH();
     if (!check) return SE_OK;
 
