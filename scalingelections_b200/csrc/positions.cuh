@@ -15,6 +15,16 @@
 
 namespace se {
 
+// Bit planes of places (the bit-sliced tally): places are below C, so B = bits of C - 1 planes
+// (at least one) hold them; kMaxPlanes covers C <= 2^20.
+constexpr int kMaxPlanes = 20;
+
+__host__ __device__ inline int planes_for(int C) {
+    int b = 0;
+    for (uint32_t x = uint32_t(C > 1 ? C - 1 : 1); x; x >>= 1) ++b;
+    return b;
+}
+
 constexpr int kPosOk = 0;
 constexpr int kPosRange = 2;   // an id outside [0, C)
 constexpr int kPosRepeat = 3;  // the same id twice

@@ -3,10 +3,12 @@
 //
 // A request is a ballot set already in device memory. It occupies a slot and is a sequence of
 // phases, each a set of independent tasks:
-//   POS     ceil(V/64) tasks: place of every candidate on every (completed) ballot, as f32
-//   TALLY   R(R+1) tasks: counts for one 128 x 64 half of an upper block pair (I <= J),
-//           written as the u32 preference matrix and, shifted into 16 bits, as the closure's
-//           working matrix (d[j][i] = V - d[i][j]; no separate defeat pass)
+//   POS     ceil(V/64) tasks: place of every candidate on every (completed) ballot, as f32,
+//           then packed into bit planes (bit k of 32 ballots' places in one word)
+//   TALLY   R(R+1) tasks: counts for one 128 x 64 half of an upper block pair (I <= J), by the
+//           bit-sliced comparison (see tally.cu), written as the u32 preference matrix and,
+//           shifted into 16 bits, as the closure's working matrix (d[j][i] = V - d[i][j]; no
+//           separate defeat pass)
 //   R == 1 (C <= 128): SMALL (closure, output, wins, ranking in one CTA)
 //   R >= 2: [PIVOT k][PANELS k][REM k] for k < R, then FIN (output + wins per block pair) and
 //           PLACE (ranking)
@@ -52,15 +54,16 @@ constexpr uint32_t kStatusTally = 8;
 constexpr int kPosChunk = 64;   // ballots per POS task
 constexpr int kVC = 32;         // voters per TALLY chunk
 constexpr int kTallyStages = 3;
-constexpr uint32_t kTallyChunkBytes = kVC * 128 * 4 + kVC * 64 * 4;  // posI [32][128] + posJ [32][64]
 constexpr size_t kEngineSmem = pcfg<16>::DATA + 16 * 8;                // data + 16 mbarrier slots
 
 struct alignas(64) Req {
     Elec e;                      // e.d = the u32 preference matrix this request's TALLY writes
-    CUtensorMap mapPos;          // positions f32 [V][Cq], box {64, 32}
+    CUtensorMap mapPl;           // bit planes u32 [ceil(V / 32) * B][Cq], box {64, B}
     const int32_t* ids;          // ballots: ids, most preferred first
     const int64_t* offsets;      // V + 1 CSR offsets, or null when every ballot has exactly C ids
     float* pos;                  // [V][Cq]
+    uint32_t* planes;            // word [ch * B + k][c]: bit k of the places of 32 ballots' candidate c
+    int32_t B;                   // bit planes per 32-ballot chunk
     uint64_t* done_host;         // host-mapped completion word of this slot
     uint32_t* tally_host;        // host-mapped: the generation, once the TALLY phase is done
     uint32_t* flags;             // [0] ballot error (2 range, 3 repeat), [1] 16-bit lane overflow
@@ -291,47 +294,68 @@ __device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v
         const int code = warp_positions<int32_t, true>(Q.ids + beg, len, C, Cq, Q.pos + v * Cq);
         if (code != kPosOk && (threadIdx.x & 31) == 0) atomicCAS(&Q.flags[0], 0u, uint32_t(code));
     }
+    // Pack the task's 32-ballot chunks into bit planes (ballots past V count as place 0). The
+    // places were written by this CTA's warps; read them back through L2.
+    __syncthreads();
+    const int B = Q.B;
+    for (int64_t ch = v0 / 32; ch * 32 < v1; ++ch)
+        for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) {
+            uint32_t pl[kMaxPlanes];
+#pragma unroll
+            for (int k = 0; k < kMaxPlanes; ++k) pl[k] = 0u;
+            for (int v = 0; v < 32; ++v) {
+                const int64_t voter = ch * 32 + v;
+                const uint32_t p = voter < Q.V ? uint32_t(__ldcg(Q.pos + voter * Cq + c)) : 0u;
+#pragma unroll
+                for (int k = 0; k < kMaxPlanes; ++k) pl[k] |= ((p >> k) & 1u) << v;
+            }
+#pragma unroll
+            for (int k = 0; k < kMaxPlanes; ++k)
+                if (k < B) Q.planes[(ch * B + k) * Cq + c] = pl[k];
+        }
 }
 
-__device__ __forceinline__ float sat_sub(float a, float b) {
-    float r;
-    asm("sub.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+__device__ __forceinline__ uint32_t borrow_step(uint32_t a, uint32_t b, uint32_t br) {
+    uint32_t r;
+    asm("lop3.b32 %0, %1, %2, %3, 0x8E;" : "=r"(r) : "r"(a), "r"(b), "r"(br));  // MAJ(~a, b, br)
     return r;
 }
 
 // ------------------------------------------------------------------------------------------
 // TALLY: counts n[i][j] = #{v : pos_v(i) < pos_v(j)} for rows I*128.. and the 64 columns
-// J*128 + h*64.. (I <= J), streamed in 32-ballot chunks through a 3-stage TMA ring. Writes the
-// u32 preferences d (both (i,j) and, for I < J, (j,i) = V - n) and, for R >= 2, the closure's
-// working matrix: kept values (d > V - d) shifted by base into 16 bits, zero elsewhere,
-// including the padding.
+// J*128 + h*64.. (I <= J), streamed in 32-ballot chunks of bit planes through a 3-stage TMA
+// ring. For each chunk the borrow of the bit-serial subtraction pos(i) - pos(j), one lop3 per
+// plane, holds the 32 answers, and a popc adds them. Writes the u32 preferences d (both (i,j)
+// and, for I < J, (j,i) = V - n) and, for R >= 2, the closure's working matrix: kept values
+// (d > V - d) shifted by base into 16 bits, zero elsewhere, including the padding.
 // ------------------------------------------------------------------------------------------
 __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8_t* smem, uint64_t* bars,
                           uint32_t& tpar) {
     const Elec& E = Q.e;
-    float* sA = reinterpret_cast<float*>(smem);                        // [3][32][128]
-    float* sB = sA + kTallyStages * kVC * 128;                         // [3][32][64]
+    const int B = Q.B;
+    const int stage_words = 3 * B * 64;  // planes of rows I (two boxes of 64) and of the 64 columns
+    uint32_t* sbuf = reinterpret_cast<uint32_t*>(smem);
     const int64_t V = Q.V;
     const int nch = int((V + kVC - 1) / kVC);
     const int xI = I * 128, xJ = J * 128 + h * 64;
     auto issue = [&](int ch, int st) {
-        mbar_arrive_expect_tx(&bars[st], kTallyChunkBytes);
-        tma_load_2d(sA + st * kVC * 128, &G->mapPos, &bars[st], xI, ch * kVC);
-        tma_load_2d(sA + st * kVC * 128 + kVC * 64, &G->mapPos, &bars[st], xI + 64, ch * kVC);
-        tma_load_2d(sB + st * kVC * 64, &G->mapPos, &bars[st], xJ, ch * kVC);
+        uint32_t* base = sbuf + st * stage_words;
+        mbar_arrive_expect_tx(&bars[st], uint32_t(stage_words) * 4u);
+        tma_load_2d(base, &G->mapPl, &bars[st], xI, ch * B);
+        tma_load_2d(base + B * 64, &G->mapPl, &bars[st], xI + 64, ch * B);
+        tma_load_2d(base + 2 * B * 64, &G->mapPl, &bars[st], xJ, ch * B);
     };
-    // posI [32][128] arrives as two [32][64] boxes: columns 0-63 then 64-127.
     if (threadIdx.x == 0) {
-        fence_tensormap(&G->mapPos);
+        fence_tensormap(&G->mapPl);
         fence_proxy_async();
         for (int st = 0; st < kTallyStages && st < nch; ++st) issue(st, st);
     }
     const geom g(threadIdx.x);
-    float acc[8][8];
+    uint32_t acc[8][8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[r][q] = 0.0f;
+        for (int q = 0; q < 8; ++q) acc[r][q] = 0u;
     bool ok = true;
     // Row r of the thread lives in box (row0 + r) / 64 at column (row0 + r) % 64.
     const int boxA = g.row0 / 64, colA = g.row0 % 64;
@@ -342,22 +366,29 @@ __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8
         if (ok && !mbar_wait_bounded(&bars[st], par, 1u << 26)) ok = false;
         tpar ^= 1u << st;
         if (ok) {
-            const float* A = sA + st * kVC * 128 + boxA * kVC * 64;
-            const float* B = sB + st * kVC * 64;
-#pragma unroll 4
-            for (int v = 0; v < kVC; ++v) {
-                float a[8], b[8];
-                const float4 a0 = *reinterpret_cast<const float4*>(A + v * 64 + colA);
-                const float4 a1 = *reinterpret_cast<const float4*>(A + v * 64 + colA + 4);
-                const float4 b0 = *reinterpret_cast<const float4*>(B + v * 64 + g.wbase);
-                const float4 b1 = *reinterpret_cast<const float4*>(B + v * 64 + g.wbase + 32);
-                a[0] = a0.x, a[1] = a0.y, a[2] = a0.z, a[3] = a0.w, a[4] = a1.x, a[5] = a1.y, a[6] = a1.z, a[7] = a1.w;
-                b[0] = b0.x, b[1] = b0.y, b[2] = b0.z, b[3] = b0.w, b[4] = b1.x, b[5] = b1.y, b[6] = b1.z, b[7] = b1.w;
+            const uint32_t* A = sbuf + st * stage_words + boxA * B * 64;
+            const uint32_t* Bp = sbuf + st * stage_words + 2 * B * 64;
+            uint32_t br[8][8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) br[r][q] = 0u;
+#pragma unroll 1
+            for (int k = 0; k < B; ++k) {
+                uint32_t a[8], b[8];
+                ld4(a, A + k * 64 + colA);
+                ld4(a + 4, A + k * 64 + colA + 4);
+                ld4(b, Bp + k * 64 + g.wbase);
+                ld4(b + 4, Bp + k * 64 + g.wbase + 32);
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) acc[r][q] += sat_sub(b[q], a[r]);
+                    for (int q = 0; q < 8; ++q) br[r][q] = borrow_step(a[r], b[q], br[r][q]);
             }
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[r][q] += __popc(br[r][q]);
         }
         __syncthreads();  // everyone is done with stage st
         if (threadIdx.x == 0 && ok && ch + kTallyStages < nch) {
@@ -377,7 +408,7 @@ __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int j = xJ + g.wbase + (q < 4 ? q : 28 + q);
-            const uint32_t n = uint32_t(acc[r][q]), m = Vu - n;
+            const uint32_t n = acc[r][q], m = Vu - n;
             const bool live = i < C && j < C && i != j;
             if (i < C && j < C) {
                 uint32_t* d = const_cast<uint32_t*>(E.d);
@@ -793,9 +824,12 @@ extern "C" int64_t se_engine_request_scratch_bytes(int64_t V, int C) {
     return scratch_layout(C).total;
 }
 
+// Places f32 [V][Cq], then the bit planes u32 [ceil(V / 32) * B][Cq].
+static int64_t planes_offset(int64_t V, int C) { return round_up(V * round_up(C, kT) * 4, 256); }
+
 extern "C" int64_t se_engine_request_positions_bytes(int64_t V, int C) {
     if (V < 1 || C < 1) return -1;
-    return V * round_up(C, kT) * 4;
+    return planes_offset(V, C) + (V + kVC - 1) / kVC * planes_for(C) * round_up(C, kT) * 4;
 }
 
 extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, void* stream_, int* slot_out,
@@ -855,7 +889,10 @@ extern "C" se_status_t se_engine_submit(se_engine_t* h, const se_request_t* rq, 
         if (se_status_t st = make_map(&e.mapDT, e.dT, kT, kT, kT * 4, kT, kKC)) return st;
     }
     q.pos = static_cast<float*>(rq->d_positions);
-    if (se_status_t st = make_map(&q.mapPos, q.pos, uint64_t(L.Cq), uint64_t(V), uint64_t(L.Cq) * 4, 64, kVC))
+    q.B = planes_for(C);
+    q.planes = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(rq->d_positions) + planes_offset(V, C));
+    if (se_status_t st = make_map(&q.mapPl, q.planes, uint64_t(L.Cq), uint64_t((V + kVC - 1) / kVC * q.B),
+                                  uint64_t(L.Cq) * 4, 64, uint32_t(q.B)))
         return st;
     q.ids = rq->d_ids;
     q.offsets = rq->d_offsets;

@@ -89,14 +89,7 @@ void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, in
 // C - 1 planes that is about (B + 2) / 32 ALU instructions per voter pair, against two FP32
 // instructions in the direct form.
 // ------------------------------------------------------------------------------------------
-constexpr int kMaxPlanes = 20;  // C <= 2^20
 constexpr int kBitStages = 4;
-
-__host__ __device__ inline int planes_for(int C) {
-    int b = 0;
-    for (uint32_t x = uint32_t(C > 1 ? C - 1 : 1); x; x >>= 1) ++b;
-    return b;
-}
 
 // planes[(ch * B + k) * Cq + c] for the chunks of voters [0, V); voters past V count as place 0.
 __global__ void __launch_bounds__(256)
@@ -267,7 +260,7 @@ using namespace se;
 using namespace se::tally;
 
 // Error word (256 B), then the places f32 [V][Cq], then the bit planes u32 [ceil(V/32) * B][Cq].
-int64_t planes_offset(int64_t V, int C) { return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256); }
+static int64_t planes_offset(int64_t V, int C) { return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256); }
 
 extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
     if (V < 0 || C < 1) return -1;
