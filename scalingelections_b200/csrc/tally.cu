@@ -33,7 +33,7 @@ namespace tally {
 
 constexpr int kTile = 128;     // candidates per tile edge
 constexpr int kVC = 32;        // voters per TMA chunk
-constexpr int kThreads = 256;  // 8 x 8 cells per thread
+constexpr int kThreads = 512;  // 8 x 4 cells per thread
 constexpr uint32_t kErrRange = 2;
 constexpr uint32_t kErrRepeat = 3;
 constexpr uint32_t kErrTimeout = 1;
@@ -163,14 +163,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_load_2d(sJ + s * stage_words, &mapPl, &bars[s], J * kTile, (ch0 + s) * B);
         }
     }
+    // 16 warps: rows row0..row0+7 and columns col0..col0+3 of the tile per thread. A warp's 8
+    // column groups read 128 contiguous bytes of a plane; its 4 row groups read 4 x 32 bytes.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row0 = (warp & 3) * 32 + (lane >> 3) * 8;
-    const int col0 = (warp >> 2) * 64 + (lane & 7) * 4;  // cols col0..+3 and col0+32..+35
-    uint32_t acc[8][8];
+    const int col0 = (warp >> 2) * 32 + (lane & 7) * 4;
+    uint32_t acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0u;
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0u;
 
     bool ok = true;
 #pragma unroll 1
@@ -180,29 +182,28 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (ok) {
             const uint32_t* pI = sI + s * stage_words;
             const uint32_t* pJ = sJ + s * stage_words;
-            uint32_t br[8][8];
+            uint32_t br[8][4];
 #pragma unroll
             for (int r = 0; r < 8; ++r)
 #pragma unroll
-                for (int q = 0; q < 8; ++q) br[r][q] = 0u;
+                for (int q = 0; q < 4; ++q) br[r][q] = 0u;
 #pragma unroll 2
             for (int k = 0; k < B; ++k) {
-                uint32_t a[8], b[8];
+                uint32_t a[8], b[4];
                 const uint4 a0 = *reinterpret_cast<const uint4*>(pI + k * kTile + row0);
                 const uint4 a1 = *reinterpret_cast<const uint4*>(pI + k * kTile + row0 + 4);
                 const uint4 b0 = *reinterpret_cast<const uint4*>(pJ + k * kTile + col0);
-                const uint4 b1 = *reinterpret_cast<const uint4*>(pJ + k * kTile + col0 + 32);
                 a[0] = a0.x, a[1] = a0.y, a[2] = a0.z, a[3] = a0.w, a[4] = a1.x, a[5] = a1.y, a[6] = a1.z, a[7] = a1.w;
-                b[0] = b0.x, b[1] = b0.y, b[2] = b0.z, b[3] = b0.w, b[4] = b1.x, b[5] = b1.y, b[6] = b1.z, b[7] = b1.w;
+                b[0] = b0.x, b[1] = b0.y, b[2] = b0.z, b[3] = b0.w;
 #pragma unroll
                 for (int r = 0; r < 8; ++r)
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) br[r][q] = borrow_step(a[r], b[q], br[r][q]);
+                    for (int q = 0; q < 4; ++q) br[r][q] = borrow_step(a[r], b[q], br[r][q]);
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r)
 #pragma unroll
-                for (int q = 0; q < 8; ++q) acc[r][q] += __popc(br[r][q]);
+                for (int q = 0; q < 4; ++q) acc[r][q] += __popc(br[r][q]);
         }
         __syncthreads();  // every thread is done with stage s
         if (threadIdx.x == 0 && ok && ch + kBitStages < nch) {
@@ -222,8 +223,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int r = 0; r < 8; ++r) {
         const int i = I * kTile + row0 + r;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int j = J * kTile + col0 + (q < 4 ? q : 28 + q);
+        for (int q = 0; q < 4; ++q) {
+            const int j = J * kTile + col0 + q;
             const uint32_t n = acc[r][q];
             if (i < C && j < C) {
                 uint32_t* ij = out + int64_t(i) * ld_out + j;
