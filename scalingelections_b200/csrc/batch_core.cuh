@@ -211,9 +211,15 @@ constexpr int kTileRem = 2;
 // mapB / kb: where the pivot rows S[K][*] (B of row and remainder tiles, D of column tiles)
 // are read: by default G->mapS at row block K; a sharded closure passes the map of a
 // received panel buffer (kb = 0) or of its own slab (kb = the local row block).
+// kvalid / rvalid: pivots of round K and rows of the tile that lie inside the C candidates
+// (by default from K and the tile's row block; a sharded closure, whose K and I are local,
+// passes them). Padding holds zeros in both operands, and a cell's relaxation through a zero
+// operand leaves it unchanged, so 32-pivot chunks and 32-row warps wholly past C skip the
+// product (their copies too), with identical results.
 template <int LB, bool GLOBAL_MAPS = true>
 __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
-                         uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1) {
+                         uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1,
+                         int kvalid = -1, int rvalid = -1) {
     using CF = cfg<LB>;
     constexpr int TW = CF::TW;
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);
@@ -227,6 +233,10 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     uint32_t* Ct;
     if (mapB == nullptr) mapB = &G->mapS;
     if (kb < 0) kb = K;
+    if (kvalid < 0) kvalid = E.C - K * kT;
+    if (rvalid < 0) rvalid = E.C - (kind == kTileRow ? K : I) * kT;
+    const int nch = kvalid >= kT ? kChunks : (kvalid + kKC - 1) / kKC;  // chunks holding pivots
+    const bool live = (g.row0 & ~31) < rvalid;                         // this warp holds real rows
     if (kind != kTileCol) {
         const bool rem = kind == kTileRem;
         const CUtensorMap* mapA = rem ? &G->mapAT : &G->mapDT;
@@ -238,6 +248,10 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
+                if (ch >= nch) {
+                    mbar_arrive(&bars[ch]);
+                    continue;
+                }
                 mbar_arrive_expect_tx(&bars[ch], CF::A_BYTES + CF::B_BYTES);
                 tma_load_2d(As + ch * CF::A_CHUNK, mapA, &bars[ch], rem ? I * kT : 0, ch * kKC);
                 tma_load_2d(Bs + ch * CF::B_CHUNK, mapB, &bars[ch], J * TW, kb * kT + ch * kKC);
@@ -281,6 +295,10 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             fence_proxy_async();
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
+                if (ch >= nch) {
+                    mbar_arrive(&bars[kChunks + ch]);
+                    continue;
+                }
                 mbar_arrive_expect_tx(&bars[kChunks + ch], CF::B_BYTES);
                 tma_load_2d(Bs + ch * CF::B_CHUNK, mapB, &bars[kChunks + ch], K * TW, kb * kT + ch * kKC);
             }
@@ -292,13 +310,14 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
         par_b ^= 1u;
     }
     if (ok) {
+        // Chunks past nch: thread 0 completed their phases without a copy; nobody waits.
 #pragma unroll 1
-        for (int ch = 0; ch < kChunks; ++ch) {
+        for (int ch = 0; ch < nch; ++ch) {
             if (!mbar_wait_bounded(&wait_bars[ch], wait_par, 1u << 26)) {
                 ok = false;
                 break;
             }
-            relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+            if (live) relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
         }
     }
     if (ok) {

@@ -77,7 +77,8 @@ constexpr int kPhaseColPanel = 1;
 constexpr int kPhaseRemainder = 2;
 
 // One phase of round k on the slab. E describes the slab: S is its first row, mapS covers its
-// rows, AT is indexed by local row block. own: this shard holds row block k (local kl), so the
+// rows, AT is indexed by local row block; b0 is the slab's first global row block. own: this
+// shard holds row block k (local kl), so the
 // pivot rows are read from its own slab; otherwise from the panel buffer (mapP, row block 0).
 // fuse_next >= 0 (remainder phase only): this shard also holds row block k + 1, at local index
 // fuse_next. Block 0 then takes tile (k+1, k+1) and, after updating it, closes it as round
@@ -87,7 +88,7 @@ constexpr int kPhaseRemainder = 2;
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     shard_tiles_kernel(const __grid_constant__ Elec E, const __grid_constant__ CUtensorMap mapP, int phase, int k,
-                       int kl, int own, int fuse_next, int kmax_next, uint32_t* __restrict__ err) {
+                       int kl, int b0, int own, int fuse_next, int kmax_next, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
@@ -123,7 +124,9 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         J = jj + (jj >= k);
     }
     uint32_t pa = 0, pb = 0;
-    const bool ok = run_tile<LB, false>(E, &E, kind, K, I, J, smem, bars, pa, pb, mapB, kb);
+    const int rblock = kind == kTileRow ? k : b0 + I;  // the tile's global row block
+    const bool ok = run_tile<LB, false>(E, &E, kind, K, I, J, smem, bars, pa, pb, mapB, kb, E.C - k * kT,
+                                        E.C - rblock * kT);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
@@ -288,7 +291,7 @@ template <int LB> se_status_t pivot_impl(se_shard& h, int k, cudaStream_t s) {
     h.pivot_ready = -1;
     if (E.R > 1) {
         shard_tiles_kernel<LB><<<unsigned(E.R - 1), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseRowPanel, k,
-                                                                                         kl, 1, -1, 0, h.err);
+                                                                                         kl, h.b0, 1, -1, 0, h.err);
         SE_CHECK_LAUNCH();
     }
     return SE_OK;
@@ -302,7 +305,7 @@ template <int LB> se_status_t update_impl(se_shard& h, int k, cudaStream_t s) {
     const int rows = own ? h.nloc - 1 : h.nloc;  // local row blocks other than k
     if (rows <= 0) return SE_OK;
     shard_tiles_kernel<LB><<<unsigned(rows), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseColPanel, k, kl,
-                                                                                  own ? 1 : 0, -1, 0, h.err);
+                                                                                  h.b0, own ? 1 : 0, -1, 0, h.err);
     SE_CHECK_LAUNCH();
     if (E.R > 1) {
         // Close round k+1's pivot inside this launch when this shard holds row block k+1.
@@ -310,7 +313,7 @@ template <int LB> se_status_t update_impl(se_shard& h, int k, cudaStream_t s) {
         const int fuse = next < E.R && next >= h.b0 && next < h.b1 ? next - h.b0 : -1;
         const int kmax_next = fuse >= 0 ? (E.C - next * kT < kT ? E.C - next * kT : kT) : 0;
         shard_tiles_kernel<LB><<<unsigned(rows * (E.R - 1)), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(
-            E, h.mapP, kPhaseRemainder, k, kl, own ? 1 : 0, fuse, kmax_next, h.err);
+            E, h.mapP, kPhaseRemainder, k, kl, h.b0, own ? 1 : 0, fuse, kmax_next, h.err);
         SE_CHECK_LAUNCH();
         if (fuse >= 0) h.pivot_ready = next;
     }

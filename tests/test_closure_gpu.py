@@ -40,6 +40,17 @@ def test_odd_sizes_against_oracle(orc, C):
             assert np.array_equal(gpu_closure(P, lanes), S_ref), (C, hi, lanes)
 
 
+@pytest.mark.parametrize("C", [160, 161, 192, 193, 224, 225, 288, 353, 415])
+def test_padding_skip_boundaries(orc, C):
+    """The last row block holds C mod 128 real pivots and rows; tiles skip the 32-pivot chunks
+    and 32-row warps wholly past C. Sizes on each side of the 32-cell steps."""
+    rng = np.random.default_rng(C + 17)
+    P = rng.integers(0, 3000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    S_ref = orc.strongest_paths(P, "blocked", tile=16)
+    for lanes in (LANES_U16, LANES_U32):
+        assert np.array_equal(gpu_closure(P, lanes), S_ref), (C, lanes)
+
+
 def test_u32_values_beyond_16_bits(orc):
     rng = np.random.default_rng(5)
     P = rng.integers(0, 2**32 - 1, size=(300, 300), dtype=np.uint64).astype(np.uint32)
