@@ -218,6 +218,17 @@ def load_traffic(lanes: int, C: int):
     return b_ref * tiles(C) / tiles(C_ref)
 
 
+def measured_hbm_gbs() -> tuple[float, str]:
+    """HBM copy bandwidth of this GPU model: the measured figure when MEASURED_PEAKS.json is
+    present, else an earlier measurement on the same B200 pool."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        v = float(json.loads(p.read_text())["hbm_gbs"])
+        return v, "measured: MEASURED_PEAKS.json hbm_gbs (STREAM-style copy)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback: 6.65 TB/s copy measured earlier on this GPU model"
+
+
 def run_ours(args, world, rank, local_rank):
     import numpy as np
     import torch
@@ -321,6 +332,31 @@ def run_ours(args, world, rank, local_rank):
                  "same_as_input": bool(torch.equal(d2.view(torch.int32), d.view(torch.int32)))}
         del tw, d2, ballots
 
+    # Ranking (se_rank: wins + stable places) of the closure's u32 output, which is larger
+    # than L2: algorithmic bytes = the C x C u32 matrix read once.
+    wins_t = torch.empty(C, dtype=torch.int32, device=dev)
+    rank_t = torch.empty(C, dtype=torch.int32, device=dev)
+
+    def rank_once():
+        _lib.check(L.se_rank(out.data_ptr(), C, C, wins_t.data_ptr(), rank_t.data_ptr(), stream.cuda_stream))
+
+    for _ in range(2):
+        rank_once()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    for _ in range(5):
+        rank_once()
+    r1.record(stream)
+    torch.cuda.synchronize()
+    rank_s = r0.elapsed_time(r1) / 5e3
+    hbm_peak, hbm_source = measured_hbm_gbs()
+    rank_bytes = float(C) * C * 4
+    ranking = {"ms": rank_s * 1e3, "kernels": ["wins_kernel", "place_kernel"],
+               "roofline": {"bound": "hbm", "achieved": rank_bytes / rank_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                            "frac": rank_bytes / rank_s / 1e9 / hbm_peak, "algorithmic_bytes": rank_bytes,
+                            "peak_source": hbm_source},
+               "winner": int(rank_t[0].item())}
+
     e2e = None
     if not args.no_e2e:
         host_in = torch.empty((C, C), dtype=torch.int32, pin_memory=True)
@@ -371,6 +407,7 @@ def run_ours(args, world, rank, local_rank):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "tally": tally,
+            "ranking": ranking,
             "clocks": clocks.summary(),
             "gpu_launches": int(L.se_closure_launch_count(C)) * args.steps,
         }

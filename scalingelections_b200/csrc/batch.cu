@@ -54,6 +54,44 @@ struct Header {
     unsigned long long wait_ns;
 };
 
+// The counter a task of election E waits for and the value it must reach; false for a task
+// with no dependency (SMALL, and PIVOT 0).
+__device__ __forceinline__ bool task_dependency(const Elec& E, uint32_t type, uint32_t k, const uint32_t*& ctr,
+                                                uint32_t& target) {
+    const uint32_t R = uint32_t(E.R);
+    if (type == kPivot && k > 0) {
+        ctr = &E.counters[2 * R + k - 1];
+        target = (R - 1) * (R - 1);
+    } else if (type == kRow || type == kCol) {
+        ctr = &E.counters[k];
+        target = 1u;
+    } else if (type == kRem) {
+        ctr = &E.counters[R + k];
+        target = 2u * (R - 1);
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// One thread: claims the next task of the queue into s_next, and records whether its
+// dependency is met already (counters only grow, so it stays met).
+__device__ __forceinline__ void claim_task(const Elec* elecs, const uint64_t* tasks, uint32_t ntasks, Header* hdr,
+                                           int queue, uint64_t& s_next, uint32_t& s_ready) {
+    uint64_t t = kNoTask;
+    uint32_t ready = 0;
+    const uint32_t n = atomicAdd(&hdr->head[queue], 1u);
+    if (n < ntasks && !ld_acquire(&hdr->abort)) {
+        t = tasks[n];
+        const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u, k = uint32_t(t >> 24) & 0xFFFu;
+        const uint32_t* ctr;
+        uint32_t target;
+        ready = !task_dependency(elecs[e], type, k, ctr, target) || ld_acquire(ctr) >= target;
+    }
+    s_next = t;
+    s_ready = ready;
+}
+
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     persistent_kernel(const Elec* __restrict__ elecs, const uint64_t* __restrict__ tasks, uint32_t ntasks,
@@ -63,39 +101,42 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
     __shared__ __align__(16) uint32_t colbuf[2][kT];
     __shared__ int32_t s_wins[kT];
-    __shared__ uint64_t s_task;
-    __shared__ uint32_t s_go;
+    __shared__ uint64_t s_task, s_next;
+    __shared__ uint32_t s_go, s_ready;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
         for (int b = 0; b < 2 * kChunks; ++b) mbar_init(&bars[b], 1);
         fence_barrier_init();
     }
+    if (threadIdx.x == 32) claim_task(elecs, tasks, ntasks, hdr, queue, s_next, s_ready);
     __syncthreads();
     uint32_t par_a = 0, par_b = 0;  // phase parity of barriers [0, 4) and [4, 8)
 
+    // The next task is claimed by thread 32 (warp 1) while the current task's first copies are
+    // in flight, so only its dependency wait, when not met at claim time, stays between tasks.
+    // No task waits while it runs, and every dependency precedes its dependents in the queue,
+    // so a task claimed ahead never blocks the tasks it depends on.
     for (;;) {
         if (threadIdx.x == 0) {
-            uint64_t t = kNoTask;
-            if (!ld_acquire(&hdr->abort)) {
-                const uint32_t n = atomicAdd(&hdr->head[queue], 1u);
-                if (n < ntasks) t = tasks[n];
-            }
+            const uint64_t t = s_next;
             s_task = t;
             s_go = 1;
             if (t != kNoTask) {
-                const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u, k = uint32_t(t >> 24) & 0xFFFu;
-                const Elec& E = elecs[e];
-                const uint32_t R = uint32_t(E.R);
-                bool ok = true;
-                const uint64_t w0 = global_ns();
-                if (type == kPivot && k > 0) ok = wait_counter(&E.counters[2 * R + k - 1], (R - 1) * (R - 1), &hdr->abort);
-                else if (type == kRow || type == kCol) ok = wait_counter(&E.counters[k], 1u, &hdr->abort);
-                else if (type == kRem) ok = wait_counter(&E.counters[R + k], 2u * (R - 1), &hdr->abort);
-                atomicAdd(&hdr->wait_ns, (unsigned long long)(global_ns() - w0));
-                if (!ok) {
-                    raise_device_error(&hdr->err, kErrDepTimeout);
-                    atomicExch(&hdr->abort, 1u);
-                    s_go = 0;
+                if (!s_ready) {
+                    const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u,
+                                   k = uint32_t(t >> 24) & 0xFFFu;
+                    const uint32_t* ctr;
+                    uint32_t target;
+                    if (task_dependency(elecs[e], type, k, ctr, target)) {
+                        const uint64_t w0 = global_ns();
+                        const bool ok = wait_counter(ctr, target, &hdr->abort);
+                        atomicAdd(&hdr->wait_ns, (unsigned long long)(global_ns() - w0));
+                        if (!ok) {
+                            raise_device_error(&hdr->err, kErrDepTimeout);
+                            atomicExch(&hdr->abort, 1u);
+                            s_go = 0;
+                        }
+                    }
                 }
                 fence_proxy_async_global();
             }
@@ -103,6 +144,7 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         __syncthreads();
         const uint64_t t = s_task;
         if (t == kNoTask || !s_go) break;
+        if (threadIdx.x == 32) claim_task(elecs, tasks, ntasks, hdr, queue, s_next, s_ready);
         const uint32_t e = uint32_t(t >> 39), type = uint32_t(t >> 36) & 7u, k = uint32_t(t >> 24) & 0xFFFu;
         const uint32_t i = uint32_t(t >> 12) & 0xFFFu, j = uint32_t(t) & 0xFFFu;
         const Elec& E = elecs[e];

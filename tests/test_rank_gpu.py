@@ -31,6 +31,19 @@ def test_ties_keep_index_order(orc):
         assert np.array_equal(r.cpu().numpy(), rank_ref)
 
 
+@pytest.mark.parametrize("C", [1, 2, 63, 64, 65, 128, 129, 2048, 2049, 4100, 6000])
+def test_wins_and_places_across_tile_and_strip_edges(orc, C):
+    """Sizes on each side of the 64-cell tile pairs and of the 128-candidate / 2048-entry strips
+    of the place count; with ties (values in [0, 3)) and without (values up to 2^32 - 1)."""
+    rng = np.random.default_rng(C + 5)
+    for hi in (3, 2**32 - 1):
+        S = rng.integers(0, hi, size=(C, C), dtype=np.uint64).astype(np.uint32)
+        wins_ref, rank_ref = orc.wins_and_ranking(S)
+        w, r = api.rank_device(api._to_device_u32(S, "cuda"))
+        assert np.array_equal(w.cpu().numpy(), wins_ref), (C, hi)
+        assert np.array_equal(r.cpu().numpy(), rank_ref), (C, hi)
+
+
 def test_candidate_labels():
     S = np.array([[0, 2, 2], [1, 0, 1], [1, 2, 0]], np.uint32)
     assert api.get_winner_and_ranking(["a", "b", "c"], S) == ("a", ["a", "c", "b"])
