@@ -826,7 +826,7 @@ def run_ingest(args, world, rank, local_rank):
             "data": "synthetic (seeded Mallows(0.8) orders, truncated to uniform lengths)",
             "config": {"workload": f"ballot file ingest: V={V} incomplete ballots, C={C}, 16-bit ids, "
                                    f"{chunk} ballots per chunk", "file_bytes": file_bytes,
-                       "chunks": stats.get("chunks"), "host_read_s_per_step": stats.get("read_s"),
+                       "chunks": stats.get("chunks"), "host_read_wait_s_per_step": stats.get("read_wait_s"),
                        "read_threads": stats.get("read_threads")},
             "file_gbs": file_bytes / e2e_s / 1e9,
             "kernel": {"ms": kernel_s * 1e3, "ballots_per_s": V / kernel_s, "pairs_per_s": pairs / kernel_s},

@@ -234,9 +234,9 @@ class BallotFile:
             yield v0, min(v0 + step, self.num_voters)
 
 
-def _pread_into(fd: int, dst: np.ndarray, file_offset: int, pool: ThreadPoolExecutor, threads: int) -> None:
-    """Fill the byte view dst from the file at file_offset with parallel pread calls, about two
-    pieces per thread (at least 1 MiB each)."""
+def _pread_pieces(fd: int, dst: np.ndarray, file_offset: int, pool: ThreadPoolExecutor, threads: int) -> list:
+    """Queues parallel pread calls that fill the byte view dst from the file at file_offset,
+    about two pieces per thread (at least 1 MiB each); returns their futures."""
     buf = dst.view(np.uint8).reshape(-1)
     n = buf.size
     mv = memoryview(buf)
@@ -251,7 +251,7 @@ def _pread_into(fd: int, dst: np.ndarray, file_offset: int, pool: ThreadPoolExec
                 raise ValueError("truncated ballot file")
             got += r
 
-    list(pool.map(read, range(0, n, piece)))
+    return [pool.submit(read, a) for a in range(0, n, piece)]
 
 
 def default_chunk_ballots(num_candidates: int, positions_bytes: int = 1 << 30) -> int:
@@ -298,50 +298,70 @@ def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | Non
         raise ValueError("invalid chunk size")
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     ragged = bf.offsets is not None
-    host_ids = [torch.empty(max(max_ids, 1), dtype=id_dtype, pin_memory=True) for _ in range(2)]
+    # Three pinned host buffers: the reads of chunk n + 1 are queued before the wait for chunk n,
+    # so the reader threads run on across chunk boundaries while a third buffer still feeds the
+    # copy of chunk n - 1. Two device buffers: the copy of chunk n waits for the tally of n - 2.
+    nh = 3
+    host_ids = [torch.empty(max(max_ids, 1), dtype=id_dtype, pin_memory=True) for _ in range(nh)]
     dev_ids = [torch.empty(max(max_ids, 1), dtype=id_dtype, device=dev) for _ in range(2)]
-    host_offs = [torch.empty(nv + 1, dtype=torch.int64, pin_memory=True) for _ in range(2)] if ragged else None
-    dev_offs = [torch.empty(nv + 1, dtype=torch.int64, device=dev) for _ in range(2)] if ragged else None
+    # The whole offsets array goes to the device once (8 bytes per ballot); each chunk's tally
+    # reads its slice there with id_base = the chunk's first id. Per-chunk host copies of it
+    # would run in this thread between the readers' calls, each one waiting for the GIL.
+    all_offs = torch.from_numpy(np.array(bf.offsets, dtype=np.int64)).to(dev) if ragged else None  # a writable copy
+    chunks = list(bf.chunks(nv))
     with torch.cuda.device(dev):
         compute = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(dev)
-        copied = [torch.cuda.Event() for _ in range(2)]
+        copied = [torch.cuda.Event() for _ in range(nh)]
         consumed = [torch.cuda.Event() for _ in range(2)]
-        used = [False, False]
+        host_used = [False] * nh
+        dev_used = [False, False]
         fd = os.open(bf.path, os.O_RDONLY)
-        read_s = 0.0
+        wait_s = 0.0
+        pending: dict[int, list] = {}
         try:
             with ThreadPoolExecutor(max_workers=max(1, threads)) as pool:
-                for n, (v0, v1) in enumerate(bf.chunks(nv)):
-                    b = n & 1
-                    if used[b]:
-                        copied[b].synchronize()  # the pinned buffer's previous copy has finished
+
+                def queue_read(n: int) -> None:
+                    hb = n % nh
+                    if host_used[hb]:
+                        copied[hb].synchronize()  # the copy out of this pinned buffer has finished
+                    v0, v1 = chunks[n]
+                    a, z = bf.span(v0, v1)
+                    pending[n] = _pread_pieces(fd, host_ids[hb][:z - a].numpy().view(np_dtype),
+                                               h.ids_offset + a * width, pool, threads)
+
+                queue_read(0)
+                for n, (v0, v1) in enumerate(chunks):
+                    if n + 1 < len(chunks):
+                        queue_read(n + 1)
+                    hb, db = n % nh, n & 1
                     a, z = bf.span(v0, v1)
                     t0 = time.perf_counter()
-                    _pread_into(fd, host_ids[b][:z - a].numpy().view(np_dtype), h.ids_offset + a * width, pool,
-                                threads)
-                    if ragged:
-                        host_offs[b][:v1 - v0 + 1].copy_(torch.from_numpy(np.array(bf.offsets[v0:v1 + 1])))
-                    read_s += time.perf_counter() - t0
+                    for f in pending.pop(n):
+                        f.result()
+                    wait_s += time.perf_counter() - t0
                     with torch.cuda.stream(copy):
-                        if used[b]:
-                            copy.wait_event(consumed[b])  # the tally of two chunks ago is done with it
-                        dev_ids[b][:z - a].copy_(host_ids[b][:z - a], non_blocking=True)
-                        if ragged:
-                            dev_offs[b][:v1 - v0 + 1].copy_(host_offs[b][:v1 - v0 + 1], non_blocking=True)
-                        copied[b].record(copy)
-                    compute.wait_event(copied[b])
+                        if dev_used[db]:
+                            copy.wait_event(consumed[db])  # the tally of two chunks ago is done with it
+                        dev_ids[db][:z - a].copy_(host_ids[hb][:z - a], non_blocking=True)
+                        copied[hb].record(copy)
+                    host_used[hb] = True
+                    compute.wait_event(copied[hb])
                     flags = SE_TALLY_ACCUMULATE | SE_TALLY_NO_SYNC | (SE_TALLY_KEEP_ERROR if n else 0)
-                    check(L.se_tally_ex(dev_ids[b].data_ptr(), width, dev_offs[b].data_ptr() if ragged else None, a,
-                                        v1 - v0, C, flags, out.data_ptr(), out.stride(0), work.data_ptr(), need,
-                                        compute.cuda_stream))
-                    consumed[b].record(compute)
-                    used[b] = True
+                    offs_ptr = all_offs.data_ptr() + 8 * v0 if ragged else None
+                    check(L.se_tally_ex(dev_ids[db].data_ptr(), width, offs_ptr, a, v1 - v0, C, flags, out.data_ptr(),
+                                        out.stride(0), work.data_ptr(), need, compute.cuda_stream))
+                    consumed[db].record(compute)
+                    dev_used[db] = True
         finally:
+            for fs in pending.values():  # an error left reads queued: let them finish before closing
+                for f in fs:
+                    f.exception()
             os.close(fd)
         code = int(work[:4].view(torch.int32).cpu().item())  # synchronises the compute stream
     if stats is not None:
-        stats.update(chunks=-(-V // nv), chunk_ballots=nv, read_s=read_s, file_bytes=os.path.getsize(bf.path),
+        stats.update(chunks=-(-V // nv), chunk_ballots=nv, read_wait_s=wait_s, file_bytes=os.path.getsize(bf.path),
                      read_threads=threads)
     if code == 2:
         raise ValueError(f"a ballot names a candidate outside [0, {C})")

@@ -5,10 +5,9 @@
 //                stable sorted(..., key=wins, reverse=True) keeps ties in input order)
 //
 // wins_kernel takes one pair of 64 x 64 tiles (I <= J, enumerated over the upper triangle so
-// that no block idles): S[I][J] is read straight into registers and S[J][I] through a
-// shared-memory transpose, every cell of S once, 128 coalesced bytes per warp load. Row wins
-// are counted by warp ballots, column wins in registers; one global atomic per candidate per
-// tile pair. place_kernel gives candidate i the place #{j : wins[j] > wins[i]} +
+// that no block idles): S[I][J] is read straight into registers and S[J][I] through a swizzled
+// shared-memory tile, every cell of S once, in 128-bit loads. Both endpoints' wins accumulate
+// in registers; one global atomic per candidate per tile pair. place_kernel gives candidate i the place #{j : wins[j] > wins[i]} +
 // #{j < i : wins[j] == wins[i]}, which is exactly the stable order, by counting over strips of
 // the wins in shared memory (four per 128-bit load, eight slices of each strip counted side
 // by side); a slice wholly before or after the block's candidates needs one compare per pair.
@@ -33,59 +32,87 @@ __device__ __forceinline__ void tile_pair(int64_t b, int nt, int& I, int& J) {
     J = int(r + (b - start(r)));
 }
 
+// Thread (ry, cx) of wins_kernel holds rows ry + 16p (p < 4) and columns 4cx .. 4cx+3 of the
+// tile S[I][J] in registers (128-bit loads), and loads the same positions of S[J][I] into
+// shared memory, where element (r, c) of that tile sits at r * 64 + (c ^ 2 * ((r >> 2) & 15)):
+// rows stay 16-byte groups (stores are one 128-bit write, conflict free), and the column reads
+// of the compare loop (row 4cx + q, column ry + 16p) fall on 32 distinct banks per warp.
+// Pair (i, j) = (i0 + r, j0 + c) is then one shared load, two compares and two adds: row wins
+// (S[i][j] > S[j][i]) and column wins (S[j][i] > S[i][j]) accumulate in registers. On a
+// diagonal tile (I = J) every ordered pair is in the tile, so only row wins are counted.
+__device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
+
 __global__ void __launch_bounds__(256)
-    wins_kernel(const uint32_t* __restrict__ S, int64_t ld, int C, int nt, int32_t* __restrict__ wins) {
-    __shared__ uint32_t t[kRT][kRT + 1];  // t[x][y] = S[j0 + y][i0 + x]
-    __shared__ int32_t wrow[2][kRT];      // row wins per half-row warp
-    __shared__ int32_t wcol[4][kRT];      // column wins per row group
+    wins_kernel(const uint32_t* __restrict__ S, int64_t ld, int C, int nt, int vec, int32_t* __restrict__ wins) {
+    __shared__ __align__(16) uint32_t bs[kRT * kRT];
+    __shared__ int32_t colpart[16][kRT];  // column wins per row group ry
     int I, J;
     tile_pair(blockIdx.x, nt, I, J);
     const int i0 = I * kRT, j0 = J * kRT;
-    const int tx = threadIdx.x & (kRT - 1), ty = threadIdx.x >> 6;  // 64 x 4
-    const int j = j0 + tx, ci = i0 + tx;
-    const bool full = i0 + kRT <= C && j0 + kRT <= C;
-    uint32_t sij[kRT / 4];
-    if (full) {  // interior tile pair: no bounds checks, addresses by one stride step
-        const uint32_t* pd = S + int64_t(i0 + ty) * ld + j;
-        const uint32_t* pt = S + int64_t(j0 + ty) * ld + ci;
-        const int64_t step = 4 * ld;
+    const int cx = threadIdx.x & 15, ry = threadIdx.x >> 4;
+    uint4 a[4], b[4];  // a[p] = S[i0 + ry + 16p][j0 + 4cx ..], b[p] = S[j0 + ry + 16p][i0 + 4cx ..]
+    if (vec && i0 + kRT <= C && j0 + kRT <= C) {  // interior pair, 16-byte aligned rows
+        const uint32_t* pa = S + int64_t(i0 + ry) * ld + j0 + 4 * cx;
+        const uint32_t* pb = S + int64_t(j0 + ry) * ld + i0 + 4 * cx;
+        const int64_t step = 16 * ld;
 #pragma unroll
-        for (int s = 0; s < kRT / 4; ++s) {
-            sij[s] = __ldg(pd + s * step);
-            t[tx][ty + 4 * s] = __ldg(pt + s * step);
+        for (int p = 0; p < 4; ++p) {
+            a[p] = ldg4(pa + p * step);
+            b[p] = ldg4(pb + p * step);
         }
     } else {
+        auto at = [&](int r, int c) -> uint32_t { return (r < C && c < C) ? __ldg(S + int64_t(r) * ld + c) : 0u; };
 #pragma unroll
-        for (int s = 0; s < kRT / 4; ++s) {
-            const int y = ty + 4 * s;
-            const int i = i0 + y, r = j0 + y;
-            sij[s] = (i < C && j < C) ? __ldg(S + int64_t(i) * ld + j) : 0u;
-            t[tx][y] = (r < C && ci < C) ? __ldg(S + int64_t(r) * ld + ci) : 0u;
+        for (int p = 0; p < 4; ++p) {
+            const int ra = i0 + ry + 16 * p, ca = j0 + 4 * cx;
+            const int rb = j0 + ry + 16 * p, cb = i0 + 4 * cx;
+            a[p] = make_uint4(at(ra, ca), at(ra, ca + 1), at(ra, ca + 2), at(ra, ca + 3));
+            b[p] = make_uint4(at(rb, cb), at(rb, cb + 1), at(rb, cb + 2), at(rb, cb + 3));
         }
     }
-    __syncthreads();
-    int wj = 0;
+    // Row r = ry + 16p: the swizzle s = 2 * ((r >> 2) & 15) moves the thread's 4-group by s & ~3
+    // and swaps its halves when bit 1 of s (bit 2 of r, which is bit 2 of ry) is set.
+    const bool swap = (ry >> 2) & 1;
 #pragma unroll
-    for (int s = 0; s < kRT / 4; ++s) {
-        const int y = ty + 4 * s;
-        const int i = i0 + y;
-        const uint32_t sji = t[y][tx];
-        const bool pair = i < C && j < C && (I != J || j > i);
-        const bool win_i = pair && sij[s] > sji;
-        wj += pair && sji > sij[s];
-        const int n = __popc(__ballot_sync(0xFFFFFFFFu, win_i));
-        if ((threadIdx.x & 31) == 0) wrow[tx >> 5][y] = n;
+    for (int p = 0; p < 4; ++p) {
+        const int r = ry + 16 * p;
+        const int g = (4 * cx) ^ (2 * ((r >> 2) & 15) & ~3);
+        const uint4 v = swap ? make_uint4(b[p].z, b[p].w, b[p].x, b[p].y) : b[p];
+        *reinterpret_cast<uint4*>(&bs[r * kRT + g]) = v;
     }
-    wcol[ty][tx] = wj;
+    __syncthreads();
+    uint32_t rw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t x[4] = {a[p].x, a[p].y, a[p].z, a[p].w};
+        const int col = (ry + 16 * p) ^ (2 * cx);  // column ry + 16p of rows 4cx + q, swizzled
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t y = bs[(4 * cx + q) * kRT + col];
+            rw[p] += x[q] > y;
+            cw[q] += y > x[q];
+        }
+    }
+    // Row wins: the 16 threads of a half warp share the rows.
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+#pragma unroll
+        for (int m = 8; m >= 1; m >>= 1) rw[p] += __shfl_xor_sync(0xFFFFFFFFu, rw[p], m);
+    }
+    if (cx < 4) {
+        const int p = cx;  // lane cx of the half warp adds row ry + 16 * cx
+        const uint32_t n = p == 0 ? rw[0] : p == 1 ? rw[1] : p == 2 ? rw[2] : rw[3];
+        if (n) atomicAdd(&wins[i0 + ry + 16 * p], int(n));
+    }
+    if (I == J) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) colpart[ry][4 * cx + q] = int(cw[q]);
     __syncthreads();
     if (threadIdx.x < kRT) {
-        const int y = threadIdx.x;
-        const int n = wrow[0][y] + wrow[1][y];
-        if (n) atomicAdd(&wins[i0 + y], n);
-    } else if (threadIdx.x < 2 * kRT) {
-        const int x = threadIdx.x - kRT;
-        const int n = wcol[0][x] + wcol[1][x] + wcol[2][x] + wcol[3][x];
-        if (n) atomicAdd(&wins[j0 + x], n);
+        int n = 0;
+#pragma unroll
+        for (int g = 0; g < 16; ++g) n += colpart[g][threadIdx.x];
+        if (n) atomicAdd(&wins[j0 + threadIdx.x], n);
     }
 }
 
@@ -161,7 +188,8 @@ extern "C" se_status_t se_rank(const uint32_t* d_S, int64_t ld, int C, int32_t* 
     SE_CUDA_TRY(cudaMemsetAsync(d_wins, 0, sizeof(int32_t) * size_t(C), s));
     const int nt = (C + rank::kRT - 1) / rank::kRT;
     const int64_t pairs = int64_t(nt) * (nt + 1) / 2;  // at most 2^27 at C = 2^20
-    rank::wins_kernel<<<unsigned(pairs), 256, 0, s>>>(d_S, ld, C, nt, d_wins);
+    const int vec = (reinterpret_cast<uintptr_t>(d_S) % 16 == 0) && ld % 4 == 0;  // rows start 16-byte aligned
+    rank::wins_kernel<<<unsigned(pairs), 256, 0, s>>>(d_S, ld, C, nt, vec, d_wins);
     SE_CHECK_LAUNCH();
     rank::place_kernel<<<(C + rank::kPlaceCand - 1) / rank::kPlaceCand, rank::kPlaceThreads, 0, s>>>(
         d_wins, C, d_ranking);

@@ -44,6 +44,21 @@ def test_wins_and_places_across_tile_and_strip_edges(orc, C):
         assert np.array_equal(r.cpu().numpy(), rank_ref), (C, hi)
 
 
+@pytest.mark.parametrize("C", [64, 200])
+def test_strided_and_unaligned_rows(orc, C):
+    """Row strides that are not a multiple of 4 cells, and a first cell off a 16-byte boundary,
+    take the scalar-load path of the wins count; same results."""
+    rng = np.random.default_rng(C)
+    S = rng.integers(0, 50, size=(C, C)).astype(np.uint32)
+    wins_ref, rank_ref = orc.wins_and_ranking(S)
+    big = torch.zeros((C, C + 3), dtype=torch.int32, device="cuda")
+    big[:, 1:C + 1] = torch.from_numpy(S.view(np.int32)).cuda()
+    for view in (big[:, 1:C + 1], big[:, :C + 3][:, 1:C + 1].contiguous()):
+        w, r = api.rank_device(view.view(torch.uint32))
+        assert np.array_equal(w.cpu().numpy(), wins_ref)
+        assert np.array_equal(r.cpu().numpy(), rank_ref)
+
+
 def test_candidate_labels():
     S = np.array([[0, 2, 2], [1, 0, 1], [1, 2, 0]], np.uint32)
     assert api.get_winner_and_ranking(["a", "b", "c"], S) == ("a", ["a", "c", "b"])
