@@ -92,23 +92,26 @@ void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, in
 constexpr int kBitStages = 4;
 
 // planes[(ch * B + k) * Cq + c] for the chunks of voters [0, V); voters past V count as place 0.
+// B is a template parameter so that only B planes of bit work are done, in registers.
+template <int B>
 __global__ void __launch_bounds__(256)
-    pack_planes_kernel(const float* __restrict__ pos, int64_t V, int64_t Cq, int B, uint32_t* __restrict__ planes) {
+    pack_planes_kernel(const float* __restrict__ pos, int64_t V, int64_t Cq, uint32_t* __restrict__ planes) {
     const int64_t c = int64_t(blockIdx.y) * blockDim.x + threadIdx.x;  // grid: (chunks, ceil(Cq / 256))
     const int64_t ch = blockIdx.x;
     if (c >= Cq) return;
-    uint32_t pl[kMaxPlanes];
+    uint32_t p[32];
 #pragma unroll
-    for (int k = 0; k < kMaxPlanes; ++k) pl[k] = 0u;
     for (int v = 0; v < 32; ++v) {
         const int64_t voter = ch * 32 + v;
-        const uint32_t p = voter < V ? uint32_t(pos[voter * Cq + c]) : 0u;
-#pragma unroll
-        for (int k = 0; k < kMaxPlanes; ++k) pl[k] |= ((p >> k) & 1u) << v;
+        p[v] = voter < V ? uint32_t(pos[voter * Cq + c]) : 0u;
     }
 #pragma unroll
-    for (int k = 0; k < kMaxPlanes; ++k)
-        if (k < B) planes[(ch * B + k) * Cq + c] = pl[k];
+    for (int k = 0; k < B; ++k) {
+        uint32_t w = 0u;
+#pragma unroll
+        for (int v = 0; v < 32; ++v) w |= ((p[v] >> k) & 1u) << v;
+        planes[(ch * B + k) * Cq + c] = w;
+    }
 }
 
 __device__ __forceinline__ uint32_t borrow_step(uint32_t a, uint32_t b, uint32_t br) {
@@ -126,15 +129,17 @@ inline size_t bits_smem(int B) { return size_t(kBitStages) * 2 * B * kTile * 4 +
 // range's counts (and, below the diagonal, the range's voters minus them) to out with atomics:
 // exact, since every count is an integer, and it keeps the grid full when there are few tiles
 // and many voters.
+// B (the planes per chunk) is a template parameter: the plane loop unrolls fully.
+template <int B>
 __global__ void __launch_bounds__(kThreads, 1)
-    count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int B, int64_t V, int C, int R, int splits,
+    count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int64_t V, int C, int R, int splits,
                       uint32_t* __restrict__ out, int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint32_t* sI = reinterpret_cast<uint32_t*>(smem_raw);  // [kBitStages][B][kTile]
     uint32_t* sJ = sI + kBitStages * B * kTile;            // [kBitStages][B][kTile]
     uint64_t* bars = reinterpret_cast<uint64_t*>(sJ + kBitStages * B * kTile);
-    const uint32_t stage_words = uint32_t(B) * kTile;
-    const uint32_t stage_bytes = 2u * stage_words * 4u;
+    constexpr uint32_t stage_words = uint32_t(B) * kTile;
+    constexpr uint32_t stage_bytes = 2u * stage_words * 4u;
 
     int64_t t = blockIdx.x / splits;
     const int split = int(blockIdx.x % splits);
@@ -187,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int r = 0; r < 8; ++r)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) br[r][q] = 0u;
-#pragma unroll 2
+#pragma unroll
             for (int k = 0; k < B; ++k) {
                 uint32_t a[8], b[4];
                 const uint4 a0 = *reinterpret_cast<const uint4*>(pI + k * kTile + row0);
@@ -254,6 +259,24 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// The pack and count kernels for each plane count 1 .. kMaxPlanes.
+struct TallyKernels {
+    void (*pack)(const float*, int64_t, int64_t, uint32_t*);
+    void (*count)(CUtensorMap, int64_t, int, int, int, uint32_t*, int64_t, bool, uint32_t*);
+};
+
+template <int... Bs> struct TallyTable {
+    static const TallyKernels* get() {
+        static const TallyKernels t[] = {{nullptr, nullptr}, {pack_planes_kernel<Bs>, count_bits_kernel<Bs>}...};
+        return t;
+    }
+};
+
+const TallyKernels& tally_kernels(int B) {
+    return TallyTable<1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20>::get()[B];
+}
+static_assert(kMaxPlanes == 20, "the table instantiates planes 1 .. 20");
+
 }  // namespace tally
 }  // namespace se
 
@@ -312,13 +335,18 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
     SE_CHECK_LAUNCH();
 
-    static bool smem_ok = cudaFuncSetAttribute(count_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               int(bits_smem(kMaxPlanes))) == cudaSuccess;
-    SE_REQUIRE(smem_ok, SE_ERR_CUDA, "cannot raise the shared-memory limit of the tally kernel");
     const int B = planes_for(C);
+    const TallyKernels& K = tally_kernels(B);
+    static bool smem_ok[kMaxPlanes + 1] = {};
+    if (!smem_ok[B]) {
+        SE_REQUIRE(cudaFuncSetAttribute(K.count, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bits_smem(B))) ==
+                       cudaSuccess,
+                   SE_ERR_CUDA, "cannot raise the shared-memory limit of the tally kernel");
+        smem_ok[B] = true;
+    }
     const int64_t nch_all = (V + kVC - 1) / kVC;
     uint32_t* planes = reinterpret_cast<uint32_t*>(work + planes_offset(V, C));
-    pack_planes_kernel<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, B, planes);
+    K.pack<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, planes);
     SE_CHECK_LAUNCH();
     CUtensorMap map;
     if (se_status_t st = se::closure::make_map(&map, planes, uint64_t(Cq), uint64_t(nch_all * B), uint64_t(Cq) * 4,
@@ -336,8 +364,8 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     if (tiles < want) splits = int(std::max<int64_t>(1, std::min<int64_t>((want + tiles - 1) / tiles, chunks / 32)));
     if (splits > 1 && !accumulate)
         SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
-    count_bits_kernel<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, B, V, C, R, splits, d_out, ld_out,
-                                                                                accumulate, err);
+    K.count<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
+                                                                      err);
     SE_CHECK_LAUNCH();
     if (!check) return SE_OK;
 
