@@ -71,6 +71,42 @@ __device__ __forceinline__ int warp_positions(const Id* __restrict__ r, int64_t 
     return kPosOk;
 }
 
+// The same places as 16-bit values in a row of shared memory (C < 2048, so every place fits),
+// with 0xFFFF marking a missing id during the completion scan. Same checks and codes: with
+// every id in range, a ballot longer than C must repeat one.
+template <typename Id>
+__device__ __forceinline__ int warp_places_u16(const Id* __restrict__ r, int64_t len, int C, int Cq,
+                                               uint16_t* __restrict__ p) {
+    const int lane = threadIdx.x & 31;
+    const bool complete = len >= C;
+    for (int c = complete ? C + lane : lane; c < Cq; c += 32) p[c] = c < C ? uint16_t(0xFFFF) : uint16_t(0);
+    __syncwarp();
+    int bad = 0;
+#pragma unroll 4
+    for (int64_t a = lane; a < len; a += 32) {
+        const int64_t id = int64_t(r[a]);
+        if (id < 0 || id >= C) bad = 1;
+        else if (len <= C) p[id] = uint16_t(a);
+    }
+    if (__any_sync(0xffffffffu, bad)) return kPosRange;
+    if (len > C) return kPosRepeat;
+    __syncwarp();
+#pragma unroll 4
+    for (int64_t a = lane; a < len; a += 32)
+        if (p[int64_t(r[a])] != uint16_t(a)) bad = 1;
+    if (__any_sync(0xffffffffu, bad)) return kPosRepeat;
+    if (complete) return kPosOk;
+    int base = int(len);
+    for (int c0 = 0; c0 < C; c0 += 32) {
+        const int c = c0 + lane;
+        const bool miss = c < C && p[c] == uint16_t(0xFFFF);
+        const uint32_t m = __ballot_sync(0xffffffffu, miss);
+        if (miss) p[c] = uint16_t(base + __popc(m & ((1u << lane) - 1u)));
+        base += __popc(m);
+    }
+    return kPosOk;
+}
+
 // The same for one ballot per CTA (all blockDim.x threads, a multiple of 32, at most 1024):
 // for long ballots, where one warp per ballot leaves too few warps in flight. Every thread of
 // the block must call it with the same ballot. scratch: 32 + 1 ints of shared memory.

@@ -10,7 +10,8 @@
 //
 // Kernel 1 (positions_kernel) writes pos as f32 [V][Cq] (exact integers), validating ids
 // (range, repeats). Kernel 2 (pack_planes_kernel) packs each 32-voter chunk into bit planes.
-// Kernel 3 (count_bits_kernel, one CTA per upper tile) streams the planes of the two
+// For C < 2048, places_planes_kernel does both in one pass and keeps the places in shared
+// memory. Kernel 3 (count_bits_kernel, one CTA per upper tile) streams the planes of the two
 // 128-candidate strips into shared memory with TMA and counts per 8 x 8 register micro-tile
 // with a bit-serial borrow chain (one lop3 per plane) and a popc per 32 voters.
 #include <cuda.h>
@@ -111,6 +112,47 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int v = 0; v < 32; ++v) w |= ((p[v] >> k) & 1u) << v;
         planes[(ch * B + k) * Cq + c] = w;
+    }
+}
+
+// Places and planes in one pass, for C < 2048: one CTA of 32 warps per 32-ballot chunk. Warp
+// w writes the places of ballot 32 ch + w as 16-bit values into row w of shared memory. Then
+// each thread takes one candidate: it reads the candidate's 32 places down the column (lanes
+// read neighbouring halfwords of one row, no bank conflicts) and builds each plane word in
+// registers. The places never leave the SM.
+constexpr int kFusedMaxCq = 2048;
+inline size_t fused_smem(int64_t Cq) { return size_t(32) * size_t(Cq + 2) * 2; }
+
+template <typename Id, int B>
+__global__ void __launch_bounds__(1024)
+    places_planes_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base,
+                         int64_t V, int C, int Cq, uint32_t* __restrict__ planes, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) uint16_t rows[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pitch = Cq + 2;  // halfwords; rows start 4 bytes apart modulo 128
+    const int64_t ch = blockIdx.x;
+    const int64_t v = ch * 32 + warp;
+    uint16_t* row = rows + warp * pitch;
+    if (v < V) {
+        const int64_t beg = offsets ? offsets[v] - id_base : v * C;
+        const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
+        const int code = warp_places_u16(ids + beg, len, C, Cq, row);
+        if (code != kPosOk && lane == 0) raise_device_error(err, uint32_t(code));
+    } else {
+        for (int c = lane; c < Cq; c += 32) row[c] = 0;  // voters past V count as place 0
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < Cq; c += blockDim.x) {
+        uint32_t p[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u) p[u] = rows[u * pitch + c];
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            uint32_t word = 0u;
+#pragma unroll
+            for (int u = 0; u < 32; ++u) word |= ((p[u] >> k) & 1u) << u;
+            planes[(ch * B + k) * int64_t(Cq) + c] = word;
+        }
     }
 }
 
@@ -260,14 +302,28 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // The pack and count kernels for each plane count 1 .. kMaxPlanes.
+template <typename Id>
+using FusedKernel = void (*)(const Id*, const int64_t*, int64_t, int64_t, int, int, uint32_t*, uint32_t*);
+
 struct TallyKernels {
     void (*pack)(const float*, int64_t, int64_t, uint32_t*);
     void (*count)(CUtensorMap, int64_t, int, int, int, uint32_t*, int64_t, bool, uint32_t*);
+    FusedKernel<uint8_t> fused8;  // places + planes for C < 2048 (B <= 11), else null
+    FusedKernel<uint16_t> fused16;
+    FusedKernel<int32_t> fused32;
 };
+
+template <int B> constexpr TallyKernels tally_entry() {
+    if constexpr (B <= 11)
+        return {pack_planes_kernel<B>, count_bits_kernel<B>, places_planes_kernel<uint8_t, B>,
+                places_planes_kernel<uint16_t, B>, places_planes_kernel<int32_t, B>};
+    else
+        return {pack_planes_kernel<B>, count_bits_kernel<B>, nullptr, nullptr, nullptr};
+}
 
 template <int... Bs> struct TallyTable {
     static const TallyKernels* get() {
-        static const TallyKernels t[] = {{nullptr, nullptr}, {pack_planes_kernel<Bs>, count_bits_kernel<Bs>}...};
+        static const TallyKernels t[] = {{nullptr, nullptr, nullptr, nullptr, nullptr}, tally_entry<Bs>()...};
         return t;
     }
 };
@@ -283,8 +339,11 @@ static_assert(kMaxPlanes == 20, "the table instantiates planes 1 .. 20");
 using namespace se;
 using namespace se::tally;
 
-// Error word (256 B), then the places f32 [V][Cq], then the bit planes u32 [ceil(V/32) * B][Cq].
-static int64_t planes_offset(int64_t V, int C) { return 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256); }
+// Error word (256 B), then the places f32 [V][Cq] (only from C = 2048 on: below that the places
+// stay in shared memory), then the bit planes u32 [ceil(V/32) * B][Cq].
+static int64_t planes_offset(int64_t V, int C) {
+    return C < kFusedMaxCq ? 256 : 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256);
+}
 
 extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
     if (V < 0 || C < 1) return -1;
@@ -327,14 +386,6 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         if (!accumulate) SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
         return SE_OK;
     }
-    if (id_bytes == 4)
-        launch_positions(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
-    else if (id_bytes == 2)
-        launch_positions(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
-    else
-        launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
-    SE_CHECK_LAUNCH();
-
     const int B = planes_for(C);
     const TallyKernels& K = tally_kernels(B);
     static bool smem_ok[kMaxPlanes + 1] = {};
@@ -346,22 +397,69 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     }
     const int64_t nch_all = (V + kVC - 1) / kVC;
     uint32_t* planes = reinterpret_cast<uint32_t*>(work + planes_offset(V, C));
-    K.pack<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, planes);
-    SE_CHECK_LAUNCH();
+    if (C < kFusedMaxCq) {  // places and planes in one pass, places in shared memory
+        const size_t smem = fused_smem(Cq);
+        static bool fused_ok[3][kMaxPlanes + 1] = {};
+        const int w = id_bytes == 1 ? 0 : id_bytes == 2 ? 1 : 2;
+        const void* fn = w == 0 ? reinterpret_cast<const void*>(K.fused8)
+                       : w == 1 ? reinterpret_cast<const void*>(K.fused16)
+                                : reinterpret_cast<const void*>(K.fused32);
+        if (!fused_ok[w][B]) {
+            SE_REQUIRE(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fused_smem(kFusedMaxCq))) ==
+                           cudaSuccess,
+                       SE_ERR_CUDA, "cannot raise the shared-memory limit of the places kernel");
+            fused_ok[w][B] = true;
+        }
+        if (w == 0)
+            K.fused8<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C,
+                                                           int(Cq), planes, err);
+        else if (w == 1)
+            K.fused16<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V,
+                                                            C, int(Cq), planes, err);
+        else
+            K.fused32<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V,
+                                                            C, int(Cq), planes, err);
+        SE_CHECK_LAUNCH();
+    } else {
+        if (id_bytes == 4)
+            launch_positions(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+        else if (id_bytes == 2)
+            launch_positions(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+        else
+            launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+        SE_CHECK_LAUNCH();
+        K.pack<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, planes);
+        SE_CHECK_LAUNCH();
+    }
     CUtensorMap map;
     if (se_status_t st = se::closure::make_map(&map, planes, uint64_t(Cq), uint64_t(nch_all * B), uint64_t(Cq) * 4,
                                                kTile, uint32_t(B)))
         return st;
     const int64_t tiles = int64_t(R) * (R + 1) / 2;
-    // Few tiles and many voters: split the voters so that the grid covers every SM about four
-    // times, keeping at least 32 chunks (1024 voters) per range.
+    // Voter splits: each of the tiles x splits CTAs counts 1/splits of the voters, one CTA per
+    // SM at a time, so a launch takes ceil(tiles x splits / SMs) waves of (the tile's counting
+    // over all voters / splits + its output). Split outputs are atomic adds, dearer than the
+    // plain stores of an unsplit launch. Costs in microseconds, measured on B200: counting
+    // 0.15 per 32-voter chunk and plane-plus-two, output 12 (atomic) or 3 (stores) per tile.
+    // Take the cheapest split count (the smallest within 1 %), keeping at least 32 chunks (1024
+    // voters) per range. With few tiles and many voters this fills the SMs (C = 1024, 2^16
+    // voters: 36 tiles x 37 splits = 9 full waves on 148 SMs); with many tiles it stays 1.
     int sms = 0, dev = 0;
     SE_CUDA_TRY(cudaGetDevice(&dev));
     SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t want = 4 * int64_t(sms);
     const int64_t chunks = (V + kVC - 1) / kVC;
+    const int64_t max_splits = std::min<int64_t>(std::max<int64_t>(1, chunks / 32), 256);
+    const double full_us = 0.15 * double(chunks) * double(B + 2);
     int splits = 1;
-    if (tiles < want) splits = int(std::max<int64_t>(1, std::min<int64_t>((want + tiles - 1) / tiles, chunks / 32)));
+    double best = 0.0;
+    for (int64_t sp = 1; sp <= max_splits; ++sp) {
+        const double waves = double((tiles * sp + sms - 1) / sms);
+        const double cost = waves * (full_us / double(sp) + (sp > 1 ? 12.0 : 3.0));
+        if (sp == 1 || cost < best * 0.99) {
+            best = cost;
+            splits = int(sp);
+        }
+    }
     if (splits > 1 && !accumulate)
         SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
     K.count<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
