@@ -71,10 +71,11 @@ __device__ __forceinline__ int warp_positions(const Id* __restrict__ r, int64_t 
     return kPosOk;
 }
 
-// The same places as 16-bit values in a row of shared memory (C < 2048, so every place fits),
+// The same places as 16-bit values in a row of shared memory (C < 65535, so every place fits),
 // with 0xFFFF marking a missing id during the completion scan. Same checks and codes: with
-// every id in range, a ballot longer than C must repeat one.
-template <typename Id>
+// every id in range, a ballot longer than C must repeat one. COHERENT: read the ballot
+// through L2, as warp_positions does.
+template <typename Id, bool COHERENT = false>
 __device__ __forceinline__ int warp_places_u16(const Id* __restrict__ r, int64_t len, int C, int Cq,
                                                uint16_t* __restrict__ p) {
     const int lane = threadIdx.x & 31;
@@ -84,7 +85,7 @@ __device__ __forceinline__ int warp_places_u16(const Id* __restrict__ r, int64_t
     int bad = 0;
 #pragma unroll 4
     for (int64_t a = lane; a < len; a += 32) {
-        const int64_t id = int64_t(r[a]);
+        const int64_t id = int64_t(pos_load<COHERENT>(r + a));
         if (id < 0 || id >= C) bad = 1;
         else if (len <= C) p[id] = uint16_t(a);
     }
@@ -93,7 +94,7 @@ __device__ __forceinline__ int warp_places_u16(const Id* __restrict__ r, int64_t
     __syncwarp();
 #pragma unroll 4
     for (int64_t a = lane; a < len; a += 32)
-        if (p[int64_t(r[a])] != uint16_t(a)) bad = 1;
+        if (p[int64_t(pos_load<COHERENT>(r + a))] != uint16_t(a)) bad = 1;
     if (__any_sync(0xffffffffu, bad)) return kPosRepeat;
     if (complete) return kPosOk;
     int base = int(len);

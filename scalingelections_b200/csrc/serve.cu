@@ -286,32 +286,54 @@ __device__ void run_place(const Elec& E, uint8_t* smem) {
 // order (the reference's completion rule, scaling_elections.py:75-83). Out-of-range or repeated
 // ids set the request's ballot error word.
 // ------------------------------------------------------------------------------------------
-__device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v1) {
-    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// smem: the task's free operand region (bytes). When a 16-bit row per warp fits there, each
+// warp builds its ballot's places in its row (scatter, check and completion scan in shared
+// memory) and then writes the row out with coalesced stores; otherwise it works in global
+// memory through L2.
+__device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v1, uint8_t* smem, size_t smem_bytes) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const bool rows = size_t(nw) * size_t(Cq) * 2 <= smem_bytes && C < 0xFFFF;
+    uint16_t* row = reinterpret_cast<uint16_t*>(smem) + size_t(warp) * Cq;
     for (int64_t v = v0 + warp; v < v1; v += nw) {  // one ballot per warp at a time
         const int64_t beg = Q.offsets ? __ldcg(Q.offsets + v) : v * C;
         const int64_t len = Q.offsets ? __ldcg(Q.offsets + v + 1) - beg : C;
-        const int code = warp_positions<int32_t, true>(Q.ids + beg, len, C, Cq, Q.pos + v * Cq);
-        if (code != kPosOk && (threadIdx.x & 31) == 0) atomicCAS(&Q.flags[0], 0u, uint32_t(code));
+        int code;
+        if (rows) {
+            code = warp_places_u16<int32_t, true>(Q.ids + beg, len, C, Cq, row);
+            __syncwarp();
+            if (code == kPosOk)
+                for (int c = lane; c < Cq; c += 32) Q.pos[v * Cq + c] = float(row[c]);
+            __syncwarp();  // the row is read before the next ballot rewrites it
+        } else {
+            code = warp_positions<int32_t, true>(Q.ids + beg, len, C, Cq, Q.pos + v * Cq);
+        }
+        if (code != kPosOk && lane == 0) atomicCAS(&Q.flags[0], 0u, uint32_t(code));
     }
     // Pack the task's 32-ballot chunks into bit planes (ballots past V count as place 0). The
     // places were written by this CTA's warps; read them back through L2.
+    // Each thread turns one candidate's 32 places into the request's B plane words, one bit
+    // extract and one bit insert per voter and plane (a loop over B, not over all 20 planes).
     __syncthreads();
     const int B = Q.B;
     for (int64_t ch = v0 / 32; ch * 32 < v1; ++ch)
         for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) {
-            uint32_t pl[kMaxPlanes];
+            uint32_t p[32];
 #pragma unroll
-            for (int k = 0; k < kMaxPlanes; ++k) pl[k] = 0u;
             for (int v = 0; v < 32; ++v) {
                 const int64_t voter = ch * 32 + v;
-                const uint32_t p = voter < Q.V ? uint32_t(__ldcg(Q.pos + voter * Cq + c)) : 0u;
-#pragma unroll
-                for (int k = 0; k < kMaxPlanes; ++k) pl[k] |= ((p >> k) & 1u) << v;
+                p[v] = voter < Q.V ? uint32_t(__ldcg(Q.pos + voter * Cq + c)) : 0u;
             }
+#pragma unroll 1
+            for (int k = 0; k < B; ++k) {
+                uint32_t word = 0u;
 #pragma unroll
-            for (int k = 0; k < kMaxPlanes; ++k)
-                if (k < B) Q.planes[(ch * B + k) * Cq + c] = pl[k];
+                for (int v = 0; v < 32; ++v) {
+                    uint32_t bit;
+                    asm("bfe.u32 %0, %1, %2, 1;" : "=r"(bit) : "r"(p[v]), "r"(k));
+                    asm("bfi.b32 %0, %1, %2, %3, 1;" : "=r"(word) : "r"(bit), "r"(word), "r"(v));
+                }
+                Q.planes[(ch * B + k) * Cq + c] = word;
+            }
         }
 }
 
@@ -550,7 +572,7 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         if (f == 0) {
             const int64_t v0 = int64_t(t) * kPosChunk;
             const int64_t v1 = v0 + kPosChunk < Q.V ? v0 + kPosChunk : Q.V;
-            run_positions(Q, E.C, E.Cp, v0, v1);
+            run_positions(Q, E.C, E.Cp, v0, v1, smem, pcfg<16>::DATA);
         } else if (f == 1) {
             int q = int(t) >> 1, I = 0;
             while (q >= R - I) {
