@@ -395,7 +395,7 @@ __device__ bool run_tally(const Req& Q, const Req* G, int I, int J, int h, uint8
             for (int r = 0; r < 8; ++r)
 #pragma unroll
                 for (int q = 0; q < 8; ++q) br[r][q] = 0u;
-#pragma unroll 1
+#pragma unroll 2
             for (int k = 0; k < B; ++k) {
                 uint32_t a[8], b[8];
                 ld4(a, A + k * 64 + colA);
