@@ -182,4 +182,29 @@ __device__ __forceinline__ void raise_device_error(uint32_t* err, uint32_t code)
     if (err) atomicCAS(err, 0u, code);
 }
 
+// Tile pair b of the upper triangle of an nt x nt tile grid, row by row: row I holds the pairs
+// (I, I) .. (I, nt - 1), so pair b is (I, J) with I <= J.
+__device__ __forceinline__ void upper_pair(int64_t b, int nt, int& I, int& J) {
+    const double n2 = 2.0 * nt + 1.0;
+    int64_t r = int64_t((n2 - sqrt(n2 * n2 - 8.0 * double(b))) * 0.5);
+    auto start = [nt](int64_t x) { return x * nt - x * (x - 1) / 2; };
+    while (r > 0 && start(r) > b) --r;
+    while (r + 1 < nt && start(r + 1) <= b) ++r;
+    I = int(r);
+    J = int(r + (b - start(r)));
+}
+
+// A 64 x 64 tile of u32 cells staged in shared memory so that both its rows and its columns
+// read conflict-free: element (r, c) sits at r * 64 + (c ^ 2 * ((r >> 2) & 15)). Row r's
+// 4-groups stay 16-byte groups, and a warp reading column r of rows 4cx + q (cx = 0..15) for
+// two neighbouring r hits 32 distinct banks.
+__device__ __forceinline__ int swz64(int r, int c) { return r * 64 + (c ^ (2 * ((r >> 2) & 15))); }
+
+// Stores cells (r, c0 .. c0+3), c0 a multiple of 4, of a swizzled tile with one 128-bit write.
+__device__ __forceinline__ void swz64_store4(uint32_t* tile, int r, int c0, uint4 v) {
+    const int s = 2 * ((r >> 2) & 15);
+    if (s & 2) v = make_uint4(v.z, v.w, v.x, v.y);  // the two halves of the group swap
+    *reinterpret_cast<uint4*>(tile + r * 64 + (c0 ^ (s & ~3))) = v;
+}
+
 }  // namespace se

@@ -21,17 +21,6 @@ namespace rank {
 
 constexpr int kRT = 64;  // tile edge of wins_kernel
 
-// Tile pair b of the upper triangle, row by row: row I holds pairs (I, I) .. (I, nt - 1).
-__device__ __forceinline__ void tile_pair(int64_t b, int nt, int& I, int& J) {
-    const double n2 = 2.0 * nt + 1.0;
-    int64_t r = int64_t((n2 - sqrt(n2 * n2 - 8.0 * double(b))) * 0.5);
-    auto start = [nt](int64_t x) { return x * nt - x * (x - 1) / 2; };
-    while (r > 0 && start(r) > b) --r;
-    while (r + 1 < nt && start(r + 1) <= b) ++r;
-    I = int(r);
-    J = int(r + (b - start(r)));
-}
-
 // Thread (ry, cx) of wins_kernel holds rows ry + 16p (p < 4) and columns 4cx .. 4cx+3 of the
 // tile S[I][J] in registers (128-bit loads), and loads the same positions of S[J][I] into
 // shared memory, where element (r, c) of that tile sits at r * 64 + (c ^ 2 * ((r >> 2) & 15)):
@@ -47,7 +36,7 @@ __global__ void __launch_bounds__(256)
     __shared__ __align__(16) uint32_t bs[kRT * kRT];
     __shared__ int32_t colpart[16][kRT];  // column wins per row group ry
     int I, J;
-    tile_pair(blockIdx.x, nt, I, J);
+    upper_pair(blockIdx.x, nt, I, J);
     const int i0 = I * kRT, j0 = J * kRT;
     const int cx = threadIdx.x & 15, ry = threadIdx.x >> 4;
     uint4 a[4], b[4];  // a[p] = S[i0 + ry + 16p][j0 + 4cx ..], b[p] = S[j0 + ry + 16p][i0 + 4cx ..]
