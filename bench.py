@@ -474,8 +474,9 @@ def run_batch(args, world, rank, local_rank):
         from scalingelections_b200 import autotune
 
         t0 = time.perf_counter()
-        tuned = autotune.tune(V=100000, per_bucket=32, reps=3, path=Path("gpurun_out") / "autotune.json"
-                              if Path("gpurun_out").exists() else None)
+        report_dir = os.environ.get("SE_REPORT_DIR")  # where to keep the tuning table, if anywhere
+        tuned = autotune.tune(V=100000, per_bucket=32, reps=3,
+                              path=Path(report_dir) / "autotune.json" if report_dir else None)
         tune_s = time.perf_counter() - t0
         lanes, order, ctas = autotune.choose(tuned, [C for (C, _, _, _) in specs], [V for (_, V, _, _) in specs])
     cells = float(sum(C ** 3 for (C, _, _, _) in all_specs))
