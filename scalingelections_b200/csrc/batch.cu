@@ -98,8 +98,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
                       Header* __restrict__ hdr, int queue) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     __shared__ int32_t s_wins[kT];
     __shared__ uint64_t s_task, s_next;
     __shared__ uint32_t s_go, s_ready;

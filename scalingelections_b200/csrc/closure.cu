@@ -84,8 +84,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
         for (int c = 0; c < kChunks; ++c) mbar_init(&bars[c], 1);
@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
                 uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     __shared__ uint32_t s_t;
     __shared__ int s_go;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
@@ -365,8 +365,8 @@ template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     diag_kernel(uint32_t* __restrict__ S, int64_t ldw, int K, uint32_t* __restrict__ dT) {
     using CF = cfg<LB>;
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     const geom g(threadIdx.x);
     uint32_t c[8][8];
     uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * CF::TW;

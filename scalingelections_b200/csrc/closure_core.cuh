@@ -145,54 +145,82 @@ __device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8]
         }
 }
 
+// Rows of the pivot-closure staging buffers (rowbuf[kPivotBufs][TW], colbuf[kPivotBufs][kT]):
+// two phases, each holding the rows and columns of two pivots.
+constexpr int kPivotBufs = 4;
+
+// Publishes row k and column k of the tile (the thread's share of them) into staging slot s.
+template <int LB>
+__device__ __forceinline__ void publish_pivot(const uint32_t (&c)[8][8], const geom& g, int k, uint32_t* row,
+                                              uint32_t* col) {
+    constexpr int CPW = cfg<LB>::CPW;
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+        if (g.row0 + r == k) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) row[g.word(q)] = c[r][q];
+        }
+    const int wk = k / CPW, hk = k % CPW;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (g.word(q) == wk) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) col[g.row0 + r] = cell_splat<LB>(c[r][q], hk);
+        }
+}
+
 // Closes the 128 x 128 tile held in registers (the thread's 8 x 8 words) in place over
-// pivots k = 0 .. kmax-1, one k at a time: the k-th row and column are broadcast through
-// double-buffered shared rows, one barrier per k. Every thread of the block must call it.
-// Pivots >= kmax are skipped, which is exact when those rows/columns are zero padding.
+// pivots k = 0 .. kmax-1, two at a time. Rows and columns k and k+1 are published together
+// (before this pair's steps) through double-buffered shared slots, one barrier per pair. Each
+// thread applies step k to the row and column k+1 it reads:
+//   c'[i][k+1] = max(c[i][k+1], min(c[i][k], c[k][k+1]))
+//   c'[k+1][j] = max(c[k+1][j], min(c[k+1][k], c[k][j]))
+// and then does both steps in one pass over its words:
+//   c[i][j] = max(c[i][j], min(c[i][k], c[k][j]), min(c'[i][k+1], c'[k+1][j]))
+// which is exactly two Floyd-Warshall steps. Every thread of the block must call it. Pivots
+// >= kmax are skipped, which is exact when those rows/columns are zero padding.
 template <int LB>
 __device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][8], const geom& g, int kmax,
                                                         uint32_t (*rowbuf)[cfg<LB>::TW],
                                                         uint32_t (*colbuf)[kT]) {
     using L = lanes<LB>;
     constexpr int CPW = cfg<LB>::CPW;
-    // Publish row 0 and column 0.
-    if (g.row0 == 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) rowbuf[0][g.word(q)] = c[0][q];
-    }
-    if (g.wbase == 0) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) colbuf[0][g.row0 + r] = cell_splat<LB>(c[r][0], 0);
-    }
+    publish_pivot<LB>(c, g, 0, rowbuf[0], colbuf[0]);
+    publish_pivot<LB>(c, g, 1, rowbuf[1], colbuf[1]);
     __syncthreads();
 #pragma unroll 1
-    for (int k = 0; k < kmax; ++k) {
-        const int buf = k & 1;
-        uint32_t a[8], b[8];
-        ld4(a, &colbuf[buf][g.row0]);
-        ld4(a + 4, &colbuf[buf][g.row0 + 4]);
-        ld4(b, &rowbuf[buf][g.wbase]);
-        ld4(b + 4, &rowbuf[buf][g.wbase + 32]);
+    for (int k = 0; k < kmax; k += 2) {
+        const int s = ((k >> 1) & 1) * 2;  // this pair's slots
+        uint32_t a0[8], b0[8];
+        ld4(a0, &colbuf[s][g.row0]);
+        ld4(a0 + 4, &colbuf[s][g.row0 + 4]);
+        ld4(b0, &rowbuf[s][g.wbase]);
+        ld4(b0 + 4, &rowbuf[s][g.wbase + 32]);
+        if (k + 1 < kmax) {
+            uint32_t a1[8], b1[8];
+            ld4(a1, &colbuf[s + 1][g.row0]);
+            ld4(a1 + 4, &colbuf[s + 1][g.row0 + 4]);
+            ld4(b1, &rowbuf[s + 1][g.wbase]);
+            ld4(b1 + 4, &rowbuf[s + 1][g.wbase + 32]);
+            const uint32_t ckk1 = cell_splat<LB>(rowbuf[s][(k + 1) / CPW], (k + 1) % CPW);  // c[k][k+1]
+            const uint32_t ck1k = colbuf[s][k + 1];                                        // c[k+1][k]
 #pragma unroll
-        for (int r = 0; r < 8; ++r)
+            for (int r = 0; r < 8; ++r) a1[r] = L::vmax(a1[r], L::vmin(a0[r], ckk1));
 #pragma unroll
-            for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a[r], b[q]));
-        const int k1 = k + 1;
-        if (k1 < kmax) {
+            for (int q = 0; q < 8; ++q) b1[q] = L::vmax(b1[q], L::vmin(ck1k, b0[q]));
 #pragma unroll
             for (int r = 0; r < 8; ++r)
-                if (g.row0 + r == k1) {
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) rowbuf[buf ^ 1][g.word(q)] = c[r][q];
-                }
-            const int wk = k1 / CPW, hk = k1 % CPW;
+                for (int q = 0; q < 8; ++q) c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
+        } else {
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (g.word(q) == wk) {
+            for (int r = 0; r < 8; ++r)
 #pragma unroll
-                    for (int r = 0; r < 8; ++r) colbuf[buf ^ 1][g.row0 + r] = cell_splat<LB>(c[r][q], hk);
-                }
+                for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a0[r], b0[q]));
         }
+        const int k2 = k + 2, t = s ^ 2;  // the next pair, into the other phase's slots
+        if (k2 < kmax) publish_pivot<LB>(c, g, k2, rowbuf[t], colbuf[t]);
+        if (k2 + 1 < kmax) publish_pivot<LB>(c, g, k2 + 1, rowbuf[t + 1], colbuf[t + 1]);
         __syncthreads();
     }
 }

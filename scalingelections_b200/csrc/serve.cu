@@ -458,8 +458,8 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
                   EngineHeader* __restrict__ hdr, uint64_t idle_ns) {
     using CF = cfg<16>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     __shared__ int32_t s_wins[kT];
     __shared__ __align__(64) Req s_q;
     __shared__ uint32_t s_slot, s_t, s_cnt;

@@ -61,8 +61,8 @@ template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     shard_pivot_kernel(uint32_t* __restrict__ S, int64_t ldw, int kl, int k, int kmax, uint32_t* __restrict__ dT) {
     using CF = cfg<LB>;
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     const geom g(threadIdx.x);
     uint32_t c[8][8];
     uint32_t* D = S + int64_t(kl) * kT * ldw + int64_t(k) * CF::TW;
@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
                        int kl, int b0, int own, int fuse_next, int kmax_next, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(16) uint32_t rowbuf[2][CF::TW];
-    __shared__ __align__(16) uint32_t colbuf[2][kT];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
         for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
