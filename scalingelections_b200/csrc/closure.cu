@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// Pivot tile (phase 1): close D = S[K][K] in place, one k at a time, then emit dT.
+// Pivot tile (phase 1): close D = S[K][K] in place, two pivots per barrier, then emit dT.
 // ------------------------------------------------------------------------------------------
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
