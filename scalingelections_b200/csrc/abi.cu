@@ -4,6 +4,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -21,6 +24,27 @@ void set_error(const char* fmt, ...) {
 }
 
 void clear_error() { g_last_error[0] = 0; }
+
+se_status_t raise_smem_limit(const void* fn, int bytes, const char* what) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cannot raise the shared-memory limit of %s: no current device", what);
+        return SE_ERR_CUDA;
+    }
+    static std::mutex m;
+    static std::set<std::tuple<const void*, int, int>> done;
+    std::lock_guard<std::mutex> lock(m);
+    if (done.count({fn, dev, bytes})) return SE_OK;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cannot raise the shared-memory limit of %s: %s", what, cudaGetErrorString(e));
+        return SE_ERR_CUDA;
+    }
+    done.insert({fn, dev, bytes});
+    return SE_OK;
+}
 
 }  // namespace se
 

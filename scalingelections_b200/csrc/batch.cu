@@ -491,10 +491,8 @@ template <int LB> int occupancy() {
 }
 
 template <int LB> se_status_t set_persistent_smem() {
-    static const cudaError_t e = cudaFuncSetAttribute(persistent_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      int(pcfg<LB>::SMEM));
-    SE_REQUIRE(e == cudaSuccess, SE_ERR_CUDA, "cannot raise the shared-memory limit of the batched closure");
-    return SE_OK;
+    return raise_smem_limit(reinterpret_cast<const void*>(persistent_kernel<LB>), int(pcfg<LB>::SMEM),
+                            "the batched closure");
 }
 
 se_status_t enqueue(const Plan& P, cudaStream_t s) {

@@ -543,18 +543,12 @@ layout plan(int C, int lane_bits) {
 std::atomic<int> g_closure_mode{1};
 
 template <int LB> se_status_t set_smem_limits() {
-    static se_status_t st = [] {
-        const int bytes = int(batch::pcfg<LB>::SMEM);
-        if (cudaFuncSetAttribute(panels_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-            cudaFuncSetAttribute(rem_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-            cudaFuncSetAttribute(flow_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return se_status_t(SE_ERR_CUDA);
-        }
-        return se_status_t(SE_OK);
-    }();
-    SE_REQUIRE(st == SE_OK, SE_ERR_CUDA, "cannot raise the shared-memory limit of the closure kernels");
-    return SE_OK;
+    const int bytes = int(batch::pcfg<LB>::SMEM);
+    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB>), bytes, "the panel kernel"))
+        return st;
+    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB>), bytes, "the remainder kernel"))
+        return st;
+    return raise_smem_limit(reinterpret_cast<const void*>(flow_kernel<LB>), bytes, "the dataflow closure");
 }
 
 // Rounds of the blocked closure on an initialised working matrix.

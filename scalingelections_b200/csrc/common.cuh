@@ -25,6 +25,11 @@ namespace se {
 void set_error(const char* fmt, ...);
 void clear_error();
 
+// Raises kernel fn's dynamic shared-memory limit to `bytes` on the current device. The setting
+// is per device, so it is remembered per (kernel, device, bytes); thread-safe. On failure it
+// records "cannot raise the shared-memory limit of <what>" and returns SE_ERR_CUDA.
+se_status_t raise_smem_limit(const void* fn, int bytes, const char* what);
+
 #define SE_CUDA_TRY(expr)                                                                     \
     do {                                                                                      \
         cudaError_t se_err_ = (expr);                                                         \

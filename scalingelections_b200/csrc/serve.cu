@@ -767,9 +767,9 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
     SE_REQUIRE(d_work && work_bytes >= need, SE_ERR_WORKSPACE, "engine workspace of %lld bytes is below %lld",
                (long long)work_bytes, (long long)need);
     SE_REQUIRE((reinterpret_cast<uintptr_t>(d_work) & 255) == 0, SE_ERR_INVALID, "workspace must be 256-byte aligned");
-    static const cudaError_t attr = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         int(kEngineSmem));
-    SE_CUDA_TRY(attr);
+    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(engine_kernel), int(kEngineSmem),
+                                          "the serving engine"))
+        return st;
     auto* h = new se_engine();
     Engine& E = h->e;
     E.work = static_cast<uint8_t*>(d_work);

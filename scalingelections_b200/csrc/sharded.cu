@@ -180,10 +180,8 @@ Layout layout(int C, int b0, int b1, int lanes) {
 }
 
 template <int LB> se_status_t set_smem() {
-    static const cudaError_t e = cudaFuncSetAttribute(shard_tiles_kernel<LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      int(pcfg<LB>::SMEM));
-    SE_REQUIRE(e == cudaSuccess, SE_ERR_CUDA, "cannot raise the shared-memory limit of the sharded closure");
-    return SE_OK;
+    return raise_smem_limit(reinterpret_cast<const void*>(shard_tiles_kernel<LB>), int(pcfg<LB>::SMEM),
+                            "the sharded closure");
 }
 
 }  // namespace shard

@@ -388,28 +388,17 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     }
     const int B = planes_for(C);
     const TallyKernels& K = tally_kernels(B);
-    static bool smem_ok[kMaxPlanes + 1] = {};
-    if (!smem_ok[B]) {
-        SE_REQUIRE(cudaFuncSetAttribute(K.count, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bits_smem(B))) ==
-                       cudaSuccess,
-                   SE_ERR_CUDA, "cannot raise the shared-memory limit of the tally kernel");
-        smem_ok[B] = true;
-    }
+    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(K.count), int(bits_smem(B)), "the tally kernel"))
+        return st;
     const int64_t nch_all = (V + kVC - 1) / kVC;
     uint32_t* planes = reinterpret_cast<uint32_t*>(work + planes_offset(V, C));
     if (C < kFusedMaxCq) {  // places and planes in one pass, places in shared memory
         const size_t smem = fused_smem(Cq);
-        static bool fused_ok[3][kMaxPlanes + 1] = {};
         const int w = id_bytes == 1 ? 0 : id_bytes == 2 ? 1 : 2;
         const void* fn = w == 0 ? reinterpret_cast<const void*>(K.fused8)
                        : w == 1 ? reinterpret_cast<const void*>(K.fused16)
                                 : reinterpret_cast<const void*>(K.fused32);
-        if (!fused_ok[w][B]) {
-            SE_REQUIRE(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fused_smem(kFusedMaxCq))) ==
-                           cudaSuccess,
-                       SE_ERR_CUDA, "cannot raise the shared-memory limit of the places kernel");
-            fused_ok[w][B] = true;
-        }
+        if (se_status_t st = raise_smem_limit(fn, int(fused_smem(kFusedMaxCq)), "the places kernel")) return st;
         if (w == 0)
             K.fused8<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C,
                                                            int(Cq), planes, err);
