@@ -13,7 +13,9 @@ runs, on seeded inputs:
   * get_winner_and_ranking               (scaling_elections.py:274-296)
 and the participation-paradox ballots of validate_paradox.py:26-28 through the same calls.
 Each case is stored as a compressed .npz holding its inputs and the reference's outputs, so
-the fixtures do not depend on any random generator at test time.
+the fixtures do not depend on any random generator at test time. With --configs it writes
+the configuration-size cases instead (see config_cases): hashes of the reference's outputs on
+ballots regenerated from a seed, since the inputs would be tens of megabytes.
 """
 from __future__ import annotations
 
@@ -60,12 +62,39 @@ def csr(rankings):
     return ids, offs
 
 
+def config_cases(ref) -> None:
+    """Configuration-size cases kept as hashes: the ballots are regenerated from their seed by
+    scalingelections_b200.ballots at test time, so only the reference's outputs are stored.
+      * config_c4096_v4096: C = 4096, V = 4096 uniform permutations (seed 4096), the
+        single-election configuration with the reference's tile sweep. Tally by
+        build_pairwise_preferences, closure by the serial and the tiled Numba paths (checked
+        equal), ranking by get_winner_and_ranking. A few minutes on 8 cores."""
+    from scalingelections_b200.ballots import uniform_ballots
+
+    C, V, seed = 4096, 4096, 4096
+    rankings = list(uniform_ballots(V, C, seed=seed))
+    d = ref.build_pairwise_preferences(rankings)
+    S = ref.compute_strongest_paths_numba_parallel(np.ascontiguousarray(d, dtype=np.uint32), tile_size=16)
+    S_serial = ref.compute_strongest_paths_numba_serial(np.ascontiguousarray(d, dtype=np.uint32))
+    assert np.array_equal(S, S_serial)
+    winner, ranking = ref.get_winner_and_ranking(list(range(C)), S)
+    case = dict(C=C, V=V, seed=seed, ballots="scalingelections_b200.ballots.uniform_ballots(V, C, seed)",
+                tally_sha256=sha(d), strongest_sha256=sha(S), winner=int(winner),
+                ranking=[int(x) for x in ranking])
+    (HERE / "config_c4096_v4096.json").write_text(json.dumps(case) + "\n")
+    print({k: v for k, v in case.items() if k != "ranking"})
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--configs", action="store_true", help="(re)generate only the configuration-size cases")
     args = ap.parse_args()
     ref = load_reference(Path(args.ref))
     sys.path.insert(0, str(HERE.parent.parent))
+    if args.configs:
+        config_cases(ref)
+        return
     from scalingelections_b200.ballots import mallows_ballots, random_preferences, uniform_ballots
 
     index = {}

@@ -1,0 +1,46 @@
+"""The single-election configuration C = 4096, V = 4096 (uniform permutations) against the
+reference's own outputs on the same ballots, produced by tests/golden/make_golden.py --configs
+from scaling_elections.py:
+  * the tally of build_pairwise_preferences (py:51-88),
+  * the strongest paths of compute_strongest_paths_numba_parallel, tile 16 (py:162-271), checked
+    there equal to the serial Numba path (py:91-125),
+  * the ranking and winner of get_winner_and_ranking (py:274-296).
+The fixture holds hashes and the ranking; the ballots are regenerated from their seed."""
+import hashlib
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from scalingelections_b200 import LANES_U16, LANES_U32, api
+from scalingelections_b200.ballots import uniform_ballots
+
+CASE = json.loads((Path(__file__).parent / "golden" / "config_c4096_v4096.json").read_text())
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint32).tobytes()).hexdigest()
+
+
+def ballots():
+    return uniform_ballots(CASE["V"], CASE["C"], seed=CASE["seed"])
+
+
+@pytest.mark.gpu
+def test_config_c4096_matches_reference():
+    d = api.build_pairwise_preferences(ballots())
+    assert sha(d) == CASE["tally_sha256"]
+    for lanes in (LANES_U16, LANES_U32):  # V < 65536: both lane modes are exact here
+        S = api.compute_strongest_paths(d, allow_gpu=True, tile_size=32, lanes=lanes)
+        assert sha(S) == CASE["strongest_sha256"], lanes
+    winner, ranking = api.get_winner_and_ranking(list(range(CASE["C"])), S)
+    assert winner == CASE["winner"]
+    assert list(ranking) == CASE["ranking"]
+
+
+@pytest.mark.skipif(not os.environ.get("SE_TEST_SLOW"), reason="about a minute on one core; set SE_TEST_SLOW=1")
+def test_oracle_tally_at_config_size(orc):
+    """The C oracle's tally on the same ballots gives the reference's tally (CPU)."""
+    assert sha(orc.tally(list(ballots()))) == CASE["tally_sha256"]
