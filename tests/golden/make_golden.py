@@ -62,38 +62,51 @@ def csr(rankings):
     return ids, offs
 
 
-def config_cases(ref) -> None:
+def config_cases(ref, only: list[str] | None = None) -> None:
     """Configuration-size cases kept as hashes: the ballots are regenerated from their seed by
     scalingelections_b200.ballots at test time, so only the reference's outputs are stored.
       * config_c4096_v4096: C = 4096, V = 4096 uniform permutations (seed 4096), the
-        single-election configuration with the reference's tile sweep. Tally by
-        build_pairwise_preferences, closure by the serial and the tiled Numba paths (checked
-        equal), ranking by get_winner_and_ranking. A few minutes on 8 cores."""
-    from scalingelections_b200.ballots import uniform_ballots
+        single-election configuration with the reference's tile sweep. Closure by the tiled and
+        the serial Numba paths (checked equal). A few minutes on 8 cores.
+      * config_c16384_v4096: C = 16384, V = 4096 Mallows(0.8) ballots (seed 16384), the
+        headline size. Closure by the tiled Numba path only (the serial one would take hours;
+        the two are equal at every size checked). About an hour on 8 cores.
+    Each: tally by build_pairwise_preferences, ranking by get_winner_and_ranking."""
+    from scalingelections_b200.ballots import mallows_ballots, uniform_ballots
 
-    C, V, seed = 4096, 4096, 4096
-    rankings = list(uniform_ballots(V, C, seed=seed))
-    d = ref.build_pairwise_preferences(rankings)
-    S = ref.compute_strongest_paths_numba_parallel(np.ascontiguousarray(d, dtype=np.uint32), tile_size=16)
-    S_serial = ref.compute_strongest_paths_numba_serial(np.ascontiguousarray(d, dtype=np.uint32))
-    assert np.array_equal(S, S_serial)
-    winner, ranking = ref.get_winner_and_ranking(list(range(C)), S)
-    case = dict(C=C, V=V, seed=seed, ballots="scalingelections_b200.ballots.uniform_ballots(V, C, seed)",
-                tally_sha256=sha(d), strongest_sha256=sha(S), winner=int(winner),
-                ranking=[int(x) for x in ranking])
-    (HERE / "config_c4096_v4096.json").write_text(json.dumps(case) + "\n")
-    print({k: v for k, v in case.items() if k != "ranking"})
+    cases = {
+        "config_c4096_v4096": (4096, 4096, 4096, None, "scalingelections_b200.ballots.uniform_ballots(V, C, seed)",
+                               True),
+        "config_c16384_v4096": (16384, 4096, 16384, 0.8,
+                                "scalingelections_b200.ballots.mallows_ballots(V, C, phi, seed)", False),
+    }
+    for name, (C, V, seed, phi, how, serial) in cases.items():
+        if only and name not in only:
+            continue
+        B = uniform_ballots(V, C, seed=seed) if phi is None else mallows_ballots(V, C, phi, seed=seed)
+        d = ref.build_pairwise_preferences(list(B))
+        del B
+        d = np.ascontiguousarray(d, dtype=np.uint32)
+        S = ref.compute_strongest_paths_numba_parallel(d, tile_size=16)
+        if serial:
+            assert np.array_equal(S, ref.compute_strongest_paths_numba_serial(d))
+        winner, ranking = ref.get_winner_and_ranking(list(range(C)), S)
+        case = dict(C=C, V=V, seed=seed, phi=phi, ballots=how, tally_sha256=sha(d), strongest_sha256=sha(S),
+                    winner=int(winner), ranking=[int(x) for x in ranking])
+        (HERE / f"{name}.json").write_text(json.dumps(case) + "\n")
+        print(name, {k: v for k, v in case.items() if k != "ranking"}, flush=True)
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--configs", action="store_true", help="(re)generate only the configuration-size cases")
+    ap.add_argument("--only", nargs="*", help="with --configs: these cases only")
     args = ap.parse_args()
     ref = load_reference(Path(args.ref))
     sys.path.insert(0, str(HERE.parent.parent))
     if args.configs:
-        config_cases(ref)
+        config_cases(ref, args.only)
         return
     from scalingelections_b200.ballots import mallows_ballots, random_preferences, uniform_ballots
 

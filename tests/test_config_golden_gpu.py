@@ -1,9 +1,10 @@
-"""The single-election configuration C = 4096, V = 4096 (uniform permutations) against the
-reference's own outputs on the same ballots, produced by tests/golden/make_golden.py --configs
-from scaling_elections.py:
+"""Single-election configurations against the reference's own outputs on the same ballots:
+C = 4096, V = 4096 uniform permutations, and the headline C = 16384, V = 4096 Mallows(0.8)
+ballots. The outputs were produced by tests/golden/make_golden.py --configs from
+scaling_elections.py:
   * the tally of build_pairwise_preferences (py:51-88),
-  * the strongest paths of compute_strongest_paths_numba_parallel, tile 16 (py:162-271), checked
-    there equal to the serial Numba path (py:91-125),
+  * the strongest paths of compute_strongest_paths_numba_parallel, tile 16 (py:162-271); at
+    C = 4096 also checked there equal to the serial Numba path (py:91-125),
   * the ranking and winner of get_winner_and_ranking (py:274-296).
 The fixture holds hashes and the ranking; the ballots are regenerated from their seed."""
 import hashlib
@@ -17,7 +18,8 @@ import pytest
 from scalingelections_b200 import LANES_U16, LANES_U32, api
 from scalingelections_b200.ballots import uniform_ballots
 
-CASE = json.loads((Path(__file__).parent / "golden" / "config_c4096_v4096.json").read_text())
+GOLDEN = Path(__file__).parent / "golden"
+CASE = json.loads((GOLDEN / "config_c4096_v4096.json").read_text())
 
 
 def sha(a: np.ndarray) -> str:
@@ -44,3 +46,22 @@ def test_config_c4096_matches_reference():
 def test_oracle_tally_at_config_size(orc):
     """The C oracle's tally on the same ballots gives the reference's tally (CPU)."""
     assert sha(orc.tally(list(ballots()))) == CASE["tally_sha256"]
+
+
+@pytest.mark.gpu
+def test_config_c16384_matches_reference(orc):
+    """The headline size. The ballots come from the oracle's C decode of the package's host
+    Mallows sampler (the same stream, 15x faster); the tally hash pins them."""
+    path = GOLDEN / "config_c16384_v4096.json"
+    if not path.exists():
+        pytest.skip("fixture not generated")
+    case = json.loads(path.read_text())
+    B = orc.mallows_ballots(case["V"], case["C"], case["phi"], seed=case["seed"])
+    d = api.build_pairwise_preferences(B)
+    del B
+    assert sha(d) == case["tally_sha256"]
+    S = api.compute_strongest_paths(d, allow_gpu=True, tile_size=32)  # 16-bit lanes: V < 65536
+    assert sha(S) == case["strongest_sha256"]
+    winner, ranking = api.get_winner_and_ranking(list(range(case["C"])), S)
+    assert winner == case["winner"]
+    assert list(ranking) == case["ranking"]
