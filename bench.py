@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per offered load")
     ap.add_argument("--loads", default="0.3,0.6,0.9", help="serve: offered loads as fractions of capacity")
     ap.add_argument("--budget-gb", type=float, default=40.0, help="serve: HBM admission budget")
+    ap.add_argument("--serve-priority", choices=["arrival", "largest"], default="arrival",
+                    help="serve: admission order of requests waiting together")
     ap.add_argument("--elections", type=int, default=4096, help="batch: number of elections")
     ap.add_argument("--max-candidates", type=int, default=2048, help="batch: largest C")
     ap.add_argument("--no-autotune", action="store_true", help="batch: skip the autotuner (use defaults)")
@@ -586,7 +588,8 @@ def run_serve(args, world, rank, local_rank):
     reqs = [(V, C, mallows_ballots_device(V, C, phi, seed=sd, device=dev)) for (V, C, phi, sd) in specs]
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
-    server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=5)
+    server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=5,
+                    priority=args.serve_priority)
     # Warm-up, then capacity: every request arrives at once (closed loop, admission-bound).
     run_arrivals(server, reqs[: min(8, len(reqs))], [0.0] * min(8, len(reqs)))
     p0 = server.stats(profile=True)
@@ -628,7 +631,8 @@ def run_serve(args, world, rank, local_rank):
             "data": "synthetic (seeded Mallows ballots resident on the GPU before arrival)",
             "config": {"workload": f"{args.requests} requests, C log-uniform [8, 8192], V log-uniform [100, 100000], "
                                    f"Mallows phi ~ U[0.2, 1]; HBM budget {args.budget_gb:g} GB",
-                       "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum())},
+                       "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum()),
+                       "admission_priority": args.serve_priority},
             "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan,
                            "engine_launches": sat_launches, "grid": grid,
                            "engine_profile": sat_profile},
