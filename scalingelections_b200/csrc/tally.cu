@@ -43,42 +43,30 @@ constexpr uint32_t kMaxPolls = 1u << 26;
 int64_t padded(int C) { return round_up(C, kTile); }
 
 // ------------------------------------------------------------------------------------------
-// Positions: pos[v][c] = place of candidate c on completed ballot v, one warp per ballot
-// (positions.cuh), 8 ballots per CTA. Id is int32_t, or uint16_t / uint8_t for packed ballots.
+// Positions (from C = 2048 on; below that places_planes_kernel keeps them on the SM):
+// pos[v][c] = place of candidate c on completed ballot v, one CTA per ballot
+// (block_positions in positions.cuh). Id is int32_t, or uint16_t / uint8_t for packed ballots.
 // Ballot v is ids[offsets[v] - id_base, offsets[v + 1] - id_base), or ids[v * C, (v + 1) * C)
 // when offsets is null (complete ballots).
 // ------------------------------------------------------------------------------------------
-constexpr int kPosWarps = 8;
-constexpr int kPosBlockFromC = 2048;  // from this many candidates on, one CTA per ballot
+constexpr int kPosThreads = 256;
 
-// PER_WARP: one ballot per warp, kPosWarps ballots per CTA; else one ballot per CTA.
-template <typename Id, bool PER_WARP>
-__global__ void __launch_bounds__(32 * kPosWarps)
+template <typename Id>
+__global__ void __launch_bounds__(kPosThreads)
     positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int64_t V,
                      int C, int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
-    const int64_t v = PER_WARP ? int64_t(blockIdx.x) * kPosWarps + (threadIdx.x >> 5) : int64_t(blockIdx.x);
-    if (v >= V) return;  // warp-uniform (and CTA-uniform for one ballot per CTA)
+    const int64_t v = blockIdx.x;
     const int64_t beg = offsets ? offsets[v] - id_base : v * C;
     const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
-    int code;
-    if constexpr (PER_WARP) {
-        code = warp_positions(ids + beg, len, C, Cq, pos + v * Cq);
-        if (code != kPosOk && (threadIdx.x & 31) == 0) raise_device_error(err, uint32_t(code));
-    } else {
-        __shared__ int scratch[33];
-        code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
-        if (code != kPosOk && threadIdx.x == 0) raise_device_error(err, uint32_t(code));
-    }
+    __shared__ int scratch[33];
+    const int code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
+    if (code != kPosOk && threadIdx.x == 0) raise_device_error(err, uint32_t(code));
 }
 
 template <typename Id>
 void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, int64_t V, int C, int64_t Cq,
                       float* pos, uint32_t* err, cudaStream_t s) {
-    if (C >= kPosBlockFromC)
-        positions_kernel<Id, false><<<unsigned(V), 32 * kPosWarps, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
-    else
-        positions_kernel<Id, true><<<unsigned((V + kPosWarps - 1) / kPosWarps), 32 * kPosWarps, 0, s>>>(
-            ids, offsets, id_base, V, C, Cq, pos, err);
+    positions_kernel<Id><<<unsigned(V), kPosThreads, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
 }
 
 // ------------------------------------------------------------------------------------------

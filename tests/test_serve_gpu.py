@@ -67,6 +67,26 @@ def test_admission_under_a_tight_budget(orc):
         assert np.array_equal(t.ranking, rank_ref), t.rid
 
 
+def test_large_candidate_counts_beside_small_ones():
+    """POS tasks build each ballot's places in a 16-bit shared-memory row per warp while four
+    rows fit (C up to 12288), and in global memory beyond that: one request on each side of the
+    limit, served together with small ones, each equal to the same election run alone."""
+    reqs = []
+    for i, (C, V) in enumerate([(12288, 150), (12400, 130), (300, 500), (50, 70000)]):
+        reqs.append((V, C, mallows_ballots_device(V, C, 0.7, seed=900 + i)))
+    torch.cuda.synchronize()
+    server = Server(budget_bytes=8 << 30, max_slots=16, idle_ms=20)
+    done, _ = run_arrivals(server, reqs, [0.0, 0.0, 0.001, 0.001], keep_paths=True)
+    server.close()
+    assert len(done) == len(reqs)
+    for t in done:
+        V, C, b = reqs[t.rid]
+        assert t.status == 0, (t.rid, t.status)
+        S, ranking = alone(V, C, b)
+        assert np.array_equal(t.strongest_paths, S), t.rid
+        assert np.array_equal(t.ranking, ranking), t.rid
+
+
 def test_malformed_ballots_reported_in_status():
     V, C = 10, 6
     b = torch.arange(C, dtype=torch.int32, device="cuda").repeat(V, 1)
