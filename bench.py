@@ -308,9 +308,9 @@ def run_ours(args, world, rank, local_rank):
     cell_bytes = 2 if lanes in (0, 16) else 4
     algo_bytes = float(R - 1) ** 2 * 128 * 128 * cell_bytes * 2  # each remainder tile read + written once
 
-    # End to end through the public host API: pinned host in, pinned host out.
-    # The tally half of the path on the same ballots (device-resident), against the FP32 pipe:
-    # B lop3 + 1 popc + 1 add per 32 voter pairs of the upper block triangle (B = bits of C - 1).
+    # The tally half of the path on the same ballots (device-resident), against the integer
+    # ALU pipe: B lop3 + 1 popc + 1 add per 32 voter pairs of the upper block triangle
+    # (B = bits of C - 1).
     tally = None
     if args.input == "mallows":
         tw = torch.empty(api.tally_workspace_bytes(V, C), dtype=torch.uint8, device=dev)
@@ -359,6 +359,7 @@ def run_ours(args, world, rank, local_rank):
                             "peak_source": hbm_source},
                "winner": int(rank_t[0].item())}
 
+    # End to end through the public host API: pinned host in, pinned host out.
     e2e = None
     if not args.no_e2e:
         host_in = torch.empty((C, C), dtype=torch.int32, pin_memory=True)
