@@ -186,6 +186,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int nch = ch1 - ch0;
     const int64_t vlo = int64_t(ch0) * kVC, vhi = int64_t(ch1) * kVC < V ? int64_t(ch1) * kVC : V;
 
+    // done[s]: warps finished with stage s's current chunk. The last of them refills the stage
+    // (see the end of the chunk loop), so no warp waits for another except on the data.
+    __shared__ uint32_t done[kBitStages];
+    if (threadIdx.x < kBitStages) done[threadIdx.x] = 0u;
     if (threadIdx.x == 0) {
         for (int s = 0; s < kBitStages; ++s) mbar_init(&bars[s], 1);
         fence_barrier_init();
@@ -240,12 +244,22 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc[r][q] += __popc(br[r][q]);
         }
-        __syncthreads();  // every thread is done with stage s
-        if (threadIdx.x == 0 && ok && ch + kBitStages < nch) {
-            fence_proxy_async();
-            mbar_arrive_expect_tx(&bars[s], stage_bytes);
-            tma_load_2d(sI + s * stage_words, &mapPl, &bars[s], I * kTile, (ch0 + ch + kBitStages) * B);
-            tma_load_2d(sJ + s * stage_words, &mapPl, &bars[s], J * kTile, (ch0 + ch + kBitStages) * B);
+        // This warp is done reading stage s. The last warp to get here refills it with chunk
+        // ch + kBitStages: its lane 0 has seen every other warp's count (and, through the warp
+        // barrier and the block fence, their reads of the stage come before the copy). Waiters
+        // on bars[s] acquire the reset of done[s] with the stage's next phase.
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&done[s], 1u) == uint32_t(kThreads / 32 - 1)) {
+                done[s] = 0u;
+                if (ok && ch + kBitStages < nch) {
+                    fence_proxy_async();
+                    mbar_arrive_expect_tx(&bars[s], stage_bytes);
+                    tma_load_2d(sI + s * stage_words, &mapPl, &bars[s], I * kTile, (ch0 + ch + kBitStages) * B);
+                    tma_load_2d(sJ + s * stage_words, &mapPl, &bars[s], J * kTile, (ch0 + ch + kBitStages) * B);
+                }
+            }
         }
     }
     if (!ok) {
