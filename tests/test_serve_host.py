@@ -40,3 +40,57 @@ def test_arena_random_workload_never_overlaps():
     for off, n in list(live.items()):
         a.free(off, n)
     assert a.used == 0 and a.alloc(a.capacity) == 0
+
+
+def _host_server(priority, max_slots=100, free_bytes=1 << 40, fits=lambda t: True):
+    """A Server with only its admission state (no engine, no GPU): try_submit records the
+    order and admits what `fits` accepts."""
+    from scalingelections_b200 import serve
+
+    srv = object.__new__(serve.Server)
+    srv.priority, srv.by_slot, srv.max_slots = priority, {}, max_slots
+
+    class _Arena:
+        pass
+
+    srv.arena = _Arena()
+    srv.arena.free_bytes = free_bytes
+    srv.order = []
+
+    def try_submit(t, ballots):
+        if not fits(t):
+            return False
+        srv.order.append(t.rid)
+        srv.by_slot[len(srv.by_slot)] = t
+        return True
+
+    srv.try_submit = try_submit
+    return srv
+
+
+def _tickets(Cs, arrivals=None):
+    from scalingelections_b200.serve import Ticket
+
+    arrivals = arrivals or [0.0] * len(Cs)
+    return [Ticket(rid=i, V=100, C=C, arrival=a) for i, (C, a) in enumerate(zip(Cs, arrivals))]
+
+
+def test_admission_priority_orders_a_burst():
+    for priority, expect in (("arrival", [0, 1, 2, 3]), ("largest", [3, 1, 2, 0])):
+        srv = _host_server(priority)
+        pending = _tickets([10, 300, 50, 2000])
+        assert srv.admit(pending, lambda t: None, now=0.0) == 4
+        assert pending == [] and srv.order == expect, priority
+
+
+def test_admission_priority_keeps_what_does_not_fit_and_no_starvation():
+    # Largest first, but C = 2000 does not fit: the others pass it while it is young ...
+    srv = _host_server("largest", fits=lambda t: t.C != 2000)
+    pending = _tickets([10, 2000, 300])
+    assert srv.admit(pending, lambda t: None, now=0.0) == 2
+    assert srv.order == [2, 0] and [t.rid for t in pending] == [1]
+    # ... and once the oldest has waited past the bypass limit, nothing passes it.
+    srv = _host_server("largest", fits=lambda t: t.C != 2000)
+    pending = _tickets([2000, 10, 300])
+    assert srv.admit(pending, lambda t: None, now=1.0, max_bypass_s=0.25) == 0
+    assert [t.rid for t in pending] == [0, 1, 2]
