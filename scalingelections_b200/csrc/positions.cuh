@@ -153,4 +153,53 @@ __device__ __forceinline__ int block_positions(const Id* __restrict__ r, int64_t
     return kPosOk;
 }
 
+// block_positions with the place row in shared memory as 16-bit values (C < 65535; the
+// caller provides Cq halfwords of p): the scatter and the repeat check stay on the SM, and the
+// finished row goes out to `out` as f32 with coalesced stores. Same checks and codes.
+template <typename Id>
+__device__ __forceinline__ int block_places_u16(const Id* __restrict__ r, int64_t len, int C, int Cq,
+                                                uint16_t* __restrict__ p, float* __restrict__ out, int* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool complete = len >= C;
+    for (int c = complete ? C + threadIdx.x : threadIdx.x; c < Cq; c += blockDim.x)
+        p[c] = c < C ? uint16_t(0xFFFF) : uint16_t(0);
+    __syncthreads();
+    int bad = 0;
+#pragma unroll 4
+    for (int64_t a = threadIdx.x; a < len; a += blockDim.x) {
+        const int64_t id = int64_t(r[a]);
+        if (id < 0 || id >= C) bad = 1;
+        else if (len <= C) p[id] = uint16_t(a);
+    }
+    if (__syncthreads_or(bad)) return kPosRange;
+    if (len > C) return kPosRepeat;  // every id is in range, so one repeats
+#pragma unroll 4
+    for (int64_t a = threadIdx.x; a < len; a += blockDim.x)
+        if (p[int64_t(r[a])] != uint16_t(a)) bad = 1;
+    if (__syncthreads_or(bad)) return kPosRepeat;
+    if (!complete) {  // missing ids in ascending order: a block-wide exclusive scan
+        int* warp_sums = scratch;
+        int base = int(len);
+        for (int c0 = 0; c0 < C; c0 += blockDim.x) {
+            const int c = c0 + threadIdx.x;
+            const bool miss = c < C && p[c] == uint16_t(0xFFFF);
+            const uint32_t m = __ballot_sync(0xffffffffu, miss);
+            if (lane == 0) warp_sums[warp] = __popc(m);
+            __syncthreads();
+            int before = __popc(m & ((1u << lane) - 1u)), total = 0;
+            for (int w = 0; w < nw; ++w) {
+                const int x = warp_sums[w];
+                before += w < warp ? x : 0;
+                total += x;
+            }
+            if (miss) p[c] = uint16_t(base + before);
+            base += total;
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < Cq; c += blockDim.x) out[c] = float(p[c]);
+    return kPosOk;
+}
+
 }  // namespace se

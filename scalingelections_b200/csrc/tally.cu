@@ -44,29 +44,43 @@ int64_t padded(int C) { return round_up(C, kTile); }
 
 // ------------------------------------------------------------------------------------------
 // Positions (from C = 2048 on; below that places_planes_kernel keeps them on the SM):
-// pos[v][c] = place of candidate c on completed ballot v, one CTA per ballot
-// (block_positions in positions.cuh). Id is int32_t, or uint16_t / uint8_t for packed ballots.
+// pos[v][c] = place of candidate c on completed ballot v, one CTA per ballot, the row built in
+// shared memory up to C = 23552 (block_places_u16 in positions.cuh) and in global memory
+// beyond (block_positions). Id is int32_t, or uint16_t / uint8_t for packed ballots.
 // Ballot v is ids[offsets[v] - id_base, offsets[v + 1] - id_base), or ids[v * C, (v + 1) * C)
 // when offsets is null (complete ballots).
 // ------------------------------------------------------------------------------------------
 constexpr int kPosThreads = 256;
 
-template <typename Id>
+// 16-bit place rows up to 46 KiB of dynamic shared memory: with the kernel's static shared
+// memory that stays within the 48 KiB a block gets without raising its limit.
+constexpr int kPosRowMaxCq = 23552;
+
+// ROW: the place row is built in shared memory (block_places_u16, Cq halfwords of dynamic
+// shared memory) and written out coalesced; else in global memory (block_positions).
+template <typename Id, bool ROW>
 __global__ void __launch_bounds__(kPosThreads)
     positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int64_t V,
                      int C, int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) uint16_t row[];
     const int64_t v = blockIdx.x;
     const int64_t beg = offsets ? offsets[v] - id_base : v * C;
     const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
     __shared__ int scratch[33];
-    const int code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
+    int code;
+    if constexpr (ROW) code = block_places_u16(ids + beg, len, C, int(Cq), row, pos + v * Cq, scratch);
+    else code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
     if (code != kPosOk && threadIdx.x == 0) raise_device_error(err, uint32_t(code));
 }
 
 template <typename Id>
 void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, int64_t V, int C, int64_t Cq,
                       float* pos, uint32_t* err, cudaStream_t s) {
-    positions_kernel<Id><<<unsigned(V), kPosThreads, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
+    if (Cq <= kPosRowMaxCq)
+        positions_kernel<Id, true><<<unsigned(V), kPosThreads, size_t(Cq) * 2, s>>>(ids, offsets, id_base, V, C, Cq,
+                                                                                 pos, err);
+    else
+        positions_kernel<Id, false><<<unsigned(V), kPosThreads, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
 }
 
 // ------------------------------------------------------------------------------------------

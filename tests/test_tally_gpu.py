@@ -50,6 +50,19 @@ def test_long_ballots_one_cta_per_ballot(orc, C, complete):
         api.build_pairwise_preferences(bad + [np.array([C - 1])])
 
 
+@pytest.mark.parametrize("C", [23552, 23553])
+def test_place_rows_either_side_of_the_shared_memory_limit(orc, C):
+    """Up to C = 23552 a ballot's place row is built in shared memory, beyond it in global
+    memory: incomplete ballots on both sides, and a repeated id, against the oracle."""
+    rng = np.random.default_rng(C)
+    ballots = [rng.permutation(C)[: rng.integers(C // 2, C + 1)] for _ in range(5)] + [np.array([C - 1])]
+    assert np.array_equal(api.build_pairwise_preferences(ballots), orc.tally(ballots, "scatter"))
+    bad = [ballots[0].copy(), np.array([C - 1])]
+    bad[0][-1] = bad[0][0]
+    with pytest.raises(ValueError, match="twice"):
+        api.build_pairwise_preferences(bad)
+
+
 def test_many_voters_beyond_16_bits(orc):
     """V = 70000 > 65535: counts need 32-bit lanes downstream; the tally itself is exact."""
     from scalingelections_b200.ballots import mallows_ballots
