@@ -3,8 +3,6 @@ checks answer without touching a GPU."""
 import ctypes
 import re
 
-import pytest
-
 from conftest import ROOT
 
 

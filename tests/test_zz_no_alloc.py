@@ -8,7 +8,6 @@ The test calls it through the C ABI and compares its output with se_closure (whi
 caller-provided workspace) bit for bit, on two calls in a row: the static array keeps the
 previous call's contents, and the second call must not be affected by them. This file is
 collected last so that a run stopping at its first failure has run every other test."""
-import ctypes
 
 import numpy as np
 import pytest
