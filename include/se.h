@@ -42,6 +42,7 @@ typedef int se_status_t;
 #define SE_ERR_DEVICE 4      /* a kernel raised its device-side error word */
 #define SE_ERR_OVERFLOW 5    /* a count does not fit the requested 16-bit lanes */
 #define SE_ERR_WORKSPACE 6   /* d_work missing or smaller than the *_workspace_bytes() query */
+#define SE_ERR_HOST 7        /* a host-side resource (memory, a lock) could not be obtained */
 
 /* Lane modes for the closure: 16 = two u16 cells per 32-bit word (every count < 65536),
  * 32 = one u32 cell per word, 0 = choose on the device: 16-bit lanes whenever the kept

@@ -19,6 +19,7 @@ SE_ERR_UNSUPPORTED = 3
 SE_ERR_DEVICE = 4
 SE_ERR_OVERFLOW = 5
 SE_ERR_WORKSPACE = 6
+SE_ERR_HOST = 7
 
 LANES_AUTO = 0
 LANES_U16 = 16

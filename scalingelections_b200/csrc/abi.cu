@@ -32,18 +32,20 @@ se_status_t raise_smem_limit(const void* fn, int bytes, const char* what) {
         set_error("cannot raise the shared-memory limit of %s: no current device", what);
         return SE_ERR_CUDA;
     }
-    static std::mutex m;
-    static std::set<std::tuple<const void*, int, int>> done;
-    std::lock_guard<std::mutex> lock(m);
-    if (done.count({fn, dev, bytes})) return SE_OK;
-    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        set_error("cannot raise the shared-memory limit of %s: %s", what, cudaGetErrorString(e));
-        return SE_ERR_CUDA;
-    }
-    done.insert({fn, dev, bytes});
-    return SE_OK;
+    return host_guard([&]() -> se_status_t {  // the cache's insert can throw std::bad_alloc
+        static std::mutex m;
+        static std::set<std::tuple<const void*, int, int>> done;
+        std::lock_guard<std::mutex> lock(m);
+        if (done.count({fn, dev, bytes})) return SE_OK;
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cannot raise the shared-memory limit of %s: %s", what, cudaGetErrorString(e));
+            return SE_ERR_CUDA;
+        }
+        done.insert({fn, dev, bytes});
+        return SE_OK;
+    });
 }
 
 }  // namespace se

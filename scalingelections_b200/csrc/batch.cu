@@ -536,13 +536,20 @@ using namespace se::batch;
 extern "C" int64_t se_batch_workspace_bytes(int n, const se_election_t* elections) {
     clear_error();
     if (n > 0 && elections == nullptr) return -1;
-    Sizes z;
-    if (size_batch(n, elections, z) != SE_OK) return -1;
-    return z.total;
+    int64_t total = -1;
+    host_guard([&] {  // size_batch fills host vectors
+        Sizes z;
+        const se_status_t st = size_batch(n, elections, z);
+        if (st == SE_OK) total = z.total;
+        return st;
+    });
+    return total;
 }
 
-extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_work, int64_t work_bytes, int order,
-                                        int ctas_per_sm, se_batch_plan_t* plan_out) {
+// The batch's host-side planning: sizes, the task queues and their dependency prefixes, all in
+// host vectors that are filled before anything is written to the device.
+static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_work, int64_t work_bytes, int order,
+                                      int ctas_per_sm, se_batch_plan_t* plan_out) {
     clear_error();
     SE_REQUIRE(plan_out != nullptr, SE_ERR_INVALID, "null plan");
     SE_REQUIRE(n == 0 || el != nullptr, SE_ERR_INVALID, "null election array");
@@ -687,6 +694,11 @@ extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_
     P.graph = nullptr;
     std::memcpy(plan_out, &P, sizeof(P));
     return SE_OK;
+}
+
+extern "C" se_status_t se_batch_prepare(int n, const se_election_t* el, void* d_work, int64_t work_bytes, int order,
+                                        int ctas_per_sm, se_batch_plan_t* plan_out) {
+    return host_guard([&] { return batch_prepare_impl(n, el, d_work, work_bytes, order, ctas_per_sm, plan_out); });
 }
 
 extern "C" se_status_t se_batch_run(const se_batch_plan_t* plan, void* stream) {

@@ -797,14 +797,17 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
 
 extern "C" se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
                                   int lane_bits, int tile, void* d_work, int64_t work_bytes, void* stream) {
-    return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, nullptr);
+    return host_guard([&] {
+        return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, nullptr);
+    });
 }
 
 extern "C" se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out,
                                            int64_t ld_out, int lane_bits, int tile, void* d_work, int64_t work_bytes,
                                            void* stream, double* phase_ms, int* launches) {
-    se_status_t st =
-        closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
+    se_status_t st = host_guard([&] {  // the phase events' vector is filled before any event exists
+        return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
+    });
     if (launches) *launches = se_closure_launch_count(C);
     return st;
 }

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <exception>
 
 #include "../../include/se.h"
 
@@ -57,6 +58,22 @@ se_status_t raise_smem_limit(const void* fn, int bytes, const char* what);
             return (code);                                                                    \
         }                                                                                     \
     } while (0)
+
+// No C++ exception may leave an extern "C" entry point: its callers (C, ctypes, cgo) cannot
+// catch one, and the process would end in std::terminate. The entry points that fill host
+// containers (which can throw std::bad_alloc) run their body through this guard, which turns
+// an exception into SE_ERR_HOST with its message.
+template <class F>
+se_status_t host_guard(F&& body) noexcept {
+    try {
+        return body();
+    } catch (const std::exception& x) {
+        set_error("host-side failure: %s", x.what());
+    } catch (...) {
+        set_error("host-side failure");
+    }
+    return SE_ERR_HOST;
+}
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 

@@ -187,9 +187,10 @@ peak_kernel_t pick(int recipe, int* cells) {
 }  // namespace
 }  // namespace se
 
-extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per_sm_clock,
-                                      double* sm_mhz, double* kernel_ms, double* relax_per_s) {
-    using namespace se;
+namespace se {
+namespace {
+se_status_t minmax_peak_impl(int recipe, int k_steps, double* relax_per_sm_clock, double* sm_mhz,
+                             double* kernel_ms, double* relax_per_s) {
     clear_error();
     int cells = 1;
     peak_kernel_t kernel = pick(recipe, &cells);
@@ -203,6 +204,9 @@ extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per
     SE_REQUIRE(per_sm >= 1, SE_ERR_CUDA, "min/max peak kernel cannot be resident");
     const int grid = sms * per_sm;
 
+    // Host buffer for the per-block clock stamps, allocated before any device resource so
+    // that a failed allocation (an exception, turned into a status by the caller) leaks none.
+    std::vector<unsigned long long> host(static_cast<size_t>(grid) * 2);
     uint32_t* sink = nullptr;
     unsigned long long* stamps = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -217,7 +221,6 @@ extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per
     if (st == SE_OK && (e = cudaEventCreate(&e0)) != cudaSuccess) fail(e, "cudaEventCreate");
     if (st == SE_OK && (e = cudaEventCreate(&e1)) != cudaSuccess) fail(e, "cudaEventCreate");
     float ms = 0.f;
-    std::vector<unsigned long long> host;
     if (st == SE_OK) {
         kernel<<<grid, kPeakThreads>>>(12345u, 64, sink, stamps);  // warm-up
         cudaEventRecord(e0);
@@ -228,7 +231,6 @@ extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per
     if (st == SE_OK && (e = cudaGetLastError()) != cudaSuccess) fail(e, "min/max peak launch");
     if (st == SE_OK) {
         cudaEventElapsedTime(&ms, e0, e1);
-        host.resize(static_cast<size_t>(grid) * 2);
         if ((e = cudaMemcpy(host.data(), stamps, host.size() * sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost)) != cudaSuccess)
             fail(e, "cudaMemcpy");
@@ -255,4 +257,13 @@ extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per
     if (sink) cudaFree(sink);
     if (stamps) cudaFree(stamps);
     return st;
+}
+
+}  // namespace
+}  // namespace se
+
+extern "C" se_status_t se_minmax_peak(int recipe, int k_steps, double* relax_per_sm_clock,
+                                      double* sm_mhz, double* kernel_ms, double* relax_per_s) {
+    return se::host_guard(
+        [&] { return se::minmax_peak_impl(recipe, k_steps, relax_per_sm_clock, sm_mhz, kernel_ms, relax_per_s); });
 }

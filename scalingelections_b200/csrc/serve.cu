@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <vector>
 
 #include "batch_core.cuh"
@@ -770,16 +771,24 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(engine_kernel), int(kEngineSmem),
                                           "the serving engine"))
         return st;
-    auto* h = new se_engine();
+    auto* h = new (std::nothrow) se_engine();
+    SE_REQUIRE(h != nullptr, SE_ERR_HOST, "cannot allocate the engine's host state");
     Engine& E = h->e;
+    try {  // the host vectors first, while no CUDA resource is held yet
+        E.gen.assign(max_slots, 0);
+        E.busy.assign(max_slots, 0);
+        E.tally_reported.assign(max_slots, 0);
+    } catch (const std::exception& x) {
+        delete h;
+        set_error("cannot allocate the engine's host state: %s", x.what());
+        return SE_ERR_HOST;
+    }
     E.work = static_cast<uint8_t*>(d_work);
     E.max_slots = max_slots;
     E.hdr = reinterpret_cast<EngineHeader*>(E.work);
     E.slots = reinterpret_cast<Req*>(E.work + so);
     E.claims = reinterpret_cast<uint64_t*>(E.work + co);
     E.dones = reinterpret_cast<uint32_t*>(E.work + dof);
-    E.gen.assign(max_slots, 0);
-    E.busy.assign(max_slots, 0);
     E.idle_ns = uint64_t(idle_ms) * 1000000ull;
     auto fail = [&](cudaError_t err, const char* what) {
         set_error("%s failed: %s", what, cudaGetErrorString(err));
@@ -806,7 +815,6 @@ extern "C" se_status_t se_engine_create(void* d_work, int64_t work_bytes, int ma
     std::memset(E.tally_host, 0, sizeof(uint32_t) * size_t(max_slots));
     if ((err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&E.tally_dev), E.tally_host, 0)) != cudaSuccess)
         return fail(err, "cudaHostGetDevicePointer");
-    E.tally_reported.assign(max_slots, 0);
     if ((err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&E.done_dev), E.done_host, 0)) != cudaSuccess)
         return fail(err, "cudaHostGetDevicePointer");
     if ((err = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking)) != cudaSuccess)

@@ -50,3 +50,36 @@ def test_closure_argument_errors_need_no_gpu():
     assert L.se_closure(p, 4, 4, p, 4, 16, 0, p, 16, None) == _lib.SE_ERR_WORKSPACE
     assert L.se_tally(None, None, 5, 4, p, 4, p, 1 << 20, None) == _lib.SE_ERR_INVALID
     assert L.se_rank(p, 2, 4, p, p, None) == _lib.SE_ERR_INVALID
+
+
+HOST_ALLOC_FAILURE = r"""
+import ctypes, resource, sys
+
+L = ctypes.CDLL(sys.argv[1])
+L.se_batch_workspace_bytes.restype = ctypes.c_int64
+L.se_last_error.restype = ctypes.c_char_p
+el = ctypes.create_string_buffer(64)  # one se_election_t, C = 0
+vm = next(int(l.split()[1]) for l in open("/proc/self/status") if l.startswith("VmSize:")) * 1024
+resource.setrlimit(resource.RLIMIT_AS, (vm + (32 << 20), resource.getrlimit(resource.RLIMIT_AS)[1]))
+n = (1 << 24) - 1  # size_batch's first host vector alone takes 134 MB
+print(L.se_batch_workspace_bytes(n, el), L.se_last_error().decode())
+"""
+
+
+def test_a_host_allocation_failure_is_a_status_not_an_abort():
+    """A std::bad_alloc inside an entry point comes back through the C ABI as an error (here
+    se_batch_workspace_bytes's -1 with its message), not as std::terminate. The process caps
+    its own address space so that the batch sizer's host vectors cannot be allocated; the
+    sizer throws before it reads an election, and the one election it is given would fail its
+    candidate-count check if the cap did not take effect."""
+    import subprocess
+    import sys
+
+    from scalingelections_b200 import _lib
+
+    r = subprocess.run([sys.executable, "-c", HOST_ALLOC_FAILURE, str(_lib.LIB_PATH)], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    total, _, message = r.stdout.strip().partition(" ")
+    assert total == "-1"
+    assert message.startswith("host-side failure"), message
