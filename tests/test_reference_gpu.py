@@ -99,6 +99,7 @@ def test_speed_against_reference_kernels(ref_gpu):
             "reference_call": "compute_strongest_paths(P, allow_gpu=True, allow_tma=False, tile_size=32)"}
     out_dir = os.environ.get("SE_REPORT_DIR")
     if out_dir:
+        os.makedirs(out_dir, exist_ok=True)
         with open(os.path.join(out_dir, "reference_gpu.json"), "w") as f:
             json.dump(line, f)
     print(json.dumps(line))
