@@ -130,9 +130,16 @@ class BatchedElections:
             check(_lib.lib().se_batch_check(ctypes.byref(self.plan), torch.cuda.current_stream().cuda_stream))
 
     def close(self) -> None:
+        """Releases the captured CUDA graph, if any."""
         if getattr(self, "plan", None) is not None and self._graph:
             _lib.lib().se_batch_release(ctypes.byref(self.plan))
             self._graph = False
+
+    def __enter__(self) -> "BatchedElections":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
 
     def __del__(self):
         try:

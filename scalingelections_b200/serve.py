@@ -296,9 +296,17 @@ class Server:
         return out
 
     def close(self) -> None:
+        """Stops the engine kernel (waiting for it) and frees its host state. The device
+        buffers stay valid until the Server itself is released, so close() before that."""
         if self.engine:
             self.L.se_engine_destroy(self.engine)
             self.engine = ctypes.c_void_p()
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
 
     def __del__(self):
         try:

@@ -54,9 +54,8 @@ def test_admission_under_a_tight_budget(orc):
     """A budget too small for all requests at once: they queue on the host and are admitted
     as memory frees up; results stay exact."""
     reqs = make_requests(2, 10)
-    server = Server(budget_bytes=64 << 20, max_slots=8, idle_ms=5)
-    done, _ = run_arrivals(server, reqs, [0.0] * len(reqs), keep_paths=True)
-    server.close()
+    with Server(budget_bytes=64 << 20, max_slots=8, idle_ms=5) as server:
+        done, _ = run_arrivals(server, reqs, [0.0] * len(reqs), keep_paths=True)
     assert len(done) == len(reqs)
     for t in done:
         V, C, b = reqs[t.rid]
