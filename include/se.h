@@ -286,12 +286,15 @@ SE_API se_status_t se_shard_check(se_shard_t* shard, void* stream);
  * Ballot tally. Replaces build_pairwise_preferences (scaling_elections.py:51-88).
  *
  *   Ballots are given in CSR form: ballot v is d_ids[d_offsets[v] .. d_offsets[v+1]), the
- *   candidate ids from most to least preferred. A ballot that omits candidates is completed
- *   by appending the missing ids in ascending order (scaling_elections.py:75-83). C must be
- *   at least max(id) + 1 (the reference uses exactly max(id) + 1, :63-66).
- *   d_out receives d[i][j] = #ballots ranking i above j (uint32, diagonal 0), row stride
- *   ld_out. Ids outside [0, C) or repeated within a ballot return SE_ERR_DEVICE with a
- *   message (the reference does not validate these).
+ *   candidate ids from most to least preferred. A ballot whose length differs from C is
+ *   completed by appending the ids it lacks in ascending order (scaling_elections.py:75-83).
+ *   C must be at least max(id) + 1 (the reference uses exactly max(id) + 1, :63-66).
+ *   d_out receives d[i][j] = the number of (ballot, position of i, later position of j)
+ *   triples (uint32, row stride ld_out), the reference's pair-by-pair count (py:46-48): for
+ *   ballots that name each id once, the number of ballots ranking i above j, with diagonal 0.
+ *   A ballot that repeats an id is counted the same way, so its pairs can reach the diagonal
+ *   and push counts above V. Ids outside [0, C) return SE_ERR_DEVICE with a message (the
+ *   reference takes C = max(id) + 1, so it never meets one).
  * ------------------------------------------------------------------------------------- */
 SE_API int64_t se_tally_workspace_bytes(int64_t V, int C);
 SE_API se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
@@ -299,8 +302,8 @@ SE_API se_status_t se_tally(const int32_t* d_ids, const int64_t* d_offsets, int6
                      void* stream);
 
 /* se_tally without the final synchronisation: fully stream-ordered. Malformed ballots are
- * reported in the first 4 bytes of d_work (0 = fine, 2 = id out of range, 3 = repeated id,
- * 1 = lost TMA completion), which the caller reads after the stream reaches that point. */
+ * reported in the first 4 bytes of d_work (0 = fine, 2 = id out of range, 1 = lost TMA
+ * completion), which the caller reads after the stream reaches that point. */
 SE_API se_status_t se_tally_enqueue(const int32_t* d_ids, const int64_t* d_offsets, int64_t V, int C,
                                     uint32_t* d_out, int64_t ld_out, void* d_work,
                                     int64_t work_bytes, void* stream);

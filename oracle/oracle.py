@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes
 import importlib.machinery
 import importlib.util
+import os
 import subprocess
 import sysconfig
 from pathlib import Path
@@ -35,12 +36,19 @@ _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 
 
+def reference_dir() -> Path | None:
+    """The reference checkout named by SE_REFERENCE_DIR, when that directory holds its sources."""
+    d = os.environ.get("SE_REFERENCE_DIR")
+    return Path(d) if d and (Path(d) / "scaling_elections.cu").exists() else None
+
+
 def build(reference: bool = True) -> None:
-    """Compile liboracle.so and, when the reference sources are present, oracle/_ref."""
+    """Compile liboracle.so and, when SE_REFERENCE_DIR names the reference sources, oracle/_ref."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    if reference and Path("/root/reference/scaling_elections.cu").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref_gpu"], check=True)
+    ref = reference_dir()
+    if reference and ref is not None:
+        for target in ("ref", "ref_gpu"):
+            subprocess.run(["make", "-s", "-C", str(HERE), target, f"REF={ref}"], check=True)
 
 
 def lib() -> ctypes.CDLL:

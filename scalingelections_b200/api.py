@@ -285,9 +285,10 @@ def _tally_host(ballots: Ballots, dev) -> torch.Tensor:
 
 def build_pairwise_preferences(voter_rankings: Sequence[np.ndarray] | np.ndarray) -> np.ndarray:
     """GPU form of scaling_elections.py:51-88: uint32 [C, C] with d[i][j] = number of voters
-    ranking i above j, C = max id + 1. Incomplete ballots get the missing ids appended in
-    ascending order (py:75-83). A ballot repeating an id raises ValueError (the reference
-    counts such ballots without complaint)."""
+    ranking i above j, C = max id + 1. A ballot whose length differs from C gets the ids it
+    lacks appended in ascending order (py:75-83). A ballot that repeats an id is counted pair
+    by pair like the reference's (py:46-48): d[x][y] gains one for every position of x before
+    a position of y, so the diagonal and counts above V can be non-zero."""
     _require_cuda()
     b = Ballots.from_rankings(voter_rankings)
     d = _tally_host(b, torch.cuda.current_device())
@@ -323,15 +324,16 @@ class SchulzeResult:
 
 def schulze(voter_rankings: Sequence[np.ndarray] | np.ndarray, *, return_paths: bool = False) -> SchulzeResult:
     """Whole Schulze election on the GPU: tally -> closure -> ranking, matrices kept in HBM.
-    Uses 16-bit closure lanes when every count fits (fewer than 65536 voters)."""
+    The closure's lanes are chosen on the device from the kept counts: 16-bit (shifted if need
+    be) whenever they fit a 16-bit window, else 32-bit."""
     _require_cuda()
     b = Ballots.from_rankings(voter_rankings)
     dev = torch.cuda.current_device()
     d = _tally_host(b, dev)
-    # Below 65536 ballots every count fits 16 bits; above, the automatic mode still finds a
-    # shifted 16-bit window (kept counts lie in (V/2, V]) up to 131070 ballots.
-    lanes = LANES_U16 if b.num_voters < 65536 else LANES_AUTO
-    S = strongest_paths_device(d, lanes=lanes)
+    # Permutation ballots keep every count within (V/2, V], a 16-bit window up to 131070
+    # ballots; ballots that repeat an id can raise counts above V, which the measured window
+    # also covers.
+    S = strongest_paths_device(d, lanes=LANES_AUTO)
     wins, ranking = rank_device(S)
     ranking_h = ranking.cpu().numpy()
     return SchulzeResult(int(ranking_h[0]), ranking_h, wins.cpu().numpy(),

@@ -266,7 +266,8 @@ def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | Non
                stats: dict | None = None) -> torch.Tensor:
     """Pairwise preference counts (uint32 [C, C] on ``device``) of every ballot in the file,
     streamed through the GPU in chunks of ``chunk_ballots``. Equals ``build_pairwise_preferences``
-    of the same ballots. Raises ValueError for an id outside [0, C) or repeated in a ballot."""
+    of the same ballots, including ballots that repeat an id (counted pair by pair, as the
+    reference does). Raises ValueError for an id outside [0, C)."""
     bf = BallotFile(path)
     h = bf.header
     threads = int(threads) if threads else min(32, os.cpu_count() or 1)
@@ -365,8 +366,6 @@ def tally_file(path: str | os.PathLike, *, device=None, chunk_ballots: int | Non
                      read_threads=threads)
     if code == 2:
         raise ValueError(f"a ballot names a candidate outside [0, {C})")
-    if code == 3:
-        raise ValueError("a ballot names the same candidate twice")
     if code:
         raise SchulzeError(_lib.SE_ERR_DEVICE, f"tally kernel reported device error {code}")
     return out

@@ -10,6 +10,13 @@
 //
 // Kernel 1 (positions_kernel) writes pos as f32 [V][Cq] (exact integers), validating ids
 // (range, repeats). Kernel 2 (pack_planes_kernel) packs each 32-voter chunk into bit planes.
+//
+// A ballot that names a candidate more than once is not a permutation, and the reference
+// counts it pair by pair all the same (py:46-48; py:75 completes it only when its length
+// differs from C). Such an "irregular" ballot gets place 0 for every candidate, so the
+// bit-sliced count sees no pair for it in either direction, and it is left out of the
+// complement V - d[i][j]. irregular_kernel then adds its pairs exactly as the reference does,
+// diagonal included, with atomics.
 // For C < 2048, places_planes_kernel does both in one pass and keeps the places in shared
 // memory. Kernel 3 (count_bits_kernel, one CTA per upper tile) streams the planes of the two
 // 128-candidate strips into shared memory with TMA and counts per 8 x 8 register micro-tile
@@ -36,11 +43,24 @@ constexpr int kTile = 128;     // candidates per tile edge
 constexpr int kVC = 32;        // voters per TMA chunk
 constexpr int kThreads = 512;  // 8 x 4 cells per thread
 constexpr uint32_t kErrRange = 2;
-constexpr uint32_t kErrRepeat = 3;
 constexpr uint32_t kErrTimeout = 1;
 constexpr uint32_t kMaxPolls = 1u << 26;
 
 int64_t padded(int C) { return round_up(C, kTile); }
+
+// Irregular ballots (a repeated id) of one call, in the workspace after the error word:
+// a count, the number per 32-voter chunk (the count kernel leaves them out of V - d[i][j]) and
+// the list of their ballot indices (for irregular_kernel).
+struct Irregular {
+    uint32_t* n;         // irregular ballots recorded
+    uint32_t* chunk;     // [ceil(V / 32)]: irregular ballots per 32-voter chunk
+    uint32_t* list;      // [V]: their ballot indices, in no particular order
+};
+
+__device__ __forceinline__ void record_irregular(const Irregular& irr, int64_t v) {
+    irr.list[atomicAdd(irr.n, 1u)] = uint32_t(v);
+    atomicAdd(irr.chunk + v / 32, 1u);
+}
 
 // ------------------------------------------------------------------------------------------
 // Positions (from C = 2048 on; below that places_planes_kernel keeps them on the SM):
@@ -61,7 +81,7 @@ constexpr int kPosRowMaxCq = 23552;
 template <typename Id, bool ROW>
 __global__ void __launch_bounds__(kPosThreads)
     positions_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int64_t V,
-                     int C, int64_t Cq, float* __restrict__ pos, uint32_t* __restrict__ err) {
+                     int C, int64_t Cq, float* __restrict__ pos, Irregular irr, uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) uint16_t row[];
     const int64_t v = blockIdx.x;
     const int64_t beg = offsets ? offsets[v] - id_base : v * C;
@@ -70,17 +90,23 @@ __global__ void __launch_bounds__(kPosThreads)
     int code;
     if constexpr (ROW) code = block_places_u16(ids + beg, len, C, int(Cq), row, pos + v * Cq, scratch);
     else code = block_positions(ids + beg, len, C, Cq, pos + v * Cq, scratch);
-    if (code != kPosOk && threadIdx.x == 0) raise_device_error(err, uint32_t(code));
+    if (code == kPosRepeat) {  // every thread got the same code after the block-wide check
+        for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) pos[v * Cq + c] = 0.0f;
+        if (threadIdx.x == 0) record_irregular(irr, v);
+    } else if (code != kPosOk && threadIdx.x == 0) {
+        raise_device_error(err, uint32_t(code));
+    }
 }
 
 template <typename Id>
 void launch_positions(const Id* ids, const int64_t* offsets, int64_t id_base, int64_t V, int C, int64_t Cq,
-                      float* pos, uint32_t* err, cudaStream_t s) {
+                      float* pos, const Irregular& irr, uint32_t* err, cudaStream_t s) {
     if (Cq <= kPosRowMaxCq)
         positions_kernel<Id, true><<<unsigned(V), kPosThreads, size_t(Cq) * 2, s>>>(ids, offsets, id_base, V, C, Cq,
-                                                                                 pos, err);
+                                                                                 pos, irr, err);
     else
-        positions_kernel<Id, false><<<unsigned(V), kPosThreads, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, err);
+        positions_kernel<Id, false><<<unsigned(V), kPosThreads, 0, s>>>(ids, offsets, id_base, V, C, Cq, pos, irr,
+                                                                        err);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -128,7 +154,8 @@ inline size_t fused_smem(int64_t Cq) { return size_t(32) * size_t(Cq + 2) * 2; }
 template <typename Id, int B>
 __global__ void __launch_bounds__(1024)
     places_planes_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base,
-                         int64_t V, int C, int Cq, uint32_t* __restrict__ planes, uint32_t* __restrict__ err) {
+                         int64_t V, int C, int Cq, uint32_t* __restrict__ planes, Irregular irr,
+                         uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) uint16_t rows[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pitch = Cq + 2;  // halfwords; rows start 4 bytes apart modulo 128
@@ -139,7 +166,13 @@ __global__ void __launch_bounds__(1024)
         const int64_t beg = offsets ? offsets[v] - id_base : v * C;
         const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
         const int code = warp_places_u16(ids + beg, len, C, Cq, row);
-        if (code != kPosOk && lane == 0) raise_device_error(err, uint32_t(code));
+        if (code == kPosRepeat) {  // an irregular ballot: place 0 everywhere, counted apart
+            __syncwarp();
+            for (int c = lane; c < Cq; c += 32) row[c] = 0;
+            if (lane == 0) record_irregular(irr, v);
+        } else if (code != kPosOk && lane == 0) {
+            raise_device_error(err, uint32_t(code));
+        }
     } else {
         for (int c = lane; c < Cq; c += 32) row[c] = 0;  // voters past V count as place 0
     }
@@ -177,7 +210,8 @@ inline size_t bits_smem(int B) { return size_t(kBitStages) * 2 * B * kTile * 4 +
 template <int B>
 __global__ void __launch_bounds__(kThreads, 1)
     count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int64_t V, int C, int R, int splits,
-                      uint32_t* __restrict__ out, int64_t ld_out, bool accumulate, uint32_t* __restrict__ err) {
+                      uint32_t* __restrict__ out, int64_t ld_out, bool accumulate,
+                      const uint32_t* __restrict__ irr_chunk, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint32_t* sI = reinterpret_cast<uint32_t*>(smem_raw);  // [kBitStages][B][kTile]
     uint32_t* sJ = sI + kBitStages * B * kTile;            // [kBitStages][B][kTile]
@@ -203,7 +237,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     // done[s]: warps finished with stage s's current chunk. The last of them refills the stage
     // (see the end of the chunk loop), so no warp waits for another except on the data.
     __shared__ uint32_t done[kBitStages];
+    __shared__ uint32_t irr_in_range;  // irregular ballots among this CTA's voters
     if (threadIdx.x < kBitStages) done[threadIdx.x] = 0u;
+    if (threadIdx.x < 32) {
+        uint32_t n = 0u;
+        for (int c = ch0 + int(threadIdx.x); c < ch1; c += 32) n += irr_chunk[c];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+        if (threadIdx.x == 0) irr_in_range = n;
+    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < kBitStages; ++s) mbar_init(&bars[s], 1);
         fence_barrier_init();
@@ -280,7 +322,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         raise_device_error(err, kErrTimeout);
         return;
     }
-    const uint32_t Vu = uint32_t(vhi - vlo);
+    // Voters with a permutation ballot: each of them is counted in exactly one of d[i][j] and
+    // d[j][i]. Irregular ballots (place 0 everywhere) are in neither and are added apart.
+    const uint32_t Vu = uint32_t(vhi - vlo) - irr_in_range;
     if (nch == 0) return;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -317,13 +361,71 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// The pairs of the irregular ballots, as the reference counts them (py:46-48 over the ballot
+// completed by py:75-83): with r the ballot as given (length len, ids in [0, C)) and M the ids
+// absent from it in ascending order, appended only when len != C, the completed ballot is
+// r ++ M and every position a before position b adds one to d[x_a][x_b]:
+//   1. a < b within r;
+//   2. every a of r with every m of M;
+//   3. m1 < m2 within M.
+// Every warp of the grid takes rows (a, or m1) of one ballot at a time, its lanes stride the
+// partners, and each adds with an atomic. Each CTA keeps the ballot's presence bitmap
+// (ceil(C / 32) words of dynamic shared memory) for 2 and 3. A call without irregular
+// ballots returns at once.
+constexpr int kIrrThreads = 512;
+
+template <typename Id>
+__global__ void __launch_bounds__(kIrrThreads)
+    irregular_kernel(const Id* __restrict__ ids, const int64_t* __restrict__ offsets, int64_t id_base, int C,
+                     const uint32_t* __restrict__ irr_n, const uint32_t* __restrict__ irr_list,
+                     uint32_t* __restrict__ out, int64_t ld_out) {
+    extern __shared__ uint32_t present[];
+    const uint32_t n = *irr_n;
+    if (n == 0u) return;
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int64_t gw = int64_t(blockIdx.x) * warps + (threadIdx.x >> 5);
+    const int64_t GW = int64_t(gridDim.x) * warps;
+    const int words = (C + 31) >> 5;
+    for (uint32_t q = 0; q < n; ++q) {
+        const int64_t v = irr_list[q];
+        const int64_t beg = offsets ? offsets[v] - id_base : v * C;
+        const int64_t len = offsets ? offsets[v + 1] - offsets[v] : C;
+        const Id* r = ids + beg;
+        for (int64_t a = gw; a < len; a += GW) {
+            uint32_t* row = out + int64_t(r[a]) * ld_out;
+            for (int64_t b = a + 1 + lane; b < len; b += 32) atomicAdd(row + int64_t(r[b]), 1u);
+        }
+        if (len == int64_t(C)) continue;  // the same for every thread of the block
+        __syncthreads();                  // the previous ballot's bitmap is no longer read
+        for (int w = threadIdx.x; w < words; w += blockDim.x) present[w] = 0u;
+        __syncthreads();
+        for (int64_t a = threadIdx.x; a < len; a += blockDim.x) {
+            const uint32_t id = uint32_t(r[a]);
+            atomicOr(present + (id >> 5), 1u << (id & 31));
+        }
+        __syncthreads();
+        auto absent = [&](int c) { return !((present[c >> 5] >> (c & 31)) & 1u); };
+        for (int64_t a = gw; a < len; a += GW) {
+            uint32_t* row = out + int64_t(r[a]) * ld_out;
+            for (int m = lane; m < C; m += 32)
+                if (absent(m)) atomicAdd(row + m, 1u);
+        }
+        for (int64_t m1 = gw; m1 < C; m1 += GW) {
+            if (!absent(int(m1))) continue;
+            uint32_t* row = out + m1 * ld_out;
+            for (int64_t m2 = m1 + 1 + lane; m2 < C; m2 += 32)
+                if (absent(int(m2))) atomicAdd(row + m2, 1u);
+        }
+    }
+}
+
 // The pack and count kernels for each plane count 1 .. kMaxPlanes.
 template <typename Id>
-using FusedKernel = void (*)(const Id*, const int64_t*, int64_t, int64_t, int, int, uint32_t*, uint32_t*);
+using FusedKernel = void (*)(const Id*, const int64_t*, int64_t, int64_t, int, int, uint32_t*, Irregular, uint32_t*);
 
 struct TallyKernels {
     void (*pack)(const float*, int64_t, int64_t, uint32_t*);
-    void (*count)(CUtensorMap, int64_t, int, int, int, uint32_t*, int64_t, bool, uint32_t*);
+    void (*count)(CUtensorMap, int64_t, int, int, int, uint32_t*, int64_t, bool, const uint32_t*, uint32_t*);
     FusedKernel<uint8_t> fused8;  // places + planes for C < 2048 (B <= 11), else null
     FusedKernel<uint16_t> fused16;
     FusedKernel<int32_t> fused32;
@@ -355,16 +457,22 @@ static_assert(kMaxPlanes == 20, "the table instantiates planes 1 .. 20");
 using namespace se;
 using namespace se::tally;
 
-// Error word (256 B), then the places f32 [V][Cq] (only from C = 2048 on: below that the places
-// stay in shared memory), then the bit planes u32 [ceil(V/32) * B][Cq].
+// Error word (256 B); the irregular-ballot record (16 B header holding the count, then one
+// word per 32-voter chunk, then the ballot list, V words); the places f32 [V][Cq] (only from
+// C = 2048 on: below that the places stay in shared memory); the bit planes u32
+// [ceil(V/32) * B][Cq].
+static int64_t chunks_of(int64_t V) { return (std::max<int64_t>(V, 1) + kVC - 1) / kVC; }
+static int64_t irregular_header_bytes(int64_t V) { return 16 + 4 * chunks_of(V); }
+static int64_t places_offset(int64_t V) {
+    return 256 + round_up(irregular_header_bytes(V) + 4 * std::max<int64_t>(V, 1), 256);
+}
 static int64_t planes_offset(int64_t V, int C) {
-    return C < kFusedMaxCq ? 256 : 256 + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256);
+    return C < kFusedMaxCq ? places_offset(V) : places_offset(V) + round_up(std::max<int64_t>(V, 1) * padded(C) * 4, 256);
 }
 
 extern "C" int64_t se_tally_workspace_bytes(int64_t V, int C) {
     if (V < 0 || C < 1) return -1;
-    const int64_t nch = (std::max<int64_t>(V, 1) + kVC - 1) / kVC;
-    return planes_offset(V, C) + round_up(nch * planes_for(C) * padded(C) * 4, 256);
+    return planes_offset(V, C) + round_up(chunks_of(V) * planes_for(C) * padded(C) * 4, 256);
 }
 
 namespace {
@@ -393,7 +501,11 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     cudaStream_t s = static_cast<cudaStream_t>(stream_);
     uint8_t* work = static_cast<uint8_t*>(d_work);
     uint32_t* err = reinterpret_cast<uint32_t*>(work);
-    float* pos = reinterpret_cast<float*>(work + 256);
+    Irregular irr;
+    irr.n = reinterpret_cast<uint32_t*>(work + 256);
+    irr.chunk = irr.n + 4;
+    irr.list = irr.chunk + chunks_of(V);
+    float* pos = reinterpret_cast<float*>(work + places_offset(V));
     const int64_t Cq = padded(C);
     const int R = int(Cq / kTile);
 
@@ -402,6 +514,7 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         if (!accumulate) SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
         return SE_OK;
     }
+    SE_CUDA_TRY(cudaMemsetAsync(irr.n, 0, size_t(irregular_header_bytes(V)), s));
     const int B = planes_for(C);
     const TallyKernels& K = tally_kernels(B);
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(K.count), int(bits_smem(B)), "the tally kernel"))
@@ -417,21 +530,21 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
         if (se_status_t st = raise_smem_limit(fn, int(fused_smem(kFusedMaxCq)), "the places kernel")) return st;
         if (w == 0)
             K.fused8<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C,
-                                                           int(Cq), planes, err);
+                                                           int(Cq), planes, irr, err);
         else if (w == 1)
             K.fused16<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V,
-                                                            C, int(Cq), planes, err);
+                                                            C, int(Cq), planes, irr, err);
         else
             K.fused32<<<unsigned(nch_all), 1024, smem, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V,
-                                                            C, int(Cq), planes, err);
+                                                            C, int(Cq), planes, irr, err);
         SE_CHECK_LAUNCH();
     } else {
         if (id_bytes == 4)
-            launch_positions(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+            launch_positions(static_cast<const int32_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, irr, err, s);
         else if (id_bytes == 2)
-            launch_positions(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+            launch_positions(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, irr, err, s);
         else
-            launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, err, s);
+            launch_positions(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, V, C, Cq, pos, irr, err, s);
         SE_CHECK_LAUNCH();
         K.pack<<<dim3(unsigned(nch_all), unsigned((Cq + 255) / 256)), 256, 0, s>>>(pos, V, Cq, planes);
         SE_CHECK_LAUNCH();
@@ -468,7 +581,30 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     if (splits > 1 && !accumulate)
         SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
     K.count<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
-                                                                      err);
+                                                                      irr.chunk, err);
+    SE_CHECK_LAUNCH();
+    // The irregular ballots' pairs, after the count's stores. Without any it returns at once.
+    const size_t irr_smem = size_t((C + 31) / 32) * 4;
+    const unsigned irr_grid = unsigned(2 * sms);
+    if (id_bytes == 4) {
+        auto fn = irregular_kernel<int32_t>;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+            return st;
+        fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, C, irr.n,
+                                                  irr.list, d_out, ld_out);
+    } else if (id_bytes == 2) {
+        auto fn = irregular_kernel<uint16_t>;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+            return st;
+        fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, C, irr.n,
+                                                  irr.list, d_out, ld_out);
+    } else {
+        auto fn = irregular_kernel<uint8_t>;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+            return st;
+        fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, C, irr.n,
+                                                  irr.list, d_out, ld_out);
+    }
     SE_CHECK_LAUNCH();
     if (!check) return SE_OK;
 
@@ -476,7 +612,6 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     SE_CUDA_TRY(cudaMemcpyAsync(&code, err, 4, cudaMemcpyDeviceToHost, s));
     SE_CUDA_TRY(cudaStreamSynchronize(s));
     SE_REQUIRE(code != kErrRange, SE_ERR_DEVICE, "a ballot names a candidate outside [0, %d)", C);
-    SE_REQUIRE(code != kErrRepeat, SE_ERR_DEVICE, "a ballot names the same candidate twice");
     SE_REQUIRE(code == 0, SE_ERR_DEVICE, "tally kernel reported device error %u (TMA wait timed out)", code);
     return SE_OK;
 }

@@ -20,8 +20,24 @@ def golden_names():
 
 
 def load_golden(name):
+    """A golden case. Cases kept small store hashes and ballots only: their preference matrix is
+    re-tallied here by the oracle's scatter form and must match the reference's tally hash."""
     with np.load(GOLDEN / f"{name}.npz") as z:
-        return {k: z[k] for k in z.files}
+        case = {k: z[k] for k in z.files}
+    if "preferences" not in case:
+        import hashlib
+
+        from oracle import oracle
+
+        d = oracle.tally(ballots_of(case), "scatter")
+        assert hashlib.sha256(d.tobytes()).hexdigest() == str(case["tally_sha256"]), name
+        case["preferences"] = d
+    return case
+
+
+def has_repeats(case):
+    """True if some ballot of the case names a candidate twice."""
+    return any(len(np.unique(b)) != len(b) for b in ballots_of(case))
 
 
 def ballots_of(case):

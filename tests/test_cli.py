@@ -13,8 +13,9 @@ import pytest
 from scalingelections_b200 import cli
 
 ROOT = Path(__file__).resolve().parent.parent
-REF = Path("/root/reference/scaling_elections.py")
-needs_ref = pytest.mark.skipif(not REF.exists(), reason="reference script not present")
+REF = Path(os.environ.get("SE_REFERENCE_DIR", "")) / "scaling_elections.py"
+needs_ref = pytest.mark.skipif(not os.environ.get("SE_REFERENCE_DIR") or not REF.exists(),
+                               reason="reference script not present (set SE_REFERENCE_DIR)")
 
 
 def reference_namespace():

@@ -4,19 +4,24 @@ compiled OpenMP closure where it was built."""
 import numpy as np
 import pytest
 
-from conftest import ballots_of, golden_names, load_golden
+from conftest import ballots_of, golden_names, has_repeats, load_golden
 
 NAMES = golden_names()
 
 
 @pytest.mark.parametrize("name", NAMES)
 def test_oracle_closure_matches_reference(orc, name):
+    import hashlib
+
     case = load_golden(name)
     P = case["preferences"]
+    if P.shape[0] > 1024:  # the serial C^3 loop would take minutes on one core
+        S = orc.strongest_paths(P, "blocked", tile=16)
+        assert hashlib.sha256(S.tobytes()).hexdigest() == str(case["strongest_sha256"])
+        return
     S = orc.strongest_paths(P, "serial")
     if "strongest" in case:
         assert np.array_equal(S, case["strongest"])
-    import hashlib
     assert hashlib.sha256(S.tobytes()).hexdigest() == str(case["strongest_sha256"])
     Sb = orc.strongest_paths(P, "blocked", tile=16)
     assert np.array_equal(S, Sb)
@@ -27,7 +32,8 @@ def test_oracle_closure_matches_reference(orc, name):
 @pytest.mark.parametrize("name", NAMES)
 def test_oracle_ranking_matches_reference(orc, name):
     case = load_golden(name)
-    S = orc.strongest_paths(case["preferences"], "serial")
+    P = case["preferences"]
+    S = orc.strongest_paths(P, "serial" if P.shape[0] <= 1024 else "blocked")
     winner, ranking = orc.winner_and_ranking(S)
     assert winner == int(case["winner"])
     assert ranking == list(case["ranking"])
@@ -39,6 +45,10 @@ def test_oracle_tally_matches_reference(orc, name):
     ballots = ballots_of(case)
     d = orc.tally(ballots, "scatter")
     assert np.array_equal(d, case["preferences"])
+    if has_repeats(case):  # the positions form holds for permutations only, and says so
+        with pytest.raises(ValueError):
+            orc.tally(ballots, "positions")
+        return
     d2 = orc.tally(ballots, "positions")
     assert np.array_equal(d2, case["preferences"])
 
