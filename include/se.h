@@ -85,6 +85,24 @@ SE_API se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, ui
                        int64_t ld_out, int lane_bits, int tile, void* d_work,
                        int64_t work_bytes, void* stream);
 
+/* se_closure without its closing synchronisation (same reference interface, cu:863-989):
+ * every step is queued on `stream` and the call returns at once, so a caller can queue
+ * several closures, or overlap their host<->device copies on another stream. lane_bits is
+ * 16 or 32 (the automatic mode reads the matrix's range back and is not available here).
+ * value_offset shifts 16-bit lanes as in se_batch (a kept count v is held as v - value_offset,
+ * which must lie in [1, 65535]; 0 = no shift). Errors of the arguments return at once; errors
+ * found on the device (a count outside the 16-bit window, a timed-out wait) are kept in the
+ * first 8 bytes of d_work until se_closure_check reads them. d_work must not be reused by
+ * another call before that check. */
+SE_API se_status_t se_closure_enqueue(const uint32_t* d_pref, int64_t ld_pref, int C,
+                                      uint32_t* d_out, int64_t ld_out, int lane_bits,
+                                      uint32_t value_offset, void* d_work, int64_t work_bytes,
+                                      void* stream);
+
+/* Synchronises `stream` and reports what the closure enqueued with d_work found on the
+ * device: SE_OK, SE_ERR_OVERFLOW (a count outside the 16-bit window) or SE_ERR_DEVICE. */
+SE_API se_status_t se_closure_check(const void* d_work, void* stream);
+
 /* Same as se_closure, and also fills phase_ms[4] with the summed device time of the four
  * kernel kinds (pivot tile, pivot-row panel, pivot-column panel, remainder) from CUDA events
  * recorded between the launches, and *launches with the number of kernels launched.
@@ -121,11 +139,13 @@ SE_API int se_closure_launch_count(int C);
  * budget, and latency-critical code that cannot afford cudaMalloc/cudaFree (cudaFree
  * synchronises the device). The scratch space is a static 18 MiB device array inside this
  * library, held on every GPU that loads it until the process exits, so C is limited to
- * 1..SE_NOALLOC_MAX_CANDIDATES; larger C returns SE_ERR_INVALID with a message. Nothing is
+ * 1..SE_NOALLOC_MAX_CANDIDATES in any lane mode; larger C returns SE_ERR_INVALID with a
+ * message. It always runs round by round (se_closure_set_mode does not apply). Nothing is
  * allocated or freed. The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress): make that first call before any stream capture. All calls share
- * the array; calls that overlap on the GPU (e.g. on different streams) race and must be
- * serialised by the caller. Synchronises `stream` once at the end, like se_closure. */
+ * (cudaGetSymbolAddress), and looks it up again after cudaDeviceReset: make that first call
+ * before any stream capture. All calls share the array; calls that overlap on the GPU (e.g.
+ * on different streams) race and must be serialised by the caller. Synchronises `stream`
+ * once at the end, like se_closure. */
 SE_API se_status_t se_closure_noalloc(const uint32_t* d_pref, int64_t ld_pref, int C,
                                       uint32_t* d_out, int64_t ld_out, int lane_bits,
                                       void* stream);

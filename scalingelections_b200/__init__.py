@@ -6,6 +6,7 @@ module with the reference's native-module surface.
 """
 from .api import (  # noqa: F401
     Ballots,
+    ClosureStream,
     LANES_AUTO,
     LANES_U16,
     LANES_U32,

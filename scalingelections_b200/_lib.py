@@ -40,6 +40,8 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure_workspace_bytes": (_c_i64, [_c_int, _c_int, _c_int]),
     "se_closure": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp]),
     "se_closure_profiled": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _dp, _ip]),
+    "se_closure_enqueue": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, ctypes.c_uint32, _vp, _c_i64, _vp]),
+    "se_closure_check": (_c_int, [_vp, _vp]),
     "se_closure_launch_count": (_c_int, [_c_int]),
     "se_closure_workspace_bytes_flow": (_c_i64, [_c_int, _c_int, _c_int]),
     "se_closure_set_mode": (_c_int, [_c_int]),

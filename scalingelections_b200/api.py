@@ -220,6 +220,97 @@ def compute_strongest_paths(preferences, *, allow_tma: bool = False, allow_gpu: 
     return _to_host_u32(out, pinned=True)
 
 
+class ClosureStream:
+    """Closures of a sequence of host preference matrices of one size, pipelined over copies.
+
+    ``compute_strongest_paths`` copies a matrix in, closes it and copies the result out, one
+    step after another. Here, while election k closes on the compute stream, election k + 1's
+    matrix is copied in and election k - 1's result is copied out on two copy streams, so in
+    steady state a step costs the closure alone (or the copies, when they are slower). Each
+    closure runs through ``se_closure_enqueue`` and is checked with ``se_closure_check`` when
+    its result is handed out. Two device slots (input, output, workspace) alternate.
+
+    lanes: LANES_U16 (with ``value_offset``, a kept count v is held as v - value_offset, which
+    must lie in [1, 65535]) or LANES_U32. A count outside the 16-bit window raises
+    SchulzeError(SE_ERR_OVERFLOW) when that election's result is handed out."""
+
+    def __init__(self, num_candidates: int, *, lanes: int = LANES_U16, value_offset: int = 0, device=None):
+        _require_cuda()
+        if lanes not in (LANES_U16, LANES_U32):
+            raise ValueError("lanes must be LANES_U16 or LANES_U32")
+        self.C = int(num_candidates)
+        if self.C < 1:
+            raise ValueError("Number of candidates must be positive")
+        self.lanes, self.value_offset = int(lanes), int(value_offset)
+        self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
+        C = self.C
+        self.work_bytes = closure_workspace_bytes(C, self.lanes)
+        with torch.cuda.device(self.dev):
+            self.d_in = [torch.empty((C, C), dtype=torch.int32, device=self.dev) for _ in range(2)]
+            self.d_out = [torch.empty((C, C), dtype=torch.int32, device=self.dev) for _ in range(2)]
+            self.work = [_workspace(self.work_bytes, self.dev) for _ in range(2)]
+            self.compute = torch.cuda.Stream(self.dev)
+            self.h2d = torch.cuda.Stream(self.dev)
+            self.d2h = torch.cuda.Stream(self.dev)
+            self.checks = torch.cuda.Stream(self.dev)
+            self.copied_in = [torch.cuda.Event() for _ in range(2)]
+            self.closed = [torch.cuda.Event() for _ in range(2)]
+            self.copied_out = [torch.cuda.Event() for _ in range(2)]
+
+    def _host_in(self, m) -> torch.Tensor:
+        t = m if isinstance(m, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(_host_u32_matrix(m)))
+        if t.shape != (self.C, self.C):
+            raise ValueError(f"every matrix must be {self.C} x {self.C}")
+        if t.dtype == torch.uint32:
+            t = t.view(torch.int32)
+        elif t.dtype != torch.int32:
+            t = torch.from_numpy(np.ascontiguousarray(t.cpu().numpy().astype(np.uint32)).view(np.int32))
+        return t.contiguous()
+
+    def map(self, matrices):
+        """Yields the strongest-path matrix (uint32 [C, C], pinned host memory) of every input
+        matrix, in order. Inputs in pinned memory are copied asynchronously; others through
+        the driver's staging, which blocks this thread but not the GPU."""
+        L = _lib.lib()
+        pending = []  # (slot, host output) in flight
+        k = 0
+        with torch.cuda.device(self.dev):
+            for m in matrices:
+                b = k & 1
+                src = self._host_in(m)
+                with torch.cuda.stream(self.h2d):
+                    if k >= 2:
+                        self.h2d.wait_event(self.closed[b])  # election k - 2 no longer reads d_in[b]
+                    self.d_in[b].copy_(src, non_blocking=True)
+                    self.copied_in[b].record(self.h2d)
+                self.compute.wait_event(self.copied_in[b])
+                if k >= 2:
+                    self.compute.wait_event(self.copied_out[b])  # d_out[b] and work[b] are free again
+                check(L.se_closure_enqueue(self.d_in[b].data_ptr(), self.C, self.C, self.d_out[b].data_ptr(), self.C,
+                                           self.lanes, self.value_offset, self.work[b].data_ptr(), self.work_bytes,
+                                           self.compute.cuda_stream))
+                self.closed[b].record(self.compute)
+                host = torch.empty((self.C, self.C), dtype=torch.int32, pin_memory=True)
+                with torch.cuda.stream(self.d2h):
+                    self.d2h.wait_event(self.closed[b])
+                    host.copy_(self.d_out[b], non_blocking=True)
+                    self.copied_out[b].record(self.d2h)
+                pending.append((b, host))
+                k += 1
+                if len(pending) == 2:
+                    yield self._finish(*pending.pop(0))
+            while pending:
+                yield self._finish(*pending.pop(0))
+
+    def _finish(self, b: int, host: torch.Tensor) -> np.ndarray:
+        # The check runs on a stream of its own that waits for this slot's result copy only:
+        # on the output stream it would also wait for the next election's copy, and so for
+        # the closure running now.
+        self.checks.wait_event(self.copied_out[b])
+        check(_lib.lib().se_closure_check(self.work[b].data_ptr(), self.checks.cuda_stream))
+        return host.numpy().view(np.uint32)
+
+
 def log_gpus() -> None:
     """Prints every CUDA device as scaling_elections.cu:996-1016 does."""
     L = _lib.lib()

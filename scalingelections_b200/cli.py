@@ -53,18 +53,18 @@ def format_throughput(cells_per_sec: float) -> str:
 def parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser(description="Benchmark the Schulze method on B200")
     ap.add_argument("--num-voters", type=int, default=0,
-                    help="Number of voters in the population, 0 for random preference matrix")
-    ap.add_argument("--num-candidates", type=int, default=256, help="Number of candidates in the election")
-    ap.add_argument("--run-cpu", action="store_true", help="Run CPU implementations (none in this package)")
-    ap.add_argument("--run-gpu", action="store_true", help="Run GPU implementation")
-    ap.add_argument("--no-serial", action="store_true", help="Skip the lane-mode cross-check")
-    ap.add_argument("--cpu-tile-size", type=int, default=16, help="Accepted for compatibility")
+                    help="ballots to draw and tally; 0 draws a random preference matrix instead")
+    ap.add_argument("--num-candidates", type=int, default=256, help="candidates C (the matrix is C x C)")
+    ap.add_argument("--run-cpu", action="store_true", help="accepted; this package has no CPU closure")
+    ap.add_argument("--run-gpu", action="store_true", help="time the GPU closure")
+    ap.add_argument("--no-serial", action="store_true", help="skip the 16-bit against 32-bit lane cross-check")
+    ap.add_argument("--cpu-tile-size", type=int, default=16, help="accepted and ignored (no CPU closure here)")
     ap.add_argument("--gpu-tile-size", type=int, default=32,
-                    help="Validated like the reference (4, 8, 16 or 32); the kernels use 128-cell tiles")
-    ap.add_argument("--warmup", type=int, default=1, help="Number of warmup iterations (default: 1)")
-    ap.add_argument("--repeat", type=int, default=1, help="Number of benchmark iterations (default: 1)")
-    ap.add_argument("--seed", type=int, default=None, help="Seed of NumPy's global generator")
-    ap.add_argument("--lanes", choices=["auto", "16", "32"], default="auto", help="Closure lane mode")
+                    help="checked against 4, 8, 16 and 32 like the reference's; the kernels use 128-cell tiles")
+    ap.add_argument("--warmup", type=int, default=1, help="untimed runs before timing (default %(default)s)")
+    ap.add_argument("--repeat", type=int, default=1, help="timed runs, averaged (default %(default)s)")
+    ap.add_argument("--seed", type=int, default=None, help="seed NumPy's global generator, for a repeatable input")
+    ap.add_argument("--lanes", choices=["auto", "16", "32"], default="auto", help="closure lanes: auto picks 16 bits whenever the counts fit")
     ap.add_argument("--device-ballots", action="store_true",
                     help="Draw the random matrix, or uniform ballots tallied in place, on the GPU "
                          "(fast at large V x C; not NumPy's stream)")

@@ -725,15 +725,27 @@ extern "C" int64_t se_closure_workspace_bytes(int C, int lane_bits, int tile) {
     return plan(C, lane_bits == 16 ? 16 : 32).total;
 }
 
-namespace {
-se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
-                         int lane_bits, int tile, void* d_work, int64_t work_bytes, void* stream_, double* phase_ms) {
+namespace se {
+namespace closure {
+se_status_t check_flags(const void* flags_dev, cudaStream_t s);
+
+// The closure behind every entry point. mode: 0/1 round by round, 2 dataflow, -1 the
+// process-wide choice (se_closure_set_mode). sync: read the flags back and report overflow or
+// a device error (else the call is stream-ordered and se_closure_check reports them later).
+// value_offset: the 16-bit lane shift when lane_bits is 16 (0 = none); the automatic mode
+// (lane_bits 0) measures its own and needs sync.
+se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
+                        int lane_bits, uint32_t value_offset, int tile, void* d_work, int64_t work_bytes,
+                        void* stream_, double* phase_ms, int mode_override, bool sync) {
     clear_error();
     SE_REQUIRE(C >= 1, SE_ERR_INVALID, "Number of candidates must be positive");
     SE_REQUIRE(C <= (1 << 20), SE_ERR_INVALID, "Number of candidates too large (%d)", C);
     SE_REQUIRE(d_pref && d_out, SE_ERR_INVALID, "null matrix pointer");
     SE_REQUIRE(ld_pref >= C && ld_out >= C, SE_ERR_INVALID, "row stride smaller than the number of candidates");
     SE_REQUIRE(lane_bits == 0 || lane_bits == 16 || lane_bits == 32, SE_ERR_INVALID, "lane_bits must be 0, 16 or 32");
+    SE_REQUIRE(lane_bits != 0 || sync, SE_ERR_INVALID,
+               "automatic lanes read the matrix's range back to the host; pass 16 or 32 to enqueue");
+    SE_REQUIRE(value_offset == 0 || lane_bits == 16, SE_ERR_INVALID, "a value offset applies to 16-bit lanes only");
     SE_REQUIRE(tile == 0 || tile == kT, SE_ERR_UNSUPPORTED, "Unsupported tile size");
     const int64_t need = se_closure_workspace_bytes(C, lane_bits, tile);
     SE_REQUIRE(d_work != nullptr && work_bytes >= need, SE_ERR_WORKSPACE,
@@ -744,7 +756,7 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
     uint8_t* work = static_cast<uint8_t*>(d_work);
 
     int lb = lane_bits == 0 ? 16 : lane_bits;
-    uint32_t base = 0;
+    uint32_t base = value_offset;
     SE_CUDA_TRY(cudaMemsetAsync(work, 0, 256, s));
     if (lane_bits == 0) {
         // Automatic lanes: 16-bit (shifted by a base if need be) whenever the kept values fit
@@ -773,7 +785,7 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
     } else {
         if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
-    const int mode = g_closure_mode.load();
+    const int mode = mode_override >= 0 ? mode_override : g_closure_mode.load();
     const bool flow = mode == 2 && P.Cp > kT;
     SE_REQUIRE(mode != 2 || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
                "the dataflow closure needs a workspace of %lld bytes", (long long)P.flow_total);
@@ -783,9 +795,14 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
     st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, base, s)
                   : launch_finalize<32>(P, work, C, d_out, ld_out, 0, s);
     if (st) return st;
+    return sync ? check_flags(work + P.flags_off, s) : SE_OK;
+}
 
+// The flags word pair a closure leaves at the start of its workspace: [0] device error (a wait
+// that timed out), [1] a kept value outside the 16-bit window. Synchronises s.
+se_status_t check_flags(const void* flags_dev, cudaStream_t s) {
     uint32_t flags[2] = {0, 0};
-    SE_CUDA_TRY(cudaMemcpyAsync(flags, work + P.flags_off, 8, cudaMemcpyDeviceToHost, s));
+    SE_CUDA_TRY(cudaMemcpyAsync(flags, flags_dev, 8, cudaMemcpyDeviceToHost, s));
     SE_CUDA_TRY(cudaStreamSynchronize(s));
     SE_REQUIRE(flags[1] == 0, SE_ERR_OVERFLOW,
                "a preference count exceeds 65535, which 16-bit lanes cannot hold; use 32-bit lanes");
@@ -793,12 +810,31 @@ se_status_t closure_impl(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_
                flags[0]);
     return SE_OK;
 }
-}  // namespace
+}  // namespace closure
+}  // namespace se
 
 extern "C" se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out, int64_t ld_out,
                                   int lane_bits, int tile, void* d_work, int64_t work_bytes, void* stream) {
     return host_guard([&] {
-        return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, nullptr);
+        return closure_run(d_pref, ld_pref, C, d_out, ld_out, lane_bits, 0, tile, d_work, work_bytes, stream, nullptr,
+                           -1, true);
+    });
+}
+
+extern "C" se_status_t se_closure_enqueue(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t* d_out,
+                                          int64_t ld_out, int lane_bits, uint32_t value_offset, void* d_work,
+                                          int64_t work_bytes, void* stream) {
+    return host_guard([&] {
+        return closure_run(d_pref, ld_pref, C, d_out, ld_out, lane_bits, value_offset, 0, d_work, work_bytes, stream,
+                           nullptr, -1, false);
+    });
+}
+
+extern "C" se_status_t se_closure_check(const void* d_work, void* stream) {
+    return host_guard([&] {
+        clear_error();
+        SE_REQUIRE(d_work != nullptr, SE_ERR_INVALID, "null workspace");
+        return check_flags(d_work, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -806,7 +842,8 @@ extern "C" se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pr
                                            int64_t ld_out, int lane_bits, int tile, void* d_work, int64_t work_bytes,
                                            void* stream, double* phase_ms, int* launches) {
     se_status_t st = host_guard([&] {  // the phase events' vector is filled before any event exists
-        return closure_impl(d_pref, ld_pref, C, d_out, ld_out, lane_bits, tile, d_work, work_bytes, stream, phase_ms);
+        return closure_run(d_pref, ld_pref, C, d_out, ld_out, lane_bits, 0, tile, d_work, work_bytes, stream, phase_ms,
+                           -1, true);
     });
     if (launches) *launches = se_closure_launch_count(C);
     return st;

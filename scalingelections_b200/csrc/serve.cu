@@ -3,8 +3,9 @@
 //
 // A request is a ballot set already in device memory. It occupies a slot and is a sequence of
 // phases, each a set of independent tasks:
-//   POS     ceil(V/64) tasks: place of every candidate on every (completed) ballot, as f32,
-//           then packed into bit planes (bit k of 32 ballots' places in one word)
+//   POS     ceil(V/64) tasks: place of every candidate on every (completed) ballot, built per
+//           warp in a 16-bit row of shared memory when the rows fit and stored as exact
+//           integers, then packed into bit planes (bit k of 32 ballots' places in one word)
 //   TALLY   R(R+1) tasks: counts for one 128 x 64 half of an upper block pair (I <= J), by the
 //           bit-sliced comparison (see tally.cu), written as the u32 preference matrix and,
 //           shifted into 16 bits, as the closure's working matrix (d[j][i] = V - d[i][j]; no
@@ -17,7 +18,8 @@
 // claimable: all tasks of the previous phase are done. Nothing waits on a dependency, so a
 // request that arrives while others are mid-closure gets SMs as soon as the older ones have no
 // claimable work: requests join and leave the running kernel at phase granularity, and the
-// tally (FP32 pipe) of one request overlaps the closure (integer min/max pipe) of another.
+// bit-sliced tally of one request (lop3 and popc on the integer ALU) shares the SMs with the
+// closure of another (min/max).
 //
 // Slots are reused. Every claim counter carries the request's generation in its upper 32 bits
 // and is advanced only by compare-and-swap against the expected generation, so a CTA that

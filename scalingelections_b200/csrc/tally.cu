@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 // (ceil(C / 32) words of dynamic shared memory) for 2 and 3. A call without irregular
 // ballots returns at once.
 constexpr int kIrrThreads = 512;
+constexpr int kIrrMaxSmem = (1 << 20) / 8;  // the bitmap at the largest C (2^20 candidates)
 
 template <typename Id>
 __global__ void __launch_bounds__(kIrrThreads)
@@ -588,19 +589,19 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     const unsigned irr_grid = unsigned(2 * sms);
     if (id_bytes == 4) {
         auto fn = irregular_kernel<int32_t>;
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), kIrrMaxSmem, "the irregular-ballot kernel"))
             return st;
         fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const int32_t*>(d_ids), d_offsets, id_base, C, irr.n,
                                                   irr.list, d_out, ld_out);
     } else if (id_bytes == 2) {
         auto fn = irregular_kernel<uint16_t>;
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), kIrrMaxSmem, "the irregular-ballot kernel"))
             return st;
         fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const uint16_t*>(d_ids), d_offsets, id_base, C, irr.n,
                                                   irr.list, d_out, ld_out);
     } else {
         auto fn = irregular_kernel<uint8_t>;
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), int(irr_smem), "the irregular-ballot kernel"))
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(fn), kIrrMaxSmem, "the irregular-ballot kernel"))
             return st;
         fn<<<irr_grid, kIrrThreads, irr_smem, s>>>(static_cast<const uint8_t*>(d_ids), d_offsets, id_base, C, irr.n,
                                                   irr.list, d_out, ld_out);

@@ -1,6 +1,8 @@
 """Continuous-batching Schulze server on one GPU.
 
-Requests are ballot sets already in device memory (V ballots of C candidates, int32 [V, C]).
+Requests are ballot sets (V ballots of C candidates, int32 [V, C]) in device memory or in host
+memory; host ballots are copied into the server's HBM block when the request is admitted, on
+the submission stream, and that copy counts against the budget until the tally is done.
 The server admits a request when its working memory fits the HBM budget (an arena carved
 from one preallocated block) and hands it to the serving engine (include/se.h, se_engine_*):
 one persistent kernel that tallies, closes and ranks every admitted election, task by task,
@@ -109,6 +111,9 @@ class Ticket:
     nbytes: int = 0
     pos_offset: int = -1
     pos_nbytes: int = 0
+    ids_offset: int = -1       # host ballots: their copy in the server's block, until tallied
+    ids_nbytes: int = 0
+    cancelled: bool = False
     slot: int = -1
     gen: int = 0
     admitted: float = 0.0
@@ -162,30 +167,38 @@ class Server:
         self.base_ptr = self.block.data_ptr()
 
     # -- admission -------------------------------------------------------------------------
-    def try_submit(self, ticket: Ticket, ballots: torch.Tensor) -> bool:
+    def try_submit(self, ticket: Ticket, ballots: torch.Tensor | np.ndarray) -> bool:
         """Admit and publish one request if its memory fits and a slot is free; else False.
-        ballots: CUDA int32 [V, C], one ballot per row listing each of the C candidates once,
-        most preferred first."""
+        ballots: int32 [V, C], one ballot per row listing each of the C candidates once, most
+        preferred first; a CUDA tensor (used in place), or host memory (a tensor, pinned for an
+        asynchronous copy, or a NumPy array), copied into the server's block on admission."""
         if len(self.by_slot) >= self.max_slots:
             return False
         V, C = ticket.V, ticket.C
-        if ballots.shape != (V, C) or ballots.dtype != torch.int32 or not ballots.is_cuda:
-            raise ValueError("ballots must be a CUDA int32 [V, C] tensor")
+        if isinstance(ballots, np.ndarray):
+            ballots = torch.from_numpy(np.ascontiguousarray(ballots, dtype=np.int32))
+        if ballots.shape != (V, C) or ballots.dtype != torch.int32:
+            raise ValueError("ballots must be an int32 [V, C] tensor or array")
+        on_host = not ballots.is_cuda
         lanes, offset = lanes_for_voters(V)
         if lanes != 16:
             raise ValueError("the server handles up to 131070 ballots per request")
         if ticket.parts is None:
             ticket.parts = request_bytes(V, C)
         parts = ticket.parts
-        if parts["total"] > self.arena.free_bytes:
+        ids_bytes = (4 * V * C + ALIGN - 1) // ALIGN * ALIGN if on_host else 0
+        if parts["total"] + ids_bytes > self.arena.free_bytes:
             return False
-        off = self.arena.alloc(parts["main"])
-        if off is None:
-            return False
-        pos_off = self.arena.alloc(parts["positions"])
-        if pos_off is None:
-            self.arena.free(off, parts["main"])
-            return False
+        blocks = []
+        for n in (parts["main"], parts["positions"], ids_bytes):
+            o = self.arena.alloc(n) if n else -1
+            if o is None:
+                for o2, n2 in blocks:
+                    if o2 >= 0:
+                        self.arena.free(o2, n2)
+                return False
+            blocks.append((o, n))
+        (off, _), (pos_off, _), (ids_off, _) = blocks
         ticket.offset, ticket.nbytes = off, parts["main"]
         ticket.pos_offset, ticket.pos_nbytes = pos_off, parts["positions"]
         pos = off
@@ -194,18 +207,39 @@ class Server:
             ptrs[name] = self.base_ptr + pos
             ticket.views[name] = (pos, parts[name])
             pos += parts[name]
-        rq = _lib.Request(ballots.data_ptr(), None, V, C, offset, ptrs["prefs"], ptrs["out"], ptrs["wins"],
-                          ptrs["ranking"], ptrs["scratch"], parts["scratch"], self.base_ptr + pos_off,
-                          parts["positions"])
-        slot, gen = ctypes.c_int(), ctypes.c_uint32()
         with torch.cuda.device(self.device):
+            if on_host:
+                # A plain copy (no dtype or layout change) is a copy-engine transfer, which runs
+                # beside the resident engine; it precedes the request's descriptor on the stream.
+                ticket.ids_offset, ticket.ids_nbytes = ids_off, ids_bytes
+                dst = self.block[ids_off:ids_off + 4 * V * C].view(torch.int32).view(V, C)
+                with torch.cuda.stream(self.stream):
+                    dst.copy_(ballots.contiguous(), non_blocking=ballots.is_pinned())
+                ids_ptr = dst.data_ptr()
+            else:
+                ids_ptr = ballots.data_ptr()
+            rq = _lib.Request(ids_ptr, None, V, C, offset, ptrs["prefs"], ptrs["out"], ptrs["wins"],
+                              ptrs["ranking"], ptrs["scratch"], parts["scratch"], self.base_ptr + pos_off,
+                              parts["positions"])
+            slot, gen = ctypes.c_int(), ctypes.c_uint32()
             check(self.L.se_engine_submit(self.engine, ctypes.byref(rq), self.stream.cuda_stream, ctypes.byref(slot),
                                           ctypes.byref(gen)))
         ticket.slot, ticket.gen = slot.value, gen.value
         ticket.admitted = time.perf_counter()
         self.by_slot[ticket.slot] = ticket
-        ticket._ballots = ballots  # keep alive until done
+        ticket._ballots = ballots  # keep alive until done (a pinned source until its copy ends)
         return True
+
+    def cancel(self, ticket: Ticket) -> bool:
+        """Cancels a request. One still waiting for admission is dropped by the next admit()
+        and never reaches the GPU. One already admitted keeps its tasks on the engine, which
+        cannot stop a task midway; its memory returns to the arena when the engine finishes
+        it, and poll() then drops it instead of returning it. Returns True if the request was
+        waiting (nothing of it ran), False if it was in flight or already done."""
+        if ticket.status >= 0:
+            return False
+        ticket.cancelled = True
+        return ticket.slot < 0
 
     # -- completion ------------------------------------------------------------------------
     def admit(self, pending: list[Ticket], ballots_of, now: float, max_bypass_s: float = 0.25) -> int:
@@ -214,6 +248,8 @@ class Server:
         than max_bypass_s: then admission is strictly by arrival and nothing passes it (no
         starvation). Returns how many were admitted."""
         admitted = 0
+        if any(t.cancelled for t in pending):
+            pending[:] = [t for t in pending if not t.cancelled]
         strict = bool(pending) and now - pending[0].arrival > max_bypass_s
         order = list(range(len(pending)))
         if self.priority == "largest" and not strict:
@@ -243,9 +279,8 @@ class Server:
         check(self.L.se_engine_poll_tallied(self.engine, self._poll_slots, self.max_slots, ctypes.byref(n)))
         for x in range(n.value):
             t = self.by_slot.get(self._poll_slots[x])
-            if t is not None and t.pos_offset >= 0:
-                self.arena.free(t.pos_offset, t.pos_nbytes)
-                t.pos_offset = -1
+            if t is not None:
+                self._release_ballots(t)
         check(self.L.se_engine_poll(self.engine, self._poll_slots, self._poll_status, self.max_slots, ctypes.byref(n)))
         now = time.perf_counter()
         done = []
@@ -254,8 +289,18 @@ class Server:
             t.finished = now
             t.status = int(self._poll_status[x])
             self._collect(t)
-            done.append(t)
+            if not t.cancelled:
+                done.append(t)
         return done
+
+    def _release_ballots(self, t: Ticket) -> None:
+        """The ballot places and a host request's copied ballots, once its tally is done."""
+        if t.pos_offset >= 0:
+            self.arena.free(t.pos_offset, t.pos_nbytes)
+            t.pos_offset = -1
+        if t.ids_offset >= 0:
+            self.arena.free(t.ids_offset, t.ids_nbytes)
+            t.ids_offset = -1
 
     def _view(self, t: Ticket, name: str, shape, dtype) -> torch.Tensor:
         pos, _ = t.views[name]
@@ -263,15 +308,14 @@ class Server:
         return self.block[pos:pos + n].view(dtype).view(*shape)
 
     def _collect(self, t: Ticket) -> None:
-        with torch.cuda.device(self.device):
-            t.ranking = self._view(t, "ranking", (t.C,), torch.int32).cpu().numpy()
-            if t.keep_paths:
-                S = self._view(t, "out", (t.C, t.C), torch.int32)
-                t.strongest_paths = S.cpu().numpy().view(np.uint32)
+        if not t.cancelled:
+            with torch.cuda.device(self.device):
+                t.ranking = self._view(t, "ranking", (t.C,), torch.int32).cpu().numpy()
+                if t.keep_paths:
+                    S = self._view(t, "out", (t.C, t.C), torch.int32)
+                    t.strongest_paths = S.cpu().numpy().view(np.uint32)
         self.arena.free(t.offset, t.nbytes)
-        if t.pos_offset >= 0:
-            self.arena.free(t.pos_offset, t.pos_nbytes)
-            t.pos_offset = -1
+        self._release_ballots(t)
         t._ballots = None
 
     @property
@@ -330,8 +374,10 @@ def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], 
                  keep_paths: bool = False, stall_s: float = 60.0) -> tuple[list[Ticket], float]:
     """Drives the server with requests (V, C, ballots) arriving at the given offsets (seconds
     from start): admits each as soon as it has arrived and fits, polls completions, and
-    returns the finished tickets and the makespan. Raises if nothing completes for stall_s
-    seconds while requests are in flight."""
+    returns the finished tickets and the makespan. Ballots in host memory are copied to the
+    device inside each request's latency window (from arrival). Raises if nothing completes
+    for stall_s seconds while requests are in flight, or if a request can never fit the
+    budget."""
     order = np.argsort(arrival_times, kind="stable")
     pending: list[Ticket] = []
     done: list[Ticket] = []
@@ -348,8 +394,13 @@ def run_arrivals(server: Server, requests: list[tuple[int, int, torch.Tensor]], 
         now = now_abs - t0
         while nxt < n and arrival_times[order[nxt]] <= now:
             i = int(order[nxt])
-            V, C, _ = requests[i]
-            pending.append(Ticket(rid=i, V=V, C=C, arrival=t0 + arrival_times[i], keep_paths=keep_paths))
+            V, C, b = requests[i]
+            t = Ticket(rid=i, V=V, C=C, arrival=t0 + arrival_times[i], keep_paths=keep_paths)
+            t.parts = request_bytes(V, C)
+            ids = 0 if getattr(b, "is_cuda", False) else (4 * V * C + ALIGN - 1) // ALIGN * ALIGN
+            if t.parts["total"] + ids > server.arena.capacity:
+                raise ValueError(f"request {i} needs {t.parts['total'] + ids} bytes, more than the whole budget")
+            pending.append(t)
             nxt += 1
         if pending:
             ta = time.perf_counter()

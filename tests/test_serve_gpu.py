@@ -94,3 +94,47 @@ def test_malformed_ballots_reported_in_status():
     done, _ = run_arrivals(server, [(V, C, b)], [0.0])
     server.close()
     assert done[0].status & 8 and (done[0].status & 3) == 3
+
+
+def test_host_ballots_and_cancel_in_the_mix():
+    """Ballots submitted from host memory (pinned tensors and NumPy arrays, copied into the
+    server's block when admitted) beside device-resident ones, under a budget that makes them
+    queue; one waiting request and one in-flight request cancelled. Every result equals the
+    same election run alone, and the budget is whole again at the end."""
+    reqs = make_requests(3, 14)
+    mixed = []
+    for i, (V, C, b) in enumerate(reqs):
+        if i % 3 == 0:
+            h = torch.empty((V, C), dtype=torch.int32, pin_memory=True)
+            h.copy_(b)
+            mixed.append((V, C, h))
+        elif i % 3 == 1:
+            mixed.append((V, C, b.cpu().numpy()))
+        else:
+            mixed.append((V, C, b))
+    from scalingelections_b200.serve import Ticket
+
+    with Server(budget_bytes=256 << 20, max_slots=8, idle_ms=5) as server:
+        done, _ = run_arrivals(server, mixed, [0.0] * 7 + [0.003] * 7, keep_paths=True)
+        assert len(done) == len(reqs)
+        # Cancel: one request cancelled before admission never runs; one cancelled after it is
+        # admitted is not returned, and its memory comes back.
+        V, C, b = mixed[0]
+        waiting = Ticket(rid=0, V=V, C=C, arrival=0.0, keep_paths=True)
+        assert server.cancel(waiting)
+        pending = [waiting]
+        assert server.admit(pending, lambda t: b, now=0.0) == 0 and pending == []
+        flying = Ticket(rid=1, V=V, C=C, arrival=0.0)
+        assert server.try_submit(flying, b)
+        assert not server.cancel(flying)
+        import time
+        t0 = time.perf_counter()
+        while server.in_flight and time.perf_counter() - t0 < 30:
+            assert server.poll() == []
+        assert server.in_flight == 0 and server.arena.used == 0
+    for t in done:
+        V, C, b = reqs[t.rid]
+        assert t.status == 0, (t.rid, t.status)
+        S, ranking = alone(V, C, b)
+        assert np.array_equal(t.strongest_paths, S), t.rid
+        assert np.array_equal(t.ranking, ranking), t.rid

@@ -61,7 +61,8 @@ def _host_server(priority, max_slots=100, free_bytes=1 << 40, fits=lambda t: Tru
         if not fits(t):
             return False
         srv.order.append(t.rid)
-        srv.by_slot[len(srv.by_slot)] = t
+        t.slot = len(srv.by_slot)
+        srv.by_slot[t.slot] = t
         return True
 
     srv.try_submit = try_submit
@@ -94,3 +95,52 @@ def test_admission_priority_keeps_what_does_not_fit_and_no_starvation():
     pending = _tickets([2000, 10, 300])
     assert srv.admit(pending, lambda t: None, now=1.0, max_bypass_s=0.25) == 0
     assert [t.rid for t in pending] == [0, 1, 2]
+
+
+def test_cancel_drops_a_waiting_request_before_admission():
+    srv = _host_server("arrival")
+    ts = _tickets([64, 128, 256])
+    assert srv.cancel(ts[1]) is True  # still waiting: nothing of it will run
+    pending = list(ts)
+    srv.admit(pending, lambda t: None, now=0.0)
+    assert srv.order == [0, 2] and pending == []
+    assert srv.cancel(ts[0]) is False  # admitted: in flight
+
+
+def test_cancelled_request_in_flight_is_not_returned_but_its_memory_is():
+    """poll() frees a cancelled request's memory when the engine finishes it, and does not
+    hand it out. The engine is faked: it reports slot 0 tallied, then done."""
+    import ctypes
+
+    from scalingelections_b200 import serve
+
+    srv = object.__new__(serve.Server)
+    srv.arena = Arena(1 << 20)
+    srv.by_slot = {}
+    srv.max_slots = 4
+    srv._poll_slots = (ctypes.c_int * 4)()
+    srv._poll_status = (ctypes.c_uint32 * 4)()
+    srv.engine = None
+
+    class FakeLib:
+        def se_engine_poll_tallied(self, engine, slots, cap, n):
+            slots[0] = 0
+            ctypes.cast(n, ctypes.POINTER(ctypes.c_int))[0] = 1
+            return 0
+
+        def se_engine_poll(self, engine, slots, status, cap, n):
+            slots[0], status[0] = 0, 0
+            ctypes.cast(n, ctypes.POINTER(ctypes.c_int))[0] = 1
+            return 0
+
+    srv.L = FakeLib()
+    t = _tickets([64])[0]
+    t.offset, t.nbytes = srv.arena.alloc(4096), 4096
+    t.pos_offset, t.pos_nbytes = srv.arena.alloc(8192), 8192
+    t.ids_offset, t.ids_nbytes = srv.arena.alloc(1024), 1024
+    t.slot = 0
+    srv.by_slot[0] = t
+    assert srv.cancel(t) is False  # in flight
+    assert srv.poll() == []
+    assert srv.arena.used == 0 and srv.by_slot == {}
+    assert srv.cancel(t) is False  # already finished

@@ -92,8 +92,13 @@ def test_repeated_ids_count_like_the_reference(orc):
     for ballots in cases:
         d = api.build_pairwise_preferences(ballots)
         assert np.array_equal(d, orc.tally(ballots, "scatter")), ballots
+    # Eight 1s: 28 pairs on the diagonal. Its length is C = 8, so it is not completed and
+    # candidate 0 gets nothing from it; the permutation adds d[0][1] = 1.
     d = api.build_pairwise_preferences(cases[2])
-    assert d[1, 1] == 28 and d[1, 0] == 7 + 1  # 8 ones: 28 pairs among them; 7 then the completion
+    assert (d[1, 1], d[1, 0], d[0, 1]) == (28, 0, 1)
+    d = api.build_pairwise_preferences([np.array([1, 1, 1]), np.array([0, 1, 2, 3])])
+    # Length 3 != C = 4: completed to [1, 1, 1, 0, 2, 3]: 3 diagonal pairs, 1 above 0 three times.
+    assert (d[1, 1], d[1, 0], d[0, 1], d[2, 3]) == (3, 3, 1, 2)
 
 
 @pytest.mark.parametrize("C,V,width", [(40, 3000, 1), (300, 777, 2), (3000, 100, 4)])

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 import torch
 
-from scalingelections_b200 import LANES_U16, LANES_U32, _lib, api
+from scalingelections_b200 import LANES_AUTO, LANES_U16, LANES_U32, _lib, api
 
 pytestmark = pytest.mark.gpu
 
@@ -51,6 +51,33 @@ def test_noalloc_matches_workspace_closure_on_consecutive_calls():
     assert same(r2, api.strongest_paths_device(d2, lanes=LANES_U16))
     # And once more at the first input, so both lane layouts have overwritten each other.
     assert same(noalloc(d1, LANES_U32), r1)
+    # Automatic lanes over the stale contents (the range probe also lives in the array): a
+    # shifted 16-bit window, then plain 16-bit values, then a range only 32 bits can hold.
+    d3 = api._to_device_u32(np.random.default_rng(4).integers(70000, 130000, size=(MAX_C, MAX_C))
+                            .astype(np.uint32), "cuda")
+    for d in (d3, d2, d1):
+        want = api._to_device_u32(orc_closure(d), "cuda")
+        assert same(noalloc(d, LANES_AUTO), want)
+        assert same(noalloc(d, LANES_AUTO), want)
+
+
+def orc_closure(d: torch.Tensor) -> np.ndarray:
+    from oracle import oracle
+
+    return oracle.strongest_paths(api._to_host_u32(d), "blocked", tile=16)
+
+
+def test_noalloc_runs_round_by_round_whatever_the_closure_mode():
+    """The dataflow form needs more scratch than the static array holds at C = 2048 in 32-bit
+    lanes; se_closure_noalloc runs round by round whatever se_closure_set_mode chose."""
+    d = random_prefs(MAX_C, 2**32 - 1, seed=5)
+    want = api.strongest_paths_device(d, lanes=LANES_U32)
+    api.set_closure_mode(2)
+    try:
+        assert same(noalloc(d, LANES_U32), want)
+        assert same(noalloc(d, LANES_AUTO), want)
+    finally:
+        api.set_closure_mode(1)
 
 
 def test_noalloc_rejects_sizes_beyond_its_static_array():
