@@ -56,9 +56,12 @@ def parse():
     ap.add_argument("--closure-mode", type=int, default=1, choices=[1, 2],
                     help="1: round by round (default), 2: dataflow")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
+    ap.add_argument("--cpu-full-size", action="store_true",
+                    help="reference arm: also time one closure at the workload's full size (minutes)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest", "sharded"], default="closure",
+    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest", "sharded", "launch-check"],
+                    default="closure",
                     help="closure: the headline single election; batch: many mixed elections; "
                          "serve: Poisson arrivals on the continuous-batching server")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests per offered load")
@@ -66,6 +69,18 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=40.0, help="serve: HBM admission budget")
     ap.add_argument("--serve-priority", choices=["arrival", "largest"], default="arrival",
                     help="serve: admission order of requests waiting together")
+    ap.add_argument("--serve-ballots", choices=["host", "device"], default="host",
+                    help="serve: ballots wait in pinned host memory (copied on admission) or on the device")
+    ap.add_argument("--tight-budget-gb", type=float, default=4.0,
+                    help="serve: budget of the extra load point where admission binds (0: skip it)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="closure: only the headline (skip the other configurations' objects)")
+    ap.add_argument("--no-batch", action="store_true", help="closure: skip the batch object")
+    ap.add_argument("--no-serve", action="store_true", help="closure: skip the serve object")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="closure: skip timing the reference's own CUDA path on the headline matrix")
+    ap.add_argument("--sharded-candidates", type=int, default=32768,
+                    help="closure under torchrun: C of the one election closed by all ranks together")
     ap.add_argument("--elections", type=int, default=4096, help="batch: number of elections")
     ap.add_argument("--max-candidates", type=int, default=2048, help="batch: largest C")
     ap.add_argument("--no-autotune", action="store_true", help="batch: skip the autotuner (use defaults)")
@@ -141,12 +156,12 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # CPU baselines (the reference's own OpenMP closure, else the oracle's port)
 # ------------------------------------------------------------------------------------------
-def cpu_sample_matrix(args):
+def cpu_sample_matrix(args, C=None):
     """Preference matrix of the bounded CPU sample: a Mallows election with C = args.cpu_sample
-    candidates and 512 voters, drawn and tallied on the host (not timed)."""
+    candidates and the headline's V and phi, drawn and tallied on the host (not timed)."""
     from oracle import oracle
 
-    b = oracle.mallows_ballots(512, args.cpu_sample, args.phi, seed=args.seed + 7)
+    b = oracle.mallows_ballots(args.voters, C or args.cpu_sample, args.phi, seed=args.seed + 7)
     return oracle.tally(b, "positions")
 
 
@@ -172,7 +187,7 @@ def cpu_closure_sample(args, d):
         oracle.strongest_paths(d, "blocked", tile=16, threads=cores)
         t = time.perf_counter() - t0
         what = "oracle blocked closure (tile 16, OpenMP)"
-    sample = (f"{what}, one C={Cs} Mallows(phi={args.phi}) election ({Cs}^3 cells, {t:.2f} s) "
+    sample = (f"{what}, one C={Cs}, V={args.voters} Mallows(phi={args.phi}) election ({Cs}^3 cells, {t:.2f} s) "
               f"standing in for the C={args.candidates} workload; {cores} host threads")
     return Cs ** 3 / t, kind, cores, sample, t
 
@@ -188,6 +203,13 @@ def run_reference_arm(args, world, rank):
         if i >= args.warmup:
             values.append(cps)
     v = statistics.median(values) / 1e9
+    full = None
+    if args.cpu_full_size:
+        # One closure at the workload's own size, to check the per-cell rate of the sample.
+        d_full = cpu_sample_matrix(args, C=args.candidates)
+        cps_full, kind_f, cores_f, sample_f, t_full = cpu_closure_sample(args, d_full)
+        full = {"value": cps_full / 1e9, "unit": UNIT, "seconds": t_full, "candidates": args.candidates,
+                "sample": sample_f, "ratio_to_sample": cps_full / 1e9 / v}
     line = {
         "metric": metric_name(args.candidates), "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": args.cpu_sample ** 3 / (v * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -197,6 +219,8 @@ def run_reference_arm(args, world, rank):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
+    if full is not None:
+        line["full_size_point"] = full
     print(json.dumps(line), flush=True)
 
 
@@ -385,6 +409,14 @@ def run_ours(args, world, rank, local_rank):
         cps, kind, cores, sample, _ = cpu_closure_sample(args, cpu_sample_matrix(args))
         cpu = {"value": cps / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = run_extras(args, local_rank, d, out, host_in if e2e is not None else None, peak_mhz)
+    elif world > 1 and not args.no_extras:
+        del work
+        torch.cuda.empty_cache()
+        extras["sharded"] = measure_sharded(args, world, rank, local_rank, C=args.sharded_candidates)
+
     if rank == 0:
         traffic = load_traffic(lanes if lanes else 16, C)
         line = {
@@ -414,7 +446,191 @@ def run_ours(args, world, rank, local_rank):
             "clocks": clocks.summary(),
             "gpu_launches": int(L.se_closure_launch_count(C)) * args.steps,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# The other configurations, as objects of the headline line (one GPU)
+# ------------------------------------------------------------------------------------------
+def closure_object(d, lanes: int, steps: int, warmup: int, local_rank: int, workload: str) -> dict:
+    """Device-timed closure of the resident matrix d in the given lanes, with the remainder
+    kernel's roofline against the min/max peak measured now (u16x2 or u32 recipe)."""
+    import torch
+
+    from scalingelections_b200 import _lib, api
+
+    L = _lib.lib()
+    C = int(d.shape[0])
+    dev = d.device
+    peak = [ctypes.c_double() for _ in range(4)]
+    recipe = 3 if lanes == 16 else 1
+    _lib.check(L.se_minmax_peak(recipe, 65536, *[ctypes.byref(x) for x in peak]))
+    peak_relax_per_s = peak[3].value
+    need = api.closure_workspace_bytes(C, lanes)
+    work = torch.empty(need, dtype=torch.uint8, device=dev)
+    out = torch.empty((C, C), dtype=torch.uint32, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        api.strongest_paths_device(d, lanes=lanes, out=out, workspace=work)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            api.strongest_paths_device(d, lanes=lanes, out=out, workspace=work)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    phase = (ctypes.c_double * 4)()
+    launches = ctypes.c_int(0)
+    _lib.check(L.se_closure_profiled(d.data_ptr(), C, C, out.data_ptr(), C, lanes, 0, work.data_ptr(), need,
+                                     stream.cuda_stream, phase, ctypes.byref(launches)))
+    R = (C + 127) // 128
+    obj = {"workload": workload, "candidates": C, "lanes": f"u{lanes}", "tile": 128, "steps": steps,
+           "warmup": warmup, "ms": ms, "value": float(C) ** 3 / (ms * 1e-3) / 1e9, "unit": UNIT,
+           "phase_ms": {"pivot_round0": phase[0], "panels": phase[1], "remainder_with_fused_pivot": phase[3]},
+           "gpu_launches": int(launches.value) * steps, "clocks": clocks.summary()}
+    if R > 1:
+        achieved = float(R - 1) ** 2 * 128 ** 3 / (phase[3] / R * 1e-3)
+        obj["roofline"] = {"bound": "int_minmax", "kernel": f"closure remainder rem_kernel<u{lanes}>",
+                           "achieved": achieved / 1e12, "peak": peak_relax_per_s / 1e12, "unit": "Trelax/s",
+                           "frac": achieved / peak_relax_per_s,
+                           "peak_source": f"measured: se_minmax_peak recipe {recipe} in this run"}
+        obj["whole_closure_frac_of_peak"] = float(C) ** 3 / (ms * 1e-3) / peak_relax_per_s
+    return obj, out
+
+
+def election_matrix(V: int, C: int, phi: float, seed: int, dev):
+    """Ballots drawn (Mallows; phi = 1 is uniform permutations) and tallied on the device."""
+    import torch
+
+    from scalingelections_b200 import api
+    from scalingelections_b200.ballots import mallows_ballots_device
+
+    b = mallows_ballots_device(V, C, phi, seed=seed, device=dev)
+    offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
+    d = api.tally_device(b.view(-1), offs, C)
+    return d, b, offs
+
+
+def reference_gpu_leg(d_host, ours_host, local_rank: int) -> dict:
+    """Baseline leg: the reference's own CUDA path (scaling_elections.cu compiled unmodified for
+    sm_100a into oracle/_ref/gpu) on the same matrix, through its own host API, timed by wall
+    clock around the call as the reference times it (scaling_elections.py:338-357): host init,
+    managed-memory migration, kernels and the copy back."""
+    from oracle import oracle
+
+    mod = oracle.reference_gpu()
+    C = int(d_host.shape[0])
+    if mod is None:
+        return {"unavailable": "oracle/_ref/gpu not built (the reference's sources were absent at build time)"}
+    small = d_host[:256, :256].copy()
+    mod.compute_strongest_paths(small, allow_gpu=True, allow_tma=False, tile_size=32)  # CUDA init, kernels loaded
+    with ClockSampler(local_rank) as clocks:
+        t0 = time.perf_counter()
+        res = mod.compute_strongest_paths(d_host, allow_gpu=True, allow_tma=False, tile_size=32)
+        t = time.perf_counter() - t0
+    import numpy as np
+
+    return {"impl": "scaling_elections.cu compute_strongest_paths(allow_gpu=True, allow_tma=False, tile_size=32), "
+                    "the reference's CUDA path compiled unmodified for sm_100a",
+            "candidates": C, "seconds": t, "value": float(C) ** 3 / t / 1e9, "unit": UNIT, "timing": "wall clock, "
+            "one call (the reference's own convention: host init, managed memory, kernels, copy back)",
+            "bit_identical_to_ours": bool(np.array_equal(res, ours_host)), "clocks": clocks.summary()}
+
+
+def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
+    """The objects of the other configurations and comparisons, added to the headline line:
+    e2e_pipelined (the headline through api.ClosureStream), u32 (the headline in 32-bit lanes),
+    c4096 (single election, C = V = 4096 uniform ballots), c32768 (C = 32768, V = 4096
+    Mallows(0.8)), batch (4096 mixed elections), serve (Poisson arrivals), reference_gpu (the
+    reference's own CUDA path on the headline matrix)."""
+    import numpy as np
+    import torch
+
+    from scalingelections_b200 import LANES_U16, api
+
+    dev = d.device
+    C = int(d.shape[0])
+    steps = max(1, args.steps)
+    ex = {}
+    if host_in is not None:
+        cs = api.ClosureStream(C, lanes=LANES_U16)
+        for _ in cs.map([host_in]):
+            pass
+        with ClockSampler(local_rank) as clocks:
+            t0 = time.perf_counter()
+            n = 0
+            for res in cs.map([host_in] * steps):
+                n += 1
+                del res
+            t = time.perf_counter() - t0
+        ex["e2e_pipelined"] = {
+            "value": float(C) ** 3 * n / t / 1e9, "unit": UNIT, "steps": n, "ms_per_step": t / n * 1e3,
+            "h2d_bytes_per_step": C * C * 4, "d2h_bytes_per_step": C * C * 4,
+            "api": "scalingelections_b200.ClosureStream.map over pinned host matrices (se_closure_enqueue: each "
+                   "step's copy in and copy out overlap the neighbouring steps' closures)",
+            "clocks": clocks.summary()}
+        del cs
+    ours_host = None
+    if not args.no_reference_gpu:
+        ours_host = api._to_host_u32(out)  # u16-lane closure of the headline matrix, widened
+    obj, out32 = closure_object(d, 32, max(2, min(steps, 3)), 1, local_rank,
+                                f"the headline election (C={C}) in 32-bit lanes")
+    obj["bit_identical_to_u16"] = bool(torch.equal(out32.view(torch.int32), out.view(torch.int32)))
+    ex["u32"] = obj
+    del out32
+    if ours_host is not None:
+        d_host = api._to_host_u32(d)
+        ex["reference_gpu"] = reference_gpu_leg(d_host, ours_host, local_rank)
+        del d_host, ours_host
+    torch.cuda.empty_cache()
+
+    # cfg2: C = V = 4096, uniform permutations (Mallows with phi = 1).
+    d4, b4, o4 = election_matrix(4096, 4096, 1.0, args.seed + 4096, dev)
+    del b4, o4
+    obj16, o16 = closure_object(d4, 16, max(steps, 20), 3, local_rank,
+                                "single election, C=4096, V=4096 uniform permutation ballots")
+    obj32, o32 = closure_object(d4, 32, max(steps, 10), 2, local_rank, "the same election in 32-bit lanes")
+    obj16["u32"] = obj32
+    obj16["u32"]["bit_identical_to_u16"] = bool(torch.equal(o16.view(torch.int32), o32.view(torch.int32)))
+    obj16["tile_note"] = "one tile shape, 128 x 128 cells (8 x 8 words per thread)"
+    ex["c4096"] = obj16
+    del d4, o16, o32
+
+    # cfg3's larger size: C = 32768, V = 4096 Mallows(0.8).
+    d32, b32, o32 = election_matrix(4096, 32768, 0.8, args.seed + 32768, dev)
+    tw = torch.empty(api.tally_workspace_bytes(4096, 32768), dtype=torch.uint8, device=dev)
+    api.tally_device(b32.view(-1), o32, 32768, out=torch.empty_like(d32), workspace=tw)
+    te0, te1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    te0.record()
+    api.tally_device(b32.view(-1), o32, 32768, out=torch.empty_like(d32), workspace=tw)
+    te1.record()
+    torch.cuda.synchronize()
+    del b32, o32, tw
+    obj, S32 = closure_object(d32, 16, 2, 1, local_rank, "single election, C=32768, V=4096 Mallows(phi=0.8) ballots")
+    obj["tally_ms"] = te0.elapsed_time(te1)
+    wins, ranking = api.rank_device(S32)
+    obj["winner"] = int(ranking[0].item())
+    ex["c32768"] = obj
+    del d32, S32, wins, ranking
+    torch.cuda.empty_cache()
+
+    if not args.no_batch:
+        line = measure_batch(args, 1, 0, local_rank)
+        ex["batch"] = {k: line[k] for k in ("metric", "value", "unit", "ms_per_step", "loop_elections_per_s",
+                                             "speedup_vs_loop", "bit_identical_to_loop", "batched_gcells_per_s",
+                                             "config", "autotune", "clocks") if k in line}
+        ex["batch"]["steps"] = line["steps"]
+        torch.cuda.empty_cache()
+    if not args.no_serve:
+        line = measure_serve(args, 1, 0, local_rank)
+        ex["serve"] = {k: line[k] for k in ("metric", "value", "unit", "config", "data", "saturation", "loads",
+                                             "tight_budget", "clocks") if k in line}
+        ex["serve"]["saturation"].pop("engine_profile", None)
+        torch.cuda.empty_cache()
+    return ex
 
 
 # ------------------------------------------------------------------------------------------
@@ -451,6 +667,15 @@ def make_batch_inputs(specs, dev):
 
 
 def run_batch(args, world, rank, local_rank):
+    line = measure_batch(args, world, rank, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batch(args, world, rank, local_rank):
+    """cfg4: a batch of elections of uneven size closed and ranked by one persistent launch
+    (CUDA graph), against a loop of the single-election path over the same batch. Returns the
+    JSON object (rank 0's view)."""
     import torch
     import torch.distributed as dist
 
@@ -532,6 +757,7 @@ def run_batch(args, world, rank, local_rank):
 
     n_total = len(all_specs)
     value = n_total / (ms_max * 1e-3)
+    line = None
     if rank == 0:
         tasks = b.task_counts()
         line = {
@@ -558,7 +784,9 @@ def run_batch(args, world, rank, local_rank):
                 "buckets": {k: {"C": v["range"], "lanes": v["lanes"]} for k, v in tuned["buckets"].items()}},
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
+    del b, prefs, outs, ranks, ws
+    torch.cuda.empty_cache()
+    return line
 
 
 # ------------------------------------------------------------------------------------------
@@ -576,6 +804,17 @@ def serve_specs(n: int, seed: int):
 
 
 def run_serve(args, world, rank, local_rank):
+    line = measure_serve(args, world, rank, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_serve(args, world, rank, local_rank):
+    """cfg5: saturation throughput, then p50/p99 latency under Poisson arrivals at the offered
+    loads, then one load under a budget small enough that admission binds. Ballots wait in
+    pinned host memory and are copied to the GPU when their request is admitted, inside its
+    latency window (--serve-ballots device keeps them resident instead). Returns the JSON
+    object (rank 0's view)."""
     import numpy as np
     import torch
 
@@ -585,10 +824,19 @@ def run_serve(args, world, rank, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     specs = serve_specs(args.requests, args.seed + 104729 * rank)
+    host = args.serve_ballots == "host"
     t0 = time.perf_counter()
-    reqs = [(V, C, mallows_ballots_device(V, C, phi, seed=sd, device=dev)) for (V, C, phi, sd) in specs]
+    reqs = []
+    for (V, C, phi, sd) in specs:
+        b = mallows_ballots_device(V, C, phi, seed=sd, device=dev)
+        if host:
+            h = torch.empty((V, C), dtype=torch.int32, pin_memory=True)
+            h.copy_(b)
+            b = h
+        reqs.append((V, C, b))
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
+    ballot_bytes = sum(4 * V * C for (V, C, _, _) in specs)
     server = Server(budget_bytes=int(args.budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2, idle_ms=5,
                     priority=args.serve_priority)
     # Warm-up, then capacity: every request arrives at once (closed loop, admission-bound).
@@ -621,6 +869,30 @@ def run_serve(args, world, rank, local_rank):
                           "engine_launches": server.stats()["engine_launches"] - l0})
     grid = server.stats()["grid"]
     server.close()
+    del server
+    torch.cuda.empty_cache()
+    # Admission binding: the middle load again under a budget that holds the largest request
+    # but only a few at a time, so requests wait on the host for memory.
+    tight = None
+    if args.tight_budget_gb > 0:
+        frac = [float(x) for x in args.loads.split(",")][len(loads) // 2]
+        rate = frac * capacity
+        gaps = rng.exponential(1.0 / rate, size=len(reqs))
+        arrivals = list(np.cumsum(gaps) - gaps[0])
+        with ClockSampler(local_rank) as tclocks:
+            with Server(budget_bytes=int(args.tight_budget_gb * (1 << 30)), max_slots=1024, ctas_per_sm=2,
+                        idle_ms=5, priority=args.serve_priority) as ts:
+                done, span = run_arrivals(ts, reqs, arrivals)
+                launches = ts.stats()["engine_launches"]
+        r = summarize(done, rate, span)
+        waited = [t.admitted - t.arrival for t in done]
+        tight = {"budget_gb": args.tight_budget_gb, "offered_fraction": frac, "offered_per_s": rate,
+                 "achieved_per_s": r.achieved_rate, "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms,
+                 "n": r.n, "engine_launches": launches,
+                 "admission_wait_ms": {"p50": float(np.percentile(waited, 50)) * 1e3,
+                                       "p99": float(np.percentile(waited, 99)) * 1e3},
+                 "clocks": tclocks.summary()}
+    line = None
     if rank == 0:
         V = np.array([s[0] for s in specs], float)
         C = np.array([s[1] for s in specs], float)
@@ -629,19 +901,25 @@ def run_serve(args, world, rank, local_rank):
             "value": capacity * world, "unit": "elections/s", "n_gpus": world, "steps": len(loads),
             "warmup": 1, "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u16 (shifted lanes above 65535 ballots)",
-            "data": "synthetic (seeded Mallows ballots resident on the GPU before arrival)",
+            "data": ("synthetic (seeded Mallows ballots in pinned host memory, copied to the GPU on admission, "
+                     "inside the latency window)" if host else
+                     "synthetic (seeded Mallows ballots resident on the GPU before arrival)"),
             "config": {"workload": f"{args.requests} requests, C log-uniform [8, 8192], V log-uniform [100, 100000], "
                                    f"Mallows phi ~ U[0.2, 1]; HBM budget {args.budget_gb:g} GB",
+                       "ballots": "host (pinned)" if host else "device", "ballot_bytes_total": ballot_bytes,
                        "tally_pairs_total": float((V * C * C / 2).sum()), "closure_cells_total": float((C ** 3).sum()),
                        "admission_priority": args.serve_priority},
             "saturation": {"p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms, "makespan_s": makespan,
                            "engine_launches": sat_launches, "grid": grid,
                            "engine_profile": sat_profile},
             "loads": loads,
+            "tight_budget": tight,
             "input_prep_seconds": prep_s,
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
+    del reqs
+    torch.cuda.empty_cache()
+    return line
 
 
 TALLY_PEAK_SOURCE = ("SMs x 64 integer ALU lanes x SM clock x 32 / (B + 2): per 32 voter pairs, B lop3 "
@@ -655,10 +933,16 @@ def tally_alu_peak(sms: int, mhz: float, C: int) -> float:
 
 
 def run_sharded(args, world, rank, local_rank):
+    line = measure_sharded(args, world, rank, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_sharded(args, world, rank, local_rank, C=None):
     """One election closed by all ranks together (scalingelections_b200.sharded): row blocks
     split across the ranks, one pivot-row panel broadcast (NCCL) per round. Every rank draws
     and tallies the same ballots, so all hold the same preference matrix. Strong scaling: the
-    work is one C^3 closure whatever the number of GPUs."""
+    work is one C^3 closure whatever the number of GPUs. Returns rank 0's JSON object."""
     import torch
     import torch.distributed as dist
 
@@ -668,8 +952,9 @@ def run_sharded(args, world, rank, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    C, V = args.candidates, args.voters
-    if world == 1:
+    C, V = (C or args.candidates), args.voters
+    own_group = world == 1 and not dist.is_initialized()
+    if own_group:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         if "MASTER_PORT" not in os.environ:
             import socket
@@ -706,6 +991,7 @@ def run_sharded(args, world, rank, local_rank):
     ok = torch.tensor([1 if identical else 0], device=dev)
     dist.all_reduce(ok, op=dist.ReduceOp.MIN)
     R = (C + 127) // 128
+    line = None
     if rank == 0:
         line = {
             "metric": f"Gcells/s (C^3/t), one election's closure sharded over the GPUs, C={C}",
@@ -719,9 +1005,11 @@ def run_sharded(args, world, rank, local_rank):
             "gpu_launches": (R * 2 + R * 2 * world) * args.steps,
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
-    if world == 1:
+    del d, rows, single
+    torch.cuda.empty_cache()
+    if own_group:
         dist.destroy_process_group()
+    return line
 
 
 def run_ingest(args, world, rank, local_rank):
@@ -848,11 +1136,44 @@ def run_ingest(args, world, rank, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def launch_ranks(n: int) -> int:
+    """Runs this script once per GPU under torch.distributed.run (one node, rendezvous on
+    127.0.0.1) with the same arguments, and returns its exit status. Used when --gpus N > 1 is
+    given outside a torchrun launch."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--standalone", "--local-addr", "127.0.0.1", "--nnodes", "1",
+           "--nproc-per-node", str(n), str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def launch_check(world, rank):
+    """Each rank joins the process group (NCCL with GPUs, else gloo), agrees on the world size
+    with an all-reduce and prints one line; for testing the launcher without GPUs."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
+    t = torch.ones(1, device="cuda" if backend == "nccl" else "cpu")
+    dist.all_reduce(t)
+    print(json.dumps({"rank": rank, "world_size": world, "ranks_seen": int(t.item()), "backend": backend}),
+          flush=True)
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args.gpus))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "launch-check":
+        launch_check(world, rank)
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
         return

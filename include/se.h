@@ -202,6 +202,11 @@ SE_API se_status_t se_batch_graph_build(se_batch_plan_t* plan);
 SE_API se_status_t se_batch_graph_launch(const se_batch_plan_t* plan, void* stream);
 SE_API se_status_t se_batch_release(se_batch_plan_t* plan);
 SE_API se_status_t se_batch_check(const se_batch_plan_t* plan, void* stream);
+/* Limit of one dependency wait of the batch's persistent kernel (default 5 s): a task whose
+ * prerequisite is not complete within it sets the batch's error word, every CTA drains the
+ * queue and exits, and se_batch_check returns SE_ERR_DEVICE; the GPU stays usable. Applies
+ * to runs enqueued after the call; a graph built before it is released (build it again). */
+SE_API se_status_t se_batch_set_wait_limit(se_batch_plan_t* plan, uint64_t limit_ns);
 /* Profile of the last run (synchronises `stream`): per task kind (small election, pivot,
  * row panel, column panel, remainder) CTA-milliseconds busy and tasks run, and the
  * CTA-milliseconds spent waiting for dependencies. Any pointer may be NULL. */

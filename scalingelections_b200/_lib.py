@@ -54,6 +54,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_batch_graph_launch": (_c_int, [_vp, _vp]),
     "se_batch_release": (_c_int, [_vp]),
     "se_batch_check": (_c_int, [_vp, _vp]),
+    "se_batch_set_wait_limit": (_c_int, [_vp, ctypes.c_uint64]),
     "se_batch_task_count": (_c_i64, [_vp, _c_int]),
     "se_batch_profile": (_c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int64), _dp, _vp]),
     "se_engine_workspace_bytes": (_c_i64, [_c_int]),

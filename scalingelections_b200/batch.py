@@ -124,6 +124,13 @@ class BatchedElections:
         return {"busy_cta_ms": dict(zip(self.KINDS, busy)), "tasks": dict(zip(self.KINDS, tasks)),
                 "wait_cta_ms": wait.value}
 
+    def set_wait_limit(self, seconds: float) -> None:
+        """Limit of one dependency wait of the persistent kernel (default 5 s). A wait that
+        runs out ends the run with an error that check() raises; the GPU stays usable. Applies
+        to later runs; a built graph is released and rebuilt on the next launch_graph()."""
+        check(_lib.lib().se_batch_set_wait_limit(ctypes.byref(self.plan), int(max(0.0, seconds) * 1e9)))
+        self._graph = False
+
     def check(self) -> None:
         """Raise if a kernel of the last run reported an error (synchronises the stream)."""
         with torch.cuda.device(self.device):

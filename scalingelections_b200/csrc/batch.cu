@@ -95,7 +95,7 @@ __device__ __forceinline__ void claim_task(const Elec* elecs, const uint64_t* ta
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     persistent_kernel(const Elec* __restrict__ elecs, const uint64_t* __restrict__ tasks, uint32_t ntasks,
-                      Header* __restrict__ hdr, int queue) {
+                      Header* __restrict__ hdr, int queue, uint64_t dep_wait_ns) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
                     uint32_t target;
                     if (task_dependency(elecs[e], type, k, ctr, target)) {
                         const uint64_t w0 = global_ns();
-                        const bool ok = wait_counter(ctr, target, &hdr->abort);
+                        const bool ok = wait_counter(ctr, target, &hdr->abort, dep_wait_ns);
                         atomicAdd(&hdr->wait_ns, (unsigned long long)(global_ns() - w0));
                         if (!ok) {
                             raise_device_error(&hdr->err, kErrDepTimeout);
@@ -406,6 +406,7 @@ struct Plan {
     int64_t init_blocks, fin_blocks, place_blocks;
     int32_t grid[2];
     cudaGraphExec_t graph;
+    uint64_t dep_wait_ns;  // limit of one dependency wait of the persistent kernel
 };
 static_assert(sizeof(Plan) <= sizeof(se_batch_plan_t), "se_batch_plan_t too small");
 
@@ -508,12 +509,12 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
     }
     if (P.ntasks[0]) {
         persistent_kernel<16><<<P.grid[0], cfg<16>::THREADS, pcfg<16>::SMEM, s>>>(
-            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[0]), P.ntasks[0], hdr, 0);
+            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[0]), P.ntasks[0], hdr, 0, P.dep_wait_ns);
         SE_CHECK_LAUNCH();
     }
     if (P.ntasks[1]) {
         persistent_kernel<32><<<P.grid[1], cfg<32>::THREADS, pcfg<32>::SMEM, s>>>(
-            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[1]), P.ntasks[1], hdr, 1);
+            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[1]), P.ntasks[1], hdr, 1, P.dep_wait_ns);
         SE_CHECK_LAUNCH();
     }
     if (P.nbig) {
@@ -692,6 +693,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     P.grid[0] = int(std::min<int64_t>(P.ntasks[0], int64_t(sms) * per16));
     P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * per32));
     P.graph = nullptr;
+    P.dep_wait_ns = kDepWaitNs;
     std::memcpy(plan_out, &P, sizeof(P));
     return SE_OK;
 }
@@ -753,6 +755,18 @@ extern "C" se_status_t se_batch_release(se_batch_plan_t* plan) {
     Plan P;
     std::memcpy(&P, plan, sizeof(P));
     if (P.graph) cudaGraphExecDestroy(P.graph);
+    P.graph = nullptr;
+    std::memcpy(plan, &P, sizeof(P));
+    return SE_OK;
+}
+
+extern "C" se_status_t se_batch_set_wait_limit(se_batch_plan_t* plan, uint64_t limit_ns) {
+    clear_error();
+    SE_REQUIRE(plan != nullptr, SE_ERR_INVALID, "null plan");
+    Plan P;
+    std::memcpy(&P, plan, sizeof(P));
+    P.dep_wait_ns = limit_ns;
+    if (P.graph) cudaGraphExecDestroy(P.graph);  // it holds the old limit
     P.graph = nullptr;
     std::memcpy(plan, &P, sizeof(P));
     return SE_OK;

@@ -75,14 +75,15 @@ __device__ __forceinline__ void fence_tensormap(const void* map) {
 }
 
 // Thread 0 only: wait until *ctr >= target or the abort flag rises or time runs out.
-__device__ inline bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag) {
+__device__ inline bool wait_counter(const uint32_t* ctr, uint32_t target, const uint32_t* abort_flag,
+                                    uint64_t limit_ns = kDepWaitNs) {
     if (ld_acquire(ctr) >= target) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t it = 0;; ++it) {
         if (ld_acquire(ctr) >= target) return true;
         if ((it & 63) == 0) {
             if (ld_acquire(abort_flag)) return false;
-            if (global_ns() - t0 > kDepWaitNs) return false;
+            if (global_ns() - t0 > limit_ns) return false;
         }
         __nanosleep(64);
     }

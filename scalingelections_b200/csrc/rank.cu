@@ -4,15 +4,19 @@
 //   ranking[r] = candidates by wins descending, ties by ascending index (py:291: Python's
 //                stable sorted(..., key=wins, reverse=True) keeps ties in input order)
 //
-// wins_kernel takes one pair of 64 x 64 tiles (I <= J, enumerated over the upper triangle so
-// that no block idles): S[I][J] is read straight into registers and S[J][I] through a swizzled
-// shared-memory tile, every cell of S once, in 128-bit loads. Both endpoints' wins accumulate
-// in registers; one global atomic per candidate per tile pair. place_kernel gives candidate i the place #{j : wins[j] > wins[i]} +
+// wins_kernel walks pairs of 64 x 64 tiles (I <= J, enumerated over the upper triangle), a few
+// resident CTAs per SM each taking every gridDim.x-th pair: S[I][J] is read straight into
+// registers and S[J][I] through a swizzled shared-memory tile, every cell of S once, in 128-bit
+// loads, and the next pair's loads are issued before the current pair is counted. Both
+// endpoints' wins accumulate in registers; one global atomic per candidate per tile pair.
+// place_kernel gives candidate i the place #{j : wins[j] > wins[i]} +
 // #{j < i : wins[j] == wins[i]}, which is exactly the stable order, by counting over strips of
 // the wins in shared memory (four per 128-bit load, eight slices of each strip counted side
 // by side); a slice wholly before or after the block's candidates needs one compare per pair.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 
@@ -20,6 +24,7 @@ namespace se {
 namespace rank {
 
 constexpr int kRT = 64;  // tile edge of wins_kernel
+constexpr int kWinsCtasPerSm = 4;
 
 // Thread (ry, cx) of wins_kernel holds rows ry + 16p (p < 4) and columns 4cx .. 4cx+3 of the
 // tile S[I][J] in registers (128-bit loads), and loads the same positions of S[J][I] into
@@ -31,15 +36,9 @@ constexpr int kRT = 64;  // tile edge of wins_kernel
 // diagonal tile (I = J) every ordered pair is in the tile, so only row wins are counted.
 __device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
 
-__global__ void __launch_bounds__(256)
-    wins_kernel(const uint32_t* __restrict__ S, int64_t ld, int C, int nt, int vec, int32_t* __restrict__ wins) {
-    __shared__ __align__(16) uint32_t bs[kRT * kRT];
-    __shared__ int32_t colpart[16][kRT];  // column wins per row group ry
-    int I, J;
-    upper_pair(blockIdx.x, nt, I, J);
-    const int i0 = I * kRT, j0 = J * kRT;
-    const int cx = threadIdx.x & 15, ry = threadIdx.x >> 4;
-    uint4 a[4], b[4];  // a[p] = S[i0 + ry + 16p][j0 + 4cx ..], b[p] = S[j0 + ry + 16p][i0 + 4cx ..]
+// Loads the thread's 4 x 4 cells of S[I][J] (a) and of S[J][I] at the same positions (b).
+__device__ __forceinline__ void load_pair(const uint32_t* __restrict__ S, int64_t ld, int C, int vec, int i0, int j0,
+                                          int ry, int cx, uint4 (&a)[4], uint4 (&b)[4]) {
     if (vec && i0 + kRT <= C && j0 + kRT <= C) {  // interior pair, 16-byte aligned rows
         const uint32_t* pa = S + int64_t(i0 + ry) * ld + j0 + 4 * cx;
         const uint32_t* pb = S + int64_t(j0 + ry) * ld + i0 + 4 * cx;
@@ -59,49 +58,80 @@ __global__ void __launch_bounds__(256)
             b[p] = make_uint4(at(rb, cb), at(rb, cb + 1), at(rb, cb + 2), at(rb, cb + 3));
         }
     }
+}
+
+// Persistent over the tile pairs: block b takes pairs b, b + gridDim.x, ... and loads the next
+// pair's cells into registers as soon as the current pair's transposed tile is in shared
+// memory, so the loads are in flight while the current pair is compared and counted.
+__global__ void __launch_bounds__(256, kWinsCtasPerSm)
+    wins_kernel(const uint32_t* __restrict__ S, int64_t ld, int C, int nt, int vec, int32_t* __restrict__ wins) {
+    __shared__ __align__(16) uint32_t bs[kRT * kRT];
+    __shared__ int32_t colpart[16][kRT];  // column wins per row group ry
+    const int64_t pairs = int64_t(nt) * (nt + 1) / 2;
+    const int cx = threadIdx.x & 15, ry = threadIdx.x >> 4;
     // Row r = ry + 16p: the swizzle s = 2 * ((r >> 2) & 15) moves the thread's 4-group by s & ~3
     // and swaps its halves when bit 1 of s (bit 2 of r, which is bit 2 of ry) is set.
     const bool swap = (ry >> 2) & 1;
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int r = ry + 16 * p;
-        const int g = (4 * cx) ^ (2 * ((r >> 2) & 15) & ~3);
-        const uint4 v = swap ? make_uint4(b[p].z, b[p].w, b[p].x, b[p].y) : b[p];
-        *reinterpret_cast<uint4*>(&bs[r * kRT + g]) = v;
+    uint4 a[4], b[4];  // a[p] = S[i0 + ry + 16p][j0 + 4cx ..], b[p] = S[j0 + ry + 16p][i0 + 4cx ..]
+    int I, J;
+    int64_t pb = blockIdx.x;
+    if (pb < pairs) {
+        upper_pair(pb, nt, I, J);
+        load_pair(S, ld, C, vec, I * kRT, J * kRT, ry, cx, a, b);
     }
-    __syncthreads();
-    uint32_t rw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
+    for (; pb < pairs; pb += gridDim.x) {
+        const int i0 = I * kRT, j0 = J * kRT;
+        const bool diag = I == J;
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const uint32_t x[4] = {a[p].x, a[p].y, a[p].z, a[p].w};
-        const int col = (ry + 16 * p) ^ (2 * cx);  // column ry + 16p of rows 4cx + q, swizzled
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint32_t y = bs[(4 * cx + q) * kRT + col];
-            rw[p] += x[q] > y;
-            cw[q] += y > x[q];
+        for (int p = 0; p < 4; ++p) {
+            const int r = ry + 16 * p;
+            const int g = (4 * cx) ^ (2 * ((r >> 2) & 15) & ~3);
+            const uint4 v = swap ? make_uint4(b[p].z, b[p].w, b[p].x, b[p].y) : b[p];
+            *reinterpret_cast<uint4*>(&bs[r * kRT + g]) = v;
         }
-    }
-    // Row wins: the 16 threads of a half warp share the rows.
+        const uint4 x0 = a[0], x1 = a[1], x2 = a[2], x3 = a[3];
+        __syncthreads();
+        const int64_t nb = pb + gridDim.x;
+        if (nb < pairs) {  // the next pair's loads, in flight during this pair's counting
+            upper_pair(nb, nt, I, J);
+            load_pair(S, ld, C, vec, I * kRT, J * kRT, ry, cx, a, b);
+        }
+        uint32_t rw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
+        const uint4 xs[4] = {x0, x1, x2, x3};
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
+        for (int p = 0; p < 4; ++p) {
+            const uint32_t x[4] = {xs[p].x, xs[p].y, xs[p].z, xs[p].w};
+            const int col = (ry + 16 * p) ^ (2 * cx);  // column ry + 16p of rows 4cx + q, swizzled
 #pragma unroll
-        for (int m = 8; m >= 1; m >>= 1) rw[p] += __shfl_xor_sync(0xFFFFFFFFu, rw[p], m);
-    }
-    if (cx < 4) {
-        const int p = cx;  // lane cx of the half warp adds row ry + 16 * cx
-        const uint32_t n = p == 0 ? rw[0] : p == 1 ? rw[1] : p == 2 ? rw[2] : rw[3];
-        if (n) atomicAdd(&wins[i0 + ry + 16 * p], int(n));
-    }
-    if (I == J) return;
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t y = bs[(4 * cx + q) * kRT + col];
+                rw[p] += x[q] > y;
+                cw[q] += y > x[q];
+            }
+        }
+        // Row wins: the 16 threads of a half warp share the rows.
 #pragma unroll
-    for (int q = 0; q < 4; ++q) colpart[ry][4 * cx + q] = int(cw[q]);
-    __syncthreads();
-    if (threadIdx.x < kRT) {
-        int n = 0;
+        for (int p = 0; p < 4; ++p) {
 #pragma unroll
-        for (int g = 0; g < 16; ++g) n += colpart[g][threadIdx.x];
-        if (n) atomicAdd(&wins[j0 + threadIdx.x], n);
+            for (int m = 8; m >= 1; m >>= 1) rw[p] += __shfl_xor_sync(0xFFFFFFFFu, rw[p], m);
+        }
+        if (cx < 4) {
+            const int p = cx;  // lane cx of the half warp adds row ry + 16 * cx
+            const uint32_t n = p == 0 ? rw[0] : p == 1 ? rw[1] : p == 2 ? rw[2] : rw[3];
+            if (n) atomicAdd(&wins[i0 + ry + 16 * p], int(n));
+        }
+        if (!diag) {  // on a diagonal tile every ordered pair was counted as a row win
+#pragma unroll
+            for (int q = 0; q < 4; ++q) colpart[ry][4 * cx + q] = int(cw[q]);
+        }
+        __syncthreads();  // bs and colpart are complete and no longer read below
+        if (!diag && threadIdx.x < kRT) {
+            int n = 0;
+#pragma unroll
+            for (int g = 0; g < 16; ++g) n += colpart[g][threadIdx.x];
+            if (n) atomicAdd(&wins[j0 + threadIdx.x], n);
+        }
+        __syncthreads();  // colpart is read before the next pair rewrites it
     }
 }
 
@@ -178,7 +208,12 @@ extern "C" se_status_t se_rank(const uint32_t* d_S, int64_t ld, int C, int32_t* 
     const int nt = (C + rank::kRT - 1) / rank::kRT;
     const int64_t pairs = int64_t(nt) * (nt + 1) / 2;  // at most 2^27 at C = 2^20
     const int vec = (reinterpret_cast<uintptr_t>(d_S) % 16 == 0) && ld % 4 == 0;  // rows start 16-byte aligned
-    rank::wins_kernel<<<unsigned(pairs), 256, 0, s>>>(d_S, ld, C, nt, vec, d_wins);
+    // A few resident CTAs per SM, each walking the tile pairs with the next pair's loads in flight.
+    int dev = 0, sms = 0;
+    SE_CUDA_TRY(cudaGetDevice(&dev));
+    SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t grid = std::min<int64_t>(pairs, int64_t(sms) * rank::kWinsCtasPerSm);
+    rank::wins_kernel<<<unsigned(grid), 256, 0, s>>>(d_S, ld, C, nt, vec, d_wins);
     SE_CHECK_LAUNCH();
     rank::place_kernel<<<(C + rank::kPlaceCand - 1) / rank::kPlaceCand, rank::kPlaceThreads, 0, s>>>(
         d_wins, C, d_ranking);

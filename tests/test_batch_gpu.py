@@ -124,3 +124,30 @@ def test_shifted_lanes_for_large_electorates(orc):
     bad.run()
     with pytest.raises(api.SchulzeError):
         bad.check()
+
+
+def test_dependency_wait_that_runs_out_reports_an_error_and_the_gpu_stays_usable(orc):
+    """Failure detection without a GPU fault. With the dependency-wait limit at zero, the panel
+    tasks, claimed as the kernel starts, find round 0's pivot tiles (tens of microseconds of
+    work) unfinished, and their waits run out: the run ends with SE_ERR_DEVICE, every CTA
+    drains the queue, and the context stays usable. With the limit restored the same plan
+    runs exactly, through a rebuilt graph too."""
+    from scalingelections_b200 import _lib
+
+    sizes = [1000, 900, 700, 600, 513]
+    host, dev = make_batch(11, sizes, [5000] * len(sizes))
+    b = BatchedElections(dev, [LANES_U16] * len(sizes))
+    b.set_wait_limit(0.0)
+    b.run()
+    with pytest.raises(_lib.SchulzeError) as e:
+        b.check()
+    assert e.value.status == _lib.SE_ERR_DEVICE and "dependency" in str(e.value)
+    x = torch.arange(1 << 20, device="cuda", dtype=torch.int64)
+    assert int(x.sum().item()) == (1 << 20) * ((1 << 20) - 1) // 2  # the context still works
+    b.set_wait_limit(5.0)
+    b.run()
+    b.check()
+    check_against_oracle(orc, host, b)
+    b.launch_graph()
+    b.check()
+    check_against_oracle(orc, host, b)

@@ -39,3 +39,13 @@ def test_reference_arm_prints_nothing_on_other_ranks():
     r = run_bench(SMALL, env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0, r.stderr
     assert not r.stdout.strip()
+
+
+def test_gpus_flag_launches_one_rank_per_gpu():
+    """--gpus N outside torchrun re-launches bench.py under torch.distributed.run with N
+    ranks; on this host (no GPU) the launch check joins them with gloo."""
+    r = run_bench(["--gpus", "2", "--workload", "launch-check"], env={"CUDA_VISIBLE_DEVICES": ""})
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert sorted(d["rank"] for d in lines) == [0, 1]
+    assert all(d["world_size"] == 2 and d["ranks_seen"] == 2 for d in lines)
