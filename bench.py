@@ -60,7 +60,8 @@ def parse():
                     help="reference arm: also time one closure at the workload's full size (minutes)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest", "sharded", "launch-check"],
+    ap.add_argument("--workload", choices=["closure", "batch", "serve", "ingest", "sharded", "reference-gpu",
+                                           "launch-check"],
                     default="closure",
                     help="closure: the headline single election; batch: many mixed elections; "
                          "serve: Poisson arrivals on the continuous-batching server")
@@ -540,6 +541,23 @@ def reference_gpu_leg(d_host, ours_host, local_rank: int) -> dict:
             "bit_identical_to_ours": bool(np.array_equal(res, ours_host)), "clocks": clocks.summary()}
 
 
+def run_reference_gpu(args, local_rank):
+    """The reference's own CUDA path alone on the headline matrix (for a launch list of its
+    kernels under ncu), beside this library's closure of the same matrix."""
+    import torch
+
+    from scalingelections_b200 import api
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    d, b, o = election_matrix(args.voters, args.candidates, args.phi, args.seed, dev)
+    del b, o
+    ours = api._to_host_u32(api.strongest_paths_device(d, lanes=args.lanes or 16))
+    line = reference_gpu_leg(api._to_host_u32(d), ours, local_rank)
+    line["workload"] = f"C={args.candidates}, V={args.voters} Mallows(phi={args.phi}) ballots"
+    print(json.dumps(line), flush=True)
+
+
 def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
     """The objects of the other configurations and comparisons, added to the headline line:
     e2e_pipelined (the headline through api.ClosureStream), u32 (the headline in 32-bit lanes),
@@ -557,7 +575,7 @@ def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
     ex = {}
     if host_in is not None:
         cs = api.ClosureStream(C, lanes=LANES_U16)
-        for _ in cs.map([host_in]):
+        for _ in cs.map([host_in] * 3):  # warm: every slot and stream used once
             pass
         with ClockSampler(local_rank) as clocks:
             t0 = time.perf_counter()
@@ -1159,8 +1177,9 @@ def launch_check(world, rank):
     dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     t = torch.ones(1, device="cuda" if backend == "nccl" else "cpu")
     dist.all_reduce(t)
-    print(json.dumps({"rank": rank, "world_size": world, "ranks_seen": int(t.item()), "backend": backend}),
-          flush=True)
+    # One write call per line: the ranks share stdout, and a short write to a pipe is atomic.
+    line = json.dumps({"rank": rank, "world_size": world, "ranks_seen": int(t.item()), "backend": backend})
+    os.write(1, (line + "\n").encode())
     dist.destroy_process_group()
 
 
@@ -1194,6 +1213,8 @@ def main():
             run_ingest(args, world, rank, local_rank)
         elif args.workload == "sharded":
             run_sharded(args, world, rank, local_rank)
+        elif args.workload == "reference-gpu":
+            run_reference_gpu(args, local_rank)
         else:
             run_ours(args, world, rank, local_rank)
     finally:

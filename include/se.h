@@ -123,12 +123,26 @@ SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
  * Host-only (no GPU needed): lets tests check the order against the dependency rules. */
 SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, int* i, int* j);
 
-/* Process-wide choice for se_closure: 0 or 1 = round by round (default), 2 = dataflow (needs
- * se_closure_workspace_bytes_flow() of workspace). For benchmarking and tests. */
+/* Process-wide schedule of se_closure (results are identical in every one):
+ *   0  automatic (default): by C, from the variant table below; 1 where it has no entry;
+ *   1  round by round: pivot, panels and remainder launches per round, panels and pivots on
+ *      the default micro-tile (8 x 8 words per thread), the next round's pivot closed by the
+ *      first CTA of the remainder launch;
+ *   2  dataflow: one persistent launch (needs se_closure_workspace_bytes_flow() of workspace);
+ *   3  as 1 with the panels on the wide micro-tile (8 x 4 words per thread, twice the warps);
+ *   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile.
+ * 3 and 4 differ from 1 in 16-bit lanes only. */
 SE_API se_status_t se_closure_set_mode(int mode);
 
-/* Number of kernels one se_closure call launches for C candidates (with lane_bits 16 or 32;
- * the automatic mode adds at most one more). */
+/* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
+ * modes[i] (1, 3 or 4); C above every entry uses 1. n <= 8; n = 0 clears it. An autotuner
+ * measures the variants per size bucket and installs the winners (scalingelections_b200
+ * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks
+ * among its kernels' tile templates (scaling_elections.cu:895-901). */
+SE_API se_status_t se_closure_set_variant_table(const int* max_c, const int* modes, int n);
+
+/* Number of kernels one se_closure call launches for C candidates in 16-bit lanes under the
+ * current schedule (automatic lanes add at most one more). */
 SE_API int se_closure_launch_count(int C);
 
 /* Largest C that se_closure_noalloc accepts. */

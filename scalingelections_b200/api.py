@@ -88,14 +88,26 @@ def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, datafl
     return n
 
 
-_closure_mode = 1
+_closure_mode = 0
 
 
 def set_closure_mode(mode: int) -> None:
-    """0 or 1: round by round (default); 2: the dataflow form (same results)."""
+    """The closure's schedule (same results in every one): 0 automatic by size (default),
+    1 round by round, 2 the dataflow form, 3 round by round with the panels on the wide
+    micro-tile, 4 as 3 with each pivot tile closed by its own wide launch (include/se.h)."""
     global _closure_mode
     check(_lib.lib().se_closure_set_mode(int(mode)))
     _closure_mode = int(mode)
+
+
+def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
+    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1, 3 or 4;
+    sizes above every entry run mode 1. An empty table clears it. autotune.tune_closure
+    measures the modes per size bucket and installs its winners through this."""
+    n = len(table)
+    max_c = (ctypes.c_int * max(n, 1))(*[int(c) for c, _ in table])
+    modes = (ctypes.c_int * max(n, 1))(*[int(m) for _, m in table])
+    check(_lib.lib().se_closure_set_variant_table(max_c, modes, n))
 
 
 def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO, out: torch.Tensor | None = None,
@@ -232,9 +244,15 @@ class ClosureStream:
 
     lanes: LANES_U16 (with ``value_offset``, a kept count v is held as v - value_offset, which
     must lie in [1, 65535]) or LANES_U32. A count outside the 16-bit window raises
-    SchulzeError(SE_ERR_OVERFLOW) when that election's result is handed out."""
+    SchulzeError(SE_ERR_OVERFLOW) when that election's result is handed out.
 
-    def __init__(self, num_candidates: int, *, lanes: int = LANES_U16, value_offset: int = 0, device=None):
+    Results are new arrays in pinned host memory from torch's pinned-memory cache. Pinning a
+    fresh block of C x C words takes a long time (a quarter second at C = 16384), so the
+    constructor fills the cache with the three result blocks a steady stream keeps alive (two
+    in flight, one with the caller); warm_results=0 skips that."""
+
+    def __init__(self, num_candidates: int, *, lanes: int = LANES_U16, value_offset: int = 0, device=None,
+                 warm_results: int = 3):
         _require_cuda()
         if lanes not in (LANES_U16, LANES_U32):
             raise ValueError("lanes must be LANES_U16 or LANES_U32")
@@ -256,6 +274,8 @@ class ClosureStream:
             self.copied_in = [torch.cuda.Event() for _ in range(2)]
             self.closed = [torch.cuda.Event() for _ in range(2)]
             self.copied_out = [torch.cuda.Event() for _ in range(2)]
+        blocks = [torch.empty((C, C), dtype=torch.int32, pin_memory=True) for _ in range(max(0, warm_results))]
+        del blocks  # back to the cache, ready for map()
 
     def _host_in(self, m) -> torch.Tensor:
         t = m if isinstance(m, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(_host_u32_matrix(m)))

@@ -1,4 +1,16 @@
-"""Autotuner for the batched closure.
+"""Autotuners for the batched closure and for the single-election closure.
+
+tune_closure: for each size bucket of the single-election closure it times the round-by-round
+schedules on a sample matrix and installs the fastest per bucket in the library's variant
+table (se_closure_set_variant_table), which the automatic schedule reads:
+  1  panels and pivots on the default micro-tile (8 x 8 words per thread, four warps in
+     16-bit lanes), the next pivot fused into the remainder launch;
+  3  panels on the wide micro-tile (8 x 4 words per thread, eight warps);
+  4  as 3, and every pivot tile closed by its own launch on the wide micro-tile.
+The schedules differ where the per-round chain (pivot, then panels) is not hidden behind the
+remainder: small and medium C.
+
+The batched closure's tuner (tune):
 
 For each election-size bucket it times, on the GPU, the batched persistent closure of a
 sample batch in both lane modes and keeps the faster:
@@ -9,9 +21,10 @@ whole persistent launch rather than to one election:
   ctas_per_sm  persistent CTAs per SM (1 or 2);
   order        elections of at most 128 candidates after the tiled ones, or before.
 A per-bucket CTA count would be tuned on a few elections of one size, where one election's
-chain of pivot rounds dominates, and would not carry over to a mixed launch. The tile (128 x 128 cells) and the register
-micro-tile (8 x 8 words) are fixed: they come from the register and shared-memory budget and
-the measured min/max issue rate. Results are stored as JSON and looked up per election.
+chain of pivot rounds dominates, and would not carry over to a mixed launch. In the batch the
+tile (128 x 128 cells) and the register micro-tile (8 x 8 words) are fixed: its persistent
+CTAs run every task kind side by side, two per SM, and the measured busy time is 96 % of the
+grid. Results are stored as JSON and looked up per election.
 """
 from __future__ import annotations
 
@@ -104,6 +117,48 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
     p.parent.mkdir(parents=True, exist_ok=True)
     p.write_text(json.dumps(table, indent=1) + "\n")
     return table
+
+
+CLOSURE_BUCKETS = [1024, 2048, 3072, 4096, 6144, 8192, 12288]  # upper bounds of the size buckets
+CLOSURE_MODES = (1, 3, 4)
+
+
+def tune_closure(sizes: Sequence[int] | None = None, reps: int = 5, V: int = 4096, seed: int = 0,
+                 install: bool = True, device=None) -> dict:
+    """Times the closure schedules CLOSURE_MODES at one size per bucket (the bucket's upper
+    bound by default; 16-bit lanes, a random tally of V ballots) and returns
+    {"sizes": {C: {mode: ms}}, "table": [(max_C, best mode), ...]}; installs the table in the
+    library when `install`. Buckets above the last size keep mode 1."""
+    from . import api
+
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    sizes = list(sizes or CLOSURE_BUCKETS)
+    out = {"sizes": {}, "table": []}
+    s = torch.cuda.current_stream()
+    try:
+        for n, C in enumerate(sizes):
+            d = _sample_batch(C, C, 1, V, seed + n, device)[0]
+            work = torch.empty(api.closure_workspace_bytes(C, LANES_U16), dtype=torch.uint8, device=device)
+            res = torch.empty_like(d)
+            times = {}
+            for mode in CLOSURE_MODES:
+                api.set_closure_mode(mode)
+                api.strongest_paths_device(d, lanes=LANES_U16, out=res, workspace=work)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                for _ in range(reps):
+                    api.strongest_paths_device(d, lanes=LANES_U16, out=res, workspace=work)
+                e1.record(s)
+                torch.cuda.synchronize()
+                times[mode] = e0.elapsed_time(e1) / reps
+            out["sizes"][int(C)] = times
+            out["table"].append((int(C), int(min(times, key=times.get))))
+            del d, work, res
+    finally:
+        api.set_closure_mode(0)
+    if install:
+        api.set_closure_variants(out["table"])
+    return out
 
 
 def load(path: Path | None = None) -> dict | None:

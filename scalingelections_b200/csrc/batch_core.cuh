@@ -178,18 +178,18 @@ __device__ void run_small(const Elec& E, uint8_t* smem, uint32_t (*rowbuf)[cfg<L
 // ------------------------------------------------------------------------------------------
 // Tile tasks of elections with R >= 2.
 // ------------------------------------------------------------------------------------------
-template <int LB>
+template <int LB, int NQ = 8>
 __device__ void run_pivot(const Elec& E, int k, uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT]) {
     using CF = cfg<LB>;
-    const geom g(threadIdx.x);
+    const geomT<NQ> g(threadIdx.x);
     const int64_t ldw = E.Cp / CF::CPW;
     uint32_t* D = E.S + int64_t(k) * kT * ldw + int64_t(k) * CF::TW;
-    uint32_t c[8][8];
-    load_tile_regs<LB, true>(c, D, ldw, g);
+    uint32_t c[8][NQ];
+    load_tile_regs<LB, true, NQ>(c, D, ldw, g);
     const int kmax = E.C - k * kT < kT ? E.C - k * kT : kT;  // pivots past C are zero padding
-    close_tile_in_registers<LB>(c, g, kmax, rowbuf, colbuf);
-    store_tile_regs<LB>(c, D, ldw, g);
-    store_transposed_splat<LB>(c, E.dT, kT, g);
+    close_tile_in_registers<LB, NQ>(c, g, kmax, rowbuf, colbuf);
+    store_tile_regs<LB, NQ>(c, D, ldw, g);
+    store_transposed_splat<LB, NQ>(c, E.dT, kT, g);
 }
 
 // Tile tasks of one pivot round K, all through one routine:
@@ -217,7 +217,9 @@ constexpr int kTileRem = 2;
 // passes them). Padding holds zeros in both operands, and a cell's relaxation through a zero
 // operand leaves it unchanged, so 32-pivot chunks and 32-row warps wholly past C skip the
 // product (their copies too), with identical results.
-template <int LB, bool GLOBAL_MAPS = true>
+// NQ: words per thread, 8 (the default micro-tile) or 4 (the wide one, 256 threads, 16-bit
+// lanes); the block must have tile_threads<LB, NQ>() threads.
+template <int LB, bool GLOBAL_MAPS = true, int NQ = 8>
 __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
                          uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1,
                          int kvalid = -1, int rvalid = -1) {
@@ -225,9 +227,9 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     constexpr int TW = CF::TW;
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);
     uint32_t* Bs = reinterpret_cast<uint32_t*>(smem + pcfg<LB>::A_REGION);
-    const geom g(threadIdx.x);
+    const geomT<NQ> g(threadIdx.x);
     const int64_t ldw = E.Cp / CF::CPW;
-    uint32_t c[8][8];
+    uint32_t c[8][NQ];
     bool ok = true;
     uint64_t* wait_bars = bars;  // the product's chunk barriers and their parity
     uint32_t wait_par = par_a;
@@ -259,7 +261,7 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             }
         }
         Ct = E.S + int64_t(rem ? I : K) * kT * ldw + int64_t(J) * TW;
-        load_tile_regs<LB, true>(c, Ct, ldw, g);
+        load_tile_regs<LB, true, NQ>(c, Ct, ldw, g);
         par_a ^= 1u;
     } else {
         // The tile itself into Bs, transposed and duplicated into As; then D into Bs.
@@ -275,7 +277,7 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
 #pragma unroll 1
         for (int ch = 0; ch < kChunks; ++ch) ok = ok && mbar_wait_bounded(&bars[ch], par_a, 1u << 26);
         if (ok) {
-            constexpr int HALVES = CF::THREADS / kT;
+            constexpr int HALVES = tile_threads<LB, NQ>() / kT;
             constexpr int SPAN = TW / HALVES;
             const int i = threadIdx.x % kT;
             const int half = threadIdx.x / kT;
@@ -286,7 +288,7 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
 #pragma unroll
                 for (int h = 0; h < CF::CPW; ++h) As[(w * CF::CPW + h) * kT + i] = cell_splat<LB>(word, h);
             }
-            load_tile_regs<LB>(c, Bs, TW, g);
+            load_tile_regs<LB, false, NQ>(c, Bs, TW, g);
         }
         __syncthreads();  // the tile region is free again
         if (threadIdx.x == 0 && ok) {
@@ -318,12 +320,12 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
                 ok = false;
                 break;
             }
-            if (live) relax_chunk<LB>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
+            if (live) relax_chunk<LB, NQ>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
         }
     }
     if (ok) {
-        store_tile_regs<LB>(c, Ct, ldw, g);
-        if (kind == kTileCol) store_transposed_splat<LB>(c, E.AT + int64_t(I) * kT, E.Cp, g);
+        store_tile_regs<LB, NQ>(c, Ct, ldw, g);
+        if (kind == kTileCol) store_transposed_splat<LB, NQ>(c, E.AT + int64_t(I) * kT, E.Cp, g);
     }
     return ok;
 }

@@ -52,8 +52,8 @@ constexpr uint32_t kMaxPolls = 1u << 26;
 // max(S[I][K], S[I][K] (x) D), which also emit the transposed panel AT. 96 KiB of shared
 // memory per CTA, so both sets are resident at once.
 // ------------------------------------------------------------------------------------------
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+template <int LB, int NQ = 8>
+__global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     panels_kernel(const __grid_constant__ batch::Elec E, int K, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
@@ -68,8 +68,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     uint32_t par_a = 0, par_b = 0;
     const bool row = b < R1;
     const int x = row ? b : b - R1;
-    ok = batch::run_tile<LB, false>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K), x + (x >= K),
-                                    smem, bars, par_a, par_b);
+    ok = batch::run_tile<LB, false, NQ>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K),
+                                        x + (x >= K), smem, bars, par_a, par_b);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -361,19 +361,19 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 // ------------------------------------------------------------------------------------------
 // Pivot tile (phase 1): close D = S[K][K] in place, two pivots per barrier, then emit dT.
 // ------------------------------------------------------------------------------------------
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+template <int LB, int NQ = 8>
+__global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     diag_kernel(uint32_t* __restrict__ S, int64_t ldw, int K, uint32_t* __restrict__ dT) {
     using CF = cfg<LB>;
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
     __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
-    const geom g(threadIdx.x);
-    uint32_t c[8][8];
+    const geomT<NQ> g(threadIdx.x);
+    uint32_t c[8][NQ];
     uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * CF::TW;
-    load_tile_regs<LB>(c, D, ldw, g);
-    close_tile_in_registers<LB>(c, g, kT, rowbuf, colbuf);
-    store_tile_regs<LB>(c, D, ldw, g);
-    store_transposed_splat<LB>(c, dT, kT, g);
+    load_tile_regs<LB, false, NQ>(c, D, ldw, g);
+    close_tile_in_registers<LB, NQ>(c, g, kT, rowbuf, colbuf);
+    store_tile_regs<LB, NQ>(c, D, ldw, g);
+    store_transposed_splat<LB, NQ>(c, dT, kT, g);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -537,25 +537,53 @@ layout plan(int C, int lane_bits) {
     return L;
 }
 
-// 0 or 1: round by round (the default: on B200 hardware block scheduling of one launch per
-// phase beats the persistent grid's claim-and-poll overhead at every size measured);
-// 2: dataflow, which then needs se_closure_workspace_bytes_flow() of workspace.
-std::atomic<int> g_closure_mode{1};
+// Closure schedules (se_closure_set_mode):
+//   0  automatic: by C, from the variant table (se_closure_set_variant_table), else 1;
+//   1  round by round, panels and pivots with the default micro-tile (8 x 8 words, 128
+//      threads in 16-bit lanes), the next round's pivot fused into the remainder launch;
+//   2  dataflow: one persistent grid (needs se_closure_workspace_bytes_flow() of workspace);
+//   3  as 1 with the panels on the wide micro-tile (8 x 4 words, 256 threads; 16-bit lanes);
+//   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile, after the
+//      whole remainder launch, instead of fused into its first CTA.
+// 3 and 4 apply to 16-bit lanes; 32-bit lanes run 1 for them. Round by round is the default:
+// on B200 hardware block scheduling of one launch per phase beats the persistent grid's
+// claim-and-poll overhead at every size measured.
+std::atomic<int> g_closure_mode{0};
+
+// The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds).
+constexpr int kMaxVariants = 8;
+std::mutex g_variant_mutex;
+int g_variant_n = 0;
+int g_variant_max_c[kMaxVariants];
+int g_variant_mode[kMaxVariants];
+
+int automatic_mode(int C) {
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    for (int i = 0; i < g_variant_n; ++i)
+        if (C <= g_variant_max_c[i]) return g_variant_mode[i];
+    return 1;
+}
 
 template <int LB> se_status_t set_smem_limits() {
     const int bytes = int(batch::pcfg<LB>::SMEM);
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB>), bytes, "the panel kernel"))
         return st;
+    if constexpr (LB == 16) {
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB, 4>), bytes,
+                                              "the wide panel kernel"))
+            return st;
+    }
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB>), bytes, "the remainder kernel"))
         return st;
     return raise_smem_limit(reinterpret_cast<const void*>(flow_kernel<LB>), bytes, "the dataflow closure");
 }
 
-// Rounds of the blocked closure on an initialised working matrix.
-// phase_ms (optional, 4 entries): accumulated device time of the diagonal, row-panel,
-// column-panel and remainder launches, from events recorded between launches.
+// Rounds of the blocked closure on an initialised working matrix, in schedule `mode` (1, 3 or
+// 4; see g_closure_mode). phase_ms (optional, 4 entries): accumulated device time of the pivot
+// launches, the panel launches, (unused) and the remainder launches, from events recorded
+// between launches.
 template <int LB>
-se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms) {
+se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms, int mode) {
     using CF = cfg<LB>;
     if (se_status_t st = set_smem_limits<LB>(); st != SE_OK) return st;
     uint32_t* S = reinterpret_cast<uint32_t*>(work + P.s_off);
@@ -564,6 +592,8 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     uint32_t* err = reinterpret_cast<uint32_t*>(work + P.flags_off);
     const int64_t ldw = P.Cp / CF::CPW;
     const int R = int(P.Cp / kT);
+    const bool wide = LB == 16 && (mode == 3 || mode == 4);
+    const bool fused = !(LB == 16 && mode == 4);
 
     batch::Elec E;
     std::memset(&E, 0, sizeof(E));
@@ -580,44 +610,64 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     E.lanes = LB;
     const size_t smem = batch::pcfg<LB>::SMEM;
 
-    // Events bracket the pivot (round 0), panel and remainder launches when profiling.
-    std::vector<cudaEvent_t> ev;
+    // Events between launches when profiling: (phase, event recorded after the launch).
+    std::vector<std::pair<int, cudaEvent_t>> ev;
+    cudaEvent_t start = nullptr;
+    se_status_t failed = SE_OK;
+    auto mark = [&](int phase) {
+        if (!phase_ms || failed) return;
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            failed = SE_ERR_CUDA;
+            set_error("cannot create a profiling event");
+            return;
+        }
+        cudaEventRecord(e, stream);
+        ev.emplace_back(phase, e);
+    };
     if (phase_ms) {
-        ev.resize(size_t(R) * 2 + 2, nullptr);
-        for (auto& e : ev)
-            if (cudaEventCreate(&e) != cudaSuccess) {
-                for (auto& x : ev)
-                    if (x) cudaEventDestroy(x);
-                SE_CUDA_TRY(cudaGetLastError());
-            }
-        cudaEventRecord(ev[0], stream);
+        if (cudaEventCreate(&start) != cudaSuccess) SE_CUDA_TRY(cudaGetLastError());
+        cudaEventRecord(start, stream);
     }
-    diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
-    if (phase_ms) cudaEventRecord(ev[1], stream);
+    auto pivot = [&](int K) {
+        if (wide) {
+            if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, K, dT);
+        } else {
+            diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, K, dT);
+        }
+        mark(0);
+    };
+    pivot(0);
     SE_CHECK_LAUNCH();
     for (int K = 0; K < R && R > 1; ++K) {
-        panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
-        if (phase_ms) cudaEventRecord(ev[2 + 2 * K], stream);
-        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, K + 1 < R ? 1 : 0, err);
-        if (phase_ms) cudaEventRecord(ev[3 + 2 * K], stream);
+        if (K > 0 && !fused) pivot(K);
+        if (wide) {
+            if constexpr (LB == 16)
+                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E, K, err);
+        } else {
+            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
+        }
+        mark(1);
+        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, err);
+        mark(3);
         SE_CHECK_LAUNCH();
     }
     if (phase_ms) {
-        const cudaEvent_t last = R > 1 ? ev[2 * R + 1] : ev[1];
-        cudaError_t e = cudaEventSynchronize(last);
-        for (int p = 0; p < 4; ++p) phase_ms[p] = 0.0;
-        float ms = 0.f;
+        for (int q = 0; q < 4; ++q) phase_ms[q] = 0.0;
+        cudaError_t e = ev.empty() ? cudaSuccess : cudaEventSynchronize(ev.back().second);
         if (e == cudaSuccess) {
-            cudaEventElapsedTime(&ms, ev[0], ev[1]);
-            phase_ms[0] += ms;
-            for (int K = 0; K < R && R > 1; ++K) {
-                cudaEventElapsedTime(&ms, K == 0 ? ev[1] : ev[1 + 2 * K], ev[2 + 2 * K]);
-                phase_ms[1] += ms;
-                cudaEventElapsedTime(&ms, ev[2 + 2 * K], ev[3 + 2 * K]);
-                phase_ms[3] += ms;
+            cudaEvent_t prev = start;
+            for (auto& x : ev) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, prev, x.second);
+                phase_ms[x.first] += ms;
+                prev = x.second;
             }
         }
-        for (auto& x : ev) cudaEventDestroy(x);
+        for (auto& x : ev) cudaEventDestroy(x.second);
+        cudaEventDestroy(start);
+        if (failed) return failed;
         SE_CUDA_TRY(e);
     }
     return SE_OK;
@@ -785,12 +835,14 @@ se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t
     } else {
         if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
-    const int mode = mode_override >= 0 ? mode_override : g_closure_mode.load();
+    int mode = mode_override >= 0 ? mode_override : g_closure_mode.load();
+    if (mode == 0) mode = automatic_mode(C);
     const bool flow = mode == 2 && P.Cp > kT;
     SE_REQUIRE(mode != 2 || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
                "the dataflow closure needs a workspace of %lld bytes", (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
-                          : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms) : run_rounds<32>(work, P, s, phase_ms));
+                          : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms, mode)
+                                      : run_rounds<32>(work, P, s, phase_ms, mode));
     if (st) return st;
     st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, base, s)
                   : launch_finalize<32>(P, work, C, d_out, ld_out, 0, s);
@@ -867,13 +919,35 @@ extern "C" se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k
 
 extern "C" se_status_t se_closure_set_mode(int mode) {
     clear_error();
-    SE_REQUIRE(mode >= 0 && mode <= 2, SE_ERR_INVALID, "closure mode must be 0, 1 or 2");
+    SE_REQUIRE(mode >= 0 && mode <= 4, SE_ERR_INVALID, "closure mode must be 0 to 4");
     g_closure_mode.store(mode);
     return SE_OK;
+}
+
+extern "C" se_status_t se_closure_set_variant_table(const int* max_c, const int* modes, int n) {
+    return host_guard([&]() -> se_status_t {
+        clear_error();
+        SE_REQUIRE(n >= 0 && n <= kMaxVariants, SE_ERR_INVALID, "at most %d table entries", kMaxVariants);
+        SE_REQUIRE(n == 0 || (max_c && modes), SE_ERR_INVALID, "null table");
+        for (int i = 0; i < n; ++i)
+            SE_REQUIRE(modes[i] == 1 || modes[i] == 3 || modes[i] == 4, SE_ERR_INVALID,
+                       "table modes must be 1, 3 or 4 (got %d)", modes[i]);
+        std::lock_guard<std::mutex> lock(g_variant_mutex);
+        for (int i = 0; i < n; ++i) {
+            g_variant_max_c[i] = max_c[i];
+            g_variant_mode[i] = modes[i];
+        }
+        g_variant_n = n;
+        return SE_OK;
+    });
 }
 
 extern "C" int se_closure_launch_count(int C) {
     if (C < 1) return 0;
     const int R = int(round_up(C, kT) / kT);
-    return R == 1 ? 3 : 3 + 2 * R;  // init, pivot of round 0, R x (panels, remainder), finalize
+    int mode = g_closure_mode.load();
+    if (mode == 0) mode = automatic_mode(C);
+    // init, pivot of round 0, R x (panels, remainder), finalize; mode 4 adds a pivot launch
+    // per later round (in 16-bit lanes).
+    return R == 1 ? 3 : 3 + 2 * R + (mode == 4 ? R - 1 : 0);
 }

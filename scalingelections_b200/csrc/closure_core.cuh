@@ -34,18 +34,31 @@ template <int LB> struct cfg {
 };
 
 // Thread geometry shared by every kernel of one lane mode: warp (wm, wn) of a 4 x WN grid,
-// lane (tr, tc) of a 4 x 8 grid. The thread owns rows row0 .. row0+7 and words
-// wbase .. wbase+3 and wbase+32 .. wbase+35 of the tile, so the 8 threads of a row group read
-// 128 contiguous bytes of B per shared load, and 4 row groups read 4 disjoint bank groups of A.
-struct geom {
+// lane (tr, tc) of a 4 x 8 grid. With NQ = 8 words per thread (the default micro-tile) the
+// thread owns rows row0 .. row0+7 and words wbase .. wbase+3 and wbase+32 .. wbase+35 of the
+// tile, so the 8 threads of a row group read 128 contiguous bytes of B per shared load, and 4
+// row groups read 4 disjoint bank groups of A. With NQ = 4 (16-bit lanes only: the wide
+// micro-tile, 256 threads) warps 4..7 take words 32..63 and the thread owns words
+// wbase .. wbase+3 of its rows: twice the warps on one tile, for tiles that run alone on an SM
+// (pivot and panels), where four warps leave every scheduler with one warp and stall on
+// instruction latency.
+template <int NQ = 8> struct geomT {
+    static_assert(NQ == 8 || NQ == 4, "8 or 4 words per thread");
     int row0, wbase;
-    __device__ __forceinline__ explicit geom(int tid) {
+    __device__ __forceinline__ explicit geomT(int tid) {
         const int warp = tid >> 5, lane = tid & 31;
         row0 = (warp & 3) * 32 + (lane >> 3) * 8;
-        wbase = (warp >> 2) * 64 + (lane & 7) * 4;
+        wbase = (warp >> 2) * (NQ == 8 ? 64 : 32) + (lane & 7) * 4;
     }
     __device__ __forceinline__ int word(int q) const { return wbase + (q < 4 ? q : 28 + q); }
 };
+using geom = geomT<8>;
+
+// Threads of a CTA that holds one tile in lane mode LB with NQ words per thread.
+template <int LB, int NQ> constexpr int tile_threads() {
+    static_assert(NQ == 8 || LB == 16, "the wide micro-tile is for 16-bit lanes");
+    return NQ == 8 ? cfg<LB>::THREADS : 256;
+}
 
 __device__ __forceinline__ void ld4(uint32_t* dst, const uint32_t* src) {
     const uint4 v = *reinterpret_cast<const uint4*>(src);
@@ -68,30 +81,30 @@ __device__ __forceinline__ void ld4_cg(uint32_t* dst, const uint32_t* src) {
     dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
 }
 
-template <int LB, bool COHERENT = false>
-__device__ __forceinline__ void load_tile_regs(uint32_t (&c)[8][8], const uint32_t* base, int64_t ldw,
-                                               const geom& g) {
+template <int LB, bool COHERENT = false, int NQ = 8>
+__device__ __forceinline__ void load_tile_regs(uint32_t (&c)[8][NQ], const uint32_t* base, int64_t ldw,
+                                               const geomT<NQ>& g) {
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
         if constexpr (COHERENT) {
             ld4_cg(&c[r][0], p);
-            ld4_cg(&c[r][4], p + 32);
+            if constexpr (NQ == 8) ld4_cg(&c[r][4], p + 32);
         } else {
             ld4(&c[r][0], p);
-            ld4(&c[r][4], p + 32);
+            if constexpr (NQ == 8) ld4(&c[r][4], p + 32);
         }
     }
 }
 
-template <int LB>
-__device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][8], uint32_t* base, int64_t ldw,
-                                                const geom& g) {
+template <int LB, int NQ = 8>
+__device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][NQ], uint32_t* base, int64_t ldw,
+                                                const geomT<NQ>& g) {
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         uint32_t* p = base + int64_t(g.row0 + r) * ldw + g.wbase;
         st4(p, &c[r][0]);
-        st4(p + 32, &c[r][4]);
+        if constexpr (NQ == 8) st4(p + 32, &c[r][4]);
     }
 }
 
@@ -101,38 +114,38 @@ __device__ __forceinline__ void store_tile_regs(const uint32_t (&c)[8][8], uint3
 // the loop overhead is negligible beside 416 instructions per iteration, and the smaller body
 // stays in the instruction cache even in the persistent kernels, whose CTAs run several task
 // routines side by side on one SM.
-template <int LB>
-__device__ __forceinline__ void relax_chunk(uint32_t (&c)[8][8], const uint32_t* __restrict__ As,
-                                            const uint32_t* __restrict__ Bs, const geom& g) {
+template <int LB, int NQ = 8>
+__device__ __forceinline__ void relax_chunk(uint32_t (&c)[8][NQ], const uint32_t* __restrict__ As,
+                                            const uint32_t* __restrict__ Bs, const geomT<NQ>& g) {
     using L = lanes<LB>;
     constexpr int TW = cfg<LB>::TW;
 #pragma unroll 4
     for (int k = 0; k < kKC; k += 2) {
-        uint32_t a0[8], a1[8], b0[8], b1[8];
+        uint32_t a0[8], a1[8], b0[NQ], b1[NQ];
         ld4(a0, As + k * kT + g.row0);
         ld4(a0 + 4, As + k * kT + g.row0 + 4);
         ld4(a1, As + (k + 1) * kT + g.row0);
         ld4(a1 + 4, As + (k + 1) * kT + g.row0 + 4);
         ld4(b0, Bs + k * TW + g.wbase);
-        ld4(b0 + 4, Bs + k * TW + g.wbase + 32);
+        if constexpr (NQ == 8) ld4(b0 + 4, Bs + k * TW + g.wbase + 32);
         ld4(b1, Bs + (k + 1) * TW + g.wbase);
-        ld4(b1 + 4, Bs + (k + 1) * TW + g.wbase + 32);
+        if constexpr (NQ == 8) ld4(b1 + 4, Bs + (k + 1) * TW + g.wbase + 32);
 #pragma unroll
         for (int r = 0; r < 8; ++r)
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
+            for (int q = 0; q < NQ; ++q)
                 c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
     }
 }
 
 // Writes the thread's cells transposed and duplicated: out[k][row] for every cell (row, k)
 // it holds; out is k-major with row stride ld_out words.
-template <int LB>
-__device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8], uint32_t* out,
-                                                       int64_t ld_out, const geom& g) {
+template <int LB, int NQ = 8>
+__device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][NQ], uint32_t* out,
+                                                       int64_t ld_out, const geomT<NQ>& g) {
     constexpr int CPW = cfg<LB>::CPW;
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+    for (int q = 0; q < NQ; ++q)
 #pragma unroll
         for (int h = 0; h < CPW; ++h) {
             const int k = g.word(q) * CPW + h;
@@ -150,19 +163,19 @@ __device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][8]
 constexpr int kPivotBufs = 4;
 
 // Publishes row k and column k of the tile (the thread's share of them) into staging slot s.
-template <int LB>
-__device__ __forceinline__ void publish_pivot(const uint32_t (&c)[8][8], const geom& g, int k, uint32_t* row,
+template <int LB, int NQ = 8>
+__device__ __forceinline__ void publish_pivot(const uint32_t (&c)[8][NQ], const geomT<NQ>& g, int k, uint32_t* row,
                                               uint32_t* col) {
     constexpr int CPW = cfg<LB>::CPW;
 #pragma unroll
     for (int r = 0; r < 8; ++r)
         if (g.row0 + r == k) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) row[g.word(q)] = c[r][q];
+            for (int q = 0; q < NQ; ++q) row[g.word(q)] = c[r][q];
         }
     const int wk = k / CPW, hk = k % CPW;
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+    for (int q = 0; q < NQ; ++q)
         if (g.word(q) == wk) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) col[g.row0 + r] = cell_splat<LB>(c[r][q], hk);
@@ -179,48 +192,48 @@ __device__ __forceinline__ void publish_pivot(const uint32_t (&c)[8][8], const g
 //   c[i][j] = max(c[i][j], min(c[i][k], c[k][j]), min(c'[i][k+1], c'[k+1][j]))
 // which is exactly two Floyd-Warshall steps. Every thread of the block must call it. Pivots
 // >= kmax are skipped, which is exact when those rows/columns are zero padding.
-template <int LB>
-__device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][8], const geom& g, int kmax,
+template <int LB, int NQ = 8>
+__device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][NQ], const geomT<NQ>& g, int kmax,
                                                         uint32_t (*rowbuf)[cfg<LB>::TW],
                                                         uint32_t (*colbuf)[kT]) {
     using L = lanes<LB>;
     constexpr int CPW = cfg<LB>::CPW;
-    publish_pivot<LB>(c, g, 0, rowbuf[0], colbuf[0]);
-    publish_pivot<LB>(c, g, 1, rowbuf[1], colbuf[1]);
+    publish_pivot<LB, NQ>(c, g, 0, rowbuf[0], colbuf[0]);
+    publish_pivot<LB, NQ>(c, g, 1, rowbuf[1], colbuf[1]);
     __syncthreads();
 #pragma unroll 1
     for (int k = 0; k < kmax; k += 2) {
         const int s = ((k >> 1) & 1) * 2;  // this pair's slots
-        uint32_t a0[8], b0[8];
+        uint32_t a0[8], b0[NQ];
         ld4(a0, &colbuf[s][g.row0]);
         ld4(a0 + 4, &colbuf[s][g.row0 + 4]);
         ld4(b0, &rowbuf[s][g.wbase]);
-        ld4(b0 + 4, &rowbuf[s][g.wbase + 32]);
+        if constexpr (NQ == 8) ld4(b0 + 4, &rowbuf[s][g.wbase + 32]);
         if (k + 1 < kmax) {
-            uint32_t a1[8], b1[8];
+            uint32_t a1[8], b1[NQ];
             ld4(a1, &colbuf[s + 1][g.row0]);
             ld4(a1 + 4, &colbuf[s + 1][g.row0 + 4]);
             ld4(b1, &rowbuf[s + 1][g.wbase]);
-            ld4(b1 + 4, &rowbuf[s + 1][g.wbase + 32]);
+            if constexpr (NQ == 8) ld4(b1 + 4, &rowbuf[s + 1][g.wbase + 32]);
             const uint32_t ckk1 = cell_splat<LB>(rowbuf[s][(k + 1) / CPW], (k + 1) % CPW);  // c[k][k+1]
             const uint32_t ck1k = colbuf[s][k + 1];                                        // c[k+1][k]
 #pragma unroll
             for (int r = 0; r < 8; ++r) a1[r] = L::vmax(a1[r], L::vmin(a0[r], ckk1));
 #pragma unroll
-            for (int q = 0; q < 8; ++q) b1[q] = L::vmax(b1[q], L::vmin(ck1k, b0[q]));
+            for (int q = 0; q < NQ; ++q) b1[q] = L::vmax(b1[q], L::vmin(ck1k, b0[q]));
 #pragma unroll
             for (int r = 0; r < 8; ++r)
 #pragma unroll
-                for (int q = 0; q < 8; ++q) c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
+                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
         } else {
 #pragma unroll
             for (int r = 0; r < 8; ++r)
 #pragma unroll
-                for (int q = 0; q < 8; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a0[r], b0[q]));
+                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a0[r], b0[q]));
         }
         const int k2 = k + 2, t = s ^ 2;  // the next pair, into the other phase's slots
-        if (k2 < kmax) publish_pivot<LB>(c, g, k2, rowbuf[t], colbuf[t]);
-        if (k2 + 1 < kmax) publish_pivot<LB>(c, g, k2 + 1, rowbuf[t + 1], colbuf[t + 1]);
+        if (k2 < kmax) publish_pivot<LB, NQ>(c, g, k2, rowbuf[t], colbuf[t]);
+        if (k2 + 1 < kmax) publish_pivot<LB, NQ>(c, g, k2 + 1, rowbuf[t + 1], colbuf[t + 1]);
         __syncthreads();
     }
 }

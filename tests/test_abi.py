@@ -52,6 +52,23 @@ def test_closure_argument_errors_need_no_gpu():
     assert L.se_rank(p, 2, 4, p, p, None) == _lib.SE_ERR_INVALID
 
 
+def test_closure_schedule_settings_need_no_gpu():
+    from scalingelections_b200 import _lib
+
+    L = _lib.lib()
+    n = 2
+    max_c = (ctypes.c_int * n)(2048, 4096)
+    ok = (ctypes.c_int * n)(4, 3)
+    bad = (ctypes.c_int * n)(4, 2)  # the dataflow form is not a table variant
+    assert L.se_closure_set_variant_table(max_c, bad, n) == _lib.SE_ERR_INVALID
+    assert L.se_closure_set_variant_table(max_c, ok, 9) == _lib.SE_ERR_INVALID
+    assert L.se_closure_set_variant_table(max_c, ok, n) == _lib.SE_OK
+    assert L.se_closure_set_variant_table(None, None, 0) == _lib.SE_OK
+    assert L.se_closure_set_mode(5) == _lib.SE_ERR_INVALID
+    for mode in (4, 0):
+        assert L.se_closure_set_mode(mode) == _lib.SE_OK
+
+
 HOST_ALLOC_FAILURE = r"""
 import ctypes, resource, sys
 
