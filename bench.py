@@ -613,7 +613,19 @@ def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
     obj32, o32 = closure_object(d4, 32, max(steps, 10), 2, local_rank, "the same election in 32-bit lanes")
     obj16["u32"] = obj32
     obj16["u32"]["bit_identical_to_u16"] = bool(torch.equal(o16.view(torch.int32), o32.view(torch.int32)))
-    obj16["tile_note"] = "one tile shape, 128 x 128 cells (8 x 8 words per thread)"
+    # The schedule sweep of this configuration: the 128-cell tile with the default micro-tile
+    # (8 x 8 words per thread) for every tile, or the wide one (8 x 4 words, twice the warps) for
+    # the panels, or for the panels and a pivot launch per round.
+    sweep = {}
+    for mode, what in ((1, "panels and pivot on 8x8 words, pivot fused"), (3, "panels on 8x4 words, pivot fused"),
+                       (4, "panels and pivot on 8x4 words, pivot launched")):
+        api.set_closure_mode(mode)
+        o, _ = closure_object(d4, 16, max(steps, 20), 3, local_rank, what)
+        sweep[str(mode)] = {"schedule": what, "ms": o["ms"], "value": o["value"],
+                            "frac_of_peak": o.get("whole_closure_frac_of_peak")}
+    api.set_closure_mode(0)
+    obj16["schedule_sweep"] = sweep
+    obj16["tile_note"] = "tile 128 x 128 cells; micro-tile 8 x 8 or 8 x 4 words per thread (schedule_sweep)"
     ex["c4096"] = obj16
     del d4, o16, o32
 

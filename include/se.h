@@ -135,7 +135,8 @@ SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, in
 SE_API se_status_t se_closure_set_mode(int mode);
 
 /* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
- * modes[i] (1, 3 or 4); C above every entry uses 1. n <= 8; n = 0 clears it. An autotuner
+ * modes[i] (1, 3 or 4); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
+ * table, measured on B200, is {C <= 1024: 4, C <= 12288: 3}. An autotuner
  * measures the variants per size bucket and installs the winners (scalingelections_b200
  * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks
  * among its kernels' tile templates (scaling_elections.cu:895-901). */

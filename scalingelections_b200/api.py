@@ -102,8 +102,10 @@ def set_closure_mode(mode: int) -> None:
 
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
     """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1, 3 or 4;
-    sizes above every entry run mode 1. An empty table clears it. autotune.tune_closure
-    measures the modes per size bucket and installs its winners through this."""
+    sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
+    the library starts with the table measured on B200, {1024: 4, 12288: 3}).
+    autotune.tune_closure measures the modes per size bucket and installs its winners through
+    this."""
     n = len(table)
     max_c = (ctypes.c_int * max(n, 1))(*[int(c) for c, _ in table])
     modes = (ctypes.c_int * max(n, 1))(*[int(m) for _, m in table])

@@ -224,106 +224,62 @@ __device__ __forceinline__ uint4 load4_u32(const uint32_t* X, int64_t ld, int C,
                       c0 + 3 < C ? __ldg(p + 3) : 0u);
 }
 
-// Both kernels below are persistent over the batch's tile pairs: a few CTAs per SM, each taking
-// pairs b, b + gridDim.x, ... and loading the next pair's cells into registers while the
-// current pair is compared and stored, so loads stay in flight between pairs.
-constexpr int kPairCtasPerSm = 2;
-
-// The pair's election and geometry.
-struct PairRef {
-    const Elec* E;
-    PairGeom g;
-    int64_t local;
-};
-
-__device__ __forceinline__ PairRef pair_ref(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
-                                            const int64_t* __restrict__ prefix, int nbig, int64_t b) {
-    PairRef r;
-    const int m = find_owner(prefix, nbig, b);
-    r.E = &elecs[big[m]];
-    r.local = b - prefix[m];
-    r.g = pair_geom(r.local, r.E->Cp);
-    return r;
-}
-
 // Defeat matrix into the padded working matrix (see init_kernel in closure.cu): S[i][j] =
 // d[i][j] if d[i][j] > d[j][i], else 0, for both tiles of the pair (on the diagonal d[i][i] >
 // d[i][i] is false, and cells past C read 0, so the padding comes out 0). Also zeroes the
 // election's wins.
-__device__ __forceinline__ void init_loads(const PairRef& P, uint4 (&a)[4], uint4 (&bt)[4]) {
-    const Elec& E = *P.E;
+__global__ void __launch_bounds__(256)
+    batch_init_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big, const int64_t* __restrict__ prefix,
+                      int nbig, Header* __restrict__ hdr) {
+    __shared__ __align__(16) uint32_t sa[kPT * kPT], sb[kPT * kPT];
+    const int64_t b = blockIdx.x;
+    const int m = find_owner(prefix, nbig, b);
+    const Elec& E = elecs[big[m]];
+    const int64_t local = b - prefix[m];
+    const int C = E.C, Cp = E.Cp;
+    const PairGeom g = pair_geom(local, Cp);
+    if (local == 0 && E.wins)
+        for (int x = threadIdx.x; x < C; x += 256) E.wins[x] = 0;
     const bool vec = E.ld % 4 == 0 && (reinterpret_cast<uintptr_t>(E.d) & 15) == 0;
+    uint4 a[4], bt[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        const int r = P.g.ry + 16 * p;
-        a[p] = load4_u32(E.d, E.ld, E.C, P.g.i0 + r, P.g.j0 + 4 * P.g.cx, vec);
-        bt[p] = load4_u32(E.d, E.ld, E.C, P.g.j0 + r, P.g.i0 + 4 * P.g.cx, vec);
+        const int r = g.ry + 16 * p;
+        a[p] = load4_u32(E.d, E.ld, C, g.i0 + r, g.j0 + 4 * g.cx, vec);
+        bt[p] = load4_u32(E.d, E.ld, C, g.j0 + r, g.i0 + 4 * g.cx, vec);
+        swz64_store4(sa, r, 4 * g.cx, a[p]);
+        swz64_store4(sb, r, 4 * g.cx, bt[p]);
     }
-}
-
-__global__ void __launch_bounds__(256, kPairCtasPerSm)
-    batch_init_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big, const int64_t* __restrict__ prefix,
-                      int nbig, int64_t total, Header* __restrict__ hdr) {
-    __shared__ __align__(16) uint32_t sa[kPT * kPT], sb[kPT * kPT];
-    int64_t b = blockIdx.x;
-    if (b >= total) return;
-    PairRef P = pair_ref(elecs, big, prefix, nbig, b);
-    uint4 a[4], bt[4];
-    init_loads(P, a, bt);
+    __syncthreads();
+    const bool u16 = E.lanes == 16;
     bool over = false;
-    for (;;) {
-        const Elec& E = *P.E;
-        const PairGeom g = P.g;
-        if (P.local == 0 && E.wins)
-            for (int x = threadIdx.x; x < E.C; x += 256) E.wins[x] = 0;
+    // One side: cells (x0 + r, y0 + 4cx + q) from own[] against their transposed partners in
+    // the other tile's staging.
+    auto emit = [&](const uint4* own, const uint32_t* other, int x0, int y0) {
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            swz64_store4(sa, g.ry + 16 * p, 4 * g.cx, a[p]);
-            swz64_store4(sb, g.ry + 16 * p, 4 * g.cx, bt[p]);
-        }
-        const uint4 a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], b0 = bt[0], b1 = bt[1], b2 = bt[2], b3 = bt[3];
-        const uint4 own_a[4] = {a0, a1, a2, a3}, own_b[4] = {b0, b1, b2, b3};
-        __syncthreads();
-        const int64_t nb = b + gridDim.x;
-        PairRef Pn = P;
-        if (nb < total) {  // the next pair's loads, in flight while this pair is written
-            Pn = pair_ref(elecs, big, prefix, nbig, nb);
-            init_loads(Pn, a, bt);
-        }
-        const bool u16 = E.lanes == 16;
-        const int Cp = E.Cp;
-        // One side: cells (x0 + r, y0 + 4cx + q) from own[] against their transposed partners
-        // in the other tile's staging.
-        auto emit = [&](const uint4* own, const uint32_t* other, int x0, int y0) {
+            const int r = g.ry + 16 * p;
+            const uint32_t x[4] = {own[p].x, own[p].y, own[p].z, own[p].w};
+            uint32_t v[4];
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const int r = g.ry + 16 * p;
-                const uint32_t x[4] = {own[p].x, own[p].y, own[p].z, own[p].w};
-                uint32_t v[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t y = other[swz64(4 * g.cx + q, r)];
-                    v[q] = x[q] > y ? x[q] : 0u;
-                }
-                const int64_t at = int64_t(x0 + r) * Cp + y0 + 4 * g.cx;
-                if (u16) {
-                    uint32_t h[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) h[q] = to_lane16(v[q], E.base, over);
-                    *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(E.S) + at) =
-                        make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
-                } else {
-                    *reinterpret_cast<uint4*>(E.S + at) = make_uint4(v[0], v[1], v[2], v[3]);
-                }
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t y = other[swz64(4 * g.cx + q, r)];
+                v[q] = x[q] > y ? x[q] : 0u;
             }
-        };
-        emit(own_a, sb, g.i0, g.j0);
-        if (g.I != g.J) emit(own_b, sa, g.j0, g.i0);
-        if (nb >= total) break;
-        __syncthreads();  // the staging is read before the next pair rewrites it
-        b = nb;
-        P = Pn;
-    }
+            const int64_t at = int64_t(x0 + r) * Cp + y0 + 4 * g.cx;
+            if (u16) {
+                uint32_t h[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) h[q] = to_lane16(v[q], E.base, over);
+                *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(E.S) + at) =
+                    make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+            } else {
+                *reinterpret_cast<uint4*>(E.S + at) = make_uint4(v[0], v[1], v[2], v[3]);
+            }
+        }
+    };
+    emit(a, sb, g.i0, g.j0);
+    if (g.I != g.J) emit(bt, sa, g.j0, g.i0);
     if (over) raise_device_error(&hdr->err, kErrOverflow);
 }
 
@@ -331,9 +287,16 @@ __global__ void __launch_bounds__(256, kPairCtasPerSm)
 // working matrix (u16 lanes store v - base); wins compare the widened values, as the
 // single-election ranking does. On a diagonal pair every ordered pair of the block is in the
 // tile, so only row wins are counted there.
-__device__ __forceinline__ void finalize_loads(const PairRef& P, uint4 (&a)[4], uint4 (&bt)[4]) {
-    const Elec& E = *P.E;
-    const int Cp = E.Cp;
+__global__ void __launch_bounds__(256)
+    batch_finalize_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
+                          const int64_t* __restrict__ prefix, int nbig) {
+    __shared__ __align__(16) uint32_t sb[kPT * kPT];  // X[J][I] staged: the transposed partners of a[]
+    __shared__ int32_t colpart[16][kPT];
+    const int64_t b = blockIdx.x;
+    const int m = find_owner(prefix, nbig, b);
+    const Elec& E = elecs[big[m]];
+    const int C = E.C, Cp = E.Cp;
+    const PairGeom g = pair_geom(b - prefix[m], Cp);
     const bool u16 = E.lanes == 16;
     auto load = [&](int row, int c0) -> uint4 {  // the working matrix covers Cp x Cp: no bounds
         const int64_t at = int64_t(row) * Cp + c0;
@@ -345,93 +308,62 @@ __device__ __forceinline__ void finalize_loads(const PairRef& P, uint4 (&a)[4], 
         }
         return __ldg(reinterpret_cast<const uint4*>(E.S + at));
     };
+    uint4 a[4], bt[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        const int r = P.g.ry + 16 * p;
-        a[p] = load(P.g.i0 + r, P.g.j0 + 4 * P.g.cx);
-        bt[p] = load(P.g.j0 + r, P.g.i0 + 4 * P.g.cx);
+        const int r = g.ry + 16 * p;
+        a[p] = load(g.i0 + r, g.j0 + 4 * g.cx);
+        bt[p] = load(g.j0 + r, g.i0 + 4 * g.cx);
+        swz64_store4(sb, r, 4 * g.cx, bt[p]);
     }
-}
-
-__global__ void __launch_bounds__(256, kPairCtasPerSm)
-    batch_finalize_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
-                          const int64_t* __restrict__ prefix, int nbig, int64_t total) {
-    __shared__ __align__(16) uint32_t sb[kPT * kPT];  // X[J][I] staged: the transposed partners of a[]
-    __shared__ int32_t colpart[16][kPT];
-    int64_t b = blockIdx.x;
-    if (b >= total) return;
-    PairRef P = pair_ref(elecs, big, prefix, nbig, b);
-    uint4 a[4], bt[4];
-    finalize_loads(P, a, bt);
-    for (;;) {
-        const Elec& E = *P.E;
-        const PairGeom g = P.g;
-        const int C = E.C;
+    auto store = [&](const uint4* own, int x0, int y0) {
 #pragma unroll
-        for (int p = 0; p < 4; ++p) swz64_store4(sb, g.ry + 16 * p, 4 * g.cx, bt[p]);
-        const uint4 a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], b0 = bt[0], b1 = bt[1], b2 = bt[2], b3 = bt[3];
-        const uint4 own_a[4] = {a0, a1, a2, a3}, own_b[4] = {b0, b1, b2, b3};
-        const int64_t nb = b + gridDim.x;
-        PairRef Pn = P;
-        if (nb < total) {  // the next pair's loads, in flight while this pair is written
-            Pn = pair_ref(elecs, big, prefix, nbig, nb);
-            finalize_loads(Pn, a, bt);
-        }
-        auto store = [&](const uint4* own, int x0, int y0) {
+        for (int p = 0; p < 4; ++p) {
+            const int i = x0 + g.ry + 16 * p;
+            if (i >= C) continue;
+            const uint32_t x[4] = {own[p].x, own[p].y, own[p].z, own[p].w};
+            uint32_t* row = E.out + int64_t(i) * E.ld_out;
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const int i = x0 + g.ry + 16 * p;
-                if (i >= C) continue;
-                const uint32_t x[4] = {own[p].x, own[p].y, own[p].z, own[p].w};
-                uint32_t* row = E.out + int64_t(i) * E.ld_out;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = y0 + 4 * g.cx + q;
-                    if (j < C) row[j] = i == j ? 0u : x[q];
-                }
-            }
-        };
-        store(own_a, g.i0, g.j0);
-        if (g.I != g.J) store(own_b, g.j0, g.i0);
-        __syncthreads();  // sb complete
-        if (E.wins != nullptr) {  // election-uniform, so CTA-uniform
-            uint32_t rw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const int r = g.ry + 16 * p;
-                const uint32_t x[4] = {own_a[p].x, own_a[p].y, own_a[p].z, own_a[p].w};
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t y = sb[swz64(4 * g.cx + q, r)];  // S[j][i] for (i, j) = (i0 + r, j0 + 4cx + q)
-                    rw[p] += x[q] > y;
-                    cw[q] += y > x[q];
-                }
-            }
-#pragma unroll
-            for (int p = 0; p < 4; ++p)
-#pragma unroll
-                for (int msk = 8; msk >= 1; msk >>= 1) rw[p] += __shfl_xor_sync(0xFFFFFFFFu, rw[p], msk);
-            if (g.cx < 4) {  // lane cx of the half warp adds row ry + 16 cx
-                const uint32_t n = g.cx == 0 ? rw[0] : g.cx == 1 ? rw[1] : g.cx == 2 ? rw[2] : rw[3];
-                const int i = g.i0 + g.ry + 16 * g.cx;
-                if (n && i < C) atomicAdd(&E.wins[i], int(n));
-            }
-            if (g.I != g.J) {  // CTA-uniform
-#pragma unroll
-                for (int q = 0; q < 4; ++q) colpart[g.ry][4 * g.cx + q] = int(cw[q]);
-                __syncthreads();
-                if (threadIdx.x < kPT) {
-                    int n = 0;
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) n += colpart[r][threadIdx.x];
-                    if (n && g.j0 + int(threadIdx.x) < C) atomicAdd(&E.wins[g.j0 + threadIdx.x], n);
-                }
+            for (int q = 0; q < 4; ++q) {
+                const int j = y0 + 4 * g.cx + q;
+                if (j < C) row[j] = i == j ? 0u : x[q];
             }
         }
-        if (nb >= total) break;
-        __syncthreads();  // sb and colpart are read before the next pair rewrites them
-        b = nb;
-        P = Pn;
+    };
+    store(a, g.i0, g.j0);
+    if (g.I != g.J) store(bt, g.j0, g.i0);
+    if (E.wins == nullptr) return;  // election-uniform
+    __syncthreads();
+    uint32_t rw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int r = g.ry + 16 * p;
+        const uint32_t x[4] = {a[p].x, a[p].y, a[p].z, a[p].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t y = sb[swz64(4 * g.cx + q, r)];  // S[j][i] for (i, j) = (i0 + r, j0 + 4cx + q)
+            rw[p] += x[q] > y;
+            cw[q] += y > x[q];
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int msk = 8; msk >= 1; msk >>= 1) rw[p] += __shfl_xor_sync(0xFFFFFFFFu, rw[p], msk);
+    if (g.cx < 4) {  // lane cx of the half warp adds row ry + 16 cx
+        const uint32_t n = g.cx == 0 ? rw[0] : g.cx == 1 ? rw[1] : g.cx == 2 ? rw[2] : rw[3];
+        const int i = g.i0 + g.ry + 16 * g.cx;
+        if (n && i < C) atomicAdd(&E.wins[i], int(n));
+    }
+    if (g.I == g.J) return;  // CTA-uniform
+#pragma unroll
+    for (int q = 0; q < 4; ++q) colpart[g.ry][4 * g.cx + q] = int(cw[q]);
+    __syncthreads();
+    if (threadIdx.x < kPT) {
+        int n = 0;
+#pragma unroll
+        for (int r = 0; r < 16; ++r) n += colpart[r][threadIdx.x];
+        if (n && g.j0 + int(threadIdx.x) < C) atomicAdd(&E.wins[g.j0 + threadIdx.x], n);
     }
 }
 
@@ -475,7 +407,6 @@ struct Plan {
     int32_t grid[2];
     cudaGraphExec_t graph;
     uint64_t dep_wait_ns;  // limit of one dependency wait of the persistent kernel
-    int64_t pair_grid;     // CTAs of the persistent init and output kernels
 };
 static_assert(sizeof(Plan) <= sizeof(se_batch_plan_t), "se_batch_plan_t too small");
 
@@ -572,8 +503,8 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
     SE_CUDA_TRY(cudaMemsetAsync(P.work, 0, 256, s));
     if (P.counters_bytes) SE_CUDA_TRY(cudaMemsetAsync(P.work + P.counters_off, 0, size_t(P.counters_bytes), s));
     if (P.nbig) {
-        batch_init_kernel<<<unsigned(std::min<int64_t>(P.init_blocks, P.pair_grid)), 256, 0, s>>>(
-            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.init_prefix_off), P.nbig, P.init_blocks, hdr);
+        batch_init_kernel<<<unsigned(P.init_blocks), 256, 0, s>>>(
+            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.init_prefix_off), P.nbig, hdr);
         SE_CHECK_LAUNCH();
     }
     if (P.ntasks[0]) {
@@ -587,8 +518,8 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
         SE_CHECK_LAUNCH();
     }
     if (P.nbig) {
-        batch_finalize_kernel<<<unsigned(std::min<int64_t>(P.fin_blocks, P.pair_grid)), 256, 0, s>>>(
-            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.fin_prefix_off), P.nbig, P.fin_blocks);
+        batch_finalize_kernel<<<unsigned(P.fin_blocks), 256, 0, s>>>(
+            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.fin_prefix_off), P.nbig);
         SE_CHECK_LAUNCH();
         batch_place_kernel<<<unsigned(P.place_blocks), 256, 0, s>>>(
             elecs, big, reinterpret_cast<const int64_t*>(P.work + P.place_prefix_off), P.nbig);
@@ -763,7 +694,6 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * per32));
     P.graph = nullptr;
     P.dep_wait_ns = kDepWaitNs;
-    P.pair_grid = int64_t(sms) * kPairCtasPerSm;
     std::memcpy(plan_out, &P, sizeof(P));
     return SE_OK;
 }

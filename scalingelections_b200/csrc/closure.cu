@@ -550,12 +550,16 @@ layout plan(int C, int lane_bits) {
 // claim-and-poll overhead at every size measured.
 std::atomic<int> g_closure_mode{0};
 
-// The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds).
+// The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds). The
+// built-in table is autotune.tune_closure's result on one B200 (16-bit lanes, ms per closure,
+// modes 1 / 3 / 4): C = 1024 0.766 / 0.728 / 0.688, C = 2048 1.486 / 1.449 / 1.538,
+// C = 4096 4.000 / 3.921 / 5.194, C = 8192 25.11 / 24.97 / 27.54, C = 12288 82.67 / 82.48 /
+// 86.34, C = 16384 191.5 / 191.7 / 196.3.
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
-int g_variant_n = 0;
-int g_variant_max_c[kMaxVariants];
-int g_variant_mode[kMaxVariants];
+int g_variant_n = 2;
+int g_variant_max_c[kMaxVariants] = {1024, 12288};
+int g_variant_mode[kMaxVariants] = {4, 3};
 
 int automatic_mode(int C) {
     std::lock_guard<std::mutex> lock(g_variant_mutex);

@@ -67,6 +67,8 @@ def test_closure_schedule_settings_need_no_gpu():
     assert L.se_closure_set_mode(5) == _lib.SE_ERR_INVALID
     for mode in (4, 0):
         assert L.se_closure_set_mode(mode) == _lib.SE_OK
+    builtin = ((ctypes.c_int * 2)(1024, 12288), (ctypes.c_int * 2)(4, 3))  # put the built-in table back
+    assert L.se_closure_set_variant_table(builtin[0], builtin[1], 2) == _lib.SE_OK
 
 
 HOST_ALLOC_FAILURE = r"""
