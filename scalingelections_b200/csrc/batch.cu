@@ -224,18 +224,25 @@ __device__ __forceinline__ uint4 load4_u32(const uint32_t* X, int64_t ld, int C,
                       c0 + 3 < C ? __ldg(p + 3) : 0u);
 }
 
+// Resident CTAs per SM the init and output kernels are compiled for (registers): more CTAs keep
+// more tile loads in flight.
+constexpr int kPairCtasPerSm = 5;
+
+// Block b of the init and output kernels works on pair `local` of election `e`.
+struct PairOwner {
+    int32_t e, local;
+};
+
 // Defeat matrix into the padded working matrix (see init_kernel in closure.cu): S[i][j] =
 // d[i][j] if d[i][j] > d[j][i], else 0, for both tiles of the pair (on the diagonal d[i][i] >
 // d[i][i] is false, and cells past C read 0, so the padding comes out 0). Also zeroes the
 // election's wins.
-__global__ void __launch_bounds__(256)
-    batch_init_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big, const int64_t* __restrict__ prefix,
-                      int nbig, Header* __restrict__ hdr) {
+__global__ void __launch_bounds__(256, kPairCtasPerSm)
+    batch_init_kernel(const Elec* __restrict__ elecs, const PairOwner* __restrict__ owner, Header* __restrict__ hdr) {
     __shared__ __align__(16) uint32_t sa[kPT * kPT], sb[kPT * kPT];
-    const int64_t b = blockIdx.x;
-    const int m = find_owner(prefix, nbig, b);
-    const Elec& E = elecs[big[m]];
-    const int64_t local = b - prefix[m];
+    const PairOwner o = owner[blockIdx.x];
+    const Elec& E = elecs[o.e];
+    const int64_t local = o.local;
     const int C = E.C, Cp = E.Cp;
     const PairGeom g = pair_geom(local, Cp);
     if (local == 0 && E.wins)
@@ -287,16 +294,14 @@ __global__ void __launch_bounds__(256)
 // working matrix (u16 lanes store v - base); wins compare the widened values, as the
 // single-election ranking does. On a diagonal pair every ordered pair of the block is in the
 // tile, so only row wins are counted there.
-__global__ void __launch_bounds__(256)
-    batch_finalize_kernel(const Elec* __restrict__ elecs, const int32_t* __restrict__ big,
-                          const int64_t* __restrict__ prefix, int nbig) {
+__global__ void __launch_bounds__(256, kPairCtasPerSm)
+    batch_finalize_kernel(const Elec* __restrict__ elecs, const PairOwner* __restrict__ owner) {
     __shared__ __align__(16) uint32_t sb[kPT * kPT];  // X[J][I] staged: the transposed partners of a[]
     __shared__ int32_t colpart[16][kPT];
-    const int64_t b = blockIdx.x;
-    const int m = find_owner(prefix, nbig, b);
-    const Elec& E = elecs[big[m]];
+    const PairOwner o = owner[blockIdx.x];
+    const Elec& E = elecs[o.e];
     const int C = E.C, Cp = E.Cp;
-    const PairGeom g = pair_geom(b - prefix[m], Cp);
+    const PairGeom g = pair_geom(o.local, Cp);
     const bool u16 = E.lanes == 16;
     auto load = [&](int row, int c0) -> uint4 {  // the working matrix covers Cp x Cp: no bounds
         const int64_t at = int64_t(row) * Cp + c0;
@@ -407,6 +412,7 @@ struct Plan {
     int32_t grid[2];
     cudaGraphExec_t graph;
     uint64_t dep_wait_ns;  // limit of one dependency wait of the persistent kernel
+    int64_t pair_owner_off;  // PairOwner per block of the init and output kernels
 };
 static_assert(sizeof(Plan) <= sizeof(se_batch_plan_t), "se_batch_plan_t too small");
 
@@ -414,7 +420,7 @@ int64_t align256(int64_t x) { return round_up(x, 256); }
 
 struct Sizes {
     int64_t total = 0, elec_off, big_off, init_prefix_off, fin_prefix_off, place_prefix_off, counters_off,
-            counters_bytes, tasks_off[2];
+            counters_bytes, tasks_off[2], pair_owner_off, pairs = 0;
     std::vector<int64_t> s_off, at_off, dt_off, ctr_off;
     std::vector<int> lanes, R, Cp;
     int nbig = 0, nsmall = 0;
@@ -458,6 +464,8 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
         off = align256(off + int64_t(kT) * kT * 4);
         const uint64_t R = uint64_t(z.R[e]);
         z.ntasks[z.lanes[e] == 16 ? 0 : 1] += uint32_t(R * R * R);
+        const int64_t nt = z.Cp[e] / kPT;
+        z.pairs += nt * (nt + 1) / 2;
     }
     z.counters_off = off;
     int64_t ctr = 0;
@@ -476,6 +484,8 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
     off = align256(off + int64_t(z.nbig + 1) * 8);
     z.place_prefix_off = off;
     off = align256(off + int64_t(z.nbig + 1) * 8);
+    z.pair_owner_off = off;
+    off = align256(off + z.pairs * 8);
     for (int q = 0; q < 2; ++q) {
         z.tasks_off[q] = off;
         off = align256(off + int64_t(z.ntasks[q]) * 8);
@@ -504,7 +514,7 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
     if (P.counters_bytes) SE_CUDA_TRY(cudaMemsetAsync(P.work + P.counters_off, 0, size_t(P.counters_bytes), s));
     if (P.nbig) {
         batch_init_kernel<<<unsigned(P.init_blocks), 256, 0, s>>>(
-            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.init_prefix_off), P.nbig, hdr);
+            elecs, reinterpret_cast<const PairOwner*>(P.work + P.pair_owner_off), hdr);
         SE_CHECK_LAUNCH();
     }
     if (P.ntasks[0]) {
@@ -519,7 +529,7 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
     }
     if (P.nbig) {
         batch_finalize_kernel<<<unsigned(P.fin_blocks), 256, 0, s>>>(
-            elecs, big, reinterpret_cast<const int64_t*>(P.work + P.fin_prefix_off), P.nbig);
+            elecs, reinterpret_cast<const PairOwner*>(P.work + P.pair_owner_off));
         SE_CHECK_LAUNCH();
         batch_place_kernel<<<unsigned(P.place_blocks), 256, 0, s>>>(
             elecs, big, reinterpret_cast<const int64_t*>(P.work + P.place_prefix_off), P.nbig);
@@ -639,15 +649,21 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     for (int l = 0; l < 2; ++l)
         SE_REQUIRE(q[l].size() == z.ntasks[l], SE_ERR_INVALID, "internal: task count mismatch");
 
-    // Block prefixes of the batched elementwise kernels.
+    // Block prefixes of the batched elementwise kernels, and for init and finalize (one CTA per
+    // pair of 64 x 64 tiles) each block's election and pair, so a CTA finds its work with one
+    // load instead of a binary search over the prefixes.
     std::vector<int64_t> ip(big.size() + 1, 0), fp(big.size() + 1, 0), pp(big.size() + 1, 0);
+    std::vector<PairOwner> owner;
+    owner.reserve(size_t(z.pairs));
     for (size_t m = 0; m < big.size(); ++m) {
         const Elec& E = host[big[m]];
-        const int64_t nt = E.Cp / kPT;  // init and finalize take one CTA per pair of 64 x 64 tiles
+        const int64_t nt = E.Cp / kPT;
         ip[m + 1] = ip[m] + nt * (nt + 1) / 2;
         fp[m + 1] = fp[m] + nt * (nt + 1) / 2;
         pp[m + 1] = pp[m] + (E.C + 255) / 256;
+        for (int64_t l = 0; l < nt * (nt + 1) / 2; ++l) owner.push_back(PairOwner{big[m], int32_t(l)});
     }
+    SE_REQUIRE(int64_t(owner.size()) == z.pairs, SE_ERR_INVALID, "internal: pair count mismatch");
     // Upload (synchronous).
     SE_CUDA_TRY(cudaMemset(work, 0, 256));
     if (n) SE_CUDA_TRY(cudaMemcpy(work + z.elec_off, host.data(), sizeof(Elec) * size_t(n), cudaMemcpyHostToDevice));
@@ -656,6 +672,8 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
         SE_CUDA_TRY(cudaMemcpy(work + z.init_prefix_off, ip.data(), 8 * ip.size(), cudaMemcpyHostToDevice));
         SE_CUDA_TRY(cudaMemcpy(work + z.fin_prefix_off, fp.data(), 8 * fp.size(), cudaMemcpyHostToDevice));
         SE_CUDA_TRY(cudaMemcpy(work + z.place_prefix_off, pp.data(), 8 * pp.size(), cudaMemcpyHostToDevice));
+        SE_CUDA_TRY(cudaMemcpy(work + z.pair_owner_off, owner.data(), sizeof(PairOwner) * owner.size(),
+                               cudaMemcpyHostToDevice));
     }
     for (int l = 0; l < 2; ++l)
         if (!q[l].empty())
@@ -676,6 +694,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     P.init_prefix_off = z.init_prefix_off;
     P.fin_prefix_off = z.fin_prefix_off;
     P.place_prefix_off = z.place_prefix_off;
+    P.pair_owner_off = z.pair_owner_off;
     P.counters_off = z.counters_off;
     P.counters_bytes = z.counters_bytes;
     for (int l = 0; l < 2; ++l) {
