@@ -53,8 +53,9 @@ def parse():
                     help="closure input: tallied Mallows ballots, or the reference's random matrix mode")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
-    ap.add_argument("--closure-mode", type=int, default=1, choices=[1, 2],
-                    help="1: round by round (default), 2: dataflow")
+    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+                    help="the closure's schedule: 0 automatic by size (default), 1 round by round, 2 dataflow, "
+                         "3 wide panels, 4 wide panels and pivot launches, 5 two streams (include/se.h)")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--cpu-full-size", action="store_true",
                     help="reference arm: also time one closure at the workload's full size (minutes)")
@@ -102,7 +103,8 @@ def config(args, world):
         "voters": args.voters,
         "phi": args.phi,
         "lanes": f"u{args.lanes}" if args.lanes else "auto",
-        "closure_mode": {1: "round by round", 2: "dataflow"}[args.closure_mode],
+        "closure_mode": {0: "automatic by size", 1: "round by round", 2: "dataflow", 3: "wide panels",
+                         4: "wide panels and pivots", 5: "two streams"}[args.closure_mode],
         "tile": 128,
         "parallelism": f"replicas{world}" if world > 1 else "single",
         "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
@@ -289,7 +291,7 @@ def run_ours(args, world, rank, local_rank):
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
     api.set_closure_mode(args.closure_mode)
-    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode == 2)
+    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode in (0, 2, 5))
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()

@@ -130,12 +130,18 @@ SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, in
  *      first CTA of the remainder launch;
  *   2  dataflow: one persistent launch (needs se_closure_workspace_bytes_flow() of workspace);
  *   3  as 1 with the panels on the wide micro-tile (8 x 4 words per thread, twice the warps);
- *   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile.
+ *   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile;
+ *   5  as 3 on two streams: each round's remainder tiles of the next pivot row and column, and
+ *      the next round's panels, run on `stream` while the rest of the round's remainder runs
+ *      on a second, lower-priority stream of the library's (joined before the call's last
+ *      launch), so the next round's chain overlaps the current round's bulk. Needs
+ *      se_closure_workspace_bytes_flow() of workspace and C > 384 (else it runs 3); the
+ *      automatic schedule picks it only when the workspace is that large.
  * 3 and 4 differ from 1 in 16-bit lanes only. */
 SE_API se_status_t se_closure_set_mode(int mode);
 
 /* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
- * modes[i] (1, 3 or 4); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
+ * modes[i] (1, 3, 4 or 5); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
  * table, measured on B200, is {C <= 1024: 4, C <= 12288: 3}. An autotuner
  * measures the variants per size bucket and installs the winners (scalingelections_b200
  * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks

@@ -94,14 +94,15 @@ _closure_mode = 0
 def set_closure_mode(mode: int) -> None:
     """The closure's schedule (same results in every one): 0 automatic by size (default),
     1 round by round, 2 the dataflow form, 3 round by round with the panels on the wide
-    micro-tile, 4 as 3 with each pivot tile closed by its own wide launch (include/se.h)."""
+    micro-tile, 4 as 3 with each pivot tile closed by its own wide launch, 5 as 3 on two
+    streams so the next round's chain overlaps the current remainder (include/se.h)."""
     global _closure_mode
     check(_lib.lib().se_closure_set_mode(int(mode)))
     _closure_mode = int(mode)
 
 
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
-    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1, 3 or 4;
+    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1, 3, 4 or 5;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
     the library starts with the table measured on B200, {1024: 4, 12288: 3}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
@@ -127,7 +128,9 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         raise ValueError("out has the wrong shape")
     if C == 0:
         return out
-    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode == 2)
+    # The dataflow (2) and two-stream (5) schedules, which the automatic one (0) may pick, use
+    # a second AT buffer: a few MiB more than the plain workspace.
+    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5))
     if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = _workspace(need, preferences.device)
     have = workspace.numel() * workspace.element_size()

@@ -6,7 +6,9 @@ table (se_closure_set_variant_table), which the automatic schedule reads:
   1  panels and pivots on the default micro-tile (8 x 8 words per thread, four warps in
      16-bit lanes), the next pivot fused into the remainder launch;
   3  panels on the wide micro-tile (8 x 4 words per thread, eight warps);
-  4  as 3, and every pivot tile closed by its own launch on the wide micro-tile.
+  4  as 3, and every pivot tile closed by its own launch on the wide micro-tile;
+  5  as 3 on two streams: the next round's pivot row and column, pivot and panels overlap
+     the current round's remaining remainder tiles.
 The schedules differ where the per-round chain (pivot, then panels) is not hidden behind the
 remainder: small and medium C.
 
@@ -120,7 +122,7 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
 
 
 CLOSURE_BUCKETS = [1024, 2048, 3072, 4096, 6144, 8192, 12288]  # upper bounds of the size buckets
-CLOSURE_MODES = (1, 3, 4)
+CLOSURE_MODES = (1, 3, 4, 5)
 
 
 def tune_closure(sizes: Sequence[int] | None = None, reps: int = 5, V: int = 4096, seed: int = 0,
@@ -138,7 +140,8 @@ def tune_closure(sizes: Sequence[int] | None = None, reps: int = 5, V: int = 409
     try:
         for n, C in enumerate(sizes):
             d = _sample_batch(C, C, 1, V, seed + n, device)[0]
-            work = torch.empty(api.closure_workspace_bytes(C, LANES_U16), dtype=torch.uint8, device=device)
+            work = torch.empty(api.closure_workspace_bytes(C, LANES_U16, dataflow=True), dtype=torch.uint8,
+                               device=device)
             res = torch.empty_like(d)
             times = {}
             for mode in CLOSURE_MODES:

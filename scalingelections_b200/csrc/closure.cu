@@ -79,9 +79,12 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
 // round's pivot tile (and emits dT) while the other blocks continue: the next round needs no
 // separate pivot launch. Nothing else in this launch reads that tile or dT.
 // ------------------------------------------------------------------------------------------
+// subset 0: all (R-1)^2 tiles of the round. subset 1: the tiles of row and column K+1 (2R - 3,
+// tile (K+1, K+1) first); subset 2: every other tile ((R-2)^2). The two-stream schedule runs
+// subset 1 and the next round's panels on the caller's stream while subset 2 runs on another.
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
-    rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, uint32_t* __restrict__ err) {
+    rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, int subset, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
@@ -92,16 +95,33 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         fence_barrier_init();
     }
     __syncthreads();
-    const int R1 = E.R - 1;
-    int t = blockIdx.x;
-    if (fuse_pivot) {
-        const int p = K * R1 + K;  // reduced coordinates of tile (K+1, K+1)
-        t = t == 0 ? p : (t == p ? 0 : t);
+    const int R1 = E.R - 1, R2 = E.R - 2;
+    int t = blockIdx.x, I, J;
+    auto skip_k_k1 = [K](int n) { return n < K ? n : n + 2; };  // n-th block index other than K, K+1
+    if (subset == 0) {
+        if (fuse_pivot) {
+            const int p = K * R1 + K;  // reduced coordinates of tile (K+1, K+1)
+            t = t == 0 ? p : (t == p ? 0 : t);
+        }
+        const int ii = t / R1, jj = t % R1;
+        I = ii + (ii >= K);
+        J = jj + (jj >= K);
+    } else if (subset == 1) {
+        if (t == 0) {
+            I = J = K + 1;
+        } else if (t <= R2) {
+            I = K + 1;
+            J = skip_k_k1(t - 1);
+        } else {
+            I = skip_k_k1(t - 1 - R2);
+            J = K + 1;
+        }
+    } else {
+        I = skip_k_k1(t / R2);
+        J = skip_k_k1(t % R2);
     }
-    const int ii = t / R1, jj = t % R1;
     uint32_t par_a = 0, par_b = 0;
-    const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, ii + (ii >= K), jj + (jj >= K), smem, bars,
-                                               par_a, par_b);
+    const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
@@ -544,8 +564,13 @@ layout plan(int C, int lane_bits) {
 //   2  dataflow: one persistent grid (needs se_closure_workspace_bytes_flow() of workspace);
 //   3  as 1 with the panels on the wide micro-tile (8 x 4 words, 256 threads; 16-bit lanes);
 //   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile, after the
-//      whole remainder launch, instead of fused into its first CTA.
-// 3 and 4 apply to 16-bit lanes; 32-bit lanes run 1 for them. Round by round is the default:
+//      whole remainder launch, instead of fused into its first CTA;
+//   5  as 3 on two streams: round k's remainder tiles of row and column k+1 (with the fused
+//      pivot) and round k+1's panels run on the caller's stream while the rest of round k's
+//      remainder runs on a lower-priority second stream, so the next round's chain overlaps
+//      the current round's bulk. AT is double-buffered (the dataflow layout's second buffer):
+//      needs se_closure_workspace_bytes_flow() of workspace, and R >= 4.
+// 3 and 4 apply to 16-bit lanes; 32-bit lanes run 1 for them (5 without the wide panels). Round by round is the default:
 // on B200 hardware block scheduling of one launch per phase beats the persistent grid's
 // claim-and-poll overhead at every size measured.
 std::atomic<int> g_closure_mode{0};
@@ -586,6 +611,93 @@ template <int LB> se_status_t set_smem_limits() {
 // 4; see g_closure_mode). phase_ms (optional, 4 entries): accumulated device time of the pivot
 // launches, the panel launches, (unused) and the remainder launches, from events recorded
 // between launches.
+// The second stream of the two-stream schedule, one per device, at the lowest priority so that
+// the caller's stream (the per-round chain) gets SMs first.
+se_status_t side_stream(cudaStream_t* out) {
+    constexpr int kMaxDev = 64;
+    static std::mutex m;
+    static cudaStream_t streams[kMaxDev] = {};
+    int dev = 0;
+    SE_CUDA_TRY(cudaGetDevice(&dev));
+    SE_REQUIRE(dev >= 0 && dev < kMaxDev, SE_ERR_INVALID, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(m);
+    if (!streams[dev]) {
+        int least = 0, greatest = 0;
+        SE_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SE_CUDA_TRY(cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, least));
+    }
+    *out = streams[dev];
+    return SE_OK;
+}
+
+// Schedule 5 (see g_closure_mode). Per round k < R-1, with A the caller's stream and B the side
+// stream, and E[k % 2] the descriptor whose AT buffer round k uses:
+//   B: wait panels(k); remainder(k) off rows and columns k, k+1; record remB[k]
+//   A: wait remB[k-1]; remainder(k) of row and column k+1, tile (k+1, k+1) first and closed as
+//      the next pivot; panels(k+1) into the other AT buffer; record panels[k+1]
+// then the last round's whole remainder on A after remB[R-2]. Reads and writes that could meet:
+// panels(k+1) writes AT[(k+1) % 2] while remainder(k) reads AT[k % 2]; it writes rows and
+// columns k+1, which no tile of B's remainder(k) reads or writes; remainder(k+1) of row and
+// column k+2 waits for all of remainder(k) (it rewrites tiles of row k that remainder(k)
+// reads); B's remainder(k+1) follows B's remainder(k) on B and waits for panels(k+1), which
+// follows A's remainder(k) on A.
+template <int LB>
+se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, uint32_t* S, int64_t ldw,
+                            uint32_t* dT, uint32_t* err, double* phase_ms) {
+    using CF = cfg<LB>;
+    constexpr bool wide = LB == 16;
+    const size_t smem = batch::pcfg<LB>::SMEM;
+    cudaStream_t B = nullptr;
+    if (se_status_t st = side_stream(&B)) return st;
+    std::vector<cudaEvent_t> ev(size_t(2 * R + 2), nullptr);  // panels[0..R), remB[0..R), start, end
+    struct Guard {
+        std::vector<cudaEvent_t>& ev;
+        ~Guard() {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } guard{ev};
+    for (size_t i = 0; i < ev.size(); ++i) {
+        const unsigned flags = (phase_ms && i >= size_t(2 * R)) ? cudaEventDefault : cudaEventDisableTiming;
+        SE_CUDA_TRY(cudaEventCreateWithFlags(&ev[i], flags));
+    }
+    cudaEvent_t* pan = ev.data();
+    cudaEvent_t* remb = ev.data() + R;
+    if (phase_ms) SE_CUDA_TRY(cudaEventRecord(ev[2 * R], A));
+    auto panels = [&](int K) {
+        if constexpr (wide) panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, A>>>(E[K & 1], K, err);
+        else panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, A>>>(E[K & 1], K, err);
+    };
+    if constexpr (wide) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, A>>>(S, ldw, 0, dT);
+    else diag_kernel<LB><<<1, CF::THREADS, 0, A>>>(S, ldw, 0, dT);
+    panels(0);
+    SE_CHECK_LAUNCH();
+    SE_CUDA_TRY(cudaEventRecord(pan[0], A));
+    const int R2 = R - 2;
+    for (int K = 0; K + 1 < R; ++K) {
+        SE_CUDA_TRY(cudaStreamWaitEvent(B, pan[K], 0));
+        rem_kernel<LB><<<R2 * R2, CF::THREADS, smem, B>>>(E[K & 1], K, 0, 2, err);
+        SE_CUDA_TRY(cudaEventRecord(remb[K], B));
+        if (K > 0) SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[K - 1], 0));
+        rem_kernel<LB><<<2 * R - 3, CF::THREADS, smem, A>>>(E[K & 1], K, 1, 1, err);
+        panels(K + 1);
+        SE_CHECK_LAUNCH();
+        SE_CUDA_TRY(cudaEventRecord(pan[K + 1], A));
+    }
+    SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[R - 2], 0));
+    rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, A>>>(E[(R - 1) & 1], R - 1, 0, 0, err);
+    SE_CHECK_LAUNCH();
+    if (phase_ms) {
+        SE_CUDA_TRY(cudaEventRecord(ev[2 * R + 1], A));
+        SE_CUDA_TRY(cudaEventSynchronize(ev[2 * R + 1]));
+        float ms = 0.f;
+        SE_CUDA_TRY(cudaEventElapsedTime(&ms, ev[2 * R], ev[2 * R + 1]));
+        for (int q = 0; q < 4; ++q) phase_ms[q] = 0.0;
+        phase_ms[3] = ms;  // the rounds overlap across the two streams: one figure for all
+    }
+    return SE_OK;
+}
+
 template <int LB>
 se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms, int mode) {
     using CF = cfg<LB>;
@@ -613,6 +725,14 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     E.R = R;
     E.lanes = LB;
     const size_t smem = batch::pcfg<LB>::SMEM;
+    if (mode == 5) {
+        batch::Elec E2[2] = {E, E};
+        uint32_t* AT2 = reinterpret_cast<uint32_t*>(work + P.at2_off);
+        if (se_status_t st = make_map(&E2[1].mapAT, AT2, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st)
+            return st;
+        E2[1].AT = AT2;
+        return run_two_streams<LB>(E2, R, stream, S, ldw, dT, err, phase_ms);
+    }
 
     // Events between launches when profiling: (phase, event recorded after the launch).
     std::vector<std::pair<int, cudaEvent_t>> ev;
@@ -653,7 +773,7 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
         }
         mark(1);
-        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, err);
+        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, 0, err);
         mark(3);
         SE_CHECK_LAUNCH();
     }
@@ -840,10 +960,12 @@ se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t
         if (se_status_t st = launch_init<32>(d_pref, ld_pref, C, P, work, 0, s)) return st;
     }
     int mode = mode_override >= 0 ? mode_override : g_closure_mode.load();
-    if (mode == 0) mode = automatic_mode(C);
+    const bool automatic = mode == 0;
+    if (automatic) mode = automatic_mode(C);
+    if (mode == 5 && (P.Cp / kT < 4 || (automatic && work_bytes < P.flow_total))) mode = 3;
     const bool flow = mode == 2 && P.Cp > kT;
-    SE_REQUIRE(mode != 2 || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
-               "the dataflow closure needs a workspace of %lld bytes", (long long)P.flow_total);
+    SE_REQUIRE((mode != 2 && mode != 5) || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
+               "the dataflow and two-stream closures need a workspace of %lld bytes", (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
                           : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms, mode)
                                       : run_rounds<32>(work, P, s, phase_ms, mode));
@@ -923,7 +1045,7 @@ extern "C" se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k
 
 extern "C" se_status_t se_closure_set_mode(int mode) {
     clear_error();
-    SE_REQUIRE(mode >= 0 && mode <= 4, SE_ERR_INVALID, "closure mode must be 0 to 4");
+    SE_REQUIRE(mode >= 0 && mode <= 5, SE_ERR_INVALID, "closure mode must be 0 to 5");
     g_closure_mode.store(mode);
     return SE_OK;
 }
@@ -934,8 +1056,8 @@ extern "C" se_status_t se_closure_set_variant_table(const int* max_c, const int*
         SE_REQUIRE(n >= 0 && n <= kMaxVariants, SE_ERR_INVALID, "at most %d table entries", kMaxVariants);
         SE_REQUIRE(n == 0 || (max_c && modes), SE_ERR_INVALID, "null table");
         for (int i = 0; i < n; ++i)
-            SE_REQUIRE(modes[i] == 1 || modes[i] == 3 || modes[i] == 4, SE_ERR_INVALID,
-                       "table modes must be 1, 3 or 4 (got %d)", modes[i]);
+            SE_REQUIRE(modes[i] == 1 || modes[i] == 3 || modes[i] == 4 || modes[i] == 5, SE_ERR_INVALID,
+                       "table modes must be 1, 3, 4 or 5 (got %d)", modes[i]);
         std::lock_guard<std::mutex> lock(g_variant_mutex);
         for (int i = 0; i < n; ++i) {
             g_variant_max_c[i] = max_c[i];
@@ -952,6 +1074,6 @@ extern "C" int se_closure_launch_count(int C) {
     int mode = g_closure_mode.load();
     if (mode == 0) mode = automatic_mode(C);
     // init, pivot of round 0, R x (panels, remainder), finalize; mode 4 adds a pivot launch
-    // per later round (in 16-bit lanes).
-    return R == 1 ? 3 : 3 + 2 * R + (mode == 4 ? R - 1 : 0);
+    // per later round (in 16-bit lanes), mode 5 a second remainder launch per round but the last.
+    return R == 1 ? 3 : 3 + 2 * R + (mode == 4 || (mode == 5 && R >= 4) ? R - 1 : 0);
 }

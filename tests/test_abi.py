@@ -64,7 +64,7 @@ def test_closure_schedule_settings_need_no_gpu():
     assert L.se_closure_set_variant_table(max_c, ok, 9) == _lib.SE_ERR_INVALID
     assert L.se_closure_set_variant_table(max_c, ok, n) == _lib.SE_OK
     assert L.se_closure_set_variant_table(None, None, 0) == _lib.SE_OK
-    assert L.se_closure_set_mode(5) == _lib.SE_ERR_INVALID
+    assert L.se_closure_set_mode(6) == _lib.SE_ERR_INVALID
     for mode in (4, 0):
         assert L.se_closure_set_mode(mode) == _lib.SE_OK
     builtin = ((ctypes.c_int * 2)(1024, 12288), (ctypes.c_int * 2)(4, 3))  # put the built-in table back

@@ -178,7 +178,7 @@ def test_dataflow_equals_round_by_round(orc, C):
         api.set_closure_mode(0)
 
 
-@pytest.mark.parametrize("C", [1, 127, 129, 300, 640, 1000, 1700, 2305])
+@pytest.mark.parametrize("C", [1, 127, 129, 300, 385, 512, 640, 1000, 1700, 2305, 4100])
 def test_wide_micro_tile_schedules(orc, C):
     """Schedules 3 (panels on the wide micro-tile) and 4 (also a wide pivot launch per round)
     against the oracle in 16-bit lanes (shifted and not) and, where they fall back to
@@ -189,13 +189,13 @@ def test_wide_micro_tile_schedules(orc, C):
     Q = P + np.uint32(70000)
     Q_ref = orc.strongest_paths(Q, "blocked", tile=16)
     try:
-        for mode in (3, 4):
+        for mode in (3, 4, 5):
             api.set_closure_mode(mode)
             for lanes in (LANES_U16, LANES_U32, LANES_AUTO):
                 assert np.array_equal(gpu_closure(P, lanes), S_ref), (mode, lanes)
             assert np.array_equal(gpu_closure(Q, LANES_AUTO), Q_ref), mode  # shifted 16-bit lanes
         api.set_closure_mode(0)
-        for table in ([(C, 3)], [(max(C - 1, 0), 1), (C, 4)], []):
+        for table in ([(C, 3)], [(max(C - 1, 0), 1), (C, 4)], [(C, 5)], []):
             api.set_closure_variants(table)
             assert np.array_equal(gpu_closure(P, LANES_U16), S_ref), table
     finally:
