@@ -53,9 +53,10 @@ def parse():
                     help="closure input: tallied Mallows ballots, or the reference's random matrix mode")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
-    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
                     help="the closure's schedule: 0 automatic by size (default), 1 round by round, 2 dataflow, "
-                         "3 wide panels, 4 wide panels and pivot launches, 5 two streams (include/se.h)")
+                         "3 wide panels, 4 wide panels and pivot launches, 5 two streams, 6 one launch per round "
+                         "(include/se.h)")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--cpu-full-size", action="store_true",
                     help="reference arm: also time one closure at the workload's full size (minutes)")
@@ -104,7 +105,7 @@ def config(args, world):
         "phi": args.phi,
         "lanes": f"u{args.lanes}" if args.lanes else "auto",
         "closure_mode": {0: "automatic by size", 1: "round by round", 2: "dataflow", 3: "wide panels",
-                         4: "wide panels and pivots", 5: "two streams"}[args.closure_mode],
+                         4: "wide panels and pivots", 5: "two streams", 6: "one launch per round"}[args.closure_mode],
         "tile": 128,
         "parallelism": f"replicas{world}" if world > 1 else "single",
         "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
@@ -230,20 +231,40 @@ def run_reference_arm(args, world, rank):
 # ------------------------------------------------------------------------------------------
 # Our arm
 # ------------------------------------------------------------------------------------------
-def load_traffic(lanes: int, C: int):
-    """DRAM bytes (read + write) per remainder-kernel launch, from the committed ncu summary
-    of a smaller case, scaled to this C by the number of remainder tiles per launch (the
-    kernel's traffic is proportional to the tiles it processes)."""
+def main_launches(R: int, mode: int) -> dict:
+    """What se_closure_profiled's phase_ms[3] times under schedule `mode`: the kernel, its
+    launches, and the tile products they run (each 128^3 relaxations; the fused pivot's closure
+    is extra and not counted). Schedule 6 runs R - 1 round launches of (R-1)^2 remainder tiles
+    plus the next round's 2(R-1) panel tiles, then one plain remainder launch; the others run R
+    remainder launches of (R-1)^2 tiles (schedule 5: the whole closure, remainder and panels)."""
+    if mode == 6:
+        per = (R - 1) ** 2 + 2 * (R - 1)
+        return {"kernel": "round_kernel", "launches": R, "tiles_per_launch": per,
+                "tiles": (R - 1) * per + (R - 1) ** 2}
+    if mode == 5:
+        return {"kernel": "rem_kernel and panels_kernel (two streams)", "launches": R,
+                "tiles_per_launch": (R - 1) ** 2 + 2 * (R - 1), "tiles": R * ((R - 1) ** 2 + 2 * (R - 1))}
+    return {"kernel": "rem_kernel", "launches": R, "tiles_per_launch": (R - 1) ** 2, "tiles": R * (R - 1) ** 2}
+
+
+def load_traffic(lanes: int, C: int, kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel`, from the committed ncu summary of a
+    smaller case, scaled to this C by the tiles per launch (the kernel's traffic is
+    proportional to the tiles it processes)."""
     import re
 
-    p = ROOT / "profiles" / "closure_rem_kernel_u16_c12288.md"
+    name = {"rem_kernel": "closure_rem_kernel_u16_c12288.md", "round_kernel": "closure_round_kernel_u16_c12288.md"}
+    if kernel not in name:
+        return None
+    p = ROOT / "profiles" / name[kernel]
     if not p.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch: u(\d+) C=(\d+) (\d+)", p.read_text())
     if not m or int(m.group(1)) != lanes:
         return None
     C_ref, b_ref = int(m.group(2)), int(m.group(3))
-    tiles = lambda c: ((c + 127) // 128 - 1) ** 2
+    R = lambda c: (c + 127) // 128  # noqa: E731
+    tiles = (lambda c: (R(c) - 1) ** 2) if kernel == "rem_kernel" else (lambda c: (R(c) - 1) ** 2 + 2 * (R(c) - 1))
     return b_ref * tiles(C) / tiles(C_ref)
 
 
@@ -291,7 +312,7 @@ def run_ours(args, world, rank, local_rank):
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
     api.set_closure_mode(args.closure_mode)
-    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode in (0, 2, 5))
+    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode in (0, 2, 5, 6))
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()
@@ -328,20 +349,21 @@ def run_ours(args, world, rank, local_rank):
     _lib.check(L.se_closure_profiled(d.data_ptr(), C, C, out.data_ptr(), C, lanes, 0, work.data_ptr(), need,
                                      stream.cuda_stream, phase, ctypes.byref(launches)))
     R = (C + 127) // 128
-    tile_launches = R if R > 1 else 0  # one remainder launch per round when R > 1
-    relax_per_launch = float(R - 1) ** 2 * 128 ** 3
-    tile_ms_avg = phase[3] / max(tile_launches, 1)
-    achieved = relax_per_launch / (tile_ms_avg * 1e-3)
+    schedule = api.closure_schedule(C, lanes or 16, need)
+    main = main_launches(R, schedule)
+    tile_ms_avg = phase[3] / max(main["launches"], 1)
+    achieved = float(main["tiles"]) * 128 ** 3 / (phase[3] * 1e-3)
     cell_bytes = 2 if lanes in (0, 16) else 4
-    algo_bytes = float(R - 1) ** 2 * 128 * 128 * cell_bytes * 2  # each remainder tile read + written once
+    algo_bytes = float(main["tiles_per_launch"]) * 128 * 128 * cell_bytes * 2  # each tile read + written once
 
-    # The reference's own CUDA path on the same matrix, first after the headline: run later in
-    # the process (after this script has pinned gigabytes of host memory for the copies) the
-    # same call measured 66 s instead of 8.5 s.
+    # The reference's own CUDA path on the same matrix (regenerated from the same seed), in a
+    # process of its own: run inside this one after its other legs, the same call once took 66 s
+    # instead of 8.5 s, and the OpenMP sample after it ten times its usual time.
     reference_gpu = None
     if world == 1 and rank == 0 and not args.no_extras and not args.no_reference_gpu:
-        reference_gpu = reference_gpu_leg(api._to_host_u32(d), api._to_host_u32(out), local_rank)
-        torch.cuda.empty_cache()
+        reference_gpu = child_line(["--workload", "reference-gpu", "--candidates", str(C), "--voters", str(V),
+                                    "--phi", str(args.phi), "--seed", str(args.seed), "--input", args.input,
+                                    "--lanes", str(lanes)])
 
     # The tally half of the path on the same ballots (device-resident), against the integer
     # ALU pipe: B lop3 + 1 popc + 1 add per 32 voter pairs of the upper block triangle
@@ -396,6 +418,7 @@ def run_ours(args, world, rank, local_rank):
 
     # End to end through the public host API: pinned host in, pinned host out.
     e2e = None
+    e2e_numpy = None
     if not args.no_e2e:
         host_in = torch.empty((C, C), dtype=torch.int32, pin_memory=True)
         host_in.copy_(d.view(torch.int32))
@@ -414,11 +437,29 @@ def run_ours(args, world, rank, local_rank):
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e = {"value": cells / float(te.item()) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": C * C * 4, "d2h_bytes_per_step": C * C * 4}
+        if world == 1 and not args.no_extras:
+            # The call as the reference's script makes it: a pageable NumPy matrix in (staged
+            # through pinned chunks), a new NumPy matrix out.
+            np_in = host_in.numpy().copy()
+            api.compute_strongest_paths(np_in, allow_gpu=True, tile_size=32, lanes=lanes)  # warm
+            n_np = max(1, min(args.steps, 5))
+            t0 = time.perf_counter()
+            for _ in range(n_np):
+                res = api.compute_strongest_paths(np_in, allow_gpu=True, tile_size=32, lanes=lanes)
+                del res
+            t_np = time.perf_counter() - t0
+            e2e_numpy = {"value": float(C) ** 3 * n_np / t_np / 1e9, "unit": UNIT, "steps": n_np,
+                         "ms_per_step": t_np / n_np * 1e3,
+                         "input": "pageable NumPy uint32 matrix (the reference script's call)"}
+            del np_in
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cps, kind, cores, sample, _ = cpu_closure_sample(args, cpu_sample_matrix(args))
-        cpu = {"value": cps / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        # The reference arm itself, one sample, in a process of its own (see reference_gpu).
+        ref = child_line(["--impl", "reference", "--steps", "1", "--warmup", "0", "--cpu-sample",
+                          str(args.cpu_sample), "--candidates", str(C), "--voters", str(V), "--phi", str(args.phi),
+                          "--seed", str(args.seed)])
+        cpu = ref.get("cpu_baseline", {"unavailable": ref.get("unavailable", "no line")})
 
     extras = {}
     if world == 1 and not args.no_extras:
@@ -429,7 +470,7 @@ def run_ours(args, world, rank, local_rank):
         extras["sharded"] = measure_sharded(args, world, rank, local_rank, C=args.sharded_candidates)
 
     if rank == 0:
-        traffic = load_traffic(lanes if lanes else 16, C)
+        traffic = load_traffic(lanes if lanes else 16, C, main["kernel"])
         line = {
             "metric": metric_name(args.candidates), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -439,7 +480,7 @@ def run_ours(args, world, rank, local_rank):
             "config": config(args, world),
             "roofline": {
                 "bound": "int_minmax",
-                "kernel": f"closure remainder rem_kernel<u{lanes or 16}>",
+                "kernel": f"{main['kernel']}<u{lanes or 16}> (closure schedule {schedule})",
                 "achieved": achieved / 1e12, "peak": peak_relax_per_s / 1e12, "unit": "Trelax/s",
                 "frac": achieved / peak_relax_per_s,
                 "peak_source": f"measured: se_minmax_peak recipe {recipe} in this run "
@@ -447,8 +488,8 @@ def run_ours(args, world, rank, local_rank):
                 "traffic": traffic,
                 "algorithmic_bytes_per_launch": algo_bytes,
                 "hbm_gbs_achieved": algo_bytes / (tile_ms_avg * 1e-3) / 1e9,
-                "phase_ms": {"pivot_round0": phase[0], "panels": phase[1],
-                             "remainder_with_fused_pivot": phase[3]},
+                "phase_ms": {"pivot_round0": phase[0], "panels": phase[1], "main_launches": phase[3]},
+                "main_launches": main,
             },
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -458,6 +499,8 @@ def run_ours(args, world, rank, local_rank):
             "gpu_launches": int(L.se_closure_launch_count(C)) * args.steps,
         }
         line.update(extras)
+        if e2e_numpy is not None:
+            line["e2e_numpy"] = e2e_numpy
         if reference_gpu is not None:
             line["reference_gpu"] = reference_gpu
         print(json.dumps(line), flush=True)
@@ -480,7 +523,7 @@ def closure_object(d, lanes: int, steps: int, warmup: int, local_rank: int, work
     recipe = 3 if lanes == 16 else 1
     _lib.check(L.se_minmax_peak(recipe, 65536, *[ctypes.byref(x) for x in peak]))
     peak_relax_per_s = peak[3].value
-    need = api.closure_workspace_bytes(C, lanes)
+    need = api.closure_workspace_bytes(C, lanes, dataflow=True)
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()
@@ -500,13 +543,15 @@ def closure_object(d, lanes: int, steps: int, warmup: int, local_rank: int, work
     _lib.check(L.se_closure_profiled(d.data_ptr(), C, C, out.data_ptr(), C, lanes, 0, work.data_ptr(), need,
                                      stream.cuda_stream, phase, ctypes.byref(launches)))
     R = (C + 127) // 128
-    obj = {"workload": workload, "candidates": C, "lanes": f"u{lanes}", "tile": 128, "steps": steps,
-           "warmup": warmup, "ms": ms, "value": float(C) ** 3 / (ms * 1e-3) / 1e9, "unit": UNIT,
-           "phase_ms": {"pivot_round0": phase[0], "panels": phase[1], "remainder_with_fused_pivot": phase[3]},
+    schedule = api.closure_schedule(C, lanes, need)
+    obj = {"workload": workload, "candidates": C, "lanes": f"u{lanes}", "tile": 128, "schedule": schedule,
+           "steps": steps, "warmup": warmup, "ms": ms, "value": float(C) ** 3 / (ms * 1e-3) / 1e9, "unit": UNIT,
+           "phase_ms": {"pivot_round0": phase[0], "panels": phase[1], "main_launches": phase[3]},
            "gpu_launches": int(launches.value) * steps, "clocks": clocks.summary()}
     if R > 1:
-        achieved = float(R - 1) ** 2 * 128 ** 3 / (phase[3] / R * 1e-3)
-        obj["roofline"] = {"bound": "int_minmax", "kernel": f"closure remainder rem_kernel<u{lanes}>",
+        main = main_launches(R, schedule)
+        achieved = float(main["tiles"]) * 128 ** 3 / (phase[3] * 1e-3)
+        obj["roofline"] = {"bound": "int_minmax", "kernel": f"{main['kernel']}<u{lanes}>",
                            "achieved": achieved / 1e12, "peak": peak_relax_per_s / 1e12, "unit": "Trelax/s",
                            "frac": achieved / peak_relax_per_s,
                            "peak_source": f"measured: se_minmax_peak recipe {recipe} in this run"}
@@ -525,6 +570,20 @@ def election_matrix(V: int, C: int, phi: float, seed: int, dev):
     offs = torch.arange(V + 1, dtype=torch.int64, device=dev) * C
     d = api.tally_device(b.view(-1), offs, C)
     return d, b, offs
+
+
+def child_line(argv: list[str]) -> dict:
+    """Runs this script with `argv` in a new process on the same GPU (this one waits, idle) and
+    returns the JSON object of its last line."""
+    env = dict(os.environ)
+    for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE", "GROUP_RANK", "ROLE_RANK"):
+        env.pop(k, None)
+    r = subprocess.run([sys.executable, str(Path(__file__).resolve()), *argv], capture_output=True, text=True,
+                       env=env, timeout=1800)
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"child exited {r.returncode}: {r.stderr.strip().splitlines()[-1:] if r.stderr else ''}"}
+    return json.loads(lines[-1])
 
 
 def reference_gpu_leg(d_host, ours_host, local_rank: int) -> dict:
@@ -562,8 +621,13 @@ def run_reference_gpu(args, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    d, b, o = election_matrix(args.voters, args.candidates, args.phi, args.seed, dev)
-    del b, o
+    if args.input == "random":
+        from scalingelections_b200.ballots import random_preferences_device
+
+        d = random_preferences_device(args.candidates, seed=args.seed, device=dev)
+    else:
+        d, b, o = election_matrix(args.voters, args.candidates, args.phi, args.seed, dev)
+        del b, o
     ours = api._to_host_u32(api.strongest_paths_device(d, lanes=args.lanes or 16))
     line = reference_gpu_leg(api._to_host_u32(d), ours, local_rank)
     line["workload"] = f"C={args.candidates}, V={args.voters} Mallows(phi={args.phi}) ballots"
@@ -619,10 +683,12 @@ def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
     obj16["u32"]["bit_identical_to_u16"] = bool(torch.equal(o16.view(torch.int32), o32.view(torch.int32)))
     # The schedule sweep of this configuration: the 128-cell tile with the default micro-tile
     # (8 x 8 words per thread) for every tile, or the wide one (8 x 4 words, twice the warps) for
-    # the panels, or for the panels and a pivot launch per round.
+    # the panels, or for the panels and a pivot launch per round; two streams; or each round's
+    # remainder and the next round's panels in one launch.
     sweep = {}
     for mode, what in ((1, "panels and pivot on 8x8 words, pivot fused"), (3, "panels on 8x4 words, pivot fused"),
-                       (4, "panels and pivot on 8x4 words, pivot launched")):
+                       (4, "panels and pivot on 8x4 words, pivot launched"), (5, "as 3 on two streams"),
+                       (6, "remainder and next panels in one launch per round")):
         api.set_closure_mode(mode)
         o, _ = closure_object(d4, 16, max(steps, 20), 3, local_rank, what)
         sweep[str(mode)] = {"schedule": what, "ms": o["ms"], "value": o["value"],

@@ -46,6 +46,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_closure_workspace_bytes_flow": (_c_i64, [_c_int, _c_int, _c_int]),
     "se_closure_set_mode": (_c_int, [_c_int]),
     "se_closure_set_variant_table": (_c_int, [_vp, _vp, _c_int]),
+    "se_closure_schedule": (_c_int, [_c_int, _c_int, _c_i64]),
     "se_closure_flow_task": (_c_int, [ctypes.c_uint32, _c_int, _ip, _ip, _ip, _ip]),
     "se_closure_noalloc": (_c_int, [_vp, _c_i64, _c_int, _vp, _c_i64, _c_int, _vp]),
     "se_batch_workspace_bytes": (_c_i64, [_c_int, _vp]),

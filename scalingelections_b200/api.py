@@ -46,9 +46,57 @@ def _workspace(nbytes: int, device) -> torch.Tensor:
     return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
 
 
+# Pageable host matrices reach the device through two pinned chunks: while one chunk's copy
+# to the device runs, host threads fill the other (NumPy releases the GIL for large copies).
+_STAGE_CHUNK = 64 << 20
+_STAGE_THREADS = 8
+_stage_state: dict = {}
+
+
+def _stage_to_device(a: np.ndarray, dev) -> torch.Tensor:
+    """A C-contiguous host array to a new CUDA uint8 tensor of its bytes, through pinned staging."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    src = a.reshape(-1).view(np.uint8)
+    n = src.size
+    out = torch.empty(n, dtype=torch.uint8, device=dev)
+    st = _stage_state.get(dev)
+    if st is None:
+        st = {"bufs": [torch.empty(_STAGE_CHUNK, dtype=torch.uint8, pin_memory=True) for _ in range(2)],
+              "events": [torch.cuda.Event() for _ in range(2)], "used": [False, False],
+              "pool": ThreadPoolExecutor(max_workers=_STAGE_THREADS)}
+        _stage_state[dev] = st
+    part = -(-_STAGE_CHUNK // _STAGE_THREADS)
+
+    def fill(dst: np.ndarray, lo: int, hi: int) -> None:
+        futures = [st["pool"].submit(np.copyto, dst[x - lo:min(x + part, hi) - lo], src[x:min(x + part, hi)])
+                   for x in range(lo, hi, part)]
+        for f in futures:
+            f.result()
+
+    stream = torch.cuda.current_stream(dev)
+    for i, lo in enumerate(range(0, n, _STAGE_CHUNK)):
+        hi = min(lo + _STAGE_CHUNK, n)
+        b = i & 1
+        if st["used"][b]:
+            st["events"][b].synchronize()  # this buffer's previous copy has left
+        buf = st["bufs"][b]
+        fill(buf.numpy(), lo, hi)
+        out[lo:hi].copy_(buf[:hi - lo], non_blocking=True)
+        st["events"][b].record(stream)
+        st["used"][b] = True
+    return out
+
+
 def _to_device_u32(a: np.ndarray | torch.Tensor, dev) -> torch.Tensor:
     """Host uint32 array -> CUDA uint32 tensor, copied through an int32 view (torch's uint32
-    is a storage-only dtype)."""
+    is a storage-only dtype). Large pageable NumPy arrays go through pinned staging."""
+    if (isinstance(a, np.ndarray) and a.dtype.itemsize == 4 and a.nbytes >= 2 * _STAGE_CHUNK
+            and torch.cuda.is_available()):
+        a = np.ascontiguousarray(a)
+        dev = torch.device(dev) if not isinstance(dev, int) else torch.device("cuda", dev)
+        with torch.cuda.device(dev):
+            return _stage_to_device(a, dev).view(torch.int32).view(a.shape).view(torch.uint32)
     t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
     t = t.view(torch.int32)
     return t.to(device=dev, non_blocking=t.is_pinned()).view(torch.uint32)
@@ -95,16 +143,30 @@ def set_closure_mode(mode: int) -> None:
     """The closure's schedule (same results in every one): 0 automatic by size (default),
     1 round by round, 2 the dataflow form, 3 round by round with the panels on the wide
     micro-tile, 4 as 3 with each pivot tile closed by its own wide launch, 5 as 3 on two
-    streams so the next round's chain overlaps the current remainder (include/se.h)."""
+    streams so the next round's chain overlaps the current remainder, 6 each round's
+    remainder and the next round's panels in one launch (include/se.h)."""
     global _closure_mode
     check(_lib.lib().se_closure_set_mode(int(mode)))
     _closure_mode = int(mode)
 
 
+BUILTIN_CLOSURE_VARIANTS = ((1024, 4), (3072, 3), (1 << 20, 6))
+
+
+def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_bytes: int | None = None) -> int:
+    """The schedule (1 to 6) a closure of this size would run now (host-only query). The
+    workspace defaults to what strongest_paths_device allocates; -1 for no candidates."""
+    if int(num_candidates) < 1:
+        return -1
+    if workspace_bytes is None:
+        workspace_bytes = closure_workspace_bytes(num_candidates, lanes, dataflow=_closure_mode in (0, 2, 5, 6))
+    return int(_lib.lib().se_closure_schedule(int(num_candidates), int(lanes), int(workspace_bytes)))
+
+
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
-    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1, 3, 4 or 5;
+    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-6;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
-    the library starts with the table measured on B200, {1024: 4, 12288: 3}).
+    the library starts with the table measured on B200, {1024: 4, 3072: 3, 2**20: 6}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
     this."""
     n = len(table)
@@ -128,9 +190,9 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         raise ValueError("out has the wrong shape")
     if C == 0:
         return out
-    # The dataflow (2) and two-stream (5) schedules, which the automatic one (0) may pick, use
-    # a second AT buffer: a few MiB more than the plain workspace.
-    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5))
+    # The dataflow (2), two-stream (5) and one-launch-per-round (6) schedules, which the
+    # automatic one (0) may pick, use a second AT buffer: a few MiB more than the plain one.
+    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5, 6))
     if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = _workspace(need, preferences.device)
     have = workspace.numel() * workspace.element_size()

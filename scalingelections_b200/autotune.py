@@ -8,7 +8,9 @@ table (se_closure_set_variant_table), which the automatic schedule reads:
   3  panels on the wide micro-tile (8 x 4 words per thread, eight warps);
   4  as 3, and every pivot tile closed by its own launch on the wide micro-tile;
   5  as 3 on two streams: the next round's pivot row and column, pivot and panels overlap
-     the current round's remaining remainder tiles.
+     the current round's remaining remainder tiles;
+  6  each round's remainder and the next round's panels in one launch, the panels in the
+     remainder's last wave.
 The schedules differ where the per-round chain (pivot, then panels) is not hidden behind the
 remainder: small and medium C.
 
@@ -122,7 +124,7 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
 
 
 CLOSURE_BUCKETS = [1024, 2048, 3072, 4096, 6144, 8192, 12288]  # upper bounds of the size buckets
-CLOSURE_MODES = (1, 3, 4, 5)
+CLOSURE_MODES = (1, 3, 4, 5, 6)
 
 
 def tune_closure(sizes: Sequence[int] | None = None, reps: int = 5, V: int = 4096, seed: int = 0,

@@ -133,6 +133,91 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------------
+// Schedule 6: round K's remainder and round K+1's panels in one launch. Each CTA takes a
+// ticket (an atomic counter, so every ticket below its own went to a CTA that is already
+// running) and runs one task:
+//   [0, 2R-3)              remainder tiles of row and column K+1; ticket 0 is tile (K+1, K+1),
+//                          which it then closes as the next pivot (dT);
+//   [2R-3, (R-1)^2)        the other remainder tiles of round K;
+//   [(R-1)^2, +2(R-1))     the panel tiles of round K+1, which first wait (bounded) until all
+//                          of the first group, the pivot included, are done.
+// The panels then run in the remainder's last, partial wave instead of a launch of their own.
+// They write AT[(K+1) % 2] while the remainder reads AT[K % 2] (descriptors E and En), and
+// rows and columns K+1, which no remainder tile of the second group reads or writes; the tiles
+// they read are exactly the first group's. state: this round's ticket and done counters.
+// ------------------------------------------------------------------------------------------
+template <int LB>
+__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+    round_kernel(const __grid_constant__ batch::Elec E, const __grid_constant__ batch::Elec En, int K,
+                 uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
+    using CF = cfg<LB>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
+    __shared__ __align__(16) uint32_t colbuf[kPivotBufs][kT];
+    __shared__ uint32_t s_ticket;
+    __shared__ int s_go;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 2 * kChunks; ++c) mbar_init(&bars[c], 1);
+        fence_barrier_init();
+        s_ticket = atomicAdd(&state[0], 1u);
+    }
+    __syncthreads();
+    const uint32_t t = s_ticket;
+    const int R = E.R, R1 = R - 1, R2 = R - 2;
+    const uint32_t first = uint32_t(2 * R - 3), rem = uint32_t(R1) * uint32_t(R1);
+    auto skip_k_k1 = [K](int n) { return n < K ? n : n + 2; };  // n-th block index other than K, K+1
+    uint32_t par_a = 0, par_b = 0;
+    if (t < rem) {
+        int I, J;
+        if (t == 0) {
+            I = J = K + 1;
+        } else if (t < first) {
+            const int x = int(t) - 1;
+            I = x < R2 ? K + 1 : skip_k_k1(x - R2);
+            J = x < R2 ? skip_k_k1(x) : K + 1;
+        } else {
+            const int x = int(t - first);
+            I = skip_k_k1(x / R2);
+            J = skip_k_k1(x % R2);
+        }
+        const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
+        if (!ok) {
+            if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
+            return;
+        }
+        if (t == 0) {
+            __syncthreads();  // the tile's stores are visible to the whole CTA
+            batch::run_pivot<LB>(E, K + 1, rowbuf, colbuf);
+        }
+        if (t < first) {  // publish: the tile (and the pivot) are done, for TMA reads too
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                batch::fence_proxy_async_global();
+                atomicAdd(&state[1], 1u);
+            }
+        }
+        return;
+    }
+    if (threadIdx.x == 0) {  // a panel of round K+1: wait for the tiles it reads and the pivot
+        const bool ok = batch::wait_counter(&state[1], first, err, 2000000000ull);
+        if (!ok) raise_device_error(err, kErrTmaTimeout);
+        s_go = ok;
+        batch::fence_proxy_async_global();
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const int x = int(t - rem);
+    const bool row = x < R1;
+    const int y = row ? x : x - R1;
+    const int K1 = K + 1;
+    const bool ok = batch::run_tile<LB, false>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1, y + (y >= K1),
+                                               y + (y >= K1), smem, bars, par_a, par_b);
+    if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
+}
+
+// ------------------------------------------------------------------------------------------
 // Dataflow closure: the same tasks as the round-by-round launches (pivot, panels, remainder),
 // run by one persistent grid that walks a fixed task order with no barrier between rounds.
 // Each task waits only for what it reads and for the readers of what it overwrites:
@@ -569,7 +654,9 @@ layout plan(int C, int lane_bits) {
 //      pivot) and round k+1's panels run on the caller's stream while the rest of round k's
 //      remainder runs on a lower-priority second stream, so the next round's chain overlaps
 //      the current round's bulk. AT is double-buffered (the dataflow layout's second buffer):
-//      needs se_closure_workspace_bytes_flow() of workspace, and R >= 4.
+//      needs se_closure_workspace_bytes_flow() of workspace, and R >= 4;
+//   6  round K's remainder and round K+1's panels in one launch (round_kernel): the panels
+//      take the remainder's last, partial wave. AT is double-buffered as in 5.
 // 3 and 4 apply to 16-bit lanes; 32-bit lanes run 1 for them (5 without the wide panels). Round by round is the default:
 // on B200 hardware block scheduling of one launch per phase beats the persistent grid's
 // claim-and-poll overhead at every size measured.
@@ -577,14 +664,15 @@ std::atomic<int> g_closure_mode{0};
 
 // The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds). The
 // built-in table is autotune.tune_closure's result on one B200 (16-bit lanes, ms per closure,
-// modes 1 / 3 / 4): C = 1024 0.766 / 0.728 / 0.688, C = 2048 1.486 / 1.449 / 1.538,
-// C = 4096 4.000 / 3.921 / 5.194, C = 8192 25.11 / 24.97 / 27.54, C = 12288 82.67 / 82.48 /
-// 86.34, C = 16384 191.5 / 191.7 / 196.3.
+// modes 1 / 3 / 4 / 5 / 6): C = 1024 0.745 / 0.714 / 0.689 / 0.723 / 0.725, C = 2048 1.491 /
+// 1.450 / 1.541 / 1.578 / 1.774, C = 3072 2.271 / 2.202 / 2.945 / 2.713 / 2.520, C = 4096
+// 4.005 / 3.924 / 5.199 / 4.213 / 3.555, C = 8192 25.12 / 24.97 / 27.54 / 27.10 / 24.95,
+// C = 16384 191.6 / 191.4 / 196.5 / 195.0 / 190.6.
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
-int g_variant_n = 2;
-int g_variant_max_c[kMaxVariants] = {1024, 12288};
-int g_variant_mode[kMaxVariants] = {4, 3};
+int g_variant_n = 3;
+int g_variant_max_c[kMaxVariants] = {1024, 3072, 1 << 20};
+int g_variant_mode[kMaxVariants] = {4, 3, 6};
 
 int automatic_mode(int C) {
     std::lock_guard<std::mutex> lock(g_variant_mutex);
@@ -603,6 +691,8 @@ template <int LB> se_status_t set_smem_limits() {
             return st;
     }
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB>), bytes, "the remainder kernel"))
+        return st;
+    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(round_kernel<LB>), bytes, "the round kernel"))
         return st;
     return raise_smem_limit(reinterpret_cast<const void*>(flow_kernel<LB>), bytes, "the dataflow closure");
 }
@@ -732,6 +822,58 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             return st;
         E2[1].AT = AT2;
         return run_two_streams<LB>(E2, R, stream, S, ldw, dT, err, phase_ms);
+    }
+    if (mode == 6) {
+        batch::Elec E2[2] = {E, E};
+        uint32_t* AT2 = reinterpret_cast<uint32_t*>(work + P.at2_off);
+        if (se_status_t st = make_map(&E2[1].mapAT, AT2, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st)
+            return st;
+        E2[1].AT = AT2;
+        uint32_t* state = reinterpret_cast<uint32_t*>(work + P.state_off);
+        SE_CUDA_TRY(cudaMemsetAsync(state, 0, size_t(2 * R) * 4, stream));
+        // Profiling: events after the round-0 pivot (phase 0), the round-0 panels (phase 1), and
+        // every later launch (phase 3: each round's remainder with the next round's panels).
+        std::vector<cudaEvent_t> ev;
+        struct Guard {
+            std::vector<cudaEvent_t>& ev;
+            ~Guard() {
+                for (auto e : ev) cudaEventDestroy(e);
+            }
+        } guard{ev};
+        auto mark = [&]() -> se_status_t {
+            if (!phase_ms) return SE_OK;
+            cudaEvent_t e = nullptr;
+            SE_CUDA_TRY(cudaEventCreate(&e));
+            ev.push_back(e);
+            SE_CUDA_TRY(cudaEventRecord(e, stream));
+            return SE_OK;
+        };
+        if (se_status_t st = mark()) return st;
+        diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
+        if (se_status_t st = mark()) return st;
+        panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, err);
+        SE_CHECK_LAUNCH();
+        if (se_status_t st = mark()) return st;
+        for (int K = 0; K + 1 < R; ++K) {
+            round_kernel<LB><<<(R - 1) * (R - 1) + 2 * (R - 1), CF::THREADS, smem, stream>>>(
+                E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K, err);
+            SE_CHECK_LAUNCH();
+        }
+        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, err);
+        SE_CHECK_LAUNCH();
+        if (se_status_t st = mark()) return st;
+        if (phase_ms) {
+            SE_CUDA_TRY(cudaEventSynchronize(ev.back()));
+            float a = 0.f, b = 0.f, c = 0.f;
+            SE_CUDA_TRY(cudaEventElapsedTime(&a, ev[0], ev[1]));
+            SE_CUDA_TRY(cudaEventElapsedTime(&b, ev[1], ev[2]));
+            SE_CUDA_TRY(cudaEventElapsedTime(&c, ev[2], ev[3]));
+            phase_ms[0] = a;
+            phase_ms[1] = b;
+            phase_ms[2] = 0.0;
+            phase_ms[3] = c;
+        }
+        return SE_OK;
     }
 
     // Events between launches when profiling: (phase, event recorded after the launch).
@@ -963,9 +1105,11 @@ se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t
     const bool automatic = mode == 0;
     if (automatic) mode = automatic_mode(C);
     if (mode == 5 && (P.Cp / kT < 4 || (automatic && work_bytes < P.flow_total))) mode = 3;
+    if (mode == 6 && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
     const bool flow = mode == 2 && P.Cp > kT;
-    SE_REQUIRE((mode != 2 && mode != 5) || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
-               "the dataflow and two-stream closures need a workspace of %lld bytes", (long long)P.flow_total);
+    SE_REQUIRE((mode != 2 && mode != 5 && mode != 6) || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
+               "the dataflow, two-stream and one-launch-per-round closures need a workspace of %lld bytes",
+               (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
                           : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms, mode)
                                       : run_rounds<32>(work, P, s, phase_ms, mode));
@@ -1045,9 +1189,21 @@ extern "C" se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k
 
 extern "C" se_status_t se_closure_set_mode(int mode) {
     clear_error();
-    SE_REQUIRE(mode >= 0 && mode <= 5, SE_ERR_INVALID, "closure mode must be 0 to 5");
+    SE_REQUIRE(mode >= 0 && mode <= 6, SE_ERR_INVALID, "closure mode must be 0 to 6");
     g_closure_mode.store(mode);
     return SE_OK;
+}
+
+extern "C" int se_closure_schedule(int C, int lane_bits, int64_t work_bytes) {
+    if (C < 1) return -1;
+    const layout P = plan(C, lane_bits == 32 ? 32 : 16);
+    int mode = g_closure_mode.load();
+    const bool automatic = mode == 0;
+    if (automatic) mode = automatic_mode(C);
+    if (mode == 5 && (P.Cp / kT < 4 || (automatic && work_bytes < P.flow_total))) mode = 3;
+    if (mode == 6 && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
+    if (lane_bits == 32 && (mode == 3 || mode == 4)) mode = 1;
+    return mode;
 }
 
 extern "C" se_status_t se_closure_set_variant_table(const int* max_c, const int* modes, int n) {
@@ -1056,8 +1212,8 @@ extern "C" se_status_t se_closure_set_variant_table(const int* max_c, const int*
         SE_REQUIRE(n >= 0 && n <= kMaxVariants, SE_ERR_INVALID, "at most %d table entries", kMaxVariants);
         SE_REQUIRE(n == 0 || (max_c && modes), SE_ERR_INVALID, "null table");
         for (int i = 0; i < n; ++i)
-            SE_REQUIRE(modes[i] == 1 || modes[i] == 3 || modes[i] == 4 || modes[i] == 5, SE_ERR_INVALID,
-                       "table modes must be 1, 3, 4 or 5 (got %d)", modes[i]);
+            SE_REQUIRE(modes[i] == 1 || (modes[i] >= 3 && modes[i] <= 6), SE_ERR_INVALID,
+                       "table modes must be 1, 3, 4, 5 or 6 (got %d)", modes[i]);
         std::lock_guard<std::mutex> lock(g_variant_mutex);
         for (int i = 0; i < n; ++i) {
             g_variant_max_c[i] = max_c[i];
@@ -1075,5 +1231,6 @@ extern "C" int se_closure_launch_count(int C) {
     if (mode == 0) mode = automatic_mode(C);
     // init, pivot of round 0, R x (panels, remainder), finalize; mode 4 adds a pivot launch
     // per later round (in 16-bit lanes), mode 5 a second remainder launch per round but the last.
+    if (mode == 6 && R >= 2) return 3 + R + 1;  // init, pivot, panels 0, R - 1 rounds, last remainder, finalize
     return R == 1 ? 3 : 3 + 2 * R + (mode == 4 || (mode == 5 && R >= 4) ? R - 1 : 0);
 }

@@ -64,11 +64,32 @@ def test_closure_schedule_settings_need_no_gpu():
     assert L.se_closure_set_variant_table(max_c, ok, 9) == _lib.SE_ERR_INVALID
     assert L.se_closure_set_variant_table(max_c, ok, n) == _lib.SE_OK
     assert L.se_closure_set_variant_table(None, None, 0) == _lib.SE_OK
-    assert L.se_closure_set_mode(6) == _lib.SE_ERR_INVALID
+    assert L.se_closure_set_mode(7) == _lib.SE_ERR_INVALID
     for mode in (4, 0):
         assert L.se_closure_set_mode(mode) == _lib.SE_OK
-    builtin = ((ctypes.c_int * 2)(1024, 12288), (ctypes.c_int * 2)(4, 3))  # put the built-in table back
-    assert L.se_closure_set_variant_table(builtin[0], builtin[1], 2) == _lib.SE_OK
+    from scalingelections_b200 import api
+
+    table = api.BUILTIN_CLOSURE_VARIANTS  # put the built-in table back
+    max_c = (ctypes.c_int * len(table))(*[c for c, _ in table])
+    modes = (ctypes.c_int * len(table))(*[m for _, m in table])
+    assert L.se_closure_set_variant_table(max_c, modes, len(table)) == _lib.SE_OK
+
+
+def test_closure_schedule_query_needs_no_gpu():
+    """Which schedule the automatic choice gives each size, with and without the workspace the
+    one-launch-per-round schedule needs, and in 32-bit lanes (no wide micro-tile there)."""
+    from scalingelections_b200 import LANES_U16, LANES_U32, api
+
+    api.set_closure_mode(0)
+    flow = lambda C: api.closure_workspace_bytes(C, LANES_U16, dataflow=True)  # noqa: E731
+    plain = lambda C: api.closure_workspace_bytes(C, LANES_U16)  # noqa: E731
+    assert api.closure_schedule(1000, LANES_U16, flow(1000)) == 4
+    assert api.closure_schedule(2048, LANES_U16, flow(2048)) == 3
+    assert api.closure_schedule(2048, LANES_U32, flow(2048)) == 1
+    assert api.closure_schedule(16384, LANES_U16, flow(16384)) == 6
+    assert api.closure_schedule(16384, LANES_U16, plain(16384)) == 1  # too little workspace for 6
+    assert api.closure_schedule(128, LANES_U16, flow(128)) == 4
+    assert api.closure_schedule(0) == -1
 
 
 HOST_ALLOC_FAILURE = r"""

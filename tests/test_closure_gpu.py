@@ -189,15 +189,31 @@ def test_wide_micro_tile_schedules(orc, C):
     Q = P + np.uint32(70000)
     Q_ref = orc.strongest_paths(Q, "blocked", tile=16)
     try:
-        for mode in (3, 4, 5):
+        for mode in (3, 4, 5, 6):
             api.set_closure_mode(mode)
             for lanes in (LANES_U16, LANES_U32, LANES_AUTO):
                 assert np.array_equal(gpu_closure(P, lanes), S_ref), (mode, lanes)
             assert np.array_equal(gpu_closure(Q, LANES_AUTO), Q_ref), mode  # shifted 16-bit lanes
         api.set_closure_mode(0)
-        for table in ([(C, 3)], [(max(C - 1, 0), 1), (C, 4)], [(C, 5)], []):
+        for table in ([(C, 3)], [(max(C - 1, 0), 1), (C, 4)], [(C, 5)], [(C, 6)], []):
             api.set_closure_variants(table)
             assert np.array_equal(gpu_closure(P, LANES_U16), S_ref), table
     finally:
-        api.set_closure_variants([(1024, 4), (12288, 3)])  # the library's built-in table
+        api.set_closure_variants(api.BUILTIN_CLOSURE_VARIANTS)  # the library's built-in table
         api.set_closure_mode(0)
+
+
+def test_dropin_stages_large_numpy_inputs_through_pinned_memory():
+    """compute_strongest_paths with a pageable NumPy matrix of 144 MB (past the two 64 MiB
+    staging chunks, with a ragged last chunk): the same result as the device-resident path,
+    twice in a row (the staging buffers are reused)."""
+    C = 6001
+    rng = np.random.default_rng(6001)
+    P = rng.integers(0, 50000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    want = api._to_host_u32(api.strongest_paths_device(torch.from_numpy(P.view(np.int32)).cuda().view(torch.uint32),
+                                                       lanes=LANES_AUTO))
+    for _ in range(2):
+        got = api.compute_strongest_paths(P, allow_gpu=True, tile_size=32)
+        assert np.array_equal(got, want)
+    d = api._to_device_u32(P, torch.cuda.current_device())
+    assert torch.equal(d.view(torch.int32).cpu(), torch.from_numpy(P.view(np.int32)))
