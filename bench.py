@@ -53,7 +53,7 @@ def parse():
                     help="closure input: tallied Mallows ballots, or the reference's random matrix mode")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
-    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
+    ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
                     help="the closure's schedule: 0 automatic by size (default), 1 round by round, 2 dataflow, "
                          "3 wide panels, 4 wide panels and pivot launches, 5 two streams, 6 one launch per round "
                          "(include/se.h)")
@@ -105,7 +105,8 @@ def config(args, world):
         "phi": args.phi,
         "lanes": f"u{args.lanes}" if args.lanes else "auto",
         "closure_mode": {0: "automatic by size", 1: "round by round", 2: "dataflow", 3: "wide panels",
-                         4: "wide panels and pivots", 5: "two streams", 6: "one launch per round"}[args.closure_mode],
+                         4: "wide panels and pivots", 5: "two streams", 6: "one launch per round",
+                         7: "wide tiles", 8: "one wide launch per round"}[args.closure_mode],
         "tile": 128,
         "parallelism": f"replicas{world}" if world > 1 else "single",
         "l2": "inputs larger than L2 (0.5 GiB u16 working matrix), no flush",
@@ -312,7 +313,7 @@ def run_ours(args, world, rank, local_rank):
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
     api.set_closure_mode(args.closure_mode)
-    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode in (0, 2, 5, 6))
+    need = api.closure_workspace_bytes(C, lanes, dataflow=args.closure_mode in (0, 2, 5, 6, 8))
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()
@@ -688,7 +689,9 @@ def run_extras(args, local_rank, d, out, host_in, peak_mhz) -> dict:
     sweep = {}
     for mode, what in ((1, "panels and pivot on 8x8 words, pivot fused"), (3, "panels on 8x4 words, pivot fused"),
                        (4, "panels and pivot on 8x4 words, pivot launched"), (5, "as 3 on two streams"),
-                       (6, "remainder and next panels in one launch per round")):
+                       (6, "remainder and next panels in one launch per round"),
+                       (7, "every tile on 8x4 words, pivot fused"),
+                       (8, "as 6 with every tile on 8x4 words")):
         api.set_closure_mode(mode)
         o, _ = closure_object(d4, 16, max(steps, 20), 3, local_rank, what)
         sweep[str(mode)] = {"schedule": what, "ms": o["ms"], "value": o["value"],

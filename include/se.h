@@ -140,19 +140,22 @@ SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, in
  *   6  one launch per round: round k's remainder tiles and round k+1's panel tiles, the
  *      panels taking the remainder's last, partial wave (they wait, bounded, for the tiles
  *      of row and column k+1 and the next pivot, which the launch runs first). Needs
- *      se_closure_workspace_bytes_flow() of workspace (else the automatic schedule runs 1).
- * 3 and 4 differ from 1 in 16-bit lanes only. */
+ *      se_closure_workspace_bytes_flow() of workspace (else the automatic schedule runs 1);
+ *   7  as 3 with the remainder tiles on the wide micro-tile too (the fused pivot then closes
+ *      on eight warps);
+ *   8  as 6 with every tile on the wide micro-tile.
+ * 3, 4 and 7 differ from 1, and 8 from 6, in 16-bit lanes only. */
 SE_API se_status_t se_closure_set_mode(int mode);
 
 /* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
- * modes[i] (1, 3, 4, 5 or 6); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
- * table, measured on B200, is {C <= 1024: 4, C <= 3072: 3, larger: 6}. An autotuner
+ * modes[i] (1 or 3 to 8); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
+ * table, measured on B200, is {C <= 3584: 7, C <= 4096: 8, larger: 6}. An autotuner
  * measures the variants per size bucket and installs the winners (scalingelections_b200
  * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks
  * among its kernels' tile templates (scaling_elections.cu:895-901). */
 SE_API se_status_t se_closure_set_variant_table(const int* max_c, const int* modes, int n);
 
-/* The schedule (1 to 6) an se_closure call would run now for C candidates with lane_bits 16
+/* The schedule (1 to 8) an se_closure call would run now for C candidates with lane_bits 16
  * or 32 and work_bytes of workspace; -1 for C < 1. Host-only. */
 SE_API int se_closure_schedule(int C, int lane_bits, int64_t work_bytes);
 

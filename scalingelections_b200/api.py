@@ -150,7 +150,7 @@ def set_closure_mode(mode: int) -> None:
     _closure_mode = int(mode)
 
 
-BUILTIN_CLOSURE_VARIANTS = ((1024, 4), (3072, 3), (1 << 20, 6))
+BUILTIN_CLOSURE_VARIANTS = ((3584, 7), (4096, 8), (1 << 20, 6))
 
 
 def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_bytes: int | None = None) -> int:
@@ -159,14 +159,14 @@ def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_byte
     if int(num_candidates) < 1:
         return -1
     if workspace_bytes is None:
-        workspace_bytes = closure_workspace_bytes(num_candidates, lanes, dataflow=_closure_mode in (0, 2, 5, 6))
+        workspace_bytes = closure_workspace_bytes(num_candidates, lanes, dataflow=_closure_mode in (0, 2, 5, 6, 8))
     return int(_lib.lib().se_closure_schedule(int(num_candidates), int(lanes), int(workspace_bytes)))
 
 
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
     """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-6;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
-    the library starts with the table measured on B200, {1024: 4, 3072: 3, 2**20: 6}).
+    the library starts with the table measured on B200, {3584: 7, 4096: 8, 2**20: 6}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
     this."""
     n = len(table)
@@ -192,7 +192,7 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         return out
     # The dataflow (2), two-stream (5) and one-launch-per-round (6) schedules, which the
     # automatic one (0) may pick, use a second AT buffer: a few MiB more than the plain one.
-    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5, 6))
+    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5, 6, 8))
     if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = _workspace(need, preferences.device)
     have = workspace.numel() * workspace.element_size()

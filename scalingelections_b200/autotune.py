@@ -124,7 +124,7 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
 
 
 CLOSURE_BUCKETS = [1024, 2048, 3072, 4096, 6144, 8192, 12288]  # upper bounds of the size buckets
-CLOSURE_MODES = (1, 3, 4, 5, 6)
+CLOSURE_MODES = (1, 3, 4, 5, 6, 7, 8)
 
 
 def tune_closure(sizes: Sequence[int] | None = None, reps: int = 5, V: int = 4096, seed: int = 0,

@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
 // subset 0: all (R-1)^2 tiles of the round. subset 1: the tiles of row and column K+1 (2R - 3,
 // tile (K+1, K+1) first); subset 2: every other tile ((R-2)^2). The two-stream schedule runs
 // subset 1 and the next round's panels on the caller's stream while subset 2 runs on another.
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+template <int LB, int NQ = 8>
+__global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, int subset, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -121,14 +121,14 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         J = skip_k_k1(t % R2);
     }
     uint32_t par_a = 0, par_b = 0;
-    const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
+    const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
     }
     if (fuse_pivot && blockIdx.x == 0) {
         __syncthreads();  // the tile's stores are visible to the whole CTA
-        batch::run_pivot<LB>(E, K + 1, rowbuf, colbuf);
+        batch::run_pivot<LB, NQ>(E, K + 1, rowbuf, colbuf);
     }
 }
 
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
 // rows and columns K+1, which no remainder tile of the second group reads or writes; the tiles
 // they read are exactly the first group's. state: this round's ticket and done counters.
 // ------------------------------------------------------------------------------------------
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+template <int LB, int NQ = 8>
+__global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     round_kernel(const __grid_constant__ batch::Elec E, const __grid_constant__ batch::Elec En, int K,
                  uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
@@ -181,14 +181,14 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
             I = skip_k_k1(x / R2);
             J = skip_k_k1(x % R2);
         }
-        const bool ok = batch::run_tile<LB, false>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
+        const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
         if (!ok) {
             if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
             return;
         }
         if (t == 0) {
             __syncthreads();  // the tile's stores are visible to the whole CTA
-            batch::run_pivot<LB>(E, K + 1, rowbuf, colbuf);
+            batch::run_pivot<LB, NQ>(E, K + 1, rowbuf, colbuf);
         }
         if (t < first) {  // publish: the tile (and the pivot) are done, for TMA reads too
             __threadfence();
@@ -212,8 +212,8 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     const bool row = x < R1;
     const int y = row ? x : x - R1;
     const int K1 = K + 1;
-    const bool ok = batch::run_tile<LB, false>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1, y + (y >= K1),
-                                               y + (y >= K1), smem, bars, par_a, par_b);
+    const bool ok = batch::run_tile<LB, false, NQ>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1,
+                                                   y + (y >= K1), y + (y >= K1), smem, bars, par_a, par_b);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -656,7 +656,10 @@ layout plan(int C, int lane_bits) {
 //      the current round's bulk. AT is double-buffered (the dataflow layout's second buffer):
 //      needs se_closure_workspace_bytes_flow() of workspace, and R >= 4;
 //   6  round K's remainder and round K+1's panels in one launch (round_kernel): the panels
-//      take the remainder's last, partial wave. AT is double-buffered as in 5.
+//      take the remainder's last, partial wave. AT is double-buffered as in 5;
+//   7  as 3 with the remainder tiles on the wide micro-tile too, so the fused pivot closes on
+//      eight warps;
+//   8  as 6 with every tile on the wide micro-tile (16-bit lanes; 32-bit lanes run 6).
 // 3 and 4 apply to 16-bit lanes; 32-bit lanes run 1 for them (5 without the wide panels). Round by round is the default:
 // on B200 hardware block scheduling of one launch per phase beats the persistent grid's
 // claim-and-poll overhead at every size measured.
@@ -664,15 +667,15 @@ std::atomic<int> g_closure_mode{0};
 
 // The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds). The
 // built-in table is autotune.tune_closure's result on one B200 (16-bit lanes, ms per closure,
-// modes 1 / 3 / 4 / 5 / 6): C = 1024 0.745 / 0.714 / 0.689 / 0.723 / 0.725, C = 2048 1.491 /
-// 1.450 / 1.541 / 1.578 / 1.774, C = 3072 2.271 / 2.202 / 2.945 / 2.713 / 2.520, C = 4096
-// 4.005 / 3.924 / 5.199 / 4.213 / 3.555, C = 8192 25.12 / 24.97 / 27.54 / 27.10 / 24.95,
-// C = 16384 191.6 / 191.4 / 196.5 / 195.0 / 190.6.
+// three repeats agreeing within 1 % unless noted; modes 3 / 6 / 7 / 8): C = 2048 1.445 /
+// 1.713 / 1.320 / 1.517, C = 2560 1.82 / 2.05 / 1.66 / 1.68, C = 3584 2.74 / 2.97 / 2.74 /
+// 2.78, C = 4096 3.95 / 3.55 / 3.97 / 3.49, C = 4608 5.39 / 4.90 / 5.46 / 4.96, C = 6144
+// 11.07 / 11.01 / 11.35 / 11.37, C = 16384 192.2 / 190.8 / 198.0 / 199.9.
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
 int g_variant_n = 3;
-int g_variant_max_c[kMaxVariants] = {1024, 3072, 1 << 20};
-int g_variant_mode[kMaxVariants] = {4, 3, 6};
+int g_variant_max_c[kMaxVariants] = {3584, 4096, 1 << 20};
+int g_variant_mode[kMaxVariants] = {7, 8, 6};
 
 int automatic_mode(int C) {
     std::lock_guard<std::mutex> lock(g_variant_mutex);
@@ -688,6 +691,12 @@ template <int LB> se_status_t set_smem_limits() {
     if constexpr (LB == 16) {
         if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB, 4>), bytes,
                                               "the wide panel kernel"))
+            return st;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB, 4>), bytes,
+                                              "the wide remainder kernel"))
+            return st;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(round_kernel<LB, 4>), bytes,
+                                              "the wide round kernel"))
             return st;
     }
     if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB>), bytes, "the remainder kernel"))
@@ -798,7 +807,8 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     uint32_t* err = reinterpret_cast<uint32_t*>(work + P.flags_off);
     const int64_t ldw = P.Cp / CF::CPW;
     const int R = int(P.Cp / kT);
-    const bool wide = LB == 16 && (mode == 3 || mode == 4);
+    const bool wide = LB == 16 && (mode == 3 || mode == 4 || mode == 7);
+    const bool wide_rem = LB == 16 && mode == 7;
     const bool fused = !(LB == 16 && mode == 4);
 
     batch::Elec E;
@@ -823,7 +833,8 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         E2[1].AT = AT2;
         return run_two_streams<LB>(E2, R, stream, S, ldw, dT, err, phase_ms);
     }
-    if (mode == 6) {
+    if (mode == 6 || mode == 8) {
+        const bool wide8 = LB == 16 && mode == 8;
         batch::Elec E2[2] = {E, E};
         uint32_t* AT2 = reinterpret_cast<uint32_t*>(work + P.at2_off);
         if (se_status_t st = make_map(&E2[1].mapAT, AT2, uint64_t(P.Cp), kT, uint64_t(P.Cp) * 4, kT, kKC); st)
@@ -849,17 +860,39 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             return SE_OK;
         };
         if (se_status_t st = mark()) return st;
-        diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
+        if (wide8) {
+            if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, 0, dT);
+        } else {
+            diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
+        }
         if (se_status_t st = mark()) return st;
-        panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, err);
+        if (wide8) {
+            if constexpr (LB == 16)
+                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, err);
+        } else {
+            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, err);
+        }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
+        const int tasks = (R - 1) * (R - 1) + 2 * (R - 1);
         for (int K = 0; K + 1 < R; ++K) {
-            round_kernel<LB><<<(R - 1) * (R - 1) + 2 * (R - 1), CF::THREADS, smem, stream>>>(
-                E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K, err);
+            if (wide8) {
+                if constexpr (LB == 16)
+                    round_kernel<LB, 4><<<tasks, tile_threads<LB, 4>(), smem, stream>>>(E2[K & 1], E2[(K + 1) & 1], K,
+                                                                                       state + 2 * K, err);
+            } else {
+                round_kernel<LB><<<tasks, CF::THREADS, smem, stream>>>(E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K,
+                                                                       err);
+            }
             SE_CHECK_LAUNCH();
         }
-        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, err);
+        if (wide8) {
+            if constexpr (LB == 16)
+                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[(R - 1) & 1], R - 1,
+                                                                                              0, 0, err);
+        } else {
+            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, err);
+        }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
         if (phase_ms) {
@@ -915,7 +948,13 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
         }
         mark(1);
-        rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, 0, err);
+        if (wide_rem) {
+            if constexpr (LB == 16)
+                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(
+                    E, K, K + 1 < R ? 1 : 0, 0, err);
+        } else {
+            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, 0, err);
+        }
         mark(3);
         SE_CHECK_LAUNCH();
     }
@@ -1105,9 +1144,9 @@ se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t
     const bool automatic = mode == 0;
     if (automatic) mode = automatic_mode(C);
     if (mode == 5 && (P.Cp / kT < 4 || (automatic && work_bytes < P.flow_total))) mode = 3;
-    if (mode == 6 && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
+    if ((mode == 6 || mode == 8) && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
     const bool flow = mode == 2 && P.Cp > kT;
-    SE_REQUIRE((mode != 2 && mode != 5 && mode != 6) || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
+    SE_REQUIRE((mode != 2 && mode != 5 && mode != 6 && mode != 8) || work_bytes >= P.flow_total, SE_ERR_WORKSPACE,
                "the dataflow, two-stream and one-launch-per-round closures need a workspace of %lld bytes",
                (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
@@ -1189,7 +1228,7 @@ extern "C" se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k
 
 extern "C" se_status_t se_closure_set_mode(int mode) {
     clear_error();
-    SE_REQUIRE(mode >= 0 && mode <= 6, SE_ERR_INVALID, "closure mode must be 0 to 6");
+    SE_REQUIRE(mode >= 0 && mode <= 8, SE_ERR_INVALID, "closure mode must be 0 to 8");
     g_closure_mode.store(mode);
     return SE_OK;
 }
@@ -1201,8 +1240,9 @@ extern "C" int se_closure_schedule(int C, int lane_bits, int64_t work_bytes) {
     const bool automatic = mode == 0;
     if (automatic) mode = automatic_mode(C);
     if (mode == 5 && (P.Cp / kT < 4 || (automatic && work_bytes < P.flow_total))) mode = 3;
-    if (mode == 6 && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
-    if (lane_bits == 32 && (mode == 3 || mode == 4)) mode = 1;
+    if ((mode == 6 || mode == 8) && (P.Cp / kT < 2 || (automatic && work_bytes < P.flow_total))) mode = 1;
+    if (lane_bits == 32 && (mode == 3 || mode == 4 || mode == 7)) mode = 1;
+    if (lane_bits == 32 && mode == 8) mode = 6;
     return mode;
 }
 
@@ -1212,8 +1252,8 @@ extern "C" se_status_t se_closure_set_variant_table(const int* max_c, const int*
         SE_REQUIRE(n >= 0 && n <= kMaxVariants, SE_ERR_INVALID, "at most %d table entries", kMaxVariants);
         SE_REQUIRE(n == 0 || (max_c && modes), SE_ERR_INVALID, "null table");
         for (int i = 0; i < n; ++i)
-            SE_REQUIRE(modes[i] == 1 || (modes[i] >= 3 && modes[i] <= 6), SE_ERR_INVALID,
-                       "table modes must be 1, 3, 4, 5 or 6 (got %d)", modes[i]);
+            SE_REQUIRE(modes[i] == 1 || (modes[i] >= 3 && modes[i] <= 8), SE_ERR_INVALID,
+                       "table modes must be 1 or 3 to 8 (got %d)", modes[i]);
         std::lock_guard<std::mutex> lock(g_variant_mutex);
         for (int i = 0; i < n; ++i) {
             g_variant_max_c[i] = max_c[i];
@@ -1231,6 +1271,6 @@ extern "C" int se_closure_launch_count(int C) {
     if (mode == 0) mode = automatic_mode(C);
     // init, pivot of round 0, R x (panels, remainder), finalize; mode 4 adds a pivot launch
     // per later round (in 16-bit lanes), mode 5 a second remainder launch per round but the last.
-    if (mode == 6 && R >= 2) return 3 + R + 1;  // init, pivot, panels 0, R - 1 rounds, last remainder, finalize
+    if ((mode == 6 || mode == 8) && R >= 2) return 3 + R + 1;  // init, pivot, panels 0, R - 1 rounds, last, finalize
     return R == 1 ? 3 : 3 + 2 * R + (mode == 4 || (mode == 5 && R >= 4) ? R - 1 : 0);
 }

@@ -64,7 +64,7 @@ def test_closure_schedule_settings_need_no_gpu():
     assert L.se_closure_set_variant_table(max_c, ok, 9) == _lib.SE_ERR_INVALID
     assert L.se_closure_set_variant_table(max_c, ok, n) == _lib.SE_OK
     assert L.se_closure_set_variant_table(None, None, 0) == _lib.SE_OK
-    assert L.se_closure_set_mode(7) == _lib.SE_ERR_INVALID
+    assert L.se_closure_set_mode(9) == _lib.SE_ERR_INVALID
     for mode in (4, 0):
         assert L.se_closure_set_mode(mode) == _lib.SE_OK
     from scalingelections_b200 import api
@@ -83,12 +83,14 @@ def test_closure_schedule_query_needs_no_gpu():
     api.set_closure_mode(0)
     flow = lambda C: api.closure_workspace_bytes(C, LANES_U16, dataflow=True)  # noqa: E731
     plain = lambda C: api.closure_workspace_bytes(C, LANES_U16)  # noqa: E731
-    assert api.closure_schedule(1000, LANES_U16, flow(1000)) == 4
-    assert api.closure_schedule(2048, LANES_U16, flow(2048)) == 3
-    assert api.closure_schedule(2048, LANES_U32, flow(2048)) == 1
+    assert api.closure_schedule(1000, LANES_U16, flow(1000)) == 7
+    flow32 = lambda C: api.closure_workspace_bytes(C, LANES_U32, dataflow=True)  # noqa: E731
+    assert api.closure_schedule(2048, LANES_U32, flow32(2048)) == 1  # no wide micro-tile in 32-bit lanes
+    assert api.closure_schedule(4096, LANES_U16, flow(4096)) == 8
+    assert api.closure_schedule(4096, LANES_U32, flow32(4096)) == 6
+    assert api.closure_schedule(4096, LANES_U16, plain(4096)) == 1  # too little workspace for 8
     assert api.closure_schedule(16384, LANES_U16, flow(16384)) == 6
     assert api.closure_schedule(16384, LANES_U16, plain(16384)) == 1  # too little workspace for 6
-    assert api.closure_schedule(128, LANES_U16, flow(128)) == 4
     assert api.closure_schedule(0) == -1
 
 

@@ -189,7 +189,7 @@ def test_wide_micro_tile_schedules(orc, C):
     Q = P + np.uint32(70000)
     Q_ref = orc.strongest_paths(Q, "blocked", tile=16)
     try:
-        for mode in (3, 4, 5, 6):
+        for mode in (3, 4, 5, 6, 7, 8):
             api.set_closure_mode(mode)
             for lanes in (LANES_U16, LANES_U32, LANES_AUTO):
                 assert np.array_equal(gpu_closure(P, lanes), S_ref), (mode, lanes)
