@@ -237,15 +237,17 @@ def main_launches(R: int, mode: int) -> dict:
     launches, and the tile products they run (each 128^3 relaxations; the fused pivot's closure
     is extra and not counted). Schedule 6 runs R - 1 round launches of (R-1)^2 remainder tiles
     plus the next round's 2(R-1) panel tiles, then one plain remainder launch; the others run R
-    remainder launches of (R-1)^2 tiles (schedule 5: the whole closure, remainder and panels)."""
-    if mode == 6:
+    remainder launches of (R-1)^2 tiles (schedule 5: the whole closure, remainder and panels).
+    Schedules 7 and 8 run the kernels of 1 and 6 on the wide micro-tile."""
+    if mode in (6, 8):
         per = (R - 1) ** 2 + 2 * (R - 1)
-        return {"kernel": "round_kernel", "launches": R, "tiles_per_launch": per,
-                "tiles": (R - 1) * per + (R - 1) ** 2}
+        return {"kernel": "round_kernel" + (" (wide micro-tile)" if mode == 8 else ""), "launches": R,
+                "tiles_per_launch": per, "tiles": (R - 1) * per + (R - 1) ** 2}
     if mode == 5:
         return {"kernel": "rem_kernel and panels_kernel (two streams)", "launches": R,
                 "tiles_per_launch": (R - 1) ** 2 + 2 * (R - 1), "tiles": R * ((R - 1) ** 2 + 2 * (R - 1))}
-    return {"kernel": "rem_kernel", "launches": R, "tiles_per_launch": (R - 1) ** 2, "tiles": R * (R - 1) ** 2}
+    return {"kernel": "rem_kernel" + (" (wide micro-tile)" if mode == 7 else ""), "launches": R,
+            "tiles_per_launch": (R - 1) ** 2, "tiles": R * (R - 1) ** 2}
 
 
 def load_traffic(lanes: int, C: int, kernel: str):
