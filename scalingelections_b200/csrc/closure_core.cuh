@@ -162,79 +162,97 @@ __device__ __forceinline__ void store_transposed_splat(const uint32_t (&c)[8][NQ
 // two phases, each holding the rows and columns of two pivots.
 constexpr int kPivotBufs = 4;
 
-// Publishes row k and column k of the tile (the thread's share of them) into staging slot s.
-template <int LB, int NQ = 8>
-__device__ __forceinline__ void publish_pivot(const uint32_t (&c)[8][NQ], const geomT<NQ>& g, int k, uint32_t* row,
-                                              uint32_t* col) {
+// Publishes row k8 + J and column k8 + J of the tile into staging slot (row, col), for k8 a
+// multiple of 8 and J < 8 known at compile time. Row k8 + J is register row J of the threads
+// whose row0 is k8; column k8 + J is cell J % CPW of word (J / CPW) % 4 of a 4-word group,
+// held by the threads whose wbase (or wbase + 32) starts that group. So one uniform test per
+// row and per column group decides the stores, and the registers are indexed statically.
+// Indices past the tile (k8 = 128) match no thread.
+template <int LB, int NQ, int J>
+__device__ __forceinline__ void publish_pivot8(const uint32_t (&c)[8][NQ], const geomT<NQ>& g, int k8, uint32_t* row,
+                                               uint32_t* col) {
     constexpr int CPW = cfg<LB>::CPW;
+    constexpr int QW = (J / CPW) & 3, H = J % CPW;
+    if (g.row0 == k8) {
+        st4(row + g.wbase, &c[J][0]);
+        if constexpr (NQ == 8) st4(row + g.wbase + 32, &c[J][4]);
+    }
+    const int w4 = ((k8 + J) / CPW) & ~3;
+    auto put_col = [&](int q) {
+        uint32_t v[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
-        if (g.row0 + r == k) {
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) row[g.word(q)] = c[r][q];
-        }
-    const int wk = k / CPW, hk = k % CPW;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-        if (g.word(q) == wk) {
-#pragma unroll
-            for (int r = 0; r < 8; ++r) col[g.row0 + r] = cell_splat<LB>(c[r][q], hk);
-        }
+        for (int r = 0; r < 8; ++r) v[r] = cell_splat<LB>(c[r][q], H);
+        st4(col + g.row0, v);
+        st4(col + g.row0 + 4, v + 4);
+    };
+    if (g.wbase == w4) put_col(QW);
+    if constexpr (NQ == 8) {
+        if (g.wbase + 32 == w4) put_col(4 + QW);
+    }
 }
 
-// Closes the 128 x 128 tile held in registers (the thread's 8 x 8 words) in place over
-// pivots k = 0 .. kmax-1, two at a time. Rows and columns k and k+1 are published together
-// (before this pair's steps) through double-buffered shared slots, one barrier per pair. Each
-// thread applies step k to the row and column k+1 it reads:
+// Pivots k = k8 + J and k + 1 (J even, known at compile time) from staging slots s, s + 1,
+// then the publish of k + 2 and k + 3 into the other phase's slots and one barrier.
+template <int LB, int NQ, int J>
+__device__ __forceinline__ void pivot_pair(uint32_t (&c)[8][NQ], const geomT<NQ>& g, int k8,
+                                           uint32_t (*rowbuf)[cfg<LB>::TW], uint32_t (*colbuf)[kT]) {
+    using L = lanes<LB>;
+    constexpr int CPW = cfg<LB>::CPW;
+    constexpr int s = ((J >> 1) & 1) * 2, t = s ^ 2;
+    uint32_t a0[8], b0[NQ], a1[8], b1[NQ];
+    ld4(a0, &colbuf[s][g.row0]);
+    ld4(a0 + 4, &colbuf[s][g.row0 + 4]);
+    ld4(b0, &rowbuf[s][g.wbase]);
+    if constexpr (NQ == 8) ld4(b0 + 4, &rowbuf[s][g.wbase + 32]);
+    ld4(a1, &colbuf[s + 1][g.row0]);
+    ld4(a1 + 4, &colbuf[s + 1][g.row0 + 4]);
+    ld4(b1, &rowbuf[s + 1][g.wbase]);
+    if constexpr (NQ == 8) ld4(b1 + 4, &rowbuf[s + 1][g.wbase + 32]);
+    const uint32_t ckk1 = cell_splat<LB>(rowbuf[s][k8 / CPW + (J + 1) / CPW], (J + 1) % CPW);  // c[k][k+1]
+    const uint32_t ck1k = colbuf[s][k8 + J + 1];                                             // c[k+1][k]
+#pragma unroll
+    for (int r = 0; r < 8; ++r) a1[r] = L::vmax(a1[r], L::vmin(a0[r], ckk1));
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) b1[q] = L::vmax(b1[q], L::vmin(ck1k, b0[q]));
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
+    if constexpr (J + 2 < 8) {
+        publish_pivot8<LB, NQ, J + 2>(c, g, k8, rowbuf[t], colbuf[t]);
+        publish_pivot8<LB, NQ, J + 3>(c, g, k8, rowbuf[t + 1], colbuf[t + 1]);
+    } else {
+        publish_pivot8<LB, NQ, 0>(c, g, k8 + 8, rowbuf[t], colbuf[t]);
+        publish_pivot8<LB, NQ, 1>(c, g, k8 + 8, rowbuf[t + 1], colbuf[t + 1]);
+    }
+    __syncthreads();
+}
+
+// Closes the 128 x 128 tile held in registers (the thread's 8 x NQ words) in place over its
+// first kmax pivots, two at a time. Rows and columns k and k+1 are published together (before
+// this pair's steps) through double-buffered shared slots, one barrier per pair. Each thread
+// applies step k to the row and column k+1 it reads:
 //   c'[i][k+1] = max(c[i][k+1], min(c[i][k], c[k][k+1]))
 //   c'[k+1][j] = max(c[k+1][j], min(c[k+1][k], c[k][j]))
 // and then does both steps in one pass over its words:
 //   c[i][j] = max(c[i][j], min(c[i][k], c[k][j]), min(c'[i][k+1], c'[k+1][j]))
-// which is exactly two Floyd-Warshall steps. Every thread of the block must call it. Pivots
-// >= kmax are skipped, which is exact when those rows/columns are zero padding.
+// which is exactly two Floyd-Warshall steps. The pivot loop runs in groups of 8, so kmax is
+// rounded up to a multiple of 8: the extra pivots' rows and columns are zero padding, and a
+// step over a zero row and column changes nothing. Every thread of the block must call it.
 template <int LB, int NQ = 8>
 __device__ __forceinline__ void close_tile_in_registers(uint32_t (&c)[8][NQ], const geomT<NQ>& g, int kmax,
                                                         uint32_t (*rowbuf)[cfg<LB>::TW],
                                                         uint32_t (*colbuf)[kT]) {
-    using L = lanes<LB>;
-    constexpr int CPW = cfg<LB>::CPW;
-    publish_pivot<LB, NQ>(c, g, 0, rowbuf[0], colbuf[0]);
-    publish_pivot<LB, NQ>(c, g, 1, rowbuf[1], colbuf[1]);
+    const int kend = kmax >= kT ? kT : (kmax + 7) & ~7;
+    publish_pivot8<LB, NQ, 0>(c, g, 0, rowbuf[0], colbuf[0]);
+    publish_pivot8<LB, NQ, 1>(c, g, 0, rowbuf[1], colbuf[1]);
     __syncthreads();
 #pragma unroll 1
-    for (int k = 0; k < kmax; k += 2) {
-        const int s = ((k >> 1) & 1) * 2;  // this pair's slots
-        uint32_t a0[8], b0[NQ];
-        ld4(a0, &colbuf[s][g.row0]);
-        ld4(a0 + 4, &colbuf[s][g.row0 + 4]);
-        ld4(b0, &rowbuf[s][g.wbase]);
-        if constexpr (NQ == 8) ld4(b0 + 4, &rowbuf[s][g.wbase + 32]);
-        if (k + 1 < kmax) {
-            uint32_t a1[8], b1[NQ];
-            ld4(a1, &colbuf[s + 1][g.row0]);
-            ld4(a1 + 4, &colbuf[s + 1][g.row0 + 4]);
-            ld4(b1, &rowbuf[s + 1][g.wbase]);
-            if constexpr (NQ == 8) ld4(b1 + 4, &rowbuf[s + 1][g.wbase + 32]);
-            const uint32_t ckk1 = cell_splat<LB>(rowbuf[s][(k + 1) / CPW], (k + 1) % CPW);  // c[k][k+1]
-            const uint32_t ck1k = colbuf[s][k + 1];                                        // c[k+1][k]
-#pragma unroll
-            for (int r = 0; r < 8; ++r) a1[r] = L::vmax(a1[r], L::vmin(a0[r], ckk1));
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) b1[q] = L::vmax(b1[q], L::vmin(ck1k, b0[q]));
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax3(c[r][q], L::vmin(a0[r], b0[q]), L::vmin(a1[r], b1[q]));
-        } else {
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax(c[r][q], L::vmin(a0[r], b0[q]));
-        }
-        const int k2 = k + 2, t = s ^ 2;  // the next pair, into the other phase's slots
-        if (k2 < kmax) publish_pivot<LB, NQ>(c, g, k2, rowbuf[t], colbuf[t]);
-        if (k2 + 1 < kmax) publish_pivot<LB, NQ>(c, g, k2 + 1, rowbuf[t + 1], colbuf[t + 1]);
-        __syncthreads();
+    for (int k8 = 0; k8 < kend; k8 += 8) {
+        pivot_pair<LB, NQ, 0>(c, g, k8, rowbuf, colbuf);
+        pivot_pair<LB, NQ, 2>(c, g, k8, rowbuf, colbuf);
+        pivot_pair<LB, NQ, 4>(c, g, k8, rowbuf, colbuf);
+        pivot_pair<LB, NQ, 6>(c, g, k8, rowbuf, colbuf);
     }
 }
 
