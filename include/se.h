@@ -111,11 +111,15 @@ SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, 
                                        int64_t ld_out, int lane_bits, int tile, void* d_work,
                                        int64_t work_bytes, void* stream, double* phase_ms, int* launches);
 
-/* Workspace for the dataflow form of the closure (no barrier between pivot rounds): one
- * persistent launch whose task order runs the next round's pivot and panels ahead of the
- * current round's bulk. se_closure runs it only after se_closure_set_mode(2). Results are
- * identical to the default round-by-round form, which is faster on B200 at every size
- * measured (hardware block scheduling costs less than the persistent grid's claim and poll). */
+/* Workspace for every schedule of se_closure_set_mode at its fastest, a few MiB above
+ * se_closure_workspace_bytes: the dataflow form (mode 2: one persistent launch whose task order
+ * runs the next round's pivot and panels ahead of the current round's bulk; identical results,
+ * slower on B200 than the round-by-round forms at every size measured), the second AT buffer
+ * of modes 5, 6 and 8, and the split-K area of modes 1, 3, 4 and 7: with it, while the
+ * 2(R-1) panel tiles of a round times 4 fit one wave of two CTAs per SM (R <= 38, C <= 4864),
+ * each panel tile and the next pivot tile run as 4 CTAs over disjoint pivot chunks whose
+ * partial tiles the last one folds with a lane-wise max (exact), which shortens each round's
+ * chain at small C. */
 SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
 
 /* Task t (< R^3) of the dataflow closure's fixed order for R = ceil(C / 128) pivot blocks:
@@ -127,7 +131,8 @@ SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, in
  *   0  automatic (default): by C, from the variant table below; 1 where it has no entry;
  *   1  round by round: pivot, panels and remainder launches per round, panels and pivots on
  *      the default micro-tile (8 x 8 words per thread), the next round's pivot closed by the
- *      first CTA of the remainder launch;
+ *      first CTA of the remainder launch (with se_closure_workspace_bytes_flow() of workspace
+ *      and C <= 4864, panel tiles and the next pivot tile split-K, as that function says);
  *   2  dataflow: one persistent launch (needs se_closure_workspace_bytes_flow() of workspace);
  *   3  as 1 with the panels on the wide micro-tile (8 x 4 words per thread, twice the warps);
  *   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile;

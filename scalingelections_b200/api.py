@@ -127,7 +127,11 @@ def _check_matrix(t: torch.Tensor, name: str) -> tuple[int, int]:
 # Device-resident entry points
 # ------------------------------------------------------------------------------------------
 def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, dataflow: bool = False) -> int:
-    """Workspace bytes of the closure; dataflow=True sizes it for the barrier-free form (mode 2)."""
+    """Workspace bytes of the closure. dataflow=True sizes it for every schedule at its fastest:
+    the dataflow form (mode 2), the second AT buffer of modes 5, 6 and 8, and the split panel
+    tiles of the round-by-round modes 1, 3, 4 and 7 up to C = 4864: a few MiB more than the
+    plain workspace. With the plain one those modes run their tiles whole, the automatic
+    schedule runs 1 where it would pick 5, 6 or 8, and modes 2, 5, 6 and 8 set explicitly fail."""
     L = _lib.lib()
     fn = L.se_closure_workspace_bytes_flow if dataflow else L.se_closure_workspace_bytes
     n = fn(int(num_candidates), int(lanes), 0)
@@ -144,7 +148,8 @@ def set_closure_mode(mode: int) -> None:
     1 round by round, 2 the dataflow form, 3 round by round with the panels on the wide
     micro-tile, 4 as 3 with each pivot tile closed by its own wide launch, 5 as 3 on two
     streams so the next round's chain overlaps the current remainder, 6 each round's
-    remainder and the next round's panels in one launch (include/se.h)."""
+    remainder and the next round's panels in one launch, 7 as 3 with every tile on the wide
+    micro-tile, 8 as 6 on the wide micro-tile (include/se.h)."""
     global _closure_mode
     check(_lib.lib().se_closure_set_mode(int(mode)))
     _closure_mode = int(mode)
@@ -154,17 +159,17 @@ BUILTIN_CLOSURE_VARIANTS = ((3584, 7), (4096, 8), (1 << 20, 6))
 
 
 def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_bytes: int | None = None) -> int:
-    """The schedule (1 to 6) a closure of this size would run now (host-only query). The
+    """The schedule (1 to 8) a closure of this size would run now (host-only query). The
     workspace defaults to what strongest_paths_device allocates; -1 for no candidates."""
     if int(num_candidates) < 1:
         return -1
     if workspace_bytes is None:
-        workspace_bytes = closure_workspace_bytes(num_candidates, lanes, dataflow=_closure_mode in (0, 2, 5, 6, 8))
+        workspace_bytes = closure_workspace_bytes(num_candidates, lanes, dataflow=True)
     return int(_lib.lib().se_closure_schedule(int(num_candidates), int(lanes), int(workspace_bytes)))
 
 
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
-    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-6;
+    """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-8;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
     the library starts with the table measured on B200, {3584: 7, 4096: 8, 2**20: 6}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
@@ -190,9 +195,9 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         raise ValueError("out has the wrong shape")
     if C == 0:
         return out
-    # The dataflow (2), two-stream (5) and one-launch-per-round (6) schedules, which the
-    # automatic one (0) may pick, use a second AT buffer: a few MiB more than the plain one.
-    need = closure_workspace_bytes(C, lanes, dataflow=_closure_mode in (0, 2, 5, 6, 8))
+    # Every schedule at its fastest: the second AT buffer (modes 2, 5, 6, 8) and the split
+    # panel tiles of small closures take a few MiB more than the plain workspace.
+    need = closure_workspace_bytes(C, lanes, dataflow=True)
     if workspace is None or workspace.numel() * workspace.element_size() < need:
         workspace = _workspace(need, preferences.device)
     have = workspace.numel() * workspace.element_size()

@@ -209,6 +209,20 @@ constexpr int kTileRow = 0;
 constexpr int kTileCol = 1;
 constexpr int kTileRem = 2;
 
+// Split-K form of a tile task, for tasks on the critical path of a small closure: `parts` CTAs
+// each run pivot chunks [q * kChunks / parts, (q + 1) * kChunks / parts) of the product from
+// the tile's own cells and store that partial tile to scratch; the last of them to arrive
+// folds every partial into its own with a lane-wise max and stores the tile as the unsplit
+// task would. Exact: every partial is max(tile, part of the product), and max is associative
+// and idempotent. The last part resets the counter for the next use and reports itself in
+// `last` (a fused pivot that follows runs in that CTA only).
+struct SplitK {
+    int q, parts;
+    uint32_t* scratch;  // this task's partial tiles, [parts][kT][TW] words
+    uint32_t* counter;  // arrivals of this task's parts (0 before the first)
+    bool last;
+};
+
 // mapB / kb: where the pivot rows S[K][*] (B of row and remainder tiles, D of column tiles)
 // are read: by default G->mapS at row block K; a sharded closure passes the map of a
 // received panel buffer (kb = 0) or of its own slab (kb = the local row block).
@@ -219,10 +233,11 @@ constexpr int kTileRem = 2;
 // product (their copies too), with identical results.
 // NQ: words per thread, 8 (the default micro-tile) or 4 (the wide one, 256 threads, 16-bit
 // lanes); the block must have tile_threads<LB, NQ>() threads.
+// split: the split-K form above (nullptr: the whole product in this CTA).
 template <int LB, bool GLOBAL_MAPS = true, int NQ = 8>
 __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
                          uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1,
-                         int kvalid = -1, int rvalid = -1) {
+                         int kvalid = -1, int rvalid = -1, SplitK* split = nullptr) {
     using CF = cfg<LB>;
     constexpr int TW = CF::TW;
     uint32_t* As = reinterpret_cast<uint32_t*>(smem);
@@ -240,6 +255,10 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     if (rvalid < 0) rvalid = E.C - (kind == kTileRow ? K : I) * kT;
     const int nch = kvalid >= kT ? kChunks : (kvalid + kKC - 1) / kKC;  // chunks holding pivots
     const bool live = (g.row0 & ~31) < rvalid;                         // this warp holds real rows
+    // This CTA's chunks [ch_lo, ch_hi): all of them, or its part's share.
+    const int ch_lo = split ? split->q * (kChunks / split->parts) : 0;
+    const int ch_hi = split ? ch_lo + kChunks / split->parts : kChunks;
+    const int ch_end = nch < ch_hi ? nch : ch_hi;
     if (kind != kTileCol) {
         const bool rem = kind == kTileRem;
         const CUtensorMap* mapA = rem ? &G->mapAT : &G->mapDT;
@@ -251,7 +270,7 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             fence_proxy_async();  // this CTA's earlier shared reads before the TMA rewrites them
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
-                if (ch >= nch) {
+                if (ch < ch_lo || ch >= ch_end) {
                     mbar_arrive(&bars[ch]);
                     continue;
                 }
@@ -298,7 +317,7 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             fence_proxy_async();
 #pragma unroll
             for (int ch = 0; ch < kChunks; ++ch) {
-                if (ch >= nch) {
+                if (ch < ch_lo || ch >= ch_end) {
                     mbar_arrive(&bars[kChunks + ch]);
                     continue;
                 }
@@ -313,15 +332,42 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
         par_b ^= 1u;
     }
     if (ok) {
-        // Chunks past nch: thread 0 completed their phases without a copy; nobody waits.
+        // Chunks outside [ch_lo, ch_end): thread 0 completed their phases without a copy;
+        // nobody waits.
 #pragma unroll 1
-        for (int ch = 0; ch < nch; ++ch) {
+        for (int ch = ch_lo; ch < ch_end; ++ch) {
             if (!mbar_wait_bounded(&wait_bars[ch], wait_par, 1u << 26)) {
                 ok = false;
                 break;
             }
             if (live) relax_chunk<LB, NQ>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
         }
+    }
+    if (ok && split != nullptr) {
+        using L = lanes<LB>;
+        constexpr int64_t kTileWords = int64_t(kT) * TW;
+        __shared__ uint32_t s_arrived;
+        store_tile_regs<LB, NQ>(c, split->scratch + split->q * kTileWords, TW, g);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) s_arrived = atomicAdd(split->counter, 1u);
+        __syncthreads();
+        split->last = s_arrived == uint32_t(split->parts - 1);
+        if (!split->last) return ok;
+        __threadfence();  // the other parts' partials, counted before our arrival, are visible
+        for (int p = 0; p < split->parts; ++p) {
+            if (p == split->q) continue;
+            const uint32_t* src = split->scratch + p * kTileWords;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                uint32_t v[NQ];
+                ld4_cg(v, src + int64_t(g.row0 + r) * TW + g.wbase);
+                if constexpr (NQ == 8) ld4_cg(v + 4, src + int64_t(g.row0 + r) * TW + g.wbase + 32);
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax(c[r][q], v[q]);
+            }
+        }
+        if (threadIdx.x == 0) *split->counter = 0u;
     }
     if (ok) {
         store_tile_regs<LB, NQ>(c, Ct, ldw, g);

@@ -52,9 +52,12 @@ constexpr uint32_t kMaxPolls = 1u << 26;
 // max(S[I][K], S[I][K] (x) D), which also emit the transposed panel AT. 96 KiB of shared
 // memory per CTA, so both sets are resident at once.
 // ------------------------------------------------------------------------------------------
+// With parts > 1 every panel tile runs split-K over `parts` consecutive blocks (batch::SplitK):
+// split_ctr[b] and split_scr[b * parts ...] are tile b's counter and partial tiles.
 template <int LB, int NQ = 8>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
-    panels_kernel(const __grid_constant__ batch::Elec E, int K, uint32_t* __restrict__ err) {
+    panels_kernel(const __grid_constant__ batch::Elec E, int K, int parts, uint32_t* __restrict__ split_ctr,
+                  uint32_t* __restrict__ split_scr, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + batch::pcfg<LB>::DATA);
     if (threadIdx.x == 0) {
@@ -63,13 +66,16 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     }
     __syncthreads();
     const int R1 = E.R - 1;
-    const int b = blockIdx.x;
+    const int b = blockIdx.x / parts;
     bool ok;
     uint32_t par_a = 0, par_b = 0;
     const bool row = b < R1;
     const int x = row ? b : b - R1;
+    batch::SplitK sp{int(blockIdx.x % parts), parts, split_scr + int64_t(b) * parts * kT * cfg<LB>::TW,
+                     split_ctr + b, false};
     ok = batch::run_tile<LB, false, NQ>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K),
-                                        x + (x >= K), smem, bars, par_a, par_b);
+                                        x + (x >= K), smem, bars, par_a, par_b, nullptr, -1, -1, -1,
+                                        parts > 1 ? &sp : nullptr);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -82,9 +88,13 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
 // subset 0: all (R-1)^2 tiles of the round. subset 1: the tiles of row and column K+1 (2R - 3,
 // tile (K+1, K+1) first); subset 2: every other tile ((R-2)^2). The two-stream schedule runs
 // subset 1 and the next round's panels on the caller's stream while subset 2 runs on another.
+// With fuse_pivot and parts > 1 (subset 0 only), blocks [0, parts) run tile (K+1, K+1) split-K
+// (batch::SplitK, counter split_ctr, partials split_scr) and the last of them closes the
+// pivot; the grid then has parts - 1 more blocks than tiles.
 template <int LB, int NQ = 8>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
-    rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, int subset, uint32_t* __restrict__ err) {
+    rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, int subset, int parts,
+               uint32_t* __restrict__ split_ctr, uint32_t* __restrict__ split_scr, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
@@ -97,10 +107,13 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     __syncthreads();
     const int R1 = E.R - 1, R2 = E.R - 2;
     int t = blockIdx.x, I, J;
+    const bool split = subset == 0 && fuse_pivot && parts > 1;
+    const int q = split && t < parts ? t : -1;  // this block's part of tile (K+1, K+1)
     auto skip_k_k1 = [K](int n) { return n < K ? n : n + 2; };  // n-th block index other than K, K+1
     if (subset == 0) {
         if (fuse_pivot) {
             const int p = K * R1 + K;  // reduced coordinates of tile (K+1, K+1)
+            if (split) t = q >= 0 ? 0 : t - parts + 1;
             t = t == 0 ? p : (t == p ? 0 : t);
         }
         const int ii = t / R1, jj = t % R1;
@@ -121,12 +134,14 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
         J = skip_k_k1(t % R2);
     }
     uint32_t par_a = 0, par_b = 0;
-    const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
+    batch::SplitK sp{q, parts, split_scr, split_ctr, false};
+    const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b,
+                                                   nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
     }
-    if (fuse_pivot && blockIdx.x == 0) {
+    if (fuse_pivot && (q >= 0 ? sp.last : !split && blockIdx.x == 0)) {
         __syncthreads();  // the tile's stores are visible to the whole CTA
         batch::run_pivot<LB, NQ>(E, K + 1, rowbuf, colbuf);
     }
@@ -620,9 +635,17 @@ struct layout {
     int64_t C = 0;
     int64_t Cp = 0;
     int64_t flags_off = 0, s_off = 0, at_off = 0, dt_off = 0, total = 0;
-    // Dataflow extras: second AT and dT buffers and the task state.
-    int64_t at2_off = 0, dt2_off = 0, state_off = 0, flow_total = 0;
+    // Dataflow extras: second AT and dT buffers and the task state; then the split-K area of
+    // the round-by-round schedules: 2R counters and the partial tiles of the 2(R-1) panel
+    // tiles and the next pivot tile.
+    int64_t at2_off = 0, dt2_off = 0, state_off = 0, split_ctr_off = 0, split_scr_off = 0, flow_total = 0;
 };
+
+// Parts of a split panel task for R row blocks: 4 while the 2(R-1) panel tiles times 4 fit one
+// wave of two CTAs per SM on a 148-SM B200 (R <= 38, C <= 4864), else 1. Measured on B200:
+// 15-19 % off the whole closure at C = 512-2048, neutral at 3072-4096; 2 parts at R = 40-64
+// cost 1-2 %, as the remainder bulk, not the chain, bounds those rounds.
+int split_parts(int R) { return R >= 2 && R - 1 <= 37 ? 4 : 1; }
 
 layout plan(int C, int lane_bits) {
     layout L;
@@ -638,7 +661,11 @@ layout plan(int C, int lane_bits) {
     L.at2_off = round_up(L.total, 256);
     L.dt2_off = L.at2_off + round_up(int64_t(kT) * L.Cp * 4, 256);
     L.state_off = L.dt2_off + round_up(int64_t(kT) * kT * 4, 256);
-    L.flow_total = L.state_off + (4 + R * R + 2 * R) * 4;
+    L.split_ctr_off = round_up(L.state_off + (4 + R * R + 2 * R) * 4, 256);
+    L.split_scr_off = L.split_ctr_off + round_up(2 * R * 4, 256);
+    const int parts = split_parts(int(R));
+    const int64_t split_tiles = parts > 1 ? (2 * (R - 1) + 1) * parts : 0;
+    L.flow_total = L.split_scr_off + split_tiles * kT * kT * cell;
     return L;
 }
 
@@ -764,8 +791,10 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     cudaEvent_t* remb = ev.data() + R;
     if (phase_ms) SE_CUDA_TRY(cudaEventRecord(ev[2 * R], A));
     auto panels = [&](int K) {
-        if constexpr (wide) panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, A>>>(E[K & 1], K, err);
-        else panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, A>>>(E[K & 1], K, err);
+        if constexpr (wide)
+            panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, A>>>(E[K & 1], K, 1, nullptr, nullptr,
+                                                                                 err);
+        else panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, A>>>(E[K & 1], K, 1, nullptr, nullptr, err);
     };
     if constexpr (wide) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, A>>>(S, ldw, 0, dT);
     else diag_kernel<LB><<<1, CF::THREADS, 0, A>>>(S, ldw, 0, dT);
@@ -775,16 +804,17 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     const int R2 = R - 2;
     for (int K = 0; K + 1 < R; ++K) {
         SE_CUDA_TRY(cudaStreamWaitEvent(B, pan[K], 0));
-        rem_kernel<LB><<<R2 * R2, CF::THREADS, smem, B>>>(E[K & 1], K, 0, 2, err);
+        rem_kernel<LB><<<R2 * R2, CF::THREADS, smem, B>>>(E[K & 1], K, 0, 2, 1, nullptr, nullptr, err);
         SE_CUDA_TRY(cudaEventRecord(remb[K], B));
         if (K > 0) SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[K - 1], 0));
-        rem_kernel<LB><<<2 * R - 3, CF::THREADS, smem, A>>>(E[K & 1], K, 1, 1, err);
+        rem_kernel<LB><<<2 * R - 3, CF::THREADS, smem, A>>>(E[K & 1], K, 1, 1, 1, nullptr, nullptr, err);
         panels(K + 1);
         SE_CHECK_LAUNCH();
         SE_CUDA_TRY(cudaEventRecord(pan[K + 1], A));
     }
     SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[R - 2], 0));
-    rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, A>>>(E[(R - 1) & 1], R - 1, 0, 0, err);
+    rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, A>>>(E[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr,
+                                                                err);
     SE_CHECK_LAUNCH();
     if (phase_ms) {
         SE_CUDA_TRY(cudaEventRecord(ev[2 * R + 1], A));
@@ -797,8 +827,10 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     return SE_OK;
 }
 
+// split_room: the workspace holds the split-K area (layout split_ctr_off..flow_total).
 template <int LB>
-se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms, int mode) {
+se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, double* phase_ms, int mode,
+                       bool split_room) {
     using CF = cfg<LB>;
     if (se_status_t st = set_smem_limits<LB>(); st != SE_OK) return st;
     uint32_t* S = reinterpret_cast<uint32_t*>(work + P.s_off);
@@ -868,9 +900,10 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         if (se_status_t st = mark()) return st;
         if (wide8) {
             if constexpr (LB == 16)
-                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, err);
+                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, 1, nullptr,
+                                                                                          nullptr, err);
         } else {
-            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, err);
+            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, 1, nullptr, nullptr, err);
         }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
@@ -888,10 +921,11 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         }
         if (wide8) {
             if constexpr (LB == 16)
-                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[(R - 1) & 1], R - 1,
-                                                                                              0, 0, err);
+                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(
+                    E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr, err);
         } else {
-            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, err);
+            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr,
+                                                                             nullptr, err);
         }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
@@ -929,6 +963,12 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         if (cudaEventCreate(&start) != cudaSuccess) SE_CUDA_TRY(cudaGetLastError());
         cudaEventRecord(start, stream);
     }
+    // Split-K panels and next pivot tile (batch::SplitK) where the rounds are few enough for
+    // the split tasks to fit one wave; the counters start at zero.
+    const int parts = split_room ? split_parts(R) : 1;
+    uint32_t* split_ctr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_ctr_off) : nullptr;
+    uint32_t* split_scr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_scr_off) : nullptr;
+    if (parts > 1) SE_CUDA_TRY(cudaMemsetAsync(split_ctr, 0, size_t(2 * R) * 4, stream));
     auto pivot = [&](int K) {
         if (wide) {
             if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, K, dT);
@@ -941,19 +981,26 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     SE_CHECK_LAUNCH();
     for (int K = 0; K < R && R > 1; ++K) {
         if (K > 0 && !fused) pivot(K);
+        const unsigned panel_blocks = unsigned(2 * (R - 1) * parts);
         if (wide) {
             if constexpr (LB == 16)
-                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E, K, err);
+                panels_kernel<LB, 4><<<panel_blocks, tile_threads<LB, 4>(), smem, stream>>>(E, K, parts, split_ctr,
+                                                                                           split_scr, err);
         } else {
-            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E, K, err);
+            panels_kernel<LB><<<panel_blocks, CF::THREADS, smem, stream>>>(E, K, parts, split_ctr, split_scr, err);
         }
         mark(1);
+        // Tile (K+1, K+1) and its pivot: counter and partials after the panel tiles'.
+        const int fuse = fused && K + 1 < R ? 1 : 0;
+        const unsigned rem_blocks = unsigned((R - 1) * (R - 1) + (fuse && parts > 1 ? parts - 1 : 0));
+        uint32_t* pctr = split_ctr ? split_ctr + 2 * (R - 1) : nullptr;
+        uint32_t* pscr = split_scr ? split_scr + int64_t(2 * (R - 1)) * parts * kT * CF::TW : nullptr;
         if (wide_rem) {
             if constexpr (LB == 16)
-                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(
-                    E, K, K + 1 < R ? 1 : 0, 0, err);
+                rem_kernel<LB, 4><<<rem_blocks, tile_threads<LB, 4>(), smem, stream>>>(E, K, fuse, 0, parts, pctr,
+                                                                                      pscr, err);
         } else {
-            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E, K, fused && K + 1 < R ? 1 : 0, 0, err);
+            rem_kernel<LB><<<rem_blocks, CF::THREADS, smem, stream>>>(E, K, fuse, 0, parts, pctr, pscr, err);
         }
         mark(3);
         SE_CHECK_LAUNCH();
@@ -1150,8 +1197,8 @@ se_status_t closure_run(const uint32_t* d_pref, int64_t ld_pref, int C, uint32_t
                "the dataflow, two-stream and one-launch-per-round closures need a workspace of %lld bytes",
                (long long)P.flow_total);
     se_status_t st = flow ? (lb == 16 ? run_flow<16>(work, P, s, phase_ms) : run_flow<32>(work, P, s, phase_ms))
-                          : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms, mode)
-                                      : run_rounds<32>(work, P, s, phase_ms, mode));
+                          : (lb == 16 ? run_rounds<16>(work, P, s, phase_ms, mode, work_bytes >= P.flow_total)
+                                      : run_rounds<32>(work, P, s, phase_ms, mode, work_bytes >= P.flow_total));
     if (st) return st;
     st = lb == 16 ? launch_finalize<16>(P, work, C, d_out, ld_out, base, s)
                   : launch_finalize<32>(P, work, C, d_out, ld_out, 0, s);

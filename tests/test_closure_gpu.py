@@ -5,7 +5,7 @@ import pytest
 import torch
 
 from conftest import golden_names, load_golden
-from scalingelections_b200 import LANES_AUTO, LANES_U16, LANES_U32, api
+from scalingelections_b200 import LANES_AUTO, LANES_U16, LANES_U32, _lib, api
 
 pytestmark = pytest.mark.gpu
 
@@ -200,6 +200,42 @@ def test_wide_micro_tile_schedules(orc, C):
             assert np.array_equal(gpu_closure(P, LANES_U16), S_ref), table
     finally:
         api.set_closure_variants(api.BUILTIN_CLOSURE_VARIANTS)  # the library's built-in table
+        api.set_closure_mode(0)
+
+
+def closure_with_workspace(P, lanes, work_bytes):
+    """se_closure through the C ABI with exactly work_bytes of workspace."""
+    C = P.shape[0]
+    d = api._to_device_u32(np.ascontiguousarray(P, dtype=np.uint32), "cuda")
+    out = torch.empty((C, C), dtype=torch.uint32, device="cuda")
+    work = torch.empty(work_bytes, dtype=torch.uint8, device="cuda")
+    _lib.check(_lib.lib().se_closure(d.data_ptr(), C, C, out.data_ptr(), C, int(lanes), 0, work.data_ptr(),
+                                     work_bytes, torch.cuda.current_stream().cuda_stream))
+    return api._to_host_u32(out)
+
+
+@pytest.mark.parametrize("C", [129, 257, 700, 2305, 4864, 4865])
+def test_split_panels_match_unsplit(orc, C):
+    """The round-by-round schedules split each panel tile and the next pivot tile over 4 pivot
+    chunks when the workspace has the split area (up to 38 row blocks, C = 4864): the same
+    matrix with the full and the plain workspace (which runs the tiles whole) gives identical
+    results in schedules 1, 3, 4 and 7 and both lane widths, and equals the oracle where the
+    oracle is quick."""
+    rng = np.random.default_rng(C + 11)
+    P = rng.integers(0, 9000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    S_ref = orc.strongest_paths(P, "blocked", tile=16) if C <= 2400 else None
+    try:
+        for mode in (1, 3, 4, 7):
+            api.set_closure_mode(mode)
+            for lanes in (LANES_U16, LANES_U32):
+                full = api.closure_workspace_bytes(C, lanes, dataflow=True)
+                plain = api.closure_workspace_bytes(C, lanes, dataflow=False)
+                split = closure_with_workspace(P, lanes, full)
+                whole = closure_with_workspace(P, lanes, plain)
+                assert np.array_equal(split, whole), (mode, lanes)
+                if S_ref is not None:
+                    assert np.array_equal(split, S_ref), (mode, lanes)
+    finally:
         api.set_closure_mode(0)
 
 
