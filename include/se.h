@@ -115,11 +115,10 @@ SE_API se_status_t se_closure_profiled(const uint32_t* d_pref, int64_t ld_pref, 
  * se_closure_workspace_bytes: the dataflow form (mode 2: one persistent launch whose task order
  * runs the next round's pivot and panels ahead of the current round's bulk; identical results,
  * slower on B200 than the round-by-round forms at every size measured), the second AT buffer
- * of modes 5, 6 and 8, and the split-K area of modes 1, 3, 4 and 7: with it, while the
- * 2(R-1) panel tiles of a round times 4 fit one wave of two CTAs per SM (R <= 38, C <= 4864),
- * each panel tile and the next pivot tile run as 4 CTAs over disjoint pivot chunks whose
- * partial tiles the last one folds with a lane-wise max (exact), which shortens each round's
- * chain at small C. */
+ * of modes 5, 6 and 8, and the split-K area of modes 1, 3, 4, 6, 7 and 8: with it, for R <= 28
+ * row blocks (C <= 3584), each panel tile and the next pivot tile run as 4 CTAs over disjoint
+ * pivot chunks whose partial tiles the last one folds with a lane-wise max (exact), which
+ * shortens each round's chain at small C. */
 SE_API int64_t se_closure_workspace_bytes_flow(int C, int lane_bits, int tile);
 
 /* Task t (< R^3) of the dataflow closure's fixed order for R = ceil(C / 128) pivot blocks:
@@ -132,7 +131,7 @@ SE_API se_status_t se_closure_flow_task(uint32_t t, int R, int* kind, int* k, in
  *   1  round by round: pivot, panels and remainder launches per round, panels and pivots on
  *      the default micro-tile (8 x 8 words per thread), the next round's pivot closed by the
  *      first CTA of the remainder launch (with se_closure_workspace_bytes_flow() of workspace
- *      and C <= 4864, panel tiles and the next pivot tile split-K, as that function says);
+ *      and C <= 3584, panel tiles and the next pivot tile split-K, as that function says);
  *   2  dataflow: one persistent launch (needs se_closure_workspace_bytes_flow() of workspace);
  *   3  as 1 with the panels on the wide micro-tile (8 x 4 words per thread, twice the warps);
  *   4  as 3 with every pivot tile closed by its own launch on the wide micro-tile;
@@ -154,7 +153,7 @@ SE_API se_status_t se_closure_set_mode(int mode);
 
 /* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
  * modes[i] (1 or 3 to 8); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
- * table, measured on B200, is {C <= 3584: 7, C <= 4096: 8, larger: 6}. An autotuner
+ * table, measured on B200, is {C <= 2048: 7, C <= 4096: 8, larger: 6}. An autotuner
  * measures the variants per size bucket and installs the winners (scalingelections_b200
  * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks
  * among its kernels' tile templates (scaling_elections.cu:895-901). */

@@ -129,7 +129,7 @@ def _check_matrix(t: torch.Tensor, name: str) -> tuple[int, int]:
 def closure_workspace_bytes(num_candidates: int, lanes: int = LANES_AUTO, dataflow: bool = False) -> int:
     """Workspace bytes of the closure. dataflow=True sizes it for every schedule at its fastest:
     the dataflow form (mode 2), the second AT buffer of modes 5, 6 and 8, and the split panel
-    tiles of the round-by-round modes 1, 3, 4 and 7 up to C = 4864: a few MiB more than the
+    tiles of modes 1, 3, 4, 6, 7 and 8 up to C = 3584: a few MiB more than the
     plain workspace. With the plain one those modes run their tiles whole, the automatic
     schedule runs 1 where it would pick 5, 6 or 8, and modes 2, 5, 6 and 8 set explicitly fail."""
     L = _lib.lib()
@@ -155,7 +155,7 @@ def set_closure_mode(mode: int) -> None:
     _closure_mode = int(mode)
 
 
-BUILTIN_CLOSURE_VARIANTS = ((3584, 7), (4096, 8), (1 << 20, 6))
+BUILTIN_CLOSURE_VARIANTS = ((2048, 7), (4096, 8), (1 << 20, 6))
 
 
 def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_bytes: int | None = None) -> int:
@@ -171,7 +171,7 @@ def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_byte
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
     """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-8;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
-    the library starts with the table measured on B200, {3584: 7, 4096: 8, 2**20: 6}).
+    the library starts with the table measured on B200, {2048: 7, 4096: 8, 2**20: 6}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
     this."""
     n = len(table)

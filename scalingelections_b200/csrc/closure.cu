@@ -160,11 +160,15 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
 // They write AT[(K+1) % 2] while the remainder reads AT[K % 2] (descriptors E and En), and
 // rows and columns K+1, which no remainder tile of the second group reads or writes; the tiles
 // they read are exactly the first group's. state: this round's ticket and done counters.
+// With parts > 1, tile (K+1, K+1) takes tickets [0, parts) and every panel tile `parts`
+// consecutive tickets, split-K (batch::SplitK; counters and partials as in panels_kernel and
+// rem_kernel): the last part of tile (K+1, K+1) closes the pivot and counts the tile done.
 // ------------------------------------------------------------------------------------------
 template <int LB, int NQ = 8>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     round_kernel(const __grid_constant__ batch::Elec E, const __grid_constant__ batch::Elec En, int K,
-                 uint32_t* __restrict__ state, uint32_t* __restrict__ err) {
+                 uint32_t* __restrict__ state, int parts, uint32_t* __restrict__ split_ctr,
+                 uint32_t* __restrict__ split_scr, uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
@@ -180,32 +184,40 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     __syncthreads();
     const uint32_t t = s_ticket;
     const int R = E.R, R1 = R - 1, R2 = R - 2;
-    const uint32_t first = uint32_t(2 * R - 3), rem = uint32_t(R1) * uint32_t(R1);
+    const uint32_t P = uint32_t(parts);
+    constexpr int64_t kTileWords = int64_t(kT) * CF::TW;
+    // Remainder tickets: tile (K+1, K+1) in [0, P), the rest of the first group (row and column
+    // K+1) up to P - 1 + first, the other tiles up to nrem.
+    const uint32_t first = uint32_t(2 * R - 3), rem = uint32_t(R1) * uint32_t(R1), nrem = rem + P - 1;
     auto skip_k_k1 = [K](int n) { return n < K ? n : n + 2; };  // n-th block index other than K, K+1
     uint32_t par_a = 0, par_b = 0;
-    if (t < rem) {
+    if (t < nrem) {
         int I, J;
-        if (t == 0) {
+        const int q = P > 1 && t < P ? int(t) : -1;  // this ticket's part of tile (K+1, K+1)
+        if (t < P) {
             I = J = K + 1;
-        } else if (t < first) {
-            const int x = int(t) - 1;
+        } else if (t < P - 1 + first) {
+            const int x = int(t - P);
             I = x < R2 ? K + 1 : skip_k_k1(x - R2);
             J = x < R2 ? skip_k_k1(x) : K + 1;
         } else {
-            const int x = int(t - first);
+            const int x = int(t - (P - 1) - first);
             I = skip_k_k1(x / R2);
             J = skip_k_k1(x % R2);
         }
-        const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b);
+        batch::SplitK sp{q, parts, split_scr + int64_t(2 * R1) * parts * kTileWords, split_ctr + 2 * R1, false};
+        const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b,
+                                                       nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
         if (!ok) {
             if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
             return;
         }
-        if (t == 0) {
+        if (q >= 0 && !sp.last) return;  // an earlier part: the last one finishes the tile
+        if (t < P) {
             __syncthreads();  // the tile's stores are visible to the whole CTA
             batch::run_pivot<LB, NQ>(E, K + 1, rowbuf, colbuf);
         }
-        if (t < first) {  // publish: the tile (and the pivot) are done, for TMA reads too
+        if (t < P - 1 + first) {  // publish: the tile (and the pivot) are done, for TMA reads too
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -223,12 +235,14 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     }
     __syncthreads();
     if (!s_go) return;
-    const int x = int(t - rem);
-    const bool row = x < R1;
-    const int y = row ? x : x - R1;
+    const int b = int((t - nrem) / P);  // the panel tile
+    const bool row = b < R1;
+    const int y = row ? b : b - R1;
     const int K1 = K + 1;
+    batch::SplitK sp{int((t - nrem) % P), parts, split_scr + int64_t(b) * parts * kTileWords, split_ctr + b, false};
     const bool ok = batch::run_tile<LB, false, NQ>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1,
-                                                   y + (y >= K1), y + (y >= K1), smem, bars, par_a, par_b);
+                                                   y + (y >= K1), y + (y >= K1), smem, bars, par_a, par_b, nullptr,
+                                                   -1, -1, -1, P > 1 ? &sp : nullptr);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -641,11 +655,12 @@ struct layout {
     int64_t at2_off = 0, dt2_off = 0, state_off = 0, split_ctr_off = 0, split_scr_off = 0, flow_total = 0;
 };
 
-// Parts of a split panel task for R row blocks: 4 while the 2(R-1) panel tiles times 4 fit one
-// wave of two CTAs per SM on a 148-SM B200 (R <= 38, C <= 4864), else 1. Measured on B200:
-// 15-19 % off the whole closure at C = 512-2048, neutral at 3072-4096; 2 parts at R = 40-64
-// cost 1-2 %, as the remainder bulk, not the chain, bounds those rounds.
-int split_parts(int R) { return R >= 2 && R - 1 <= 37 ? 4 : 1; }
+// Parts of a split panel task for R row blocks: 4 up to R = 28 (C <= 3584), else 1. Measured on
+// B200: 15-19 % off the whole closure at C = 512-2048 in the round-by-round schedules and up to
+// 11 % in the one-launch-per-round ones; from R = 32 the remainder bulk, not the chain, bounds
+// the rounds, and the split cost 7 % in the one-launch schedules at C = 4096-4608 (their unsplit
+// panels already fill the remainder's last wave) and 1-2 % at R = 40-64 with 2 parts.
+int split_parts(int R) { return R >= 2 && R <= 28 ? 4 : 1; }
 
 layout plan(int C, int lane_bits) {
     layout L;
@@ -701,7 +716,7 @@ std::atomic<int> g_closure_mode{0};
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
 int g_variant_n = 3;
-int g_variant_max_c[kMaxVariants] = {3584, 4096, 1 << 20};
+int g_variant_max_c[kMaxVariants] = {2048, 4096, 1 << 20};
 int g_variant_mode[kMaxVariants] = {7, 8, 6};
 
 int automatic_mode(int C) {
@@ -857,6 +872,12 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     E.R = R;
     E.lanes = LB;
     const size_t smem = batch::pcfg<LB>::SMEM;
+    // Split-K panels and next pivot tile (batch::SplitK) where the rounds are few enough for
+    // the split tasks to fit one wave; the counters start at zero.
+    const int parts = split_room && mode != 5 ? split_parts(R) : 1;
+    uint32_t* split_ctr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_ctr_off) : nullptr;
+    uint32_t* split_scr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_scr_off) : nullptr;
+    if (parts > 1) SE_CUDA_TRY(cudaMemsetAsync(split_ctr, 0, size_t(2 * R) * 4, stream));
     if (mode == 5) {
         batch::Elec E2[2] = {E, E};
         uint32_t* AT2 = reinterpret_cast<uint32_t*>(work + P.at2_off);
@@ -898,24 +919,25 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
             diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
         }
         if (se_status_t st = mark()) return st;
+        const unsigned panel_blocks = unsigned(2 * (R - 1) * parts);
         if (wide8) {
             if constexpr (LB == 16)
-                panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, 1, nullptr,
-                                                                                          nullptr, err);
+                panels_kernel<LB, 4><<<panel_blocks, tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, parts, split_ctr,
+                                                                                           split_scr, err);
         } else {
-            panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, stream>>>(E2[0], 0, 1, nullptr, nullptr, err);
+            panels_kernel<LB><<<panel_blocks, CF::THREADS, smem, stream>>>(E2[0], 0, parts, split_ctr, split_scr, err);
         }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
-        const int tasks = (R - 1) * (R - 1) + 2 * (R - 1);
+        const int tasks = (R - 1) * (R - 1) + (parts - 1) + 2 * (R - 1) * parts;
         for (int K = 0; K + 1 < R; ++K) {
             if (wide8) {
                 if constexpr (LB == 16)
-                    round_kernel<LB, 4><<<tasks, tile_threads<LB, 4>(), smem, stream>>>(E2[K & 1], E2[(K + 1) & 1], K,
-                                                                                       state + 2 * K, err);
+                    round_kernel<LB, 4><<<tasks, tile_threads<LB, 4>(), smem, stream>>>(
+                        E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K, parts, split_ctr, split_scr, err);
             } else {
                 round_kernel<LB><<<tasks, CF::THREADS, smem, stream>>>(E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K,
-                                                                       err);
+                                                                       parts, split_ctr, split_scr, err);
             }
             SE_CHECK_LAUNCH();
         }
@@ -963,12 +985,6 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         if (cudaEventCreate(&start) != cudaSuccess) SE_CUDA_TRY(cudaGetLastError());
         cudaEventRecord(start, stream);
     }
-    // Split-K panels and next pivot tile (batch::SplitK) where the rounds are few enough for
-    // the split tasks to fit one wave; the counters start at zero.
-    const int parts = split_room ? split_parts(R) : 1;
-    uint32_t* split_ctr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_ctr_off) : nullptr;
-    uint32_t* split_scr = parts > 1 ? reinterpret_cast<uint32_t*>(work + P.split_scr_off) : nullptr;
-    if (parts > 1) SE_CUDA_TRY(cudaMemsetAsync(split_ctr, 0, size_t(2 * R) * 4, stream));
     auto pivot = [&](int K) {
         if (wide) {
             if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, K, dT);

@@ -214,10 +214,10 @@ def closure_with_workspace(P, lanes, work_bytes):
     return api._to_host_u32(out)
 
 
-@pytest.mark.parametrize("C", [129, 257, 700, 2305, 4864, 4865])
+@pytest.mark.parametrize("C", [129, 257, 700, 2305, 3584, 3585])
 def test_split_panels_match_unsplit(orc, C):
     """The round-by-round schedules split each panel tile and the next pivot tile over 4 pivot
-    chunks when the workspace has the split area (up to 38 row blocks, C = 4864): the same
+    chunks when the workspace has the split area (up to 28 row blocks, C = 3584): the same
     matrix with the full and the plain workspace (which runs the tiles whole) gives identical
     results in schedules 1, 3, 4 and 7 and both lane widths, and equals the oracle where the
     oracle is quick."""
