@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "batch_core.cuh"
@@ -248,25 +249,80 @@ __global__ void __launch_bounds__(256, kPairCtasPerSm)
     if (local == 0 && E.wins)
         for (int x = threadIdx.x; x < C; x += 256) E.wins[x] = 0;
     const bool vec = E.ld % 4 == 0 && (reinterpret_cast<uintptr_t>(E.d) & 15) == 0;
+    // Off the diagonal with both tiles inside the C candidates (CTA-uniform; i0 < j0), every
+    // cell exists and the loads need no bounds.
+    const bool interior = g.I != g.J && g.j0 + kPT <= C;
+    // All eight 4-cell loads are issued before any is used (CTA-uniform branches around
+    // straight-line code), so the CTA has both tiles in flight at once.
     uint4 a[4], bt[4];
+    if (interior) {
+        const uint32_t* pa = E.d + int64_t(g.i0 + g.ry) * E.ld + g.j0 + 4 * g.cx;
+        const uint32_t* pb = E.d + int64_t(g.j0 + g.ry) * E.ld + g.i0 + 4 * g.cx;
+        const int64_t step = 16 * E.ld;
+        const bool half = E.ld % 2 == 0 && (reinterpret_cast<uintptr_t>(E.d) & 7) == 0;  // rows 8-byte aligned
+        if (vec) {
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                a[p] = __ldg(reinterpret_cast<const uint4*>(pa + p * step));
+                bt[p] = __ldg(reinterpret_cast<const uint4*>(pb + p * step));
+            }
+        } else if (half) {
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const uint2* x = reinterpret_cast<const uint2*>(pa + p * step);
+                const uint2* y = reinterpret_cast<const uint2*>(pb + p * step);
+                const uint2 x0 = __ldg(x), x1 = __ldg(x + 1), y0 = __ldg(y), y1 = __ldg(y + 1);
+                a[p] = make_uint4(x0.x, x0.y, x1.x, x1.y);
+                bt[p] = make_uint4(y0.x, y0.y, y1.x, y1.y);
+            }
+        } else {
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const uint32_t* x = pa + p * step;
+                const uint32_t* y = pb + p * step;
+                a[p] = make_uint4(__ldg(x), __ldg(x + 1), __ldg(x + 2), __ldg(x + 3));
+                bt[p] = make_uint4(__ldg(y), __ldg(y + 1), __ldg(y + 2), __ldg(y + 3));
+            }
+        }
+    } else if (vec) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int r = g.ry + 16 * p;
+            a[p] = load4_u32(E.d, E.ld, C, g.i0 + r, g.j0 + 4 * g.cx, true);
+            bt[p] = load4_u32(E.d, E.ld, C, g.j0 + r, g.i0 + 4 * g.cx, true);
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int r = g.ry + 16 * p;
+            a[p] = load4_u32(E.d, E.ld, C, g.i0 + r, g.j0 + 4 * g.cx, false);
+            bt[p] = load4_u32(E.d, E.ld, C, g.j0 + r, g.i0 + 4 * g.cx, false);
+        }
+    }
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
         const int r = g.ry + 16 * p;
-        a[p] = load4_u32(E.d, E.ld, C, g.i0 + r, g.j0 + 4 * g.cx, vec);
-        bt[p] = load4_u32(E.d, E.ld, C, g.j0 + r, g.i0 + 4 * g.cx, vec);
         swz64_store4(sa, r, 4 * g.cx, a[p]);
         swz64_store4(sb, r, 4 * g.cx, bt[p]);
     }
     __syncthreads();
-    const bool u16 = E.lanes == 16;
+    // Three CTA-uniform forms: u32 lanes; u16 lanes with base 0, where a kept value is its own
+    // cell and one OR per cell finds any that would not fit (checked once at the end); and u16
+    // lanes with a base, which checks each value against its window (to_lane16).
+    const int form = E.lanes != 16 ? 0 : (E.base == 0 ? 1 : 2);
+    const uint32_t base = E.base;
     bool over = false;
-    // One side: cells (x0 + r, y0 + 4cx + q) from own[] against their transposed partners in
-    // the other tile's staging.
-    auto emit = [&](const uint4* own, const uint32_t* other, int x0, int y0) {
+    uint32_t acc = 0;
+    // One side: cells (x0 + r, y0 + 4cx + q), read back from their own tile's staging (so no
+    // registers hold the tiles across the barrier), against their transposed partners in the
+    // other tile's staging.
+    auto emit = [&](auto form_tag, const uint32_t* own, const uint32_t* other, int x0, int y0) {
+        constexpr int F = decltype(form_tag)::value;
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
             const int r = g.ry + 16 * p;
-            const uint32_t x[4] = {own[p].x, own[p].y, own[p].z, own[p].w};
+            const uint4 o4 = swz64_load4(own, r, 4 * g.cx);
+            const uint32_t x[4] = {o4.x, o4.y, o4.z, o4.w};
             uint32_t v[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -274,20 +330,32 @@ __global__ void __launch_bounds__(256, kPairCtasPerSm)
                 v[q] = x[q] > y ? x[q] : 0u;
             }
             const int64_t at = int64_t(x0 + r) * Cp + y0 + 4 * g.cx;
-            if (u16) {
+            if constexpr (F == 0) {
+                *reinterpret_cast<uint4*>(E.S + at) = make_uint4(v[0], v[1], v[2], v[3]);
+            } else {
                 uint32_t h[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) h[q] = to_lane16(v[q], E.base, over);
+                for (int q = 0; q < 4; ++q) {
+                    if constexpr (F == 1) {
+                        acc |= v[q];
+                        h[q] = v[q];
+                    } else {
+                        h[q] = to_lane16(v[q], base, over);
+                    }
+                }
                 *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(E.S) + at) =
-                    make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
-            } else {
-                *reinterpret_cast<uint4*>(E.S + at) = make_uint4(v[0], v[1], v[2], v[3]);
+                    make_uint2(__byte_perm(h[0], h[1], 0x5410), __byte_perm(h[2], h[3], 0x5410));
             }
         }
     };
-    emit(a, sb, g.i0, g.j0);
-    if (g.I != g.J) emit(bt, sa, g.j0, g.i0);
-    if (over) raise_device_error(&hdr->err, kErrOverflow);
+    auto both = [&](auto form_tag) {
+        emit(form_tag, sa, sb, g.i0, g.j0);
+        if (g.I != g.J) emit(form_tag, sb, sa, g.j0, g.i0);
+    };
+    if (form == 0) both(std::integral_constant<int, 0>{});
+    else if (form == 1) both(std::integral_constant<int, 1>{});
+    else both(std::integral_constant<int, 2>{});
+    if (over || acc > 0xFFFFu) raise_device_error(&hdr->err, kErrOverflow);
 }
 
 // Output (u32, zero diagonal) and wins, on the same tile pairs. Cells are widened from the
@@ -303,25 +371,70 @@ __global__ void __launch_bounds__(256, kPairCtasPerSm)
     const int C = E.C, Cp = E.Cp;
     const PairGeom g = pair_geom(o.local, Cp);
     const bool u16 = E.lanes == 16;
-    auto load = [&](int row, int c0) -> uint4 {  // the working matrix covers Cp x Cp: no bounds
-        const int64_t at = int64_t(row) * Cp + c0;
-        if (u16) {
-            const uint2 w = __ldg(reinterpret_cast<const uint2*>(reinterpret_cast<const uint16_t*>(E.S) + at));
-            const uint32_t h[4] = {w.x & 0xFFFFu, w.x >> 16, w.y & 0xFFFFu, w.y >> 16};
-            return make_uint4(h[0] ? h[0] + E.base : 0u, h[1] ? h[1] + E.base : 0u, h[2] ? h[2] + E.base : 0u,
-                              h[3] ? h[3] + E.base : 0u);
-        }
-        return __ldg(reinterpret_cast<const uint4*>(E.S + at));
-    };
+    // The working matrix covers Cp x Cp: no bounds. All eight loads are issued before any is
+    // used (one CTA-uniform branch on the lane width around straight-line code); then the
+    // 16-bit cells are widened (u16 lanes store v - base).
     uint4 a[4], bt[4];
+    if (u16) {
+        const uint16_t* S16 = reinterpret_cast<const uint16_t*>(E.S);
+        uint2 wa[4], wb[4];
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const int r = g.ry + 16 * p;
-        a[p] = load(g.i0 + r, g.j0 + 4 * g.cx);
-        bt[p] = load(g.j0 + r, g.i0 + 4 * g.cx);
-        swz64_store4(sb, r, 4 * g.cx, bt[p]);
+        for (int p = 0; p < 4; ++p) {
+            const int r = g.ry + 16 * p;
+            wa[p] = __ldg(reinterpret_cast<const uint2*>(S16 + int64_t(g.i0 + r) * Cp + g.j0 + 4 * g.cx));
+            wb[p] = __ldg(reinterpret_cast<const uint2*>(S16 + int64_t(g.j0 + r) * Cp + g.i0 + 4 * g.cx));
+        }
+        const uint32_t base = E.base;
+        if (base == 0) {  // CTA-uniform: a cell is its value
+            auto widen = [](uint2 w) { return make_uint4(w.x & 0xFFFFu, w.x >> 16, w.y & 0xFFFFu, w.y >> 16); };
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                a[p] = widen(wa[p]);
+                bt[p] = widen(wb[p]);
+            }
+        } else {
+            auto widen = [base](uint2 w) {
+                const uint32_t h[4] = {w.x & 0xFFFFu, w.x >> 16, w.y & 0xFFFFu, w.y >> 16};
+                return make_uint4(h[0] ? h[0] + base : 0u, h[1] ? h[1] + base : 0u, h[2] ? h[2] + base : 0u,
+                                  h[3] ? h[3] + base : 0u);
+            };
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                a[p] = widen(wa[p]);
+                bt[p] = widen(wb[p]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int r = g.ry + 16 * p;
+            a[p] = __ldg(reinterpret_cast<const uint4*>(E.S + int64_t(g.i0 + r) * Cp + g.j0 + 4 * g.cx));
+            bt[p] = __ldg(reinterpret_cast<const uint4*>(E.S + int64_t(g.j0 + r) * Cp + g.i0 + 4 * g.cx));
+        }
     }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) swz64_store4(sb, g.ry + 16 * p, 4 * g.cx, bt[p]);
+    // Off the diagonal, with both tiles inside the C candidates (CTA-uniform), the cells are
+    // stored as they are: 128-bit stores where the output rows are 16-byte aligned.
+    const bool interior = g.I != g.J && g.j0 + kPT <= C;  // i0 < j0, so i0 + kPT <= C too
+    const bool vec_out = E.ld_out % 4 == 0 && (reinterpret_cast<uintptr_t>(E.out) & 15) == 0;
+    const bool half_out = E.ld_out % 2 == 0 && (reinterpret_cast<uintptr_t>(E.out) & 7) == 0;
     auto store = [&](const uint4* own, int x0, int y0) {
+        if (interior) {
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                uint32_t* at = E.out + int64_t(x0 + g.ry + 16 * p) * E.ld_out + y0 + 4 * g.cx;
+                if (vec_out) {
+                    *reinterpret_cast<uint4*>(at) = own[p];
+                } else if (half_out) {
+                    reinterpret_cast<uint2*>(at)[0] = make_uint2(own[p].x, own[p].y);
+                    reinterpret_cast<uint2*>(at)[1] = make_uint2(own[p].z, own[p].w);
+                } else {
+                    at[0] = own[p].x, at[1] = own[p].y, at[2] = own[p].z, at[3] = own[p].w;
+                }
+            }
+            return;
+        }
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
             const int i = x0 + g.ry + 16 * p;

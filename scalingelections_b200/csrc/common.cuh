@@ -229,4 +229,11 @@ __device__ __forceinline__ void swz64_store4(uint32_t* tile, int r, int c0, uint
     *reinterpret_cast<uint4*>(tile + r * 64 + (c0 ^ (s & ~3))) = v;
 }
 
+// Cells (r, c0 .. c0+3), c0 a multiple of 4, of a swizzled tile with one 128-bit read.
+__device__ __forceinline__ uint4 swz64_load4(const uint32_t* tile, int r, int c0) {
+    const int s = 2 * ((r >> 2) & 15);
+    const uint4 v = *reinterpret_cast<const uint4*>(tile + r * 64 + (c0 ^ (s & ~3)));
+    return (s & 2) ? make_uint4(v.z, v.w, v.x, v.y) : v;
+}
+
 }  // namespace se
