@@ -322,8 +322,14 @@ SE_API se_status_t se_engine_destroy(se_engine_t* engine);
  *   2. the caller broadcasts that panel, se_shard_panel_bytes() bytes at byte offset
  *      se_shard_panel_offset(k) of the owner's workspace, into the same offset of every other
  *      shard's workspace (e.g. one NCCL broadcast; the offsets differ between owner and
- *      receivers, so each rank asks its own shard);
+ *      receivers, so each rank asks its own shard; receivers have one buffer per round
+ *      parity, so panel k+1 may arrive while round k still reads panel k);
  *   3. every shard calls se_shard_update(k): column panels and remainder tiles of its rows.
+ * Look-ahead order, which lets panel k+1 cross the links during round k's remainder: in round
+ * k the shard holding row block k+1 first calls se_shard_update_part(k, 1) (that row block
+ * alone, closing the next pivot tile) and se_shard_pivot(k+1); the broadcast of panel k+1
+ * then starts (asynchronously) on every rank, and every shard calls se_shard_update_part(k, 2)
+ * (all its other rows) while it is in flight. Both orders give identical results.
  * Before round 0 each shard calls se_shard_init with the whole C x C preference matrix on its
  * GPU; after round R-1, se_shard_finalize writes its rows [128 b0, min(128 b1, C)) of the
  * strongest-path matrix (u32, zero diagonal). Results equal se_closure's bit for bit.
@@ -340,6 +346,10 @@ SE_API se_status_t se_shard_pivot(se_shard_t* shard, int k, void* stream);
 SE_API int64_t se_shard_panel_offset(const se_shard_t* shard, int k);
 SE_API int64_t se_shard_panel_bytes(const se_shard_t* shard);
 SE_API se_status_t se_shard_update(se_shard_t* shard, int k, void* stream);
+/* se_shard_update in parts: part 0 all of it; 1 row block k+1 alone (no launch unless this
+ * shard holds it), its tile (k+1, k+1) then closed as the next pivot; 2 every row but k+1.
+ * Parts 1 then 2 of one round do what part 0 does. */
+SE_API se_status_t se_shard_update_part(se_shard_t* shard, int k, int part, void* stream);
 SE_API se_status_t se_shard_finalize(se_shard_t* shard, uint32_t* d_out, int64_t ld_out, void* stream);
 SE_API se_status_t se_shard_check(se_shard_t* shard, void* stream);
 

@@ -77,6 +77,7 @@ SIGNATURES: dict[str, tuple] = {
     "se_shard_panel_offset": (_c_i64, [_vp, _c_int]),
     "se_shard_panel_bytes": (_c_i64, [_vp]),
     "se_shard_update": (_c_int, [_vp, _c_int, _vp]),
+    "se_shard_update_part": (_c_int, [_vp, _c_int, _c_int, _vp]),
     "se_shard_finalize": (_c_int, [_vp, _vp, _c_i64, _vp]),
     "se_shard_check": (_c_int, [_vp, _vp]),
     "se_tally_workspace_bytes": (_c_i64, [_c_i64, _c_int]),

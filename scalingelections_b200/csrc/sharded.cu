@@ -76,19 +76,37 @@ constexpr int kPhaseRowPanel = 0;
 constexpr int kPhaseColPanel = 1;
 constexpr int kPhaseRemainder = 2;
 
+// The local row block of the b-th row the column-panel and remainder phases update: `only`
+// >= 0 selects that row block alone; otherwise every local row block but kl (when own) and
+// `skip` (when >= 0), in order.
+__device__ __forceinline__ int selected_row(int b, int own, int kl, int only, int skip) {
+    if (only >= 0) return only;
+    int lo = own ? kl : -1, hi = skip;
+    if (lo > hi) {
+        const int t = lo;
+        lo = hi;
+        hi = t;
+    }
+    if (lo >= 0 && b >= lo) ++b;
+    if (hi >= 0 && b >= hi) ++b;
+    return b;
+}
+
 // One phase of round k on the slab. E describes the slab: S is its first row, mapS covers its
 // rows, AT is indexed by local row block; b0 is the slab's first global row block. own: this
 // shard holds row block k (local kl), so the
 // pivot rows are read from its own slab; otherwise from the panel buffer (mapP, row block 0).
+// only / skip: the rows the column-panel and remainder phases update (selected_row).
 // fuse_next >= 0 (remainder phase only): this shard also holds row block k + 1, at local index
-// fuse_next. Block 0 then takes tile (k+1, k+1) and, after updating it, closes it as round
-// k+1's pivot over kmax_next pivots and writes dT, while the other blocks go on: the next
-// round's se_shard_pivot needs only its row panel. Nothing else in this launch reads that
-// tile or dT.
+// fuse_next, and updates it in this launch. Block 0 then takes tile (k+1, k+1) and, after
+// updating it, closes it as round k+1's pivot over kmax_next pivots and writes dT, while the
+// other blocks go on: the next round's se_shard_pivot needs only its row panel. Nothing else
+// in this launch reads that tile or dT.
 template <int LB>
 __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     shard_tiles_kernel(const __grid_constant__ Elec E, const __grid_constant__ CUtensorMap mapP, int phase, int k,
-                       int kl, int b0, int own, int fuse_next, int kmax_next, uint32_t* __restrict__ err) {
+                       int kl, int b0, int own, int only, int skip, int fuse_next, int kmax_next,
+                       uint32_t* __restrict__ err) {
     using CF = cfg<LB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(16) uint32_t rowbuf[kPivotBufs][CF::TW];
@@ -104,8 +122,10 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
     int b = blockIdx.x;
     const bool fuse = phase == kPhaseRemainder && fuse_next >= 0;
     if (fuse) {
-        // Reduced coordinates of tile (k+1, k+1): local rows without kl, columns without k.
-        const int p = (own && fuse_next > kl ? fuse_next - 1 : fuse_next) * (E.R - 1) + k;
+        // Reduced coordinates of tile (k+1, k+1): its position among the selected rows (rows
+        // without kl, or the one row `only`), columns without k.
+        const int row = only >= 0 ? 0 : (own && fuse_next > kl ? fuse_next - 1 : fuse_next);
+        const int p = row * (E.R - 1) + k;
         b = b == 0 ? p : (b == p ? 0 : b);
     }
     int kind, K = k, I = 0, J = 0;
@@ -113,14 +133,14 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         kind = kTileRow;
         K = kl;
         J = b + (b >= k);
-    } else if (phase == kPhaseColPanel) {  // local row blocks other than k
+    } else if (phase == kPhaseColPanel) {  // the selected local row blocks (never k)
         kind = kTileCol;
-        I = own ? b + (b >= kl) : b;
+        I = selected_row(b, own, kl, only, skip);
     } else {
         kind = kTileRem;
         const int R1 = E.R - 1;
         const int ii = b / R1, jj = b % R1;
-        I = own ? ii + (ii >= kl) : ii;
+        I = selected_row(ii, own, kl, only, skip);
         J = jj + (jj >= k);
     }
     uint32_t pa = 0, pb = 0;
@@ -163,7 +183,7 @@ __global__ void __launch_bounds__(256)
 }
 
 struct Layout {
-    int64_t s_off, at_off, dt_off, p_off, total, panel_bytes;
+    int64_t s_off, at_off, dt_off, p_off, total, panel_bytes;  // p_off: two panel buffers (round parity)
 };
 
 Layout layout(int C, int b0, int b1, int lanes) {
@@ -175,7 +195,7 @@ Layout layout(int C, int b0, int b1, int lanes) {
     L.dt_off = round_up(L.at_off + int64_t(kT) * Cp * 4, 256);
     L.p_off = round_up(L.dt_off + int64_t(kT) * kT * 4, 256);
     L.panel_bytes = int64_t(kT) * Cp * cell;
-    L.total = round_up(L.p_off + L.panel_bytes, 256);
+    L.total = round_up(L.p_off + 2 * L.panel_bytes, 256);
     return L;
 }
 
@@ -191,8 +211,8 @@ using namespace se;
 using namespace se::shard;
 
 struct se_shard {
-    Elec E;            // the slab: maps, pointers, C, Cp, R, lanes, base
-    CUtensorMap mapP;  // the received pivot-row panel, 128 x Cp cells
+    Elec E;               // the slab: maps, pointers, C, Cp, R, lanes, base
+    CUtensorMap mapP[2];  // the received pivot-row panels of even and odd rounds, 128 x Cp cells
     uint8_t* work;
     uint32_t* err;
     uint8_t* P;
@@ -246,7 +266,8 @@ extern "C" se_status_t se_shard_create(int C, int b0, int b1, int lane_bits, uin
     se_status_t st = make_map(&E.mapS, E.S, ldw, uint64_t(h->nloc) * kT, ldw * 4, uint32_t(tw), kKC);
     if (!st) st = make_map(&E.mapAT, E.AT, uint64_t(E.Cp), kT, uint64_t(E.Cp) * 4, kT, kKC);
     if (!st) st = make_map(&E.mapDT, E.dT, kT, kT, kT * 4, kT, kKC);
-    if (!st) st = make_map(&h->mapP, h->P, ldw, kT, ldw * 4, uint32_t(tw), kKC);
+    if (!st) st = make_map(&h->mapP[0], h->P, ldw, kT, ldw * 4, uint32_t(tw), kKC);
+    if (!st) st = make_map(&h->mapP[1], h->P + h->panel_bytes, ldw, kT, ldw * 4, uint32_t(tw), kKC);
     if (st) {
         delete h;
         return st;
@@ -288,30 +309,43 @@ template <int LB> se_status_t pivot_impl(se_shard& h, int k, cudaStream_t s) {
     }
     h.pivot_ready = -1;
     if (E.R > 1) {
-        shard_tiles_kernel<LB><<<unsigned(E.R - 1), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseRowPanel, k,
-                                                                                         kl, h.b0, 1, -1, 0, h.err);
+        shard_tiles_kernel<LB><<<unsigned(E.R - 1), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(
+            E, h.mapP[k & 1], kPhaseRowPanel, k, kl, h.b0, 1, -1, -1, -1, 0, h.err);
         SE_CHECK_LAUNCH();
     }
     return SE_OK;
 }
 
-template <int LB> se_status_t update_impl(se_shard& h, int k, cudaStream_t s) {
+// part 0: every local row block but k; 1: row block k+1 alone (nothing unless this shard holds
+// it); 2: every local row block but k and k+1. Row block k+1, when updated here, also closes
+// round k+1's pivot tile inside the remainder launch.
+template <int LB> se_status_t update_impl(se_shard& h, int k, int part, cudaStream_t s) {
     const Elec& E = h.E;
     if (se_status_t st = set_smem<LB>()) return st;
     const bool own = k >= h.b0 && k < h.b1;
     const int kl = own ? k - h.b0 : 0;
-    const int rows = own ? h.nloc - 1 : h.nloc;  // local row blocks other than k
+    const int next = k + 1;
+    const int nl = next < E.R && next >= h.b0 && next < h.b1 ? next - h.b0 : -1;  // local index of k+1
+    int only = -1, skip = -1, rows = own ? h.nloc - 1 : h.nloc;
+    if (part == 1) {
+        if (nl < 0) return SE_OK;
+        only = nl;
+        rows = 1;
+    } else if (part == 2 && nl >= 0) {
+        skip = nl;
+        rows -= 1;
+    }
     if (rows <= 0) return SE_OK;
-    shard_tiles_kernel<LB><<<unsigned(rows), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(E, h.mapP, kPhaseColPanel, k, kl,
-                                                                                  h.b0, own ? 1 : 0, -1, 0, h.err);
+    const CUtensorMap& mapP = h.mapP[k & 1];
+    shard_tiles_kernel<LB><<<unsigned(rows), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(
+        E, mapP, kPhaseColPanel, k, kl, h.b0, own ? 1 : 0, only, skip, -1, 0, h.err);
     SE_CHECK_LAUNCH();
     if (E.R > 1) {
-        // Close round k+1's pivot inside this launch when this shard holds row block k+1.
-        const int next = k + 1;
-        const int fuse = next < E.R && next >= h.b0 && next < h.b1 ? next - h.b0 : -1;
+        // Close round k+1's pivot inside this launch when it updates row block k+1.
+        const int fuse = part != 2 ? nl : -1;
         const int kmax_next = fuse >= 0 ? (E.C - next * kT < kT ? E.C - next * kT : kT) : 0;
         shard_tiles_kernel<LB><<<unsigned(rows * (E.R - 1)), cfg<LB>::THREADS, pcfg<LB>::SMEM, s>>>(
-            E, h.mapP, kPhaseRemainder, k, kl, h.b0, own ? 1 : 0, fuse, kmax_next, h.err);
+            E, mapP, kPhaseRemainder, k, kl, h.b0, own ? 1 : 0, only, skip, fuse, kmax_next, h.err);
         SE_CHECK_LAUNCH();
         if (fuse >= 0) h.pivot_ready = next;
     }
@@ -332,7 +366,7 @@ extern "C" int64_t se_shard_panel_offset(const se_shard_t* sh, int k) {
     if (!sh || k < 0 || k >= sh->E.R) return -1;
     if (k >= sh->b0 && k < sh->b1)  // the owner broadcasts straight from its slab rows
         return (reinterpret_cast<const uint8_t*>(sh->E.S) - sh->work) + int64_t(k - sh->b0) * sh->panel_bytes;
-    return sh->P - sh->work;
+    return (sh->P - sh->work) + (k & 1) * sh->panel_bytes;  // a receiver's buffer of k's parity
 }
 
 extern "C" int64_t se_shard_panel_bytes(const se_shard_t* sh) { return sh ? sh->panel_bytes : -1; }
@@ -342,7 +376,16 @@ extern "C" se_status_t se_shard_update(se_shard_t* sh, int k, void* stream) {
     SE_REQUIRE(sh != nullptr, SE_ERR_INVALID, "null shard handle");
     SE_REQUIRE(k >= 0 && k < sh->E.R, SE_ERR_INVALID, "round %d outside [0, %d)", k, sh->E.R);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    return sh->E.lanes == 16 ? update_impl<16>(*sh, k, s) : update_impl<32>(*sh, k, s);
+    return sh->E.lanes == 16 ? update_impl<16>(*sh, k, 0, s) : update_impl<32>(*sh, k, 0, s);
+}
+
+extern "C" se_status_t se_shard_update_part(se_shard_t* sh, int k, int part, void* stream) {
+    clear_error();
+    SE_REQUIRE(sh != nullptr, SE_ERR_INVALID, "null shard handle");
+    SE_REQUIRE(k >= 0 && k < sh->E.R, SE_ERR_INVALID, "round %d outside [0, %d)", k, sh->E.R);
+    SE_REQUIRE(part >= 0 && part <= 2, SE_ERR_INVALID, "part must be 0, 1 or 2 (got %d)", part);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return sh->E.lanes == 16 ? update_impl<16>(*sh, k, part, s) : update_impl<32>(*sh, k, part, s);
 }
 
 extern "C" se_status_t se_shard_finalize(se_shard_t* sh, uint32_t* d_out, int64_t ld_out, void* stream) {

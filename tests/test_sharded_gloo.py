@@ -1,8 +1,9 @@
 """The sharded closure's rounds (scalingelections_b200.sharded) over two gloo ranks on CPU.
-Each rank runs the real driver, strongest_paths_sharded, with its one broadcast per round;
-a numpy model of one shard stands in for the GPU kernels. The model does the same tile
-steps: pivot closure, pivot-row panel, column panels, remainder. The gathered rows must
-equal the oracle's closure exactly."""
+Each rank runs the real driver, strongest_paths_sharded, with its one asynchronous broadcast
+per round in look-ahead order; a numpy model of one shard stands in for the GPU kernels. The
+model does the same tile steps: pivot closure, pivot-row panel, column panels, remainder, with
+a receive buffer per round parity, and it checks the order (row block k+1 before the next
+pivot, the rest after). The gathered rows must equal the oracle's closure exactly."""
 import os
 import socket
 
@@ -28,7 +29,8 @@ class ModelShard:
         self.C, self.b0, self.b1 = C, b0, b1
         self.Cp = (C + T - 1) // T * T
         self.slab = torch.zeros(((b1 - b0) * T, self.Cp), dtype=torch.int64)
-        self.P = torch.zeros((T, self.Cp), dtype=torch.int64)
+        self.P = torch.zeros((2, T, self.Cp), dtype=torch.int64)  # receive buffers by round parity
+        self.done = {}  # round -> local row blocks already updated in it
 
     def init(self, d):
         dn = d.view(torch.int32).numpy().view(np.uint32).astype(np.int64)
@@ -42,6 +44,8 @@ class ModelShard:
         return a[r * T:(r + 1) * T, c * T:(c + 1) * T]
 
     def pivot(self, k):
+        if k > 0:  # the pivot row block must have had round k-1's update
+            assert k - self.b0 in self.done.get(k - 1, set()), ("pivot before its row block's update", k)
         s = self.slab.numpy()
         kl = k - self.b0
         D = self._blk(s, kl, k)
@@ -55,14 +59,25 @@ class ModelShard:
     def panel(self, k):
         if self.b0 <= k < self.b1:
             return self.slab[(k - self.b0) * T:(k - self.b0 + 1) * T]
-        return self.P
+        return self.P[k % 2]
 
     def update(self, k):
+        self.update_part(k, 0)
+
+    def update_part(self, k, part):
         s = self.slab.numpy()
         own = self.b0 <= k < self.b1
+        nl = k + 1 - self.b0 if self.b0 <= k + 1 < self.b1 else -1
         row = self.panel(k).numpy()
         D = row[:, k * T:(k + 1) * T]
         mine = [I for I in range(self.b1 - self.b0) if not (own and I == k - self.b0)]
+        if part == 1:
+            mine = [I for I in mine if I == nl]
+        elif part == 2:
+            mine = [I for I in mine if I != nl]
+        done = self.done.setdefault(k, set())
+        assert not done & set(mine), ("row block updated twice", k)
+        done.update(mine)
         for I in mine:
             Cb = self._blk(s, I, k)
             Cb[:] = np.maximum(Cb, maxmin(Cb, D))

@@ -32,6 +32,7 @@ def test_virtual_shards_equal_single_closure(C, parts):
     single = api.strongest_paths_device(d, lanes=LANES_U16)
     assert same(strongest_paths_virtual(d, parts, lanes=LANES_U16), single)
     assert same(strongest_paths_virtual(d, parts, lanes=LANES_U32), single)
+    assert same(strongest_paths_virtual(d, parts, lanes=LANES_U16, lookahead=False), single)
 
 
 def test_virtual_shards_against_oracle(orc):
@@ -64,6 +65,10 @@ def test_shard_rejects_bad_calls():
         sh.pivot(1)
     with pytest.raises(ValueError):
         sh.panel(8)
+    with pytest.raises(_lib.SchulzeError, match="part must be"):
+        sh.update_part(0, 3)
+    assert sh.panel(0).data_ptr() != sh.panel(1).data_ptr()  # a receive buffer per round parity
+    assert sh.panel(0).data_ptr() == sh.panel(6).data_ptr()  # rounds 2-4 are this shard's own rows
     sh.close()
 
 
