@@ -223,6 +223,39 @@ struct SplitK {
     bool last;
 };
 
+// The split-K epilogue of one part (SplitK): stores its partial tile, counts itself, and in the
+// last part to arrive folds the other parts' partials into c. Returns whether this part is the
+// last (which then stores the tile).
+template <int LB, int NQ>
+__device__ __forceinline__ bool fold_split(uint32_t (&c)[8][NQ], SplitK* split, const geomT<NQ>& g) {
+    using L = lanes<LB>;
+    constexpr int TW = cfg<LB>::TW;
+    constexpr int64_t kTileWords = int64_t(kT) * TW;
+    __shared__ uint32_t s_arrived;
+    store_tile_regs<LB, NQ>(c, split->scratch + split->q * kTileWords, TW, g);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_arrived = atomicAdd(split->counter, 1u);
+    __syncthreads();
+    split->last = s_arrived == uint32_t(split->parts - 1);
+    if (!split->last) return false;
+    __threadfence();  // the other parts' partials, counted before our arrival, are visible
+    for (int p = 0; p < split->parts; ++p) {
+        if (p == split->q) continue;
+        const uint32_t* src = split->scratch + p * kTileWords;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            uint32_t v[NQ];
+            ld4_cg(v, src + int64_t(g.row0 + r) * TW + g.wbase);
+            if constexpr (NQ == 8) ld4_cg(v + 4, src + int64_t(g.row0 + r) * TW + g.wbase + 32);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax(c[r][q], v[q]);
+        }
+    }
+    if (threadIdx.x == 0) *split->counter = 0u;
+    return true;
+}
+
 // mapB / kb: where the pivot rows S[K][*] (B of row and remainder tiles, D of column tiles)
 // are read: by default G->mapS at row block K; a sharded closure passes the map of a
 // received panel buffer (kb = 0) or of its own slab (kb = the local row block).
@@ -233,8 +266,9 @@ struct SplitK {
 // product (their copies too), with identical results.
 // NQ: words per thread, 8 (the default micro-tile) or 4 (the wide one, 256 threads, 16-bit
 // lanes); the block must have tile_threads<LB, NQ>() threads.
-// split: the split-K form above (nullptr: the whole product in this CTA).
-template <int LB, bool GLOBAL_MAPS = true, int NQ = 8>
+// SPLIT / split: the split-K form above, compiled in only where a kernel may split (the whole
+// product in this CTA when split is null); without it the routine has no split logic at all.
+template <int LB, bool GLOBAL_MAPS = true, int NQ = 8, bool SPLIT = false>
 __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, int J, uint8_t* smem, uint64_t* bars,
                          uint32_t& par_a, uint32_t& par_b, const CUtensorMap* mapB = nullptr, int kb = -1,
                          int kvalid = -1, int rvalid = -1, SplitK* split = nullptr) {
@@ -255,10 +289,15 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     if (rvalid < 0) rvalid = E.C - (kind == kTileRow ? K : I) * kT;
     const int nch = kvalid >= kT ? kChunks : (kvalid + kKC - 1) / kKC;  // chunks holding pivots
     const bool live = (g.row0 & ~31) < rvalid;                         // this warp holds real rows
-    // This CTA's chunks [ch_lo, ch_hi): all of them, or its part's share.
-    const int ch_lo = split ? split->q * (kChunks / split->parts) : 0;
-    const int ch_hi = split ? ch_lo + kChunks / split->parts : kChunks;
-    const int ch_end = nch < ch_hi ? nch : ch_hi;
+    // This CTA's chunks [ch_lo, ch_end): all that hold pivots, or its part's share of them.
+    int ch_lo = 0, ch_end = nch;
+    if constexpr (SPLIT) {
+        if (split) {
+            ch_lo = split->q * (kChunks / split->parts);
+            const int ch_hi = ch_lo + kChunks / split->parts;
+            ch_end = nch < ch_hi ? nch : ch_hi;
+        }
+    }
     if (kind != kTileCol) {
         const bool rem = kind == kTileRem;
         const CUtensorMap* mapA = rem ? &G->mapAT : &G->mapDT;
@@ -343,31 +382,10 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
             if (live) relax_chunk<LB, NQ>(c, As + ch * CF::A_CHUNK, Bs + ch * CF::B_CHUNK, g);
         }
     }
-    if (ok && split != nullptr) {
-        using L = lanes<LB>;
-        constexpr int64_t kTileWords = int64_t(kT) * TW;
-        __shared__ uint32_t s_arrived;
-        store_tile_regs<LB, NQ>(c, split->scratch + split->q * kTileWords, TW, g);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) s_arrived = atomicAdd(split->counter, 1u);
-        __syncthreads();
-        split->last = s_arrived == uint32_t(split->parts - 1);
-        if (!split->last) return ok;
-        __threadfence();  // the other parts' partials, counted before our arrival, are visible
-        for (int p = 0; p < split->parts; ++p) {
-            if (p == split->q) continue;
-            const uint32_t* src = split->scratch + p * kTileWords;
-#pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                uint32_t v[NQ];
-                ld4_cg(v, src + int64_t(g.row0 + r) * TW + g.wbase);
-                if constexpr (NQ == 8) ld4_cg(v + 4, src + int64_t(g.row0 + r) * TW + g.wbase + 32);
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) c[r][q] = L::vmax(c[r][q], v[q]);
-            }
+    if constexpr (SPLIT) {
+        if (ok && split != nullptr) {
+            if (!fold_split<LB, NQ>(c, split, g)) return ok;  // an earlier part: the last one stores
         }
-        if (threadIdx.x == 0) *split->counter = 0u;
     }
     if (ok) {
         store_tile_regs<LB, NQ>(c, Ct, ldw, g);

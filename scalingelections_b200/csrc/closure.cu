@@ -35,6 +35,7 @@
 #include <cstring>
 #include <atomic>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "batch_core.cuh"
@@ -54,7 +55,7 @@ constexpr uint32_t kMaxPolls = 1u << 26;
 // ------------------------------------------------------------------------------------------
 // With parts > 1 every panel tile runs split-K over `parts` consecutive blocks (batch::SplitK):
 // split_ctr[b] and split_scr[b * parts ...] are tile b's counter and partial tiles.
-template <int LB, int NQ = 8>
+template <int LB, int NQ = 8, bool SPLIT = false>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     panels_kernel(const __grid_constant__ batch::Elec E, int K, int parts, uint32_t* __restrict__ split_ctr,
                   uint32_t* __restrict__ split_scr, uint32_t* __restrict__ err) {
@@ -66,16 +67,17 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     }
     __syncthreads();
     const int R1 = E.R - 1;
-    const int b = blockIdx.x / parts;
+    const int P = SPLIT ? parts : 1;
+    const int b = blockIdx.x / P;
     bool ok;
     uint32_t par_a = 0, par_b = 0;
     const bool row = b < R1;
     const int x = row ? b : b - R1;
-    batch::SplitK sp{int(blockIdx.x % parts), parts, split_scr + int64_t(b) * parts * kT * cfg<LB>::TW,
-                     split_ctr + b, false};
-    ok = batch::run_tile<LB, false, NQ>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K),
-                                        x + (x >= K), smem, bars, par_a, par_b, nullptr, -1, -1, -1,
-                                        parts > 1 ? &sp : nullptr);
+    batch::SplitK sp{int(blockIdx.x % P), P, SPLIT ? split_scr + int64_t(b) * P * kT * cfg<LB>::TW : nullptr,
+                     SPLIT ? split_ctr + b : nullptr, false};
+    ok = batch::run_tile<LB, false, NQ, SPLIT>(E, &E, row ? batch::kTileRow : batch::kTileCol, K, x + (x >= K),
+                                               x + (x >= K), smem, bars, par_a, par_b, nullptr, -1, -1, -1,
+                                               SPLIT ? &sp : nullptr);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
 // With fuse_pivot and parts > 1 (subset 0 only), blocks [0, parts) run tile (K+1, K+1) split-K
 // (batch::SplitK, counter split_ctr, partials split_scr) and the last of them closes the
 // pivot; the grid then has parts - 1 more blocks than tiles.
-template <int LB, int NQ = 8>
+template <int LB, int NQ = 8, bool SPLIT = false>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     rem_kernel(const __grid_constant__ batch::Elec E, int K, int fuse_pivot, int subset, int parts,
                uint32_t* __restrict__ split_ctr, uint32_t* __restrict__ split_scr, uint32_t* __restrict__ err) {
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     __syncthreads();
     const int R1 = E.R - 1, R2 = E.R - 2;
     int t = blockIdx.x, I, J;
-    const bool split = subset == 0 && fuse_pivot && parts > 1;
+    const bool split = SPLIT && subset == 0 && fuse_pivot && parts > 1;
     const int q = split && t < parts ? t : -1;  // this block's part of tile (K+1, K+1)
     auto skip_k_k1 = [K](int n) { return n < K ? n : n + 2; };  // n-th block index other than K, K+1
     if (subset == 0) {
@@ -135,8 +137,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     }
     uint32_t par_a = 0, par_b = 0;
     batch::SplitK sp{q, parts, split_scr, split_ctr, false};
-    const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b,
-                                                   nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
+    const bool ok = batch::run_tile<LB, false, NQ, SPLIT>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b,
+                                                          nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
     if (!ok) {
         if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
         return;
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
 // consecutive tickets, split-K (batch::SplitK; counters and partials as in panels_kernel and
 // rem_kernel): the last part of tile (K+1, K+1) closes the pivot and counts the tile done.
 // ------------------------------------------------------------------------------------------
-template <int LB, int NQ = 8>
+template <int LB, int NQ = 8, bool SPLIT = false>
 __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     round_kernel(const __grid_constant__ batch::Elec E, const __grid_constant__ batch::Elec En, int K,
                  uint32_t* __restrict__ state, int parts, uint32_t* __restrict__ split_ctr,
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     __syncthreads();
     const uint32_t t = s_ticket;
     const int R = E.R, R1 = R - 1, R2 = R - 2;
-    const uint32_t P = uint32_t(parts);
+    const uint32_t P = SPLIT ? uint32_t(parts) : 1u;
     constexpr int64_t kTileWords = int64_t(kT) * CF::TW;
     // Remainder tickets: tile (K+1, K+1) in [0, P), the rest of the first group (row and column
     // K+1) up to P - 1 + first, the other tiles up to nrem.
@@ -205,9 +207,10 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
             I = skip_k_k1(x / R2);
             J = skip_k_k1(x % R2);
         }
-        batch::SplitK sp{q, parts, split_scr + int64_t(2 * R1) * parts * kTileWords, split_ctr + 2 * R1, false};
-        const bool ok = batch::run_tile<LB, false, NQ>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a, par_b,
-                                                       nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
+        batch::SplitK sp{q, int(P), SPLIT ? split_scr + int64_t(2 * R1) * P * kTileWords : nullptr,
+                         SPLIT ? split_ctr + 2 * R1 : nullptr, false};
+        const bool ok = batch::run_tile<LB, false, NQ, SPLIT>(E, &E, batch::kTileRem, K, I, J, smem, bars, par_a,
+                                                              par_b, nullptr, -1, -1, -1, q >= 0 ? &sp : nullptr);
         if (!ok) {
             if (threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
             return;
@@ -239,10 +242,11 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     const bool row = b < R1;
     const int y = row ? b : b - R1;
     const int K1 = K + 1;
-    batch::SplitK sp{int((t - nrem) % P), parts, split_scr + int64_t(b) * parts * kTileWords, split_ctr + b, false};
-    const bool ok = batch::run_tile<LB, false, NQ>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1,
-                                                   y + (y >= K1), y + (y >= K1), smem, bars, par_a, par_b, nullptr,
-                                                   -1, -1, -1, P > 1 ? &sp : nullptr);
+    batch::SplitK sp{int((t - nrem) % P), int(P), SPLIT ? split_scr + int64_t(b) * P * kTileWords : nullptr,
+                     SPLIT ? split_ctr + b : nullptr, false};
+    const bool ok = batch::run_tile<LB, false, NQ, SPLIT>(En, &En, row ? batch::kTileRow : batch::kTileCol, K1,
+                                                          y + (y >= K1), y + (y >= K1), smem, bars, par_a, par_b,
+                                                          nullptr, -1, -1, -1, SPLIT && P > 1 ? &sp : nullptr);
     if (!ok && threadIdx.x == 0) raise_device_error(err, kErrTmaTimeout);
 }
 
@@ -728,24 +732,50 @@ int automatic_mode(int C) {
 
 template <int LB> se_status_t set_smem_limits() {
     const int bytes = int(batch::pcfg<LB>::SMEM);
-    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB>), bytes, "the panel kernel"))
-        return st;
+    auto raise = [bytes](const void* fn, const char* what) { return raise_smem_limit(fn, bytes, what); };
+    auto both = [&](auto tag) -> se_status_t {  // every kernel of one micro-tile, whole and split
+        constexpr int NQ = decltype(tag)::value;
+        const void* fns[6] = {reinterpret_cast<const void*>(panels_kernel<LB, NQ, false>),
+                              reinterpret_cast<const void*>(panels_kernel<LB, NQ, true>),
+                              reinterpret_cast<const void*>(rem_kernel<LB, NQ, false>),
+                              reinterpret_cast<const void*>(rem_kernel<LB, NQ, true>),
+                              reinterpret_cast<const void*>(round_kernel<LB, NQ, false>),
+                              reinterpret_cast<const void*>(round_kernel<LB, NQ, true>)};
+        for (const void* fn : fns)
+            if (se_status_t st = raise(fn, "the closure's tile kernels")) return st;
+        return SE_OK;
+    };
+    if (se_status_t st = both(std::integral_constant<int, 8>{})) return st;
     if constexpr (LB == 16) {
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(panels_kernel<LB, 4>), bytes,
-                                              "the wide panel kernel"))
-            return st;
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB, 4>), bytes,
-                                              "the wide remainder kernel"))
-            return st;
-        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(round_kernel<LB, 4>), bytes,
-                                              "the wide round kernel"))
-            return st;
+        if (se_status_t st = both(std::integral_constant<int, 4>{})) return st;
     }
-    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rem_kernel<LB>), bytes, "the remainder kernel"))
-        return st;
-    if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(round_kernel<LB>), bytes, "the round kernel"))
-        return st;
-    return raise_smem_limit(reinterpret_cast<const void*>(flow_kernel<LB>), bytes, "the dataflow closure");
+    return raise(reinterpret_cast<const void*>(flow_kernel<LB>), "the dataflow closure");
+}
+
+// Launches of the tile kernels. The split-K form (parts > 1) is a separate instantiation, so the
+// whole-tile kernels that large closures run carry no split logic.
+template <int LB, int NQ>
+void launch_panels(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, int K, int parts,
+                   uint32_t* ctr, uint32_t* scr, uint32_t* err) {
+    constexpr int T = tile_threads<LB, NQ>();
+    if (parts > 1) panels_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, K, parts, ctr, scr, err);
+    else panels_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, K, 1, nullptr, nullptr, err);
+}
+
+template <int LB, int NQ>
+void launch_rem(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, int K, int fuse, int subset,
+                int parts, uint32_t* ctr, uint32_t* scr, uint32_t* err) {
+    constexpr int T = tile_threads<LB, NQ>();
+    if (parts > 1) rem_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, K, fuse, subset, parts, ctr, scr, err);
+    else rem_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, K, fuse, subset, 1, nullptr, nullptr, err);
+}
+
+template <int LB, int NQ>
+void launch_round(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, const batch::Elec& En, int K,
+                  uint32_t* state, int parts, uint32_t* ctr, uint32_t* scr, uint32_t* err) {
+    constexpr int T = tile_threads<LB, NQ>();
+    if (parts > 1) round_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, En, K, state, parts, ctr, scr, err);
+    else round_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, En, K, state, 1, nullptr, nullptr, err);
 }
 
 // Rounds of the blocked closure on an initialised working matrix, in schedule `mode` (1, 3 or
@@ -806,10 +836,8 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     cudaEvent_t* remb = ev.data() + R;
     if (phase_ms) SE_CUDA_TRY(cudaEventRecord(ev[2 * R], A));
     auto panels = [&](int K) {
-        if constexpr (wide)
-            panels_kernel<LB, 4><<<2 * (R - 1), tile_threads<LB, 4>(), smem, A>>>(E[K & 1], K, 1, nullptr, nullptr,
-                                                                                 err);
-        else panels_kernel<LB><<<2 * (R - 1), CF::THREADS, smem, A>>>(E[K & 1], K, 1, nullptr, nullptr, err);
+        if constexpr (wide) launch_panels<LB, 4>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err);
+        else launch_panels<LB, 8>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err);
     };
     if constexpr (wide) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, A>>>(S, ldw, 0, dT);
     else diag_kernel<LB><<<1, CF::THREADS, 0, A>>>(S, ldw, 0, dT);
@@ -819,17 +847,16 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     const int R2 = R - 2;
     for (int K = 0; K + 1 < R; ++K) {
         SE_CUDA_TRY(cudaStreamWaitEvent(B, pan[K], 0));
-        rem_kernel<LB><<<R2 * R2, CF::THREADS, smem, B>>>(E[K & 1], K, 0, 2, 1, nullptr, nullptr, err);
+        launch_rem<LB, 8>(unsigned(R2 * R2), smem, B, E[K & 1], K, 0, 2, 1, nullptr, nullptr, err);
         SE_CUDA_TRY(cudaEventRecord(remb[K], B));
         if (K > 0) SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[K - 1], 0));
-        rem_kernel<LB><<<2 * R - 3, CF::THREADS, smem, A>>>(E[K & 1], K, 1, 1, 1, nullptr, nullptr, err);
+        launch_rem<LB, 8>(unsigned(2 * R - 3), smem, A, E[K & 1], K, 1, 1, 1, nullptr, nullptr, err);
         panels(K + 1);
         SE_CHECK_LAUNCH();
         SE_CUDA_TRY(cudaEventRecord(pan[K + 1], A));
     }
     SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[R - 2], 0));
-    rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, A>>>(E[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr,
-                                                                err);
+    launch_rem<LB, 8>(unsigned((R - 1) * (R - 1)), smem, A, E[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr, err);
     SE_CHECK_LAUNCH();
     if (phase_ms) {
         SE_CUDA_TRY(cudaEventRecord(ev[2 * R + 1], A));
@@ -922,10 +949,9 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         const unsigned panel_blocks = unsigned(2 * (R - 1) * parts);
         if (wide8) {
             if constexpr (LB == 16)
-                panels_kernel<LB, 4><<<panel_blocks, tile_threads<LB, 4>(), smem, stream>>>(E2[0], 0, parts, split_ctr,
-                                                                                           split_scr, err);
+                launch_panels<LB, 4>(panel_blocks, smem, stream, E2[0], 0, parts, split_ctr, split_scr, err);
         } else {
-            panels_kernel<LB><<<panel_blocks, CF::THREADS, smem, stream>>>(E2[0], 0, parts, split_ctr, split_scr, err);
+            launch_panels<LB, 8>(panel_blocks, smem, stream, E2[0], 0, parts, split_ctr, split_scr, err);
         }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
@@ -933,21 +959,21 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         for (int K = 0; K + 1 < R; ++K) {
             if (wide8) {
                 if constexpr (LB == 16)
-                    round_kernel<LB, 4><<<tasks, tile_threads<LB, 4>(), smem, stream>>>(
-                        E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K, parts, split_ctr, split_scr, err);
+                    launch_round<LB, 4>(unsigned(tasks), smem, stream, E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K,
+                                        parts, split_ctr, split_scr, err);
             } else {
-                round_kernel<LB><<<tasks, CF::THREADS, smem, stream>>>(E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K,
-                                                                       parts, split_ctr, split_scr, err);
+                launch_round<LB, 8>(unsigned(tasks), smem, stream, E2[K & 1], E2[(K + 1) & 1], K, state + 2 * K,
+                                    parts, split_ctr, split_scr, err);
             }
             SE_CHECK_LAUNCH();
         }
         if (wide8) {
             if constexpr (LB == 16)
-                rem_kernel<LB, 4><<<(R - 1) * (R - 1), tile_threads<LB, 4>(), smem, stream>>>(
-                    E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr, err);
+                launch_rem<LB, 4>(unsigned((R - 1) * (R - 1)), smem, stream, E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr,
+                                  nullptr, err);
         } else {
-            rem_kernel<LB><<<(R - 1) * (R - 1), CF::THREADS, smem, stream>>>(E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr,
-                                                                             nullptr, err);
+            launch_rem<LB, 8>(unsigned((R - 1) * (R - 1)), smem, stream, E2[(R - 1) & 1], R - 1, 0, 0, 1, nullptr,
+                              nullptr, err);
         }
         SE_CHECK_LAUNCH();
         if (se_status_t st = mark()) return st;
@@ -999,11 +1025,9 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         if (K > 0 && !fused) pivot(K);
         const unsigned panel_blocks = unsigned(2 * (R - 1) * parts);
         if (wide) {
-            if constexpr (LB == 16)
-                panels_kernel<LB, 4><<<panel_blocks, tile_threads<LB, 4>(), smem, stream>>>(E, K, parts, split_ctr,
-                                                                                           split_scr, err);
+            if constexpr (LB == 16) launch_panels<LB, 4>(panel_blocks, smem, stream, E, K, parts, split_ctr, split_scr, err);
         } else {
-            panels_kernel<LB><<<panel_blocks, CF::THREADS, smem, stream>>>(E, K, parts, split_ctr, split_scr, err);
+            launch_panels<LB, 8>(panel_blocks, smem, stream, E, K, parts, split_ctr, split_scr, err);
         }
         mark(1);
         // Tile (K+1, K+1) and its pivot: counter and partials after the panel tiles'.
@@ -1012,11 +1036,9 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         uint32_t* pctr = split_ctr ? split_ctr + 2 * (R - 1) : nullptr;
         uint32_t* pscr = split_scr ? split_scr + int64_t(2 * (R - 1)) * parts * kT * CF::TW : nullptr;
         if (wide_rem) {
-            if constexpr (LB == 16)
-                rem_kernel<LB, 4><<<rem_blocks, tile_threads<LB, 4>(), smem, stream>>>(E, K, fuse, 0, parts, pctr,
-                                                                                      pscr, err);
+            if constexpr (LB == 16) launch_rem<LB, 4>(rem_blocks, smem, stream, E, K, fuse, 0, parts, pctr, pscr, err);
         } else {
-            rem_kernel<LB><<<rem_blocks, CF::THREADS, smem, stream>>>(E, K, fuse, 0, parts, pctr, pscr, err);
+            launch_rem<LB, 8>(rem_blocks, smem, stream, E, K, fuse, 0, parts, pctr, pscr, err);
         }
         mark(3);
         SE_CHECK_LAUNCH();
