@@ -803,6 +803,7 @@ def measure_batch(args, world, rank, local_rank):
     tune_s = 0.0
     if args.no_autotune:
         lanes, order, ctas = [lanes_for_voters(V) for (_, V, _, _) in specs], 0, 0
+        micro = None
     else:
         from scalingelections_b200 import autotune
 
@@ -812,8 +813,9 @@ def measure_batch(args, world, rank, local_rank):
                               path=Path(report_dir) / "autotune.json" if report_dir else None)
         tune_s = time.perf_counter() - t0
         lanes, order, ctas = autotune.choose(tuned, [C for (C, _, _, _) in specs], [V for (_, V, _, _) in specs])
+        micro = autotune.choose_micro_tiles(tuned, [C for (C, _, _, _) in specs], lanes)
     cells = float(sum(C ** 3 for (C, _, _, _) in all_specs))
-    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas)
+    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas, micro_tiles=micro)
     b.build_graph()
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -875,7 +877,8 @@ def measure_batch(args, world, rank, local_rank):
                        "u16_elections": sum(1 for l in lanes if l[0] == 16),
                        "u16_shifted_elections": sum(1 for l in lanes if l[0] == 16 and l[1] > 0),
                        "u32_elections": sum(1 for l in lanes if l[0] == 32),
-                       "tasks": {"u16": tasks[0], "u32": tasks[1]}, "graph": True},
+                       "tasks": {"u16": tasks[0], "u32": tasks[1], "u16_wide_micro_tile": tasks[2]},
+                       "graph": True},
             "batched_gcells_per_s": cells / (ms_max * 1e-3) / 1e9,
             "loop_elections_per_s": len(specs) / loop_s,
             "loop_seconds": loop_s,
@@ -886,7 +889,8 @@ def measure_batch(args, world, rank, local_rank):
             "autotune": None if tuned is None else {
                 "seconds": tune_s, "order": order, "ctas_per_sm": ctas,
                 "launch_ms": tuned.get("launch_ms"),
-                "buckets": {k: {"C": v["range"], "lanes": v["lanes"]} for k, v in tuned["buckets"].items()}},
+                "buckets": {k: {"C": v["range"], "lanes": v["lanes"], "micro_tile": v.get("micro_tile", 8),
+                                "ms": v["ms"]} for k, v in tuned["buckets"].items()}},
             "clocks": clocks.summary(),
         }
     del b, prefs, outs, ranks, ws

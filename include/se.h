@@ -222,7 +222,10 @@ typedef struct se_election {
     int32_t C;
     int32_t lane_bits;
     uint32_t value_offset; /* 16-bit lanes only */
-    int32_t reserved;
+    /* Micro-tile of the tile tasks: 0 or 8 the default (8 x 8 words per thread), 4 the wide
+     * one (8 x 4 words, 256-thread CTAs; 16-bit lanes, used for C > 128). The batch runs each
+     * kind in its own persistent launch; the autotuner picks one per size bucket. */
+    int32_t micro_tile;
 } se_election_t;
 
 typedef struct se_batch_plan {
@@ -248,7 +251,8 @@ SE_API se_status_t se_batch_set_wait_limit(se_batch_plan_t* plan, uint64_t limit
  * CTA-milliseconds spent waiting for dependencies. Any pointer may be NULL. */
 SE_API se_status_t se_batch_profile(const se_batch_plan_t* plan, double* busy_ms, int64_t* tasks,
                                     double* wait_ms, void* stream);
-/* Number of tasks in queue 0 (16-bit lanes) or 1 (32-bit lanes) of a prepared plan. */
+/* Number of tasks in queue 0 (16-bit lanes), 1 (32-bit lanes) or 2 (16-bit lanes on the wide
+ * micro-tile) of a prepared plan. */
 SE_API int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue);
 
 /* ---------------------------------------------------------------------------------------

@@ -96,7 +96,7 @@ class Election(ctypes.Structure):
     _fields_ = [("d_pref", ctypes.c_void_p), ("ld_pref", ctypes.c_int64), ("d_out", ctypes.c_void_p),
                 ("ld_out", ctypes.c_int64), ("d_wins", ctypes.c_void_p), ("d_ranking", ctypes.c_void_p),
                 ("C", ctypes.c_int32), ("lane_bits", ctypes.c_int32), ("value_offset", ctypes.c_uint32),
-                ("reserved", ctypes.c_int32)]
+                ("micro_tile", ctypes.c_int32)]
 
 
 class Request(ctypes.Structure):

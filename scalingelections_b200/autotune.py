@@ -17,18 +17,20 @@ remainder: small and medium C.
 The batched closure's tuner (tune):
 
 For each election-size bucket it times, on the GPU, the batched persistent closure of a
-sample batch in both lane modes and keeps the faster:
-  lanes        16-bit (shifted by V // 2 when counts exceed 16 bits) or 32-bit.
+sample batch in both lane modes and keeps the faster, and in 16-bit lanes (C > 128) both
+register micro-tiles of the tile tasks:
+  lanes        16-bit (shifted by V // 2 when counts exceed 16 bits) or 32-bit;
+  micro_tile   8 (8 x 8 words per thread, 128-thread CTAs) or 4 (8 x 4 words, 256-thread
+               CTAs, each kind in its own persistent launch), the wide one only when it is at
+               least 2 % faster.
 Then, over a mixed sample with the same number of elections in every bucket (a log-uniform
 spread of sizes, like a real batch), it times every pair of the settings that belong to the
 whole persistent launch rather than to one election:
   ctas_per_sm  persistent CTAs per SM (1 or 2);
   order        elections of at most 128 candidates after the tiled ones, or before.
 A per-bucket CTA count would be tuned on a few elections of one size, where one election's
-chain of pivot rounds dominates, and would not carry over to a mixed launch. In the batch the
-tile (128 x 128 cells) and the register micro-tile (8 x 8 words) are fixed: its persistent
-CTAs run every task kind side by side, two per SM, and the measured busy time is 96 % of the
-grid. Results are stored as JSON and looked up per election.
+chain of pivot rounds dominates, and would not carry over to a mixed launch. The tile is
+128 x 128 cells everywhere. Results are stored as JSON and looked up per election.
 """
 from __future__ import annotations
 
@@ -71,8 +73,8 @@ def _sample_batch(lo: int, hi: int, n: int, V: int, seed: int, device) -> list[t
     return out
 
 
-def _time(prefs, lanes, order, ctas, reps: int) -> float:
-    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas)
+def _time(prefs, lanes, order, ctas, reps: int, micro_tiles=None) -> float:
+    b = BatchedElections(prefs, lanes, order=order, ctas_per_sm=ctas, micro_tiles=micro_tiles)
     b.build_graph()
     b.launch_graph()
     b.check()
@@ -105,14 +107,22 @@ def tune(V: int = 100000, per_bucket: int = 48, reps: int = 3, seed: int = 0, pa
                 continue
             results[f"u{lanes}"] = _time(prefs, [lane_pair] * len(prefs), 0, 2, reps)
         best = min(results, key=results.get)
-        table["buckets"][str(b)] = {"range": [lo, hi], "lanes": int(best[1:]), "ms": results}
+        micro = 8
+        if best == "u16" and hi > 128:  # the wide micro-tile, for elections with tile tasks
+            lane_pair = lanes_for_voters(V)
+            results["u16_wide"] = _time(prefs, [lane_pair] * len(prefs), 0, 2, reps, [4] * len(prefs))
+            # A margin: the queues run one after another, so a split that noise decides only
+            # costs the launches' balance.
+            micro = 4 if results["u16_wide"] < 0.98 * results["u16"] else 8
+        table["buckets"][str(b)] = {"range": [lo, hi], "lanes": int(best[1:]), "micro_tile": micro, "ms": results}
         del prefs
     mixed = []
     for b, (lo, hi) in enumerate(BUCKETS[:-1]):
         mixed += _sample_batch(lo, hi, max(2, per_bucket // 2), V, seed + 100 + b, device)
     lanes = [(LANES_U32, 0) if table["buckets"][str(bucket_of(int(p.shape[0])))]["lanes"] == 32
              else lanes_for_voters(V) for p in mixed]
-    launch = {(o, c): _time(mixed, lanes, o, c, reps) for o in (0, 1) for c in (1, 2)}
+    micro = choose_micro_tiles(table, [int(p.shape[0]) for p in mixed], lanes)
+    launch = {(o, c): _time(mixed, lanes, o, c, reps, micro) for o in (0, 1) for c in (1, 2)}
     order, ctas = min(launch, key=launch.get)
     table["order"] = int(order)
     table["ctas_per_sm"] = int(ctas)
@@ -185,3 +195,14 @@ def choose(table: dict | None, Cs: Sequence[int], Vs: Sequence[int]) -> tuple[li
     order = int((table or {}).get("order", 0))
     ctas = int((table or {}).get("ctas_per_sm", 0))
     return lanes, order, ctas
+
+
+def choose_micro_tiles(table: dict | None, Cs: Sequence[int], lanes: Sequence) -> list[int]:
+    """Micro-tile per election (BatchedElections micro_tiles): the bucket's tuned one for
+    16-bit lanes, else the default 8 (32-bit lanes have the default only)."""
+    out = []
+    for C, lp in zip(Cs, lanes):
+        entry = (table or {}).get("buckets", {}).get(str(bucket_of(int(C))))
+        lb = int(lp[0]) if isinstance(lp, (tuple, list)) else int(lp)
+        out.append(int(entry.get("micro_tile", 8)) if entry and lb == LANES_U16 else 8)
+    return out

@@ -33,13 +33,16 @@ class BatchedElections:
 
     lanes: per election, LANES_U16 or LANES_U32, or (lanes, value_offset) pairs such as
     lanes_for_voters() returns; None picks from each matrix's maximum (one device-to-host
-    read for the whole batch). order: 0 runs small elections (C <= 128) after the tiled ones,
-    1 before them. ctas_per_sm: persistent CTAs per SM (0 = as many as fit). An autotuned
-    table (scalingelections_b200.autotune) supplies lanes, order and ctas_per_sm per size
-    bucket. The batch keeps references to every buffer it uses."""
+    read for the whole batch). micro_tiles: per election, 8 (the default 8 x 8-word micro-tile)
+    or 4 (the wide 8 x 4-word one, 256-thread CTAs; 16-bit lanes), run as separate persistent
+    launches; None is 8 everywhere. order: 0 runs small elections (C <= 128) after the tiled
+    ones, 1 before them. ctas_per_sm: persistent CTAs per SM (0 = as many as fit). An autotuned
+    table (scalingelections_b200.autotune) supplies lanes, micro-tiles, order and ctas_per_sm
+    per size bucket. The batch keeps references to every buffer it uses."""
 
     def __init__(self, preferences: Sequence[torch.Tensor], lanes: Sequence | None = None, *,
-                 ranking: bool = True, order: int = 0, ctas_per_sm: int = 0):
+                 ranking: bool = True, order: int = 0, ctas_per_sm: int = 0,
+                 micro_tiles: Sequence[int] | None = None):
         if not preferences:
             raise ValueError("empty batch")
         self.device = preferences[0].device
@@ -59,6 +62,9 @@ class BatchedElections:
         self.offsets = [p[1] for p in pairs]
         if len(self.lanes) != len(self.prefs):
             raise ValueError("one lane mode per election")
+        self.micro_tiles = [8] * len(self.prefs) if micro_tiles is None else [int(m) for m in micro_tiles]
+        if len(self.micro_tiles) != len(self.prefs):
+            raise ValueError("one micro-tile per election")
         self.outs, self.wins, self.rankings = [], [], []
         arr = (_lib.Election * len(self.prefs))()
         for e, (p, (C, ld)) in enumerate(zip(self.prefs, shapes)):
@@ -73,7 +79,8 @@ class BatchedElections:
             self.wins.append(w)
             self.rankings.append(r)
             arr[e] = _lib.Election(p.data_ptr(), ld, out.data_ptr(), C, w.data_ptr() if w is not None else None,
-                                   r.data_ptr() if r is not None else None, C, self.lanes[e], self.offsets[e], 0)
+                                   r.data_ptr() if r is not None else None, C, self.lanes[e], self.offsets[e],
+                                   self.micro_tiles[e])
         self._arr = arr
         L = _lib.lib()
         need = L.se_batch_workspace_bytes(len(self.prefs), ctypes.cast(arr, ctypes.c_void_p))
@@ -90,9 +97,11 @@ class BatchedElections:
     def strongest_paths(self) -> list[torch.Tensor]:
         return self.outs
 
-    def task_counts(self) -> tuple[int, int]:
+    def task_counts(self) -> tuple[int, int, int]:
+        """Tasks of the three persistent launches: 16-bit lanes, 32-bit lanes, 16-bit lanes on
+        the wide micro-tile."""
         L = _lib.lib()
-        return (L.se_batch_task_count(ctypes.byref(self.plan), 0), L.se_batch_task_count(ctypes.byref(self.plan), 1))
+        return tuple(L.se_batch_task_count(ctypes.byref(self.plan), q) for q in range(3))
 
     def run(self) -> None:
         """Enqueue the whole batch on the current stream (asynchronous)."""

@@ -47,7 +47,8 @@ using namespace se::closure;
 struct Header {
     uint32_t err;
     uint32_t abort;
-    uint32_t head[2];  // queue heads of the u16 and u32 persistent launches
+    uint32_t head[3];  // queue heads of the persistent launches: u16, u32, u16 on the wide micro-tile
+    uint32_t pad;
     // Profile: per task kind (SMALL, PIVOT, ROW, COL, REM) CTA-nanoseconds busy and tasks run;
     // CTA-nanoseconds waiting for dependencies.
     unsigned long long busy_ns[5];
@@ -93,8 +94,11 @@ __device__ __forceinline__ void claim_task(const Elec* elecs, const uint64_t* ta
     s_ready = ready;
 }
 
-template <int LB>
-__global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
+// NQ: the tile tasks' micro-tile, 8 (8 x 8 words, the default) or 4 (8 x 4 words, 256 threads,
+// 16-bit lanes: elections with C > 128 whose size bucket the autotuner gave the wide one; small
+// elections always run on the default, whose SMALL routine is written for it).
+template <int LB, int NQ = 8>
+__global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
     persistent_kernel(const Elec* __restrict__ elecs, const uint64_t* __restrict__ tasks, uint32_t ntasks,
                       Header* __restrict__ hdr, int queue, uint64_t dep_wait_ns) {
     using CF = cfg<LB>;
@@ -152,12 +156,13 @@ __global__ void __launch_bounds__(cfg<LB>::THREADS, 1)
         bool ok = true;
         const uint64_t tb = threadIdx.x == 0 ? global_ns() : 0;
         if (type == kSmall) {
-            run_small<LB>(E, smem, rowbuf, colbuf, s_wins, &hdr->err);
+            if constexpr (NQ == 8) run_small<LB>(E, smem, rowbuf, colbuf, s_wins, &hdr->err);
+            else ok = false;  // the host never queues one here
         } else if (type == kPivot) {
-            run_pivot<LB>(E, int(k), rowbuf, colbuf);
+            run_pivot<LB, NQ>(E, int(k), rowbuf, colbuf);
         } else {
             const int kind = type == kRow ? kTileRow : (type == kCol ? kTileCol : kTileRem);
-            ok = run_tile<LB>(E, &E, kind, int(k), int(i), int(j), smem, bars, par_a, par_b);
+            ok = run_tile<LB, true, NQ>(E, &E, kind, int(k), int(i), int(j), smem, bars, par_a, par_b);
         }
         __threadfence();
         __syncthreads();
@@ -519,10 +524,10 @@ struct Plan {
     int64_t work_bytes;
     int32_t n, nbig, nsmall;
     int64_t elec_off, big_off, init_prefix_off, fin_prefix_off, place_prefix_off, counters_off, counters_bytes;
-    int64_t tasks_off[2];
-    uint32_t ntasks[2];
+    int64_t tasks_off[3];  // queues: u16, u32, u16 on the wide micro-tile
+    uint32_t ntasks[3];
     int64_t init_blocks, fin_blocks, place_blocks;
-    int32_t grid[2];
+    int32_t grid[3];
     cudaGraphExec_t graph;
     uint64_t dep_wait_ns;  // limit of one dependency wait of the persistent kernel
     int64_t pair_owner_off;  // PairOwner per block of the init and output kernels
@@ -533,12 +538,16 @@ int64_t align256(int64_t x) { return round_up(x, 256); }
 
 struct Sizes {
     int64_t total = 0, elec_off, big_off, init_prefix_off, fin_prefix_off, place_prefix_off, counters_off,
-            counters_bytes, tasks_off[2], pair_owner_off, pairs = 0;
+            counters_bytes, tasks_off[3], pair_owner_off, pairs = 0;
     std::vector<int64_t> s_off, at_off, dt_off, ctr_off;
-    std::vector<int> lanes, R, Cp;
+    std::vector<int> lanes, R, Cp, queue;
     int nbig = 0, nsmall = 0;
-    uint32_t ntasks[2] = {0, 0};
+    uint32_t ntasks[3] = {0, 0, 0};
 };
+
+// The persistent launch an election's tasks go to: 1 for 32-bit lanes; 2 for 16-bit lanes with
+// C > 128 on the wide micro-tile; 0 otherwise.
+int queue_of(int lanes, int R, int micro_tile) { return lanes != 16 ? 1 : (R > 1 && micro_tile == 4 ? 2 : 0); }
 
 se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
     SE_REQUIRE(n >= 0, SE_ERR_INVALID, "negative election count");
@@ -550,6 +559,7 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
     z.lanes.resize(n);
     z.R.resize(n);
     z.Cp.resize(n);
+    z.queue.resize(n);
     int64_t off = 256;  // header
     z.elec_off = off;
     off = align256(off + int64_t(n) * int64_t(sizeof(Elec)));
@@ -559,12 +569,15 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
         SE_REQUIRE(el[e].lane_bits == 0 || el[e].lane_bits == 16 || el[e].lane_bits == 32, SE_ERR_INVALID,
                    "election %d: lane_bits must be 0, 16 or 32", e);
         z.lanes[e] = el[e].lane_bits == 16 ? 16 : 32;
+        SE_REQUIRE(el[e].micro_tile == 0 || el[e].micro_tile == 8 || (el[e].micro_tile == 4 && z.lanes[e] == 16),
+                   SE_ERR_INVALID, "election %d: micro_tile must be 0 or 8, or 4 with 16-bit lanes", e);
         z.Cp[e] = int(round_up(el[e].C, kT));
         z.R[e] = z.Cp[e] / kT;
+        z.queue[e] = queue_of(z.lanes[e], z.R[e], el[e].micro_tile);
         SE_REQUIRE(z.R[e] <= 4095, SE_ERR_INVALID, "election %d too large for a batch", e);
         if (z.R[e] == 1) {
             ++z.nsmall;
-            z.ntasks[z.lanes[e] == 16 ? 0 : 1] += 1;
+            z.ntasks[z.queue[e]] += 1;
             continue;
         }
         ++z.nbig;
@@ -576,7 +589,7 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
         z.dt_off[e] = off;
         off = align256(off + int64_t(kT) * kT * 4);
         const uint64_t R = uint64_t(z.R[e]);
-        z.ntasks[z.lanes[e] == 16 ? 0 : 1] += uint32_t(R * R * R);
+        z.ntasks[z.queue[e]] += uint32_t(R * R * R);
         const int64_t nt = z.Cp[e] / kPT;
         z.pairs += nt * (nt + 1) / 2;
     }
@@ -599,7 +612,7 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
     off = align256(off + int64_t(z.nbig + 1) * 8);
     z.pair_owner_off = off;
     off = align256(off + z.pairs * 8);
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 3; ++q) {
         z.tasks_off[q] = off;
         off = align256(off + int64_t(z.ntasks[q]) * 8);
     }
@@ -607,15 +620,16 @@ se_status_t size_batch(int n, const se_election_t* el, Sizes& z) {
     return SE_OK;
 }
 
-template <int LB> int occupancy() {
+template <int LB, int NQ = 8> int occupancy() {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<LB>, cfg<LB>::THREADS, pcfg<LB>::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel<LB, NQ>, tile_threads<LB, NQ>(),
+                                                  pcfg<LB>::SMEM);
     cudaGetLastError();
     return per_sm;
 }
 
-template <int LB> se_status_t set_persistent_smem() {
-    return raise_smem_limit(reinterpret_cast<const void*>(persistent_kernel<LB>), int(pcfg<LB>::SMEM),
+template <int LB, int NQ = 8> se_status_t set_persistent_smem() {
+    return raise_smem_limit(reinterpret_cast<const void*>(persistent_kernel<LB, NQ>), int(pcfg<LB>::SMEM),
                             "the batched closure");
 }
 
@@ -638,6 +652,11 @@ se_status_t enqueue(const Plan& P, cudaStream_t s) {
     if (P.ntasks[1]) {
         persistent_kernel<32><<<P.grid[1], cfg<32>::THREADS, pcfg<32>::SMEM, s>>>(
             elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[1]), P.ntasks[1], hdr, 1, P.dep_wait_ns);
+        SE_CHECK_LAUNCH();
+    }
+    if (P.ntasks[2]) {
+        persistent_kernel<16, 4><<<P.grid[2], tile_threads<16, 4>(), pcfg<16>::SMEM, s>>>(
+            elecs, reinterpret_cast<const uint64_t*>(P.work + P.tasks_off[2]), P.ntasks[2], hdr, 2, P.dep_wait_ns);
         SE_CHECK_LAUNCH();
     }
     if (P.nbig) {
@@ -692,6 +711,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     }
     if (se_status_t st = set_persistent_smem<16>()) return st;
     if (se_status_t st = set_persistent_smem<32>()) return st;
+    if (se_status_t st = set_persistent_smem<16, 4>()) return st;
     uint8_t* work = static_cast<uint8_t*>(d_work);
 
     std::vector<Elec> host(n);
@@ -730,18 +750,18 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     std::stable_sort(order_big.begin(), order_big.end(), [&](int a, int b) { return host[a].R > host[b].R; });
     int Rmax = 1;
     for (int e : big) Rmax = std::max(Rmax, host[e].R);
-    std::vector<uint64_t> q[2];
+    std::vector<uint64_t> q[3];
     std::vector<uint64_t> small[2];
     for (int e = 0; e < n; ++e)
-        if (host[e].R == 1) small[host[e].lanes == 16 ? 0 : 1].push_back(pack_task(e, kSmall, 0, 0, 0));
+        if (host[e].R == 1) small[z.queue[e]].push_back(pack_task(e, kSmall, 0, 0, 0));
     if (order == 1)  // small elections first
         for (int l = 0; l < 2; ++l) q[l].insert(q[l].end(), small[l].begin(), small[l].end());
     for (int k = 0; k < Rmax; ++k) {
         for (int e : order_big)
-            if (host[e].R > k) q[host[e].lanes == 16 ? 0 : 1].push_back(pack_task(e, kPivot, k, k, k));
+            if (host[e].R > k) q[z.queue[e]].push_back(pack_task(e, kPivot, k, k, k));
         for (int e : order_big)
             if (host[e].R > k) {
-                auto& Q = q[host[e].lanes == 16 ? 0 : 1];
+                auto& Q = q[z.queue[e]];
                 for (int x = 0; x < host[e].R; ++x)
                     if (x != k) {
                         Q.push_back(pack_task(e, kRow, k, k, x));
@@ -750,7 +770,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
             }
         for (int e : order_big)
             if (host[e].R > k) {
-                auto& Q = q[host[e].lanes == 16 ? 0 : 1];
+                auto& Q = q[z.queue[e]];
                 for (int i = 0; i < host[e].R; ++i)
                     if (i != k)
                         for (int j = 0; j < host[e].R; ++j)
@@ -759,7 +779,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     }
     if (order != 1)
         for (int l = 0; l < 2; ++l) q[l].insert(q[l].end(), small[l].begin(), small[l].end());
-    for (int l = 0; l < 2; ++l)
+    for (int l = 0; l < 3; ++l)
         SE_REQUIRE(q[l].size() == z.ntasks[l], SE_ERR_INVALID, "internal: task count mismatch");
 
     // Block prefixes of the batched elementwise kernels, and for init and finalize (one CTA per
@@ -788,7 +808,7 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
         SE_CUDA_TRY(cudaMemcpy(work + z.pair_owner_off, owner.data(), sizeof(PairOwner) * owner.size(),
                                cudaMemcpyHostToDevice));
     }
-    for (int l = 0; l < 2; ++l)
+    for (int l = 0; l < 3; ++l)
         if (!q[l].empty())
             SE_CUDA_TRY(cudaMemcpy(work + z.tasks_off[l], q[l].data(), 8 * q[l].size(), cudaMemcpyHostToDevice));
 
@@ -810,20 +830,22 @@ static se_status_t batch_prepare_impl(int n, const se_election_t* el, void* d_wo
     P.pair_owner_off = z.pair_owner_off;
     P.counters_off = z.counters_off;
     P.counters_bytes = z.counters_bytes;
-    for (int l = 0; l < 2; ++l) {
+    for (int l = 0; l < 3; ++l) {
         P.tasks_off[l] = z.tasks_off[l];
         P.ntasks[l] = z.ntasks[l];
     }
     P.init_blocks = ip.back();
     P.fin_blocks = fp.back();
     P.place_blocks = pp.back();
-    const int occ16 = occupancy<16>(), occ32 = occupancy<32>();
-    SE_REQUIRE(occ16 >= 1 && occ32 >= 1, SE_ERR_CUDA, "batched closure kernel cannot be resident");
+    const int occ16 = occupancy<16>(), occ32 = occupancy<32>(), occ16w = occupancy<16, 4>();
+    SE_REQUIRE(occ16 >= 1 && occ32 >= 1 && occ16w >= 1, SE_ERR_CUDA, "batched closure kernel cannot be resident");
     SE_REQUIRE(ctas_per_sm >= 0, SE_ERR_INVALID, "ctas_per_sm must be >= 0");
     const int per16 = ctas_per_sm > 0 ? std::min(occ16, ctas_per_sm) : occ16;
     const int per32 = ctas_per_sm > 0 ? std::min(occ32, ctas_per_sm) : occ32;
+    const int per16w = ctas_per_sm > 0 ? std::min(occ16w, ctas_per_sm) : occ16w;
     P.grid[0] = int(std::min<int64_t>(P.ntasks[0], int64_t(sms) * per16));
     P.grid[1] = int(std::min<int64_t>(P.ntasks[1], int64_t(sms) * per32));
+    P.grid[2] = int(std::min<int64_t>(P.ntasks[2], int64_t(sms) * per16w));
     P.graph = nullptr;
     P.dep_wait_ns = kDepWaitNs;
     std::memcpy(plan_out, &P, sizeof(P));
@@ -938,7 +960,7 @@ extern "C" se_status_t se_batch_profile(const se_batch_plan_t* plan, double* bus
 }
 
 extern "C" int64_t se_batch_task_count(const se_batch_plan_t* plan, int queue) {
-    if (!plan || queue < 0 || queue > 1) return -1;
+    if (!plan || queue < 0 || queue > 2) return -1;
     Plan P;
     std::memcpy(&P, plan, sizeof(P));
     return P.ntasks[queue];

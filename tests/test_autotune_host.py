@@ -41,3 +41,14 @@ def test_choose_with_a_table():
     lanes, order, ctas = choose(table, [8, 300, 1000], [50, 70000, 70000])
     assert lanes == [(LANES_U16, 0), (LANES_U32, 0), (LANES_U16, 35000)]
     assert (order, ctas) == (1, 2)
+
+
+def test_choose_micro_tiles():
+    from scalingelections_b200.autotune import choose_micro_tiles
+
+    table = {"buckets": {str(bucket_of(300)): {"lanes": 16, "micro_tile": 4},
+                         str(bucket_of(1000)): {"lanes": 16, "micro_tile": 8}}}
+    lanes = [(LANES_U16, 0), (LANES_U16, 0), (LANES_U32, 0), (LANES_U16, 35000)]
+    assert choose_micro_tiles(table, [300, 1000, 300, 300], lanes) == [4, 8, 8, 4]
+    assert choose_micro_tiles(None, [300], [(LANES_U16, 0)]) == [8]
+    assert choose_micro_tiles({"buckets": {str(bucket_of(8)): {"lanes": 16}}}, [8], [LANES_U16]) == [8]

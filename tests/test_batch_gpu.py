@@ -43,6 +43,30 @@ def test_mixed_batch_matches_oracle(orc):
     check_against_oracle(orc, host, b)
 
 
+def test_wide_micro_tile_queue_matches_oracle(orc):
+    """Elections given the wide micro-tile run in a third persistent launch of 256-thread CTAs:
+    the same results as the oracle, beside default-micro-tile and 32-bit elections in one batch;
+    a small election (C <= 128) asked to be wide runs on the default, and the wide micro-tile
+    in 32-bit lanes is refused."""
+    sizes = [60, 129, 200, 257, 300, 384, 513, 700, 130, 450, 90]
+    highs = [4000] * 8 + [2**32 - 1, 2**32 - 1, 60000]
+    host, dev = make_batch(11, sizes, highs)
+    lanes = [LANES_U16] * 8 + [LANES_U32, LANES_U32, LANES_U16]
+    micro = [4, 4, 8, 4, 8, 4, 4, 4, 8, 8, 4]
+    b = BatchedElections(dev, lanes, micro_tiles=micro)
+    counts = b.task_counts()
+    assert counts[2] > 0 and counts[0] > 0 and counts[1] > 0
+    b.run()
+    b.check()
+    check_against_oracle(orc, host, b)
+    b.build_graph()
+    b.launch_graph()
+    b.check()
+    check_against_oracle(orc, host, b)
+    with pytest.raises(api.SchulzeError, match="micro_tile"):
+        BatchedElections(dev[8:9], [LANES_U32], micro_tiles=[4])
+
+
 def test_alone_equals_in_batch():
     sizes = [40, 130, 300, 520]
     host, dev = make_batch(3, sizes, [1000] * 4)
