@@ -55,8 +55,12 @@ def parse():
     ap.add_argument("--lanes", type=int, default=16, choices=[0, 16, 32])
     ap.add_argument("--closure-mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6, 7, 8],
                     help="the closure's schedule: 0 automatic by size (default), 1 round by round, 2 dataflow, "
-                         "3 wide panels, 4 wide panels and pivot launches, 5 two streams, 6 one launch per round "
-                         "(include/se.h)")
+                         "3 wide panels, 4 wide panels and pivot launches, 5 two streams, 6 one launch per round, "
+                         "7 every tile wide, 8 one launch per round, wide (include/se.h)")
+    ap.add_argument("--workspace", choices=["full", "plain"], default="full",
+                    help="closure workspace of the headline step: full (every schedule at its fastest, the "
+                         "default) or plain (se_closure_workspace_bytes: no second pivot-panel buffer and no "
+                         "split tiles)")
     ap.add_argument("--cpu-sample", type=int, default=4096, help="C of the bounded CPU sample")
     ap.add_argument("--cpu-full-size", action="store_true",
                     help="reference arm: also time one closure at the workload's full size (minutes)")
@@ -315,7 +319,7 @@ def run_ours(args, world, rank, local_rank):
     peak_relax_per_clk, peak_mhz, _, peak_relax_per_s = [x.value for x in peak]
 
     api.set_closure_mode(args.closure_mode)
-    need = api.closure_workspace_bytes(C, lanes, dataflow=True)
+    need = api.closure_workspace_bytes(C, lanes, dataflow=args.workspace == "full")
     work = torch.empty(need, dtype=torch.uint8, device=dev)
     out = torch.empty((C, C), dtype=torch.uint32, device=dev)
     stream = torch.cuda.current_stream()
@@ -848,7 +852,7 @@ def measure_batch(args, world, rank, local_rank):
 
     # The same batch through the plain single-election entry points, one election at a time,
     # checked bit for bit against the batched results.
-    ws = torch.empty(max(api.closure_workspace_bytes(C, 0) for (C, _, _, _) in specs),
+    ws = torch.empty(max(api.closure_workspace_bytes(C, 0, dataflow=True) for (C, _, _, _) in specs),
                      dtype=torch.uint8, device=dev)
     outs = [torch.empty_like(p) for p in prefs]
     torch.cuda.synchronize()

@@ -186,7 +186,10 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
     on the same device (diagonal 0), bit-identical to compute_strongest_paths_numba_serial.
 
     lanes: LANES_U16 (every count < 65536), LANES_U32, or LANES_AUTO (checked on the device,
-    one 4-byte read back)."""
+    one 4-byte read back). workspace: used as given when it holds closure_workspace_bytes(C,
+    lanes) bytes (below the dataflow=True size the automatic schedule runs what fits, as
+    closure_schedule reports, and modes 2, 5, 6 and 8 set explicitly fail); else a full one is
+    allocated (and cached)."""
     C, ld = _check_matrix(preferences, "preferences")
     if out is None:
         out = torch.empty((C, C), dtype=torch.uint32, device=preferences.device)
@@ -195,11 +198,13 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
         raise ValueError("out has the wrong shape")
     if C == 0:
         return out
-    # Every schedule at its fastest: the second AT buffer (modes 2, 5, 6, 8) and the split
-    # panel tiles of small closures take a few MiB more than the plain workspace.
-    need = closure_workspace_bytes(C, lanes, dataflow=True)
+    # A workspace the caller passes is used as it is when it holds the plain size (the library
+    # then runs the schedules that fit it); otherwise the full one, with which every schedule
+    # runs at its fastest (the second AT buffer of modes 2, 5, 6 and 8 and the split panel
+    # tiles of small closures: a few MiB more).
+    need = closure_workspace_bytes(C, lanes, dataflow=False)
     if workspace is None or workspace.numel() * workspace.element_size() < need:
-        workspace = _workspace(need, preferences.device)
+        workspace = _workspace(closure_workspace_bytes(C, lanes, dataflow=True), preferences.device)
     have = workspace.numel() * workspace.element_size()
     with torch.cuda.device(preferences.device):
         check(_lib.lib().se_closure(preferences.data_ptr(), ld, C, out.data_ptr(), ldo, int(lanes), 0,
@@ -334,7 +339,7 @@ class ClosureStream:
         self.lanes, self.value_offset = int(lanes), int(value_offset)
         self.dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index)
         C = self.C
-        self.work_bytes = closure_workspace_bytes(C, self.lanes)
+        self.work_bytes = closure_workspace_bytes(C, self.lanes, dataflow=True)  # every schedule at its fastest
         with torch.cuda.device(self.dev):
             self.d_in = [torch.empty((C, C), dtype=torch.int32, device=self.dev) for _ in range(2)]
             self.d_out = [torch.empty((C, C), dtype=torch.int32, device=self.dev) for _ in range(2)]
