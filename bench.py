@@ -121,6 +121,10 @@ def config(args, world):
 # Clock sampling during the timed region
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
+    """SM clocks and throttle reasons during a timed region: one `nvidia-smi -lms 200` process
+    for the whole region (a single NVML start-up, which happens before the region opens: entry
+    waits, bounded, for the first sample), its lines read by a thread, the process ended on
+    exit."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -128,27 +132,41 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.samples: list[list[str]] = []
-        self._stop = threading.Event()
-        self._thr = threading.Thread(target=self._run, daemon=True)
+        self._first = threading.Event()
+        self._proc = None
+        self._thr = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [x.strip() for x in line.strip().split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+                self._first.set()
+        self._first.set()  # the process ended (no GPU, or terminated): nothing more to wait for
 
     def __enter__(self):
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return self
+        self._thr = threading.Thread(target=self._read, daemon=True)
         self._thr.start()
+        self._first.wait(10.0)
         return self
 
     def __exit__(self, *exc):
-        self._stop.set()
-        self._thr.join(timeout=10)
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+                self._proc.wait(timeout=5)
+        if self._thr is not None:
+            self._thr.join(timeout=5)
 
     def summary(self):
         if not self.samples:
