@@ -308,8 +308,9 @@ SE_API se_status_t se_engine_poll(se_engine_t* engine, int* slots, uint32_t* sta
 SE_API se_status_t se_engine_poll_tallied(se_engine_t* engine, int* slots, int max, int* n);
 /* Kernel launches so far, the engine's grid size, requests in flight and, when the arrays
  * are given, a profile snapshot: busy_ms[8] / tasks[8] per task kind (positions, tally,
- * small election, pivot, panels, remainder, output + wins, ranking), summed over CTAs, and
- * the CTA-milliseconds spent looking for work (any pointer may be NULL). */
+ * small election, round 0's pivot, panels, remainder (which closes the later pivots: the task
+ * that updates a round's next pivot tile closes it), output + wins, ranking), summed over
+ * CTAs, and the CTA-milliseconds spent looking for work (any pointer may be NULL). */
 SE_API se_status_t se_engine_stats(se_engine_t* engine, int64_t* launches, int* grid, int* in_flight,
                                    double* busy_ms, int64_t* tasks, double* search_ms);
 SE_API se_status_t se_engine_stop(se_engine_t* engine);

@@ -11,8 +11,10 @@
 //           shifted into 16 bits, as the closure's working matrix (d[j][i] = V - d[i][j]; no
 //           separate defeat pass)
 //   R == 1 (C <= 128): SMALL (closure, output, wins, ranking in one CTA)
-//   R >= 2: [PIVOT k][PANELS k][REM k] for k < R, then FIN (output + wins per block pair) and
-//           PLACE (ranking)
+//   R >= 2: PIVOT 0, then [PANELS k][REM k] for k < R, then FIN (output + wins per block pair)
+//           and PLACE (ranking). REM k's task 0 is tile (k+1, k+1), which after its update
+//           closes the next round's pivot (as the single-election closure's remainder launch
+//           does), so no round but the first has a pivot phase of its own.
 // The engine's CTAs (one or two per SM, resident while there is work) repeatedly scan the
 // active slots, oldest first, and claim a task from the first request whose current phase is
 // claimable: all tasks of the previous phase are done. Nothing waits on a dependency, so a
@@ -50,7 +52,7 @@ namespace serve {
 using namespace se::batch;
 using namespace se::closure;
 
-constexpr int kMaxPhases = 3 * 256 + 4;  // R <= 256, i.e. C <= 32768
+constexpr int kMaxPhases = 3 * 256 + 4;  // R <= 256, i.e. C <= 32768 (2R + 5 phases are used)
 constexpr size_t round_up_const(size_t x, size_t m) { return (x + m - 1) / m * m; }
 constexpr uint32_t kStatusOverflow = 4;
 constexpr uint32_t kStatusTally = 8;
@@ -88,18 +90,17 @@ struct EngineHeader {
 };
 constexpr int kKindCount = 8;
 
-__host__ __device__ inline int phases_of(int R) { return R == 1 ? 3 : 3 * R + 4; }
+// Phases of a request with R row blocks: POS, TALLY, then SMALL (R = 1), or PIVOT 0,
+// [PANELS k][REM k] for k < R, FIN, PLACE.
+__host__ __device__ inline int phases_of(int R) { return R == 1 ? 3 : 2 * R + 5; }
 
 __host__ __device__ inline uint32_t phase_size(int R, int64_t V, int f) {
     if (f == 0) return uint32_t((V + kPosChunk - 1) / kPosChunk);
     if (f == 1) return uint32_t(R * (R + 1));
-    if (R == 1) return 1;
-    const int g = f - 2;
-    if (g < 3 * R) {
-        const int kind = g % 3;
-        return kind == 0 ? 1u : (kind == 1 ? uint32_t(2 * (R - 1)) : uint32_t((R - 1) * (R - 1)));
-    }
-    return g == 3 * R ? uint32_t(R * (R + 1) / 2) : 1u;
+    if (R == 1 || f == 2) return 1;
+    const int g = f - 3;
+    if (g < 2 * R) return g % 2 == 0 ? uint32_t(2 * (R - 1)) : uint32_t((R - 1) * (R - 1));
+    return g == 2 * R ? uint32_t(R * (R + 1) / 2) : 1u;
 }
 
 __device__ __forceinline__ uint64_t ld_acquire64(const uint64_t* p) {
@@ -108,7 +109,7 @@ __device__ __forceinline__ uint64_t ld_acquire64(const uint64_t* p) {
     return v;
 }
 
-__host__ __device__ inline bool is_remainder_phase(int R, int f) { return R > 1 && f >= 2 && f - 2 < 3 * R && (f - 2) % 3 == 2; }
+__host__ __device__ inline bool is_remainder_phase(int R, int f) { return R > 1 && f >= 3 && f - 3 < 2 * R && (f - 3) % 2 == 1; }
 
 // Claims the next task of slot s (generation gen); returns the phase, the first index and how
 // many consecutive tasks were taken (two remainder tiles at a time while two are left: the
@@ -586,42 +587,48 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         } else if (R == 1) {
             run_small<16>(E, smem, rowbuf, colbuf, s_wins, Q.flags + 1);  // overflow -> this request
             last = true;
+        } else if (f == 2) {
+            run_pivot<16>(E, 0, rowbuf, colbuf);
         } else {
-            const int g = f - 2;
-            if (g < 3 * R) {
-                const int k = g / 3, kind = g % 3;
-                if (kind == 0) {
-                    run_pivot<16>(E, k, rowbuf, colbuf);
-                } else {
-                    // Panels (row panels first, then column panels) or remainder tiles, one per
-                    // task; a remainder claim may hold two consecutive tiles.
-                    const int R1 = R - 1;
-                    const uint32_t cnt = s_cnt;
-                    for (uint32_t x = 0; x < cnt; ++x) {
-                        // The previous tile's shared operands are read before the next TMA;
-                        // the reduction keeps every thread's view of ok the same.
-                        if (x > 0 && !__syncthreads_and(ok)) {
-                            ok = false;
-                            break;
-                        }
-                        const int tt = int(t + x);
-                        int tk, ii, jj;
-                        if (kind == 1) {
-                            const bool row = tt < R1;
-                            const int y = row ? tt : tt - R1;
-                            tk = row ? kTileRow : kTileCol;
-                            ii = jj = y + (y >= k);
-                        } else {
-                            tk = kTileRem;
-                            ii = tt / R1;
-                            jj = tt % R1;
-                            ii += ii >= k;
-                            jj += jj >= k;
-                        }
-                        ok = run_tile<16>(E, G, tk, k, ii, jj, smem, bars, par_a, par_b);
+            const int g = f - 3;
+            if (g < 2 * R) {
+                const int k = g / 2, kind = 1 + g % 2;  // 1 panels, 2 remainder
+                // Panels (row panels first, then column panels) or remainder tiles, one per
+                // task; a remainder claim may hold two consecutive tiles. Remainder task 0 is
+                // tile (k+1, k+1) (its index swapped with that tile's), closed afterwards as the
+                // next round's pivot.
+                const int R1 = R - 1;
+                const int p_next = k * R1 + k;  // reduced coordinates of tile (k+1, k+1)
+                const uint32_t cnt = s_cnt;
+                for (uint32_t x = 0; x < cnt; ++x) {
+                    // The previous tile's shared operands are read before the next TMA;
+                    // the reduction keeps every thread's view of ok the same.
+                    if (x > 0 && !__syncthreads_and(ok)) {
+                        ok = false;
+                        break;
+                    }
+                    int tt = int(t + x);
+                    const bool pivot_next = kind == 2 && k + 1 < R && tt == 0;
+                    int tk, ii, jj;
+                    if (kind == 1) {
+                        const bool row = tt < R1;
+                        const int y = row ? tt : tt - R1;
+                        tk = row ? kTileRow : kTileCol;
+                        ii = jj = y + (y >= k);
+                    } else {
+                        if (k + 1 < R) tt = tt == 0 ? p_next : (tt == p_next ? 0 : tt);
+                        tk = kTileRem;
+                        ii = tt / R1;
+                        jj = tt % R1;
+                        ii += ii >= k;
+                        jj += jj >= k;
+                    }
+                    ok = run_tile<16>(E, G, tk, k, ii, jj, smem, bars, par_a, par_b);
+                    if (pivot_next && __syncthreads_and(ok)) {  // the tile's stores are visible
+                        run_pivot<16>(E, k + 1, rowbuf, colbuf);
                     }
                 }
-            } else if (g == 3 * R) {
+            } else if (g == 2 * R) {
                 int rem = int(t), I = 0;
                 while (rem >= R - I) {
                     rem -= R - I;
@@ -636,7 +643,8 @@ __global__ void __launch_bounds__(cfg<16>::THREADS, 1)
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
-            const int kind = f == 0 ? 0 : f == 1 ? 1 : R == 1 ? 2 : (f - 2 < 3 * R ? 3 + (f - 2) % 3 : (f - 2 == 3 * R ? 6 : 7));
+            const int kind = f == 0 ? 0 : f == 1 ? 1 : R == 1 ? 2 : f == 2 ? 3
+                           : (f - 3 < 2 * R ? 4 + (f - 3) % 2 : (f - 3 == 2 * R ? 6 : 7));
             const uint32_t cnt = s_cnt;
             atomicAdd(&hdr->busy_ns[kind], (unsigned long long)(global_ns() - t_task));
             atomicAdd(&hdr->tasks[kind], (unsigned long long)cnt);
