@@ -66,7 +66,7 @@ struct alignas(64) Req {
     CUtensorMap mapPl;           // bit planes u32 [ceil(V / 32) * B][Cq], box {64, B}
     const int32_t* ids;          // ballots: ids, most preferred first
     const int64_t* offsets;      // V + 1 CSR offsets, or null when every ballot has exactly C ids
-    float* pos;                  // [V][Cq]
+    float* pos;                  // [V][Cq] places: f32, or u16 when the POS rows fit shared memory (POS)
     uint32_t* planes;            // word [ch * B + k][c]: bit k of the places of 32 ballots' candidate c
     int32_t B;                   // bit planes per 32-ballot chunk
     uint64_t* done_host;         // host-mapped completion word of this slot
@@ -303,10 +303,15 @@ __device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v
         const int64_t len = Q.offsets ? __ldcg(Q.offsets + v + 1) - beg : C;
         int code;
         if (rows) {
+            // 16-bit places, copied out 8 at a time (Cq is a multiple of 128, so rows and
+            // destinations are 16-byte aligned).
             code = warp_places_u16<int32_t, true>(Q.ids + beg, len, C, Cq, row);
             __syncwarp();
-            if (code == kPosOk)
-                for (int c = lane; c < Cq; c += 32) Q.pos[v * Cq + c] = float(row[c]);
+            if (code == kPosOk) {
+                uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<uint16_t*>(Q.pos) + v * Cq);
+                const uint4* src = reinterpret_cast<const uint4*>(row);
+                for (int c = lane; c < Cq / 8; c += 32) dst[c] = src[c];
+            }
             __syncwarp();  // the row is read before the next ballot rewrites it
         } else {
             code = warp_positions<int32_t, true>(Q.ids + beg, len, C, Cq, Q.pos + v * Cq);
@@ -314,18 +319,27 @@ __device__ void run_positions(const Req& Q, int C, int Cq, int64_t v0, int64_t v
         if (code != kPosOk && lane == 0) atomicCAS(&Q.flags[0], 0u, uint32_t(code));
     }
     // Pack the task's 32-ballot chunks into bit planes (ballots past V count as place 0). The
-    // places were written by this CTA's warps; read them back through L2.
+    // places were written by this CTA's warps (u16 or f32, as above); read them back through L2.
     // Each thread turns one candidate's 32 places into the request's B plane words, one bit
     // extract and one bit insert per voter and plane (a loop over B, not over all 20 planes).
     __syncthreads();
     const int B = Q.B;
+    const uint16_t* pos16 = reinterpret_cast<const uint16_t*>(Q.pos);
     for (int64_t ch = v0 / 32; ch * 32 < v1; ++ch)
         for (int64_t c = threadIdx.x; c < Cq; c += blockDim.x) {
             uint32_t p[32];
+            if (rows) {  // CTA-uniform
 #pragma unroll
-            for (int v = 0; v < 32; ++v) {
-                const int64_t voter = ch * 32 + v;
-                p[v] = voter < Q.V ? uint32_t(__ldcg(Q.pos + voter * Cq + c)) : 0u;
+                for (int v = 0; v < 32; ++v) {
+                    const int64_t voter = ch * 32 + v;
+                    p[v] = voter < Q.V ? uint32_t(__ldcg(pos16 + voter * Cq + c)) : 0u;
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < 32; ++v) {
+                    const int64_t voter = ch * 32 + v;
+                    p[v] = voter < Q.V ? uint32_t(__ldcg(Q.pos + voter * Cq + c)) : 0u;
+                }
             }
 #pragma unroll 1
             for (int k = 0; k < B; ++k) {
