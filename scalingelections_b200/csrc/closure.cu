@@ -36,6 +36,7 @@
 #include <atomic>
 #include <mutex>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "batch_core.cuh"
@@ -66,6 +67,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
         fence_barrier_init();
     }
     __syncthreads();
+    pdl_trigger();  // the next launch may start filling SMs this grid has left
+    pdl_wait();     // the previous launch's tiles are complete and visible
     const int R1 = E.R - 1;
     const int P = SPLIT ? parts : 1;
     const int b = blockIdx.x / P;
@@ -107,6 +110,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
         fence_barrier_init();
     }
     __syncthreads();
+    pdl_trigger();  // the next launch may start filling SMs this grid has left
+    pdl_wait();     // the previous launch's tiles are complete and visible
     const int R1 = E.R - 1, R2 = E.R - 2;
     int t = blockIdx.x, I, J;
     const bool split = SPLIT && subset == 0 && fuse_pivot && parts > 1;
@@ -184,6 +189,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), NQ == 4 ? 2 : 1)
         s_ticket = atomicAdd(&state[0], 1u);
     }
     __syncthreads();
+    pdl_trigger();  // the next round's launch may start filling SMs this grid has left
+    pdl_wait();     // the previous launch's tiles are complete and visible
     const uint32_t t = s_ticket;
     const int R = E.R, R1 = R - 1, R2 = R - 2;
     const uint32_t P = SPLIT ? uint32_t(parts) : 1u;
@@ -753,29 +760,56 @@ template <int LB> se_status_t set_smem_limits() {
 }
 
 // Launches of the tile kernels. The split-K form (parts > 1) is a separate instantiation, so the
-// whole-tile kernels that large closures run carry no split logic.
+// whole-tile kernels that large closures run carry no split logic. Every launch is a
+// programmatic dependent launch (pdl_trigger / pdl_wait): a round's grid may occupy the SM slots
+// that the previous grid's last, partial wave leaves free and start its first tiles the moment
+// that grid completes, without the launch gap.
+template <typename... Params, typename... Args>
+void launch_pdl(bool pdl, void (*kernel)(Params...), unsigned blocks, int threads, size_t smem, cudaStream_t s,
+                Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(unsigned(threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int LB, int NQ>
 void launch_panels(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, int K, int parts,
-                   uint32_t* ctr, uint32_t* scr, uint32_t* err) {
+                   uint32_t* ctr, uint32_t* scr, uint32_t* err, bool pdl = true) {
     constexpr int T = tile_threads<LB, NQ>();
-    if (parts > 1) panels_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, K, parts, ctr, scr, err);
-    else panels_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, K, 1, nullptr, nullptr, err);
+    if (parts > 1) launch_pdl(pdl, panels_kernel<LB, NQ, true>, blocks, T, smem, s, E, K, parts, ctr, scr, err);
+    else
+        launch_pdl(pdl, panels_kernel<LB, NQ, false>, blocks, T, smem, s, E, K, 1, (uint32_t*)nullptr,
+                   (uint32_t*)nullptr, err);
 }
 
 template <int LB, int NQ>
 void launch_rem(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, int K, int fuse, int subset,
-                int parts, uint32_t* ctr, uint32_t* scr, uint32_t* err) {
+                int parts, uint32_t* ctr, uint32_t* scr, uint32_t* err, bool pdl = true) {
     constexpr int T = tile_threads<LB, NQ>();
-    if (parts > 1) rem_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, K, fuse, subset, parts, ctr, scr, err);
-    else rem_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, K, fuse, subset, 1, nullptr, nullptr, err);
+    if (parts > 1)
+        launch_pdl(pdl, rem_kernel<LB, NQ, true>, blocks, T, smem, s, E, K, fuse, subset, parts, ctr, scr, err);
+    else
+        launch_pdl(pdl, rem_kernel<LB, NQ, false>, blocks, T, smem, s, E, K, fuse, subset, 1, (uint32_t*)nullptr,
+                   (uint32_t*)nullptr, err);
 }
 
 template <int LB, int NQ>
 void launch_round(unsigned blocks, size_t smem, cudaStream_t s, const batch::Elec& E, const batch::Elec& En, int K,
                   uint32_t* state, int parts, uint32_t* ctr, uint32_t* scr, uint32_t* err) {
     constexpr int T = tile_threads<LB, NQ>();
-    if (parts > 1) round_kernel<LB, NQ, true><<<blocks, T, smem, s>>>(E, En, K, state, parts, ctr, scr, err);
-    else round_kernel<LB, NQ, false><<<blocks, T, smem, s>>>(E, En, K, state, 1, nullptr, nullptr, err);
+    if (parts > 1)
+        launch_pdl(true, round_kernel<LB, NQ, true>, blocks, T, smem, s, E, En, K, state, parts, ctr, scr, err);
+    else
+        launch_pdl(true, round_kernel<LB, NQ, false>, blocks, T, smem, s, E, En, K, state, 1, (uint32_t*)nullptr,
+                   (uint32_t*)nullptr, err);
 }
 
 // Rounds of the blocked closure on an initialised working matrix, in schedule `mode` (1, 3 or
@@ -836,8 +870,9 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     cudaEvent_t* remb = ev.data() + R;
     if (phase_ms) SE_CUDA_TRY(cudaEventRecord(ev[2 * R], A));
     auto panels = [&](int K) {
-        if constexpr (wide) launch_panels<LB, 4>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err);
-        else launch_panels<LB, 8>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err);
+        if constexpr (wide)
+            launch_panels<LB, 4>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err, false);
+        else launch_panels<LB, 8>(unsigned(2 * (R - 1)), smem, A, E[K & 1], K, 1, nullptr, nullptr, err, false);
     };
     if constexpr (wide) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, A>>>(S, ldw, 0, dT);
     else diag_kernel<LB><<<1, CF::THREADS, 0, A>>>(S, ldw, 0, dT);
@@ -847,16 +882,17 @@ se_status_t run_two_streams(const batch::Elec (&E)[2], int R, cudaStream_t A, ui
     const int R2 = R - 2;
     for (int K = 0; K + 1 < R; ++K) {
         SE_CUDA_TRY(cudaStreamWaitEvent(B, pan[K], 0));
-        launch_rem<LB, 8>(unsigned(R2 * R2), smem, B, E[K & 1], K, 0, 2, 1, nullptr, nullptr, err);
+        launch_rem<LB, 8>(unsigned(R2 * R2), smem, B, E[K & 1], K, 0, 2, 1, nullptr, nullptr, err, false);
         SE_CUDA_TRY(cudaEventRecord(remb[K], B));
         if (K > 0) SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[K - 1], 0));
-        launch_rem<LB, 8>(unsigned(2 * R - 3), smem, A, E[K & 1], K, 1, 1, 1, nullptr, nullptr, err);
+        launch_rem<LB, 8>(unsigned(2 * R - 3), smem, A, E[K & 1], K, 1, 1, 1, nullptr, nullptr, err, false);
         panels(K + 1);
         SE_CHECK_LAUNCH();
         SE_CUDA_TRY(cudaEventRecord(pan[K + 1], A));
     }
     SE_CUDA_TRY(cudaStreamWaitEvent(A, remb[R - 2], 0));
-    launch_rem<LB, 8>(unsigned((R - 1) * (R - 1)), smem, A, E[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr, err);
+    launch_rem<LB, 8>(unsigned((R - 1) * (R - 1)), smem, A, E[(R - 1) & 1], R - 1, 0, 0, 1, nullptr, nullptr, err,
+                      false);
     SE_CHECK_LAUNCH();
     if (phase_ms) {
         SE_CUDA_TRY(cudaEventRecord(ev[2 * R + 1], A));
