@@ -515,6 +515,8 @@ __global__ void __launch_bounds__(tile_threads<LB, NQ>(), 1)
     const geomT<NQ> g(threadIdx.x);
     uint32_t c[8][NQ];
     uint32_t* D = S + int64_t(K) * kT * ldw + int64_t(K) * CF::TW;
+    pdl_trigger();
+    pdl_wait();  // the tile's previous update is complete and visible
     load_tile_regs<LB, false, NQ>(c, D, ldw, g);
     close_tile_in_registers<LB, NQ>(c, g, kT, rowbuf, colbuf);
     store_tile_regs<LB, NQ>(c, D, ldw, g);
@@ -609,6 +611,7 @@ template <int LB>
 __global__ void __launch_bounds__(256)
     finalize_kernel(const void* __restrict__ Sv, int Cp, int C, uint32_t* __restrict__ out, int64_t ld_out,
                     uint32_t base) {
+    pdl_wait();  // the closure's last launch is complete and visible
     for (int i = blockIdx.y; i < C; i += gridDim.y)
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < C; j += gridDim.x * blockDim.x) {
             uint32_t v;
@@ -765,10 +768,10 @@ template <int LB> se_status_t set_smem_limits() {
 // that the previous grid's last, partial wave leaves free and start its first tiles the moment
 // that grid completes, without the launch gap.
 template <typename... Params, typename... Args>
-void launch_pdl(bool pdl, void (*kernel)(Params...), unsigned blocks, int threads, size_t smem, cudaStream_t s,
+void launch_pdl(bool pdl, void (*kernel)(Params...), dim3 grid, int threads, size_t smem, cudaStream_t s,
                 Args&&... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
+    cfg.gridDim = grid;
     cfg.blockDim = dim3(unsigned(threads));
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -977,9 +980,9 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
         };
         if (se_status_t st = mark()) return st;
         if (wide8) {
-            if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, 0, dT);
+            if constexpr (LB == 16) launch_pdl(true, diag_kernel<LB, 4>, 1u, tile_threads<LB, 4>(), 0, stream, S, ldw, 0, dT);
         } else {
-            diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, 0, dT);
+            launch_pdl(true, diag_kernel<LB>, 1u, CF::THREADS, 0, stream, S, ldw, 0, dT);
         }
         if (se_status_t st = mark()) return st;
         const unsigned panel_blocks = unsigned(2 * (R - 1) * parts);
@@ -1049,9 +1052,9 @@ se_status_t run_rounds(uint8_t* work, const layout& P, cudaStream_t stream, doub
     }
     auto pivot = [&](int K) {
         if (wide) {
-            if constexpr (LB == 16) diag_kernel<LB, 4><<<1, tile_threads<LB, 4>(), 0, stream>>>(S, ldw, K, dT);
+            if constexpr (LB == 16) launch_pdl(true, diag_kernel<LB, 4>, 1u, tile_threads<LB, 4>(), 0, stream, S, ldw, K, dT);
         } else {
-            diag_kernel<LB><<<1, CF::THREADS, 0, stream>>>(S, ldw, K, dT);
+            launch_pdl(true, diag_kernel<LB>, 1u, CF::THREADS, 0, stream, S, ldw, K, dT);
         }
         mark(0);
     };
@@ -1172,7 +1175,8 @@ se_status_t launch_finalize(const layout& P, uint8_t* work, int C, uint32_t* out
                             cudaStream_t s) {
     const int gx = int((C + 255) / 256);
     const int gy = C < 65535 ? C : 65535;
-    finalize_kernel<LB><<<dim3(gx, gy), 256, 0, s>>>(work + P.s_off, int(P.Cp), C, out, ld_out, base);
+    launch_pdl(true, finalize_kernel<LB>, dim3(unsigned(gx), unsigned(gy)), 256, 0, s,
+               static_cast<const void*>(work + P.s_off), int(P.Cp), C, out, ld_out, base);
     SE_CHECK_LAUNCH();
     return SE_OK;
 }
