@@ -153,7 +153,7 @@ SE_API se_status_t se_closure_set_mode(int mode);
 
 /* The variant table of the automatic schedule: for C <= max_c[i] (the first i that holds) use
  * modes[i] (1 or 3 to 8); C above every entry uses 1. n <= 8; n = 0 clears it. The built-in
- * table, measured on B200, is {C <= 2048: 7, C <= 4096: 8, larger: 6}. An autotuner
+ * table, measured on B200, is {C <= 1024: 7, C <= 4096: 8, larger: 6}. An autotuner
  * measures the variants per size bucket and installs the winners (scalingelections_b200
  * autotune.tune_closure). No reference counterpart: the reference's tile_size argument picks
  * among its kernels' tile templates (scaling_elections.cu:895-901). */

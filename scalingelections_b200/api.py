@@ -155,7 +155,7 @@ def set_closure_mode(mode: int) -> None:
     _closure_mode = int(mode)
 
 
-BUILTIN_CLOSURE_VARIANTS = ((2048, 7), (4096, 8), (1 << 20, 6))
+BUILTIN_CLOSURE_VARIANTS = ((1024, 7), (4096, 8), (1 << 20, 6))
 
 
 def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_bytes: int | None = None) -> int:
@@ -171,7 +171,7 @@ def closure_schedule(num_candidates: int, lanes: int = LANES_U16, workspace_byte
 def set_closure_variants(table: Sequence[tuple[int, int]]) -> None:
     """The automatic schedule's table: (max_C, mode) pairs, first match wins, modes 1 or 3-8;
     sizes above every entry run mode 1. An empty table clears it (every size then runs mode 1;
-    the library starts with the table measured on B200, {2048: 7, 4096: 8, 2**20: 6}).
+    the library starts with the table measured on B200, {1024: 7, 4096: 8, 2**20: 6}).
     autotune.tune_closure measures the modes per size bucket and installs its winners through
     this."""
     n = len(table)

@@ -730,7 +730,7 @@ std::atomic<int> g_closure_mode{0};
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
 int g_variant_n = 3;
-int g_variant_max_c[kMaxVariants] = {2048, 4096, 1 << 20};
+int g_variant_max_c[kMaxVariants] = {1024, 4096, 1 << 20};
 int g_variant_mode[kMaxVariants] = {7, 8, 6};
 
 int automatic_mode(int C) {

@@ -85,7 +85,8 @@ def test_closure_schedule_query_needs_no_gpu():
     plain = lambda C: api.closure_workspace_bytes(C, LANES_U16)  # noqa: E731
     assert api.closure_schedule(1000, LANES_U16, flow(1000)) == 7
     flow32 = lambda C: api.closure_workspace_bytes(C, LANES_U32, dataflow=True)  # noqa: E731
-    assert api.closure_schedule(2048, LANES_U32, flow32(2048)) == 1  # no wide micro-tile in 32-bit lanes
+    assert api.closure_schedule(1000, LANES_U32, flow32(1000)) == 1  # no wide micro-tile in 32-bit lanes
+    assert api.closure_schedule(2048, LANES_U32, flow32(2048)) == 6  # mode 8 on the default micro-tile
     assert api.closure_schedule(3000, LANES_U16, flow(3000)) == 8
     assert api.closure_schedule(4096, LANES_U16, flow(4096)) == 8
     assert api.closure_schedule(4096, LANES_U32, flow32(4096)) == 6
