@@ -212,6 +212,40 @@ def strongest_paths_device(preferences: torch.Tensor, *, lanes: int = LANES_AUTO
     return out
 
 
+def strongest_paths_enqueue(preferences: torch.Tensor, *, lanes: int, value_offset: int = 0,
+                            out: torch.Tensor | None = None, workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """The closure of strongest_paths_device queued on the current stream without waiting
+    (se_closure_enqueue): returns ``out`` as soon as the work is queued. lanes is LANES_U16 or
+    LANES_U32 (LANES_AUTO would read the matrix back). The call's error word stays in
+    ``workspace``, which must not serve another closure before closure_check(workspace) has
+    read it; pass one (of closure_workspace_bytes(C, lanes, dataflow=True) bytes for every
+    schedule at its fastest) to check it later."""
+    if lanes not in (LANES_U16, LANES_U32):
+        raise ValueError("lanes must be LANES_U16 or LANES_U32")
+    C, ld = _check_matrix(preferences, "preferences")
+    if out is None:
+        out = torch.empty((C, C), dtype=torch.uint32, device=preferences.device)
+    Co, ldo = _check_matrix(out, "out")
+    if Co != C:
+        raise ValueError("out has the wrong shape")
+    if C == 0:
+        return out
+    if workspace is None:
+        raise ValueError("pass the workspace: closure_check reads the call's error word from it")
+    have = workspace.numel() * workspace.element_size()
+    with torch.cuda.device(preferences.device):
+        check(_lib.lib().se_closure_enqueue(preferences.data_ptr(), ld, C, out.data_ptr(), ldo, int(lanes),
+                                            int(value_offset), workspace.data_ptr(), have, _stream()))
+    return out
+
+
+def closure_check(workspace: torch.Tensor) -> None:
+    """Waits for the current stream and raises if the closure queued with this workspace
+    reported a device error or a value outside its 16-bit window (se_closure_check)."""
+    with torch.cuda.device(workspace.device):
+        check(_lib.lib().se_closure_check(workspace.data_ptr(), _stream()))
+
+
 def tally_workspace_bytes(num_voters: int, num_candidates: int) -> int:
     n = _lib.lib().se_tally_workspace_bytes(int(num_voters), int(num_candidates))
     if n < 0:

@@ -86,3 +86,33 @@ def test_closure_stream_raises_on_overflow_in_order():
     assert first.shape == (C, C)
     with pytest.raises(api.SchulzeError):
         next(it)
+
+
+def test_python_enqueue_and_check_equal_the_synchronous_call(orc):
+    """api.strongest_paths_enqueue queues closures back to back without waiting, each with its
+    own workspace; api.closure_check then reads each call's error word. The results equal
+    strongest_paths_device's and the oracle's; a 16-bit overflow surfaces at the check."""
+    import numpy as np
+    import torch
+
+    from scalingelections_b200 import LANES_U16, LANES_U32, api
+
+    rng = np.random.default_rng(31)
+    mats = [rng.integers(0, 3000, size=(C, C), dtype=np.uint64).astype(np.uint32) for C in (130, 700, 1000)]
+    outs, works = [], []
+    for P in mats:
+        d = api._to_device_u32(P, "cuda")
+        C = P.shape[0]
+        w = torch.empty(api.closure_workspace_bytes(C, LANES_U16, dataflow=True), dtype=torch.uint8, device="cuda")
+        outs.append((P, api.strongest_paths_enqueue(d, lanes=LANES_U16, workspace=w), d))
+        works.append(w)
+    for w in works:
+        api.closure_check(w)
+    for P, o, d in outs:
+        assert np.array_equal(api._to_host_u32(o), orc.strongest_paths(P, "blocked", tile=16))
+        assert torch.equal(o.view(torch.int32), api.strongest_paths_device(d, lanes=LANES_U32).view(torch.int32))
+    big = api._to_device_u32(rng.integers(70000, 90000, size=(200, 200), dtype=np.uint64).astype(np.uint32), "cuda")
+    w = torch.empty(api.closure_workspace_bytes(200, LANES_U16, dataflow=True), dtype=torch.uint8, device="cuda")
+    api.strongest_paths_enqueue(big, lanes=LANES_U16, workspace=w)
+    with pytest.raises(api.SchulzeError, match="16-bit"):
+        api.closure_check(w)
