@@ -93,7 +93,9 @@ SE_API se_status_t se_closure(const uint32_t* d_pref, int64_t ld_pref, int C, ui
  * which must lie in [1, 65535]; 0 = no shift). Errors of the arguments return at once; errors
  * found on the device (a count outside the 16-bit window, a timed-out wait) are kept in the
  * first 8 bytes of d_work until se_closure_check reads them. d_work must not be reused by
- * another call before that check. */
+ * another call before that check. A call may be captured into a CUDA graph once a first call
+ * of the same lane width has run outside any capture (it sets the kernels' shared-memory
+ * limits); each replay closes the captured matrices again. */
 SE_API se_status_t se_closure_enqueue(const uint32_t* d_pref, int64_t ld_pref, int C,
                                       uint32_t* d_out, int64_t ld_out, int lane_bits,
                                       uint32_t value_offset, void* d_work, int64_t work_bytes,

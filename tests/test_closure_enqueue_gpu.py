@@ -116,3 +116,30 @@ def test_python_enqueue_and_check_equal_the_synchronous_call(orc):
     api.strongest_paths_enqueue(big, lanes=LANES_U16, workspace=w)
     with pytest.raises(api.SchulzeError, match="16-bit"):
         api.closure_check(w)
+
+
+@pytest.mark.parametrize("C", [700, 3000, 5000])
+def test_enqueued_closure_captures_into_a_cuda_graph(C):
+    """The stream-ordered closure captured into a CUDA graph (after a first call outside the
+    capture) replays to the synchronous call's result: schedules 7, 8 and 6 at these sizes,
+    with their split tiles and programmatic dependent launches."""
+    rng = np.random.default_rng(C)
+    P = rng.integers(0, 3000, size=(C, C), dtype=np.uint64).astype(np.uint32)
+    d = api._to_device_u32(P, "cuda")
+    ref = api.strongest_paths_device(d, lanes=LANES_U16)
+    out = torch.empty_like(d)
+    w = torch.empty(api.closure_workspace_bytes(C, LANES_U16, dataflow=True), dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        api.strongest_paths_enqueue(d, lanes=LANES_U16, out=out, workspace=w)
+        api.closure_check(w)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        api.strongest_paths_enqueue(d, lanes=LANES_U16, out=out, workspace=w)
+    out.zero_()
+    for _ in range(2):
+        g.replay()
+    torch.cuda.synchronize()
+    api.closure_check(w)
+    assert torch.equal(out.view(torch.int32), ref.view(torch.int32))
