@@ -722,11 +722,11 @@ layout plan(int C, int lane_bits) {
 std::atomic<int> g_closure_mode{0};
 
 // The variant table of mode 0: modes[i] for C <= max_c[i] (the first entry that holds). The
-// built-in table is autotune.tune_closure's result on one B200 (16-bit lanes, ms per closure,
-// three repeats agreeing within 1 % unless noted; modes 3 / 6 / 7 / 8): C = 2048 1.445 /
-// 1.713 / 1.320 / 1.517, C = 2560 1.82 / 2.05 / 1.66 / 1.68, C = 3584 2.74 / 2.97 / 2.74 /
-// 2.78, C = 4096 3.95 / 3.55 / 3.97 / 3.49, C = 4608 5.39 / 4.90 / 5.46 / 4.96, C = 6144
-// 11.07 / 11.01 / 11.35 / 11.37, C = 16384 192.2 / 190.8 / 198.0 / 199.9.
+// built-in table is autotune.tune_closure's result on one B200 with programmatic launches
+// (16-bit lanes, ms per closure, 5 closures each; modes 3 / 6 / 7 / 8): C = 1024 0.441 / 0.473
+// / 0.432 / 0.443, C = 2048 0.962 / 0.976 / 0.974 / 0.947, C = 3072 1.855 / 1.759 / 1.865 /
+// 1.750, C = 4096 3.783 / 3.398 / 4.200 / 3.397, C = 5120 6.870 / 6.392 / 7.611 / 6.452, C =
+// 6144 10.85 / 10.84 / 11.45 / 11.08. The table is within 2.2 % of the fastest mode at each.
 constexpr int kMaxVariants = 8;
 std::mutex g_variant_mutex;
 int g_variant_n = 3;
