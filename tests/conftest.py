@@ -46,6 +46,36 @@ def ballots_of(case):
     return [ids[offs[v]:offs[v + 1]] for v in range(len(offs) - 1)]
 
 
+def chain_matrix(C, seed, order="shuffled", low=1000, high=61000, noise=100, base=0):
+    """A preference matrix whose strongest paths run the length of the matrix.
+
+    Candidates perm[0] -> perm[1] -> ... -> perm[C-1] defeat each other by chain weights w drawn
+    from [low, high); the reverse counts are zero, and every other pair counts below `noise`.
+    Every off-diagonal count is then raised by `base` (a shifted window of values). A path with a
+    noise edge is weaker than any chain edge, so the strongest path from perm[s] to perm[t]
+    (s < t) is the chain's segment: base + min(w[s:t]). `order` is "shuffled", "ascending"
+    (the chain follows the indices, so it crosses pivots in loop order) or "descending"
+    (against it). Returns (P, perm, w)."""
+    rng = np.random.default_rng(seed)
+    perm = {"shuffled": rng.permutation(C), "ascending": np.arange(C), "descending": np.arange(C)[::-1]}[order]
+    P = rng.integers(0, noise, size=(C, C), dtype=np.uint64)
+    w = rng.integers(low, high, size=max(C - 1, 0), dtype=np.uint64)
+    P[perm[:-1], perm[1:]] = w
+    P[perm[1:], perm[:-1]] = 0
+    P += np.uint64(base)
+    np.fill_diagonal(P, 0)
+    return P.astype(np.uint32), perm, w
+
+
+def chain_forward_ok(S, perm, w, base=0):
+    """True if S holds the known strength of every forward pair of a chain_matrix."""
+    for s in range(len(perm) - 1):
+        want = np.minimum.accumulate(w[s:]) + np.uint64(base)
+        if not np.array_equal(S[perm[s], perm[s + 1:]].astype(np.uint64), want):
+            return False
+    return True
+
+
 @pytest.fixture(scope="session")
 def orc():
     from oracle import oracle

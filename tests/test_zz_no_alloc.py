@@ -87,3 +87,17 @@ def test_noalloc_rejects_sizes_beyond_its_static_array():
                                        LANES_U16, torch.cuda.current_stream().cuda_stream)
     assert st == _lib.SE_ERR_INVALID
     assert "2048" in _lib.last_error()
+
+
+def test_noalloc_on_a_long_chain():
+    """Strongest paths of up to 2047 hops (a chain of strong defeats against the pivot order)
+    through the static array, in every lane mode."""
+    from conftest import chain_forward_ok, chain_matrix
+
+    P, perm, w = chain_matrix(MAX_C, seed=7, order="descending")
+    d = api._to_device_u32(P, "cuda")
+    want = orc_closure(d)
+    assert chain_forward_ok(want, perm, w)
+    want_dev = api._to_device_u32(want, "cuda")
+    for lanes in (LANES_U16, LANES_U32, LANES_AUTO):
+        assert same(noalloc(d, lanes), want_dev), lanes
