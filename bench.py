@@ -38,6 +38,9 @@ sys.path.insert(0, str(ROOT))
 def metric_name(C: int) -> str:
     return f"Gcells/s (C^3/t), single-election widest-path closure, C={C}"
 UNIT = "Gcells/s"
+# se_rank places up to this many candidates from per-CTA histograms of the wins, larger C by
+# counting over strips (kHistMaxC in csrc/rank.cu).
+RANK_HIST_MAX_C = 49152
 
 
 def parse():
@@ -435,7 +438,8 @@ def run_ours(args, world, rank, local_rank):
     rank_s = r0.elapsed_time(r1) / 5e3
     hbm_peak, hbm_source = measured_hbm_gbs()
     rank_bytes = float(C) * C * 4
-    ranking = {"ms": rank_s * 1e3, "kernels": ["wins_kernel", "place_kernel"],
+    place = "place_hist_kernel" if C <= RANK_HIST_MAX_C else "place_kernel"
+    ranking = {"ms": rank_s * 1e3, "kernels": ["wins_kernel", place],
                "roofline": {"bound": "hbm", "achieved": rank_bytes / rank_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
                             "frac": rank_bytes / rank_s / 1e9 / hbm_peak, "algorithmic_bytes": rank_bytes,
                             "peak_source": hbm_source},

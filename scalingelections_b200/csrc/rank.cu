@@ -8,11 +8,17 @@
 // resident CTAs per SM each taking every gridDim.x-th pair: S[I][J] is read straight into
 // registers and S[J][I] through a swizzled shared-memory tile, every cell of S once, in 128-bit
 // loads, and the next pair's loads are issued before the current pair is counted. Both
-// endpoints' wins accumulate in registers; one global atomic per candidate per tile pair.
-// place_kernel gives candidate i the place #{j : wins[j] > wins[i]} +
-// #{j < i : wins[j] == wins[i]}, which is exactly the stable order, by counting over strips of
-// the wins in shared memory (four per 128-bit load, eight slices of each strip counted side
-// by side); a slice wholly before or after the block's candidates needs one compare per pair.
+// endpoints' wins accumulate in registers; one global atomic per candidate per tile pair. The
+// transposed tile and the column partials are double-buffered: two barriers per pair.
+//
+// Candidate i's place is #{j : wins[j] > wins[i]} + #{j < i : wins[j] == wins[i]}, which is
+// exactly the stable order. place_hist_kernel (C <= kHistMaxC) builds, per CTA, the histogram of
+// all wins in shared memory (wins lie in [0, C)), reads the counts above each candidate's value
+// from its suffix sums, and the ties before it from the histogram of the wins before the CTA's
+// first candidate plus a scan of its own candidates: O(C) per CTA. place_kernel (larger C)
+// counts over strips of the wins in shared memory (four per 128-bit load, eight slices of each
+// strip counted side by side); a slice wholly before or after the block's candidates needs one
+// compare per pair.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -63,10 +69,14 @@ __device__ __forceinline__ void load_pair(const uint32_t* __restrict__ S, int64_
 // Persistent over the tile pairs: block b takes pairs b, b + gridDim.x, ... and loads the next
 // pair's cells into registers as soon as the current pair's transposed tile is in shared
 // memory, so the loads are in flight while the current pair is compared and counted.
+//
+// Two barriers per pair. The transposed tile and the column partials are double-buffered:
+// pair n uses bs[n & 1] and colpart[n & 1], and pair n + 2 rewrites them only after pair n + 1's
+// first barrier, which every thread reaches after it has finished with pair n.
 __global__ void __launch_bounds__(256, kWinsCtasPerSm)
     wins_kernel(const uint32_t* __restrict__ S, int64_t ld, int C, int nt, int vec, int32_t* __restrict__ wins) {
-    __shared__ __align__(16) uint32_t bs[kRT * kRT];
-    __shared__ int32_t colpart[16][kRT];  // column wins per row group ry
+    __shared__ __align__(16) uint32_t tiles[2][kRT * kRT];
+    __shared__ int32_t partials[2][16][kRT];  // column wins per row group ry
     const int64_t pairs = int64_t(nt) * (nt + 1) / 2;
     const int cx = threadIdx.x & 15, ry = threadIdx.x >> 4;
     // Row r = ry + 16p: the swizzle s = 2 * ((r >> 2) & 15) moves the thread's 4-group by s & ~3
@@ -79,9 +89,11 @@ __global__ void __launch_bounds__(256, kWinsCtasPerSm)
         upper_pair(pb, nt, I, J);
         load_pair(S, ld, C, vec, I * kRT, J * kRT, ry, cx, a, b);
     }
-    for (; pb < pairs; pb += gridDim.x) {
+    for (int buf = 0; pb < pairs; pb += gridDim.x, buf ^= 1) {
         const int i0 = I * kRT, j0 = J * kRT;
         const bool diag = I == J;
+        uint32_t* bs = tiles[buf];
+        int32_t(*colpart)[kRT] = partials[buf];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
             const int r = ry + 16 * p;
@@ -124,14 +136,13 @@ __global__ void __launch_bounds__(256, kWinsCtasPerSm)
 #pragma unroll
             for (int q = 0; q < 4; ++q) colpart[ry][4 * cx + q] = int(cw[q]);
         }
-        __syncthreads();  // bs and colpart are complete and no longer read below
+        __syncthreads();  // colpart is complete
         if (!diag && threadIdx.x < kRT) {
             int n = 0;
 #pragma unroll
             for (int g = 0; g < 16; ++g) n += colpart[g][threadIdx.x];
             if (n) atomicAdd(&wins[j0 + threadIdx.x], n);
         }
-        __syncthreads();  // colpart is read before the next pair rewrites it
     }
 }
 
@@ -192,6 +203,100 @@ __global__ void __launch_bounds__(kPlaceThreads)
     }
 }
 
+// place_hist_kernel: kHistCand candidates per CTA, the histogram of all C wins in dynamic shared
+// memory (C ints). Wins lie in [0, C); a value outside is skipped, which cannot happen for the
+// wins that wins_kernel counts.
+constexpr int kHistThreads = 512;
+constexpr int kHistCand = 128;
+constexpr int kHistMaxC = 49152;  // 192 KB of counts
+
+__global__ void __launch_bounds__(kHistThreads)
+    place_hist_kernel(const int32_t* __restrict__ wins, int C, int32_t* __restrict__ ranking) {
+    extern __shared__ int32_t h[];                 // h[v] = #{j : wins[j] == v}, v < C
+    __shared__ __align__(16) int32_t own[kHistCand];  // the CTA's candidates' wins
+    __shared__ int32_t suffix[kHistThreads + 1];   // suffix[t] = counts of bins [t * L, C)
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * kHistCand;
+    const int nb = min(kHistCand, C - i0);
+    for (int v = tid; v < C; v += kHistThreads) h[v] = 0;
+    if (tid < kHistCand) own[tid] = tid < nb ? wins[i0 + tid] : -1;
+    // Adds wins[jb .. je) to the histogram; jb is 0 or i0, a multiple of 4, so 16-byte aligned
+    // wins are read four at a time.
+    const bool vec = (reinterpret_cast<uintptr_t>(wins) & 15) == 0;
+    auto add = [&](int v) {
+        if (unsigned(v) < unsigned(C)) atomicAdd(&h[v], 1);
+    };
+    auto add_range = [&](int jb, int je) {
+        int j = jb;
+        if (vec) {
+            const int4* w4 = reinterpret_cast<const int4*>(wins + jb);
+            const int n4 = (je - jb) >> 2;
+#pragma unroll 2
+            for (int q = tid; q < n4; q += kHistThreads) {
+                const int4 v = w4[q];
+                add(v.x), add(v.y), add(v.z), add(v.w);
+            }
+            j += 4 * n4;
+        }
+#pragma unroll 4
+        for (j += tid; j < je; j += kHistThreads) add(wins[j]);
+    };
+    __syncthreads();
+    add_range(0, i0);  // the wins before the CTA's first candidate
+    __syncthreads();
+    const int wi = tid < nb ? own[tid] : -1;
+    const bool mine = unsigned(wi) < unsigned(C);
+    int place = mine ? h[wi] : 0;  // ties before the CTA
+    if (tid < kHistCand) {  // ties among the CTA's own candidates before this one (own[j] = -1 past nb)
+        const int4* o4 = reinterpret_cast<const int4*>(own);
+#pragma unroll 8
+        for (int q = 0; q < kHistCand / 4; ++q) {
+            const int4 v = o4[q];
+            const int j = 4 * q;
+            place += (v.x == wi && j < tid) + (v.y == wi && j + 1 < tid) + (v.z == wi && j + 2 < tid) +
+                     (v.w == wi && j + 3 < tid);
+        }
+    }
+    __syncthreads();  // every count above is read before the rest of the wins are added
+    add_range(i0, C);
+    __syncthreads();
+    // Bins in chunks of L per thread; suffix[t] = sum of chunks t, t + 1, ... Thread t reads its
+    // chunk starting at offset t % L and wrapping, so that the lanes of a warp read 32
+    // consecutive bins at each step (distinct banks) instead of 32 bins L apart (one bank).
+    const int L = (C + kHistThreads - 1) / kHistThreads;
+    int sum = 0;
+    {
+        const int base = tid * L;
+        int o = tid % L;
+        for (int i = 0; i < L; ++i) {
+            if (base + o < C) sum += h[base + o];
+            if (++o == L) o = 0;
+        }
+    }
+    // Inclusive suffix scan of the chunk sums: within the warp (from the higher lanes), then
+    // over the warps' totals.
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_down_sync(0xFFFFFFFFu, sum, d);
+        if (lane + d < 32) sum += o;
+    }
+    __shared__ int32_t warp_total[kHistThreads / 32];
+    if (lane == 0) warp_total[warp] = sum;  // lane 0 holds its warp's total
+    __syncthreads();
+    int later = 0;  // totals of the warps after this one
+    for (int w = warp + 1; w < kHistThreads / 32; ++w) later += warp_total[w];
+    suffix[tid] = sum + later;
+    if (tid == 0) suffix[kHistThreads] = 0;
+    __syncthreads();
+    if (mine) {
+        const int c = wi / L;  // #{j : wins[j] > wi}: later chunks, then this chunk's bins above wi
+        place += suffix[c + 1];
+        for (int v = wi + 1, e = min(C, (c + 1) * L); v < e; ++v) place += h[v];
+        ranking[place] = i0 + tid;
+    }
+}
+
 }  // namespace rank
 }  // namespace se
 
@@ -215,8 +320,17 @@ extern "C" se_status_t se_rank(const uint32_t* d_S, int64_t ld, int C, int32_t* 
     const int64_t grid = std::min<int64_t>(pairs, int64_t(sms) * rank::kWinsCtasPerSm);
     rank::wins_kernel<<<unsigned(grid), 256, 0, s>>>(d_S, ld, C, nt, vec, d_wins);
     SE_CHECK_LAUNCH();
-    rank::place_kernel<<<(C + rank::kPlaceCand - 1) / rank::kPlaceCand, rank::kPlaceThreads, 0, s>>>(
-        d_wins, C, d_ranking);
+    if (C <= rank::kHistMaxC) {
+        const int bytes = int(sizeof(int32_t)) * rank::kHistMaxC;
+        if (se_status_t st = raise_smem_limit(reinterpret_cast<const void*>(rank::place_hist_kernel), bytes,
+                                              "the ranking's place kernel"))
+            return st;
+        rank::place_hist_kernel<<<(C + rank::kHistCand - 1) / rank::kHistCand, rank::kHistThreads,
+                                  sizeof(int32_t) * size_t(C), s>>>(d_wins, C, d_ranking);
+    } else {
+        rank::place_kernel<<<(C + rank::kPlaceCand - 1) / rank::kPlaceCand, rank::kPlaceThreads, 0, s>>>(
+            d_wins, C, d_ranking);
+    }
     SE_CHECK_LAUNCH();
     return SE_OK;
 }

@@ -5,7 +5,7 @@ import pytest
 import torch
 
 from conftest import ballots_of, golden_names, load_golden
-from scalingelections_b200 import api
+from scalingelections_b200 import _lib, api
 
 pytestmark = pytest.mark.gpu
 
@@ -42,6 +42,62 @@ def test_wins_and_places_across_tile_and_strip_edges(orc, C):
         w, r = api.rank_device(api._to_device_u32(S, "cuda"))
         assert np.array_equal(w.cpu().numpy(), wins_ref), (C, hi)
         assert np.array_equal(r.cpu().numpy(), rank_ref), (C, hi)
+
+
+def key_matrix(key):
+    """S[i][j] = 1 where key[i] > key[j], built on the GPU: wins[i] = #{j : key[j] < key[i]},
+    known without an O(C^2) count, so sizes of tens of thousands stay cheap to check."""
+    k = torch.from_numpy(key.astype(np.int64)).cuda()
+    return (k[:, None] > k[None, :]).to(torch.int32).view(torch.uint32)
+
+
+def key_wins_and_ranking(key):
+    wins = np.searchsorted(np.sort(key), key, side="left").astype(np.int32)
+    return wins, np.argsort(-wins, kind="stable").astype(np.int32)
+
+
+def test_key_matrix_closed_form(orc):
+    """The closed form above equals the oracle's count where the oracle is quick."""
+    rng = np.random.default_rng(3)
+    for C, distinct in ((1, 1), (7, 2), (300, 3), (300, 300), (1000, 40)):
+        key = rng.integers(0, distinct, size=C)
+        S = api._to_host_u32(key_matrix(key))
+        wins_ref, rank_ref = orc.wins_and_ranking(S)
+        wins, ranking = key_wins_and_ranking(key)
+        assert np.array_equal(wins, wins_ref) and np.array_equal(ranking, rank_ref)
+
+
+@pytest.mark.parametrize("C", [4095, 4096, 4097, 16384, 49152, 49153])
+def test_places_on_both_sides_of_the_histogram_limit(C):
+    """Up to 49152 candidates the places come from per-CTA histograms of the wins, above from
+    the strip count: both give the stable order, with every candidate tied, a few distinct wins,
+    many ties and none."""
+    rng = np.random.default_rng(C)
+    for distinct in (1, 3, C // 7 + 1, C):
+        key = rng.permutation(C) if distinct == C else rng.integers(0, distinct, size=C)
+        S = key_matrix(key)
+        w, r = api.rank_device(S)
+        del S
+        wins, ranking = key_wins_and_ranking(key)
+        assert np.array_equal(w.cpu().numpy(), wins), (C, distinct)
+        assert np.array_equal(r.cpu().numpy(), ranking), (C, distinct)
+    torch.cuda.empty_cache()
+
+
+def test_wins_buffer_off_a_16_byte_boundary(orc):
+    """A wins buffer 4 bytes past a 16-byte boundary: the place histogram reads the wins one at
+    a time instead of four; same wins and ranking."""
+    C = 3000
+    S = np.random.default_rng(11).integers(0, 4, size=(C, C)).astype(np.uint32)
+    wins_ref, rank_ref = orc.wins_and_ranking(S)
+    d = api._to_device_u32(S, "cuda")
+    buf = torch.zeros(C + 4, dtype=torch.int32, device="cuda")
+    ranking = torch.empty(C, dtype=torch.int32, device="cuda")
+    _lib.check(_lib.lib().se_rank(d.data_ptr(), C, C, buf.data_ptr() + 4, ranking.data_ptr(),
+                                  torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert np.array_equal(buf[1:C + 1].cpu().numpy(), wins_ref)
+    assert np.array_equal(ranking.cpu().numpy(), rank_ref)
 
 
 @pytest.mark.parametrize("C", [64, 200])
