@@ -76,6 +76,33 @@ def chain_forward_ok(S, perm, w, base=0):
     return True
 
 
+def cyclic_ballots(C, seed, max_count=5):
+    """Ballots whose strongest paths run around a cycle in single steps.
+
+    Ballot r ranks perm[r], perm[r + 1], ..., perm[C - 1], perm[0], ..., perm[r - 1] (the order
+    rotated by r), cast by n[r] voters (n in [1, max_count]); N = sum(n). Then perm[s] beats
+    perm[s + 1] (cyclically) by N - n[s + 1], every kept defeat is a forward jump around the
+    cycle, and a jump over the rotations (s, t] is never stronger than the single steps across
+    them. So the strongest path from perm[s] to perm[t] is the chain of single steps, with
+    strength N - max(n[u] for u in (s, t], cyclically). Needs C > 2 * max_count.
+    Returns (ballots int32 [N, C], perm, n)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(C)
+    n = rng.integers(1, max_count + 1, size=C)
+    ballots = np.concatenate([np.tile(np.roll(perm, -r), (int(n[r]), 1)) for r in range(C)])
+    return ballots.astype(np.int32), perm, n
+
+
+def cyclic_strongest_paths(perm, n):
+    """The closed-form strongest-path matrix of cyclic_ballots(...)."""
+    C, N = len(perm), int(n.sum())
+    S = np.zeros((C, C), dtype=np.uint32)
+    for s in range(C):
+        u = (s + 1 + np.arange(C - 1)) % C  # perm[s + 1], perm[s + 2], ... around the cycle
+        S[perm[s], perm[u]] = N - np.maximum.accumulate(n[u])
+    return S
+
+
 @pytest.fixture(scope="session")
 def orc():
     from oracle import oracle

@@ -1,11 +1,14 @@
-"""The oracle on matrices whose strongest paths run the length of the matrix (a chain of strong
-defeats over weak noise): its serial and blocked closures agree, and every forward pair along
-the chain has the strength known in closed form, the smallest chain weight on the segment.
+"""The oracle on inputs whose strongest paths run the length of the matrix, each with a
+closed-form answer:
+  * a chain of strong defeats over weak noise: the serial and blocked closures agree, and every
+    forward pair along the chain has the smallest chain weight on the segment;
+  * ballots that rotate one order (tallied by the oracle): every strongest path runs the cycle
+    in single steps.
 This pins the oracle on the inputs the GPU long-path tests compare against."""
 import numpy as np
 import pytest
 
-from conftest import chain_forward_ok, chain_matrix
+from conftest import chain_forward_ok, chain_matrix, cyclic_ballots, cyclic_strongest_paths
 
 
 @pytest.mark.parametrize("C", [1, 2, 3, 17, 130, 300])
@@ -35,3 +38,13 @@ def test_chain_check_catches_a_planted_error(orc):
     S = orc.strongest_paths(P, "serial")
     S[perm[3], perm[40]] -= 1
     assert not chain_forward_ok(S, perm, w)
+
+
+@pytest.mark.parametrize("C", [11, 12, 50, 300])
+def test_cyclic_ballots_known_strengths(orc, C):
+    """Rotations of one order (the reference's own ballot shape, tallied by the oracle): every
+    strongest path runs the cycle in single steps and has its closed-form strength."""
+    ballots, perm, n = cyclic_ballots(C, seed=C)
+    d = orc.tally(list(ballots), "scatter")
+    S = orc.strongest_paths(d, "serial")
+    assert np.array_equal(S, cyclic_strongest_paths(perm, n))

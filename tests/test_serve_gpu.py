@@ -138,3 +138,29 @@ def test_host_ballots_and_cancel_in_the_mix():
         S, ranking = alone(V, C, b)
         assert np.array_equal(t.strongest_paths, S), t.rid
         assert np.array_equal(t.ranking, ranking), t.rid
+
+
+def test_cyclic_ballots_in_the_mix():
+    """Ballots that rotate one order, whose strongest paths run around a cycle in single steps
+    (conftest.cyclic_ballots), served in bursts beside Mallows requests: each has its
+    closed-form strongest paths and equals the election run alone."""
+    from conftest import cyclic_ballots, cyclic_strongest_paths
+
+    reqs, want = [], {}
+    for i, C in enumerate([12, 40, 129, 300, 513, 900]):
+        ballots, perm, n = cyclic_ballots(C, seed=100 + i)
+        want[len(reqs)] = cyclic_strongest_paths(perm, n)
+        reqs.append((len(ballots), C, torch.from_numpy(ballots).cuda()))
+    reqs += make_requests(5, 6)
+    with Server(budget_bytes=2 << 30, max_slots=64, idle_ms=20) as server:
+        times = [0.0, 0.0, 0.002, 0.002, 0.004, 0.004] * 2
+        done, _ = run_arrivals(server, reqs, times, keep_paths=True)
+    assert len(done) == len(reqs)
+    for t in done:
+        assert t.status == 0, (t.rid, t.status)
+        V, C, b = reqs[t.rid]
+        S, ranking = alone(V, C, b)
+        assert np.array_equal(t.strongest_paths, S), t.rid
+        assert np.array_equal(t.ranking, ranking), t.rid
+        if t.rid in want:
+            assert np.array_equal(S, want[t.rid]), t.rid
