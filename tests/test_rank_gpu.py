@@ -31,10 +31,12 @@ def test_ties_keep_index_order(orc):
         assert np.array_equal(r.cpu().numpy(), rank_ref)
 
 
-@pytest.mark.parametrize("C", [1, 2, 63, 64, 65, 128, 129, 2048, 2049, 4100, 6000])
+@pytest.mark.parametrize("C", [1, 2, 63, 64, 65, 128, 129, 2048, 2049, 4100, 6000, 8128, 8192, 8193])
 def test_wins_and_places_across_tile_and_strip_edges(orc, C):
     """Sizes on each side of the 64-cell tile pairs and of the 128-candidate / 2048-entry strips
-    of the place count; with ties (values in [0, 3)) and without (values up to 2^32 - 1)."""
+    of the place count, and of the wins count's blocked pair order (tile grids that are a
+    multiple of 16 tiles from 128 tiles: C = 8192, not 8128 or 8193); with ties (values in
+    [0, 3)) and without (values up to 2^32 - 1)."""
     rng = np.random.default_rng(C + 5)
     for hi in (3, 2**32 - 1):
         S = rng.integers(0, hi, size=(C, C), dtype=np.uint64).astype(np.uint32)
