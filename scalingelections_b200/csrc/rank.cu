@@ -4,8 +4,9 @@
 //   ranking[r] = candidates by wins descending, ties by ascending index (py:291: Python's
 //                stable sorted(..., key=wins, reverse=True) keeps ties in input order)
 //
-// wins_kernel walks pairs of 64 x 64 tiles (I <= J, enumerated over the upper triangle), a few
-// resident CTAs per SM each taking every gridDim.x-th pair: S[I][J] is read straight into
+// wins_kernel walks pairs of 64 x 64 tiles (I <= J, over the upper triangle in row order or, for
+// a whole grid of 16 x 16 super-blocks, super-block by super-block), a few resident CTAs per SM
+// each taking every gridDim.x-th pair: S[I][J] is read straight into
 // registers and S[J][I] through a swizzled shared-memory tile, every cell of S once, in 128-bit
 // loads, and the next pair's loads are issued before the current pair is counted. Both
 // endpoints' wins accumulate in registers; one global atomic per candidate per tile pair. The
