@@ -199,6 +199,39 @@ __device__ __forceinline__ uint32_t borrow_step(uint32_t a, uint32_t b, uint32_t
 
 inline size_t bits_smem(int B) { return size_t(kBitStages) * 2 * B * kTile * 4 + kBitStages * 8; }
 
+// How the count's CTAs map to (upper tile, voter range). The first head_ctas CTAs take tiles
+// 0 .. head_ctas / splits - 1, each cut into `splits` voter ranges; the rest take the remaining
+// tiles (the launch's last, partial wave), each cut into tail_splits ranges, so that the tail
+// does not hold a whole wave's time for a few tiles.
+struct CountSplit {
+    int64_t head_ctas;
+    int splits;
+    int tail_splits;
+};
+
+// Upper tile t (row by row: row I holds tiles (I, I) .. (I, R - 1)).
+__device__ __forceinline__ void upper_tile(int64_t t, int R, int& I, int& J) {
+    I = 0;
+    while (t >= R - I) {
+        t -= R - I;
+        ++I;
+    }
+    J = I + int(t);
+}
+
+// Zeroes upper tile first + blockIdx.x and its mirror (J, I), row by row: the tiles whose counts
+// arrive as atomic adds from several voter ranges.
+__global__ void __launch_bounds__(256)
+    zero_tiles_kernel(uint32_t* __restrict__ out, int64_t ld_out, int C, int R, int64_t first) {
+    int I, J;
+    upper_tile(first + blockIdx.x, R, I, J);
+    for (int e = threadIdx.x; e < kTile * kTile; e += 256) {
+        const int r = e / kTile, c = e % kTile;
+        if (I * kTile + r < C && J * kTile + c < C) out[int64_t(I * kTile + r) * ld_out + J * kTile + c] = 0u;
+        if (J * kTile + r < C && I * kTile + c < C) out[int64_t(J * kTile + r) * ld_out + I * kTile + c] = 0u;
+    }
+}
+
 // Counting over one upper tile (I <= J): d[I][J] and, for I < J, d[J][I] = V - d[I][J]. One
 // CTA per tile (and voter range): the two 128-candidate plane strips of each 32-voter chunk
 // are staged by TMA (box {128, B}) through a 4-stage ring. With splits > 1 the voters are cut
@@ -209,7 +242,7 @@ inline size_t bits_smem(int B) { return size_t(kBitStages) * 2 * B * kTile * 4 +
 // B (the planes per chunk) is a template parameter: the plane loop unrolls fully.
 template <int B>
 __global__ void __launch_bounds__(kThreads, 1)
-    count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int64_t V, int C, int R, int splits,
+    count_bits_kernel(const __grid_constant__ CUtensorMap mapPl, int64_t V, int C, int R, CountSplit sp,
                       uint32_t* __restrict__ out, int64_t ld_out, bool accumulate,
                       const uint32_t* __restrict__ irr_chunk, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -219,14 +252,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr uint32_t stage_words = uint32_t(B) * kTile;
     constexpr uint32_t stage_bytes = 2u * stage_words * 4u;
 
-    int64_t t = blockIdx.x / splits;
-    const int split = int(blockIdx.x % splits);
-    int I = 0;
-    while (t >= R - I) {
-        t -= R - I;
-        ++I;
+    int64_t t;
+    int split, splits;
+    if (int64_t(blockIdx.x) < sp.head_ctas) {
+        t = blockIdx.x / sp.splits, split = int(blockIdx.x % sp.splits), splits = sp.splits;
+    } else {
+        const int64_t b = int64_t(blockIdx.x) - sp.head_ctas;
+        t = sp.head_ctas / sp.splits + b / sp.tail_splits, split = int(b % sp.tail_splits), splits = sp.tail_splits;
     }
-    const int J = I + int(t);
+    int I, J;
+    upper_tile(t, R, I, J);
     const int total_ch = int((V + kVC - 1) / kVC);
     const int per = (total_ch + splits - 1) / splits;
     const int ch0 = split * per < total_ch ? split * per : total_ch;
@@ -426,7 +461,7 @@ using FusedKernel = void (*)(const Id*, const int64_t*, int64_t, int64_t, int, i
 
 struct TallyKernels {
     void (*pack)(const float*, int64_t, int64_t, uint32_t*);
-    void (*count)(CUtensorMap, int64_t, int, int, int, uint32_t*, int64_t, bool, const uint32_t*, uint32_t*);
+    void (*count)(CUtensorMap, int64_t, int, int, CountSplit, uint32_t*, int64_t, bool, const uint32_t*, uint32_t*);
     FusedKernel<uint8_t> fused8;  // places + planes for C < 2048 (B <= 11), else null
     FusedKernel<uint16_t> fused16;
     FusedKernel<int32_t> fused32;
@@ -563,6 +598,9 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
     // Take the cheapest split count (the smallest within 1 %), keeping at least 32 chunks (1024
     // voters) per range. With few tiles and many voters this fills the SMs (C = 1024, 2^16
     // voters: 36 tiles x 37 splits = 9 full waves on 148 SMs); with many tiles it stays 1.
+    // Then, unsplit, the last partial wave's tiles alone may be split the same way, when that
+    // is cheaper than a whole wave for them (C = 4096, 4096 voters: 84 tiles in 3 ranges each;
+    // C = 8192: 8 tiles in 4).
     int sms = 0, dev = 0;
     SE_CUDA_TRY(cudaGetDevice(&dev));
     SE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -579,10 +617,32 @@ se_status_t tally_impl(const void* d_ids, int id_bytes, const int64_t* d_offsets
             splits = int(sp);
         }
     }
-    if (splits > 1 && !accumulate)
-        SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
-    K.count<<<unsigned(tiles * splits), kThreads, bits_smem(B), s>>>(map, V, C, R, splits, d_out, ld_out, accumulate,
-                                                                      irr.chunk, err);
+    int64_t head = tiles;  // tiles in the head of the launch
+    int tail_splits = 1;
+    if (splits == 1 && tiles > sms && tiles % sms) {
+        const int64_t rem = tiles % sms;
+        double tail = full_us + 3.0;
+        for (int64_t sp = 2; sp <= std::min<int64_t>(max_splits, 8); ++sp) {
+            const double cost = double((rem * sp + sms - 1) / sms) * (full_us / double(sp) + 12.0);
+            if (cost < tail * 0.99) {
+                tail = cost;
+                tail_splits = int(sp);
+            }
+        }
+        if (tail_splits > 1) head = tiles - rem;
+    }
+    if (!accumulate) {
+        if (splits > 1) {
+            SE_CUDA_TRY(cudaMemset2DAsync(d_out, size_t(ld_out) * 4, 0, size_t(C) * 4, size_t(C), s));
+        } else if (tail_splits > 1) {
+            zero_tiles_kernel<<<unsigned(tiles - head), 256, 0, s>>>(d_out, ld_out, C, R, head);
+            SE_CHECK_LAUNCH();
+        }
+    }
+    const CountSplit layout{head * splits, splits, tail_splits};
+    const int64_t grid = head * splits + (tiles - head) * tail_splits;
+    K.count<<<unsigned(grid), kThreads, bits_smem(B), s>>>(map, V, C, R, layout, d_out, ld_out, accumulate, irr.chunk,
+                                                           err);
     SE_CHECK_LAUNCH();
     // The irregular ballots' pairs, after the count's stores. Without any it returns at once.
     const size_t irr_smem = size_t((C + 31) / 32) * 4;

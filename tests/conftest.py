@@ -103,6 +103,22 @@ def cyclic_strongest_paths(perm, n):
     return S
 
 
+def cyclic_tally(perm, n):
+    """The preference matrix of cyclic_ballots(...): voters of rotation r rank perm[s] above
+    perm[t] unless r lies in (s, t] (for s < t), so d[perm[s]][perm[t]] = N - n[s+1 .. t] and
+    d[perm[t]][perm[s]] = n[s+1 .. t]."""
+    C = len(perm)
+    P = np.concatenate([[0], np.cumsum(n)]).astype(np.int64)  # P[k] = n[0] + ... + n[k-1]
+    s = np.arange(C)[:, None]
+    t = np.arange(C)[None, :]
+    between = np.abs(P[t + 1] - P[s + 1])  # voters of the rotations strictly after min(s, t) up to max(s, t)
+    d_rot = np.where(s < t, P[-1] - between, between)
+    np.fill_diagonal(d_rot, 0)
+    d = np.zeros((C, C), dtype=np.uint32)
+    d[np.ix_(perm, perm)] = d_rot
+    return d
+
+
 @pytest.fixture(scope="session")
 def orc():
     from oracle import oracle

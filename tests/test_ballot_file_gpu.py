@@ -179,3 +179,39 @@ def test_tally_split_voters(orc, accumulate):
         np.fill_diagonal(expect, 0)
         expect = expect + base
     assert np.array_equal(host_u32(out).astype(np.int64), expect)
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_tally_last_wave_split_over_voter_ranges(orc, accumulate):
+    """C = 4096 and 4099 voters: 528 upper tiles, so the count's last partial wave (84 tiles) is
+    split over 3 voter ranges and added with atomics, while the other tiles store whole counts.
+    The ballots rotate one order (one voter per rotation: a closed-form tally), and three more
+    repeat a candidate, in the first, a middle and the last voter chunk (added from the oracle's
+    tally of those three alone; tallies are additive). Overwrite and accumulate modes."""
+    from conftest import cyclic_ballots, cyclic_tally
+
+    C = 4096
+    ballots, perm, n = cyclic_ballots(C, seed=17, max_count=1)
+    extra = [np.concatenate([perm, perm[k:k + 1]]) for k in (0, 7, 99)]  # length C + 1: one id twice
+    B = list(ballots)
+    B.insert(3, extra[0])
+    B.insert(len(B) // 2, extra[1])
+    B.append(extra[2])
+    V = len(B)
+    lens = np.array([b.size for b in B])
+    offs = np.zeros(V + 1, dtype=np.int64)
+    np.cumsum(lens, out=offs[1:])
+    d_ids = torch.from_numpy(np.concatenate(B).astype(np.int16)).cuda()
+    d_offs = torch.from_numpy(offs).cuda()
+    L = _lib.lib()
+    need = L.se_tally_workspace_bytes(V, C)
+    work = torch.empty(need, dtype=torch.uint8, device="cuda")
+    seed = torch.randint(0, 1000, (C, C), dtype=torch.int32, device="cuda")
+    out = seed.clone().view(torch.uint32)
+    flags = bfm.SE_TALLY_ACCUMULATE if accumulate else 0
+    _lib.check(L.se_tally_ex(d_ids.data_ptr(), 2, d_offs.data_ptr(), 0, V, C, flags, out.data_ptr(), C,
+                             work.data_ptr(), need, torch.cuda.current_stream().cuda_stream))
+    expect = cyclic_tally(perm, n).astype(np.int64) + orc.tally(extra, "scatter").astype(np.int64)
+    if accumulate:
+        expect = expect + seed.cpu().numpy().astype(np.int64)
+    assert np.array_equal(host_u32(out).astype(np.int64), expect)

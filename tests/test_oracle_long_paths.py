@@ -8,7 +8,7 @@ This pins the oracle on the inputs the GPU long-path tests compare against."""
 import numpy as np
 import pytest
 
-from conftest import chain_forward_ok, chain_matrix, cyclic_ballots, cyclic_strongest_paths
+from conftest import chain_forward_ok, chain_matrix, cyclic_ballots, cyclic_strongest_paths, cyclic_tally
 
 
 @pytest.mark.parametrize("C", [1, 2, 3, 17, 130, 300])
@@ -46,5 +46,6 @@ def test_cyclic_ballots_known_strengths(orc, C):
     strongest path runs the cycle in single steps and has its closed-form strength."""
     ballots, perm, n = cyclic_ballots(C, seed=C)
     d = orc.tally(list(ballots), "scatter")
+    assert np.array_equal(d, cyclic_tally(perm, n))
     S = orc.strongest_paths(d, "serial")
     assert np.array_equal(S, cyclic_strongest_paths(perm, n))
