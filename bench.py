@@ -1292,9 +1292,12 @@ def run_ingest(args, world, rank, local_rank):
 def launch_ranks(n: int) -> int:
     """Runs this script once per GPU under torch.distributed.run (one node, rendezvous on
     127.0.0.1) with the same arguments, and returns its exit status. Used when --gpus N > 1 is
-    given outside a torchrun launch."""
-    cmd = [sys.executable, "-m", "torch.distributed.run", "--standalone", "--local-addr", "127.0.0.1", "--nnodes", "1",
-           "--nproc-per-node", str(n), str(Path(__file__).resolve()), *sys.argv[1:]]
+    given outside a torchrun launch. The ranks' process group times out a stuck collective after
+    300 s; as the last bound, well above that, `timeout` ends the whole launch after 30 minutes
+    (exit status 124)."""
+    cmd = ["timeout", "-k", "60", "1800", sys.executable, "-m", "torch.distributed.run", "--standalone",
+           "--local-addr", "127.0.0.1", "--nnodes", "1", "--nproc-per-node", str(n), str(Path(__file__).resolve()),
+           *sys.argv[1:]]
     return subprocess.call(cmd)
 
 
