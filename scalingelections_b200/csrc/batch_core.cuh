@@ -263,7 +263,9 @@ __device__ __forceinline__ bool fold_split(uint32_t (&c)[8][NQ], SplitK* split, 
 // (by default from K and the tile's row block; a sharded closure, whose K and I are local,
 // passes them). Padding holds zeros in both operands, and a cell's relaxation through a zero
 // operand leaves it unchanged, so 32-pivot chunks and 32-row warps wholly past C skip the
-// product (their copies too), with identical results.
+// product (their copies too), with identical results. On the wide micro-tile, whose warps 4..7
+// hold cells 64..127 of their rows, those warps skip it too when the tile's columns past 64 are
+// all padding (a column tile's columns are round K's pivots: kvalid; otherwise block J's).
 // NQ: words per thread, 8 (the default micro-tile) or 4 (the wide one, 256 threads, 16-bit
 // lanes); the block must have tile_threads<LB, NQ>() threads.
 // SPLIT / split: the split-K form above, compiled in only where a kernel may split (the whole
@@ -288,7 +290,9 @@ __device__ bool run_tile(const Elec& E, const Elec* G, int kind, int K, int I, i
     if (kvalid < 0) kvalid = E.C - K * kT;
     if (rvalid < 0) rvalid = E.C - (kind == kTileRow ? K : I) * kT;
     const int nch = kvalid >= kT ? kChunks : (kvalid + kKC - 1) / kKC;  // chunks holding pivots
-    const bool live = (g.row0 & ~31) < rvalid;                         // this warp holds real rows
+    const int cvalid = kind == kTileCol ? kvalid : E.C - J * kT;         // the tile's columns inside C
+    // This warp holds real rows and, on the wide micro-tile, real columns.
+    const bool live = (g.row0 & ~31) < rvalid && (NQ == 8 || (g.wbase & ~31) * CF::CPW < cvalid);
     // This CTA's chunks [ch_lo, ch_end): all that hold pivots, or its part's share of them.
     int ch_lo = 0, ch_end = nch;
     if constexpr (SPLIT) {
